@@ -1,0 +1,353 @@
+"""Benchmark of the per-step hot path: RK4 propagation + conjunction screening.
+
+One step = one Simulation::step of the whole population followed by the
+screening of that step (grid, pair filter, Hermite TCA refinement), i.e. one
+iteration of the reference CLI loop (src/main.cpp:346-407) with --conj-km 5.
+
+Workload (default): 1 000 000 objects = 28 340 seeded catalogue objects + 971 660
+fragments in 200 clouds around random LEO parents (isotropic Delta-v, log-normal
+magnitude, median 50 m/s, sigma_ln 0.8; radii 0.05-0.5 m, power law -1.6), each
+cloud released at a random time within the day before the epoch; dt = 10 s,
+threshold 5 km, radius scale 1, minimum encounter speed 10 m/s. Synthetic data.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--precision fp64]
+
+Rank 0 prints one JSON line. With N > 1 (torchrun) every rank runs its own
+independent realisation (seed + rank): weak scaling, no collective on the data
+path; the timing is the max over ranks of the device time.
+"""
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "object-steps/s at 1M objs, split-prec vs FP64 at ≤1 m/24 h error; pairs/s"
+L2_BYTES = 126 * 1024 * 1024
+FLUSH_BYTES = 256 * 1024 * 1024
+
+# Algorithmic FP64 operations per unit (as the reference writes them):
+#   object-step: acceleration x 4 (33 mul + 21 add/sub + 5 div + 3 sqrt each)
+#                + 78 RK4 combination ops = 294 mul/add + 20 div + 12 sqrt
+#   candidate pair: 6 subtractions for dr, dv, then |dr|^2, |dv|^2, dr.dv (15)
+#                   and the distance-gate comparison (4) = 25 ops; a pair that
+#                   reaches the full filter adds its ts, p, |p|, gate and
+#                   convexity terms: 30 mul/add + 1 div + 3 sqrt
+FLOPS_OBJECT_STEP = 294 + 20 + 12
+FLOPS_PAIR_CHEAP = 25
+FLOPS_PAIR_FULL = 34
+FLOPS_REFINE = 2 * 62 * 28 + 60
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=360)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--objects", type=int, default=1_000_000)
+    ap.add_argument("--base", type=int, default=28_340)
+    ap.add_argument("--parents", type=int, default=200)
+    ap.add_argument("--frag-age-s", type=float, default=86400.0)
+    ap.add_argument("--seed", type=int, default=20260801)
+    ap.add_argument("--dt", type=float, default=10.0)
+    ap.add_argument("--conj-km", type=float, default=5.0)
+    ap.add_argument("--steps-per-graph", type=int, default=32)
+    ap.add_argument("--cpu-steps", type=int, default=8, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=60)
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def config_of(a):
+    return {"workload": f"{a.objects} objects ({a.base} catalogue + {a.objects - a.base} fragments in "
+                        f"{a.parents} clouds released within {a.frag_age_s / 3600:g} h), dt {a.dt:g} s, "
+                        f"--conj-km {a.conj_km:g}, radius scale 1, min-vrel 10 m/s",
+            "objects": a.objects, "dt_s": a.dt, "threshold_km": a.conj_km, "precision": a.precision,
+            "seed": a.seed, "steps_per_graph": a.steps_per_graph,
+            "l2": f"flushed before every timed step ({FLUSH_BYTES >> 20} MiB write, outside the timed events)",
+            "parallelism": "one independent realisation per GPU (seed + rank)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def cpu_baseline(a, st, sz, al, steps):
+    """The reference CPU path (oracle/_ref, else the oracle port) on this host."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import checkers
+    threads = os.cpu_count() or 1
+    if checkers.reference_available():
+        chk, kind = checkers.Reference(), "reference"
+    else:
+        chk, kind, threads = checkers.Oracle(), "port", 1
+    t0 = time.perf_counter()
+    _, fa, conj, stats = chk.run(st, sz, al, epoch_jd=2461253.916666667, dt=a.dt, steps=steps, screen=True,
+                                 threshold_km=a.conj_km, threads=threads)
+    wall = time.perf_counter() - t0
+    obj_steps = int(np.sum(stats["alive"])) if steps else 0
+    # objects propagated = alive at the start of each step
+    alive_start = int(al.sum()) + int(np.sum(stats["alive"][:-1]))
+    return {"value": alive_start / wall, "unit": "object-steps/s", "cores": threads, "kind": kind,
+            "sample": f"first {steps} steps of the same {len(st)}-object population, screening included",
+            "pairs_per_s": float(stats["candidate_pairs"].sum()) / wall, "wall_s": wall,
+            "conjunctions": int(len(conj)), "_obj_steps_after": obj_steps}
+
+
+def run_reference_arm(a):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    ks = importlib.import_module("kessler-syndrom-simulation_b200")
+    st, sz, al = ks.generate_population(a.seed, a.base, a.objects, a.parents, a.frag_age_s)
+    steps = max(1, min(a.steps, 24))
+    warm = max(0, min(a.warmup, 1))
+    base = cpu_baseline(a, st, sz, al, warm + steps)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "object-steps/s",
+            "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * base["wall_s"] / (warm + steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)", "config": config_of(a),
+            "pairs_per_s": base["pairs_per_s"],
+            "cpu_baseline": {"value": base["value"], "unit": "object-steps/s", "cores": base["cores"],
+                             "kind": base["kind"],
+                             "sample": f"{warm + steps} steps of the {a.objects}-object workload "
+                                       f"(of the K={a.steps} requested), all host threads"},
+            "e2e": {"value": base["value"], "unit": "object-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    world, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    ks = importlib.import_module("kessler-syndrom-simulation_b200")
+    st, sz, al = ks.generate_population(a.seed + rank, a.base, a.objects, a.parents, a.frag_age_s)
+
+    eng = ks.Engine(local)
+    eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
+    eng.set_screening(True, a.conj_km, 1.0, 0.01)
+    eng.set_precision(ks.PRECISION_FP64 if a.precision == "fp64" else ks.PRECISION_SPLIT)
+    eng.set_steps_per_graph(a.steps_per_graph)
+    eng.set_l2_flush(FLUSH_BYTES)
+    eng.set_profiling(True)
+    eng.set_population(st, sz, al)
+    eng.run(a.warmup)
+    eng.take_conjunctions()
+    eng.take_step_stats()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    w0 = time.perf_counter()
+    eng.run(a.steps)
+    barrier()
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    tm = eng.timing()
+    conj = eng.take_conjunctions()
+    stats = eng.take_step_stats()
+
+    dev_ms = tm["total_ms"]
+    obj_steps = tm["object_steps"]
+    pairs = tm["candidate_pairs"]
+    if pg:
+        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_ms_max = float(t.item())
+        c = torch.tensor([obj_steps, pairs, len(conj)], device="cuda", dtype=torch.float64)
+        pg.all_reduce(c, op=pg.ReduceOp.SUM)
+        obj_total, pairs_total, conj_total = (float(x) for x in c.tolist())
+    else:
+        dev_ms_max, obj_total, pairs_total, conj_total = dev_ms, float(obj_steps), float(pairs), float(len(conj))
+
+    value = obj_total / (dev_ms_max * 1e-3)
+    steps = max(1, tm["steps"])
+    phases = {k: tm[k] / steps for k in ("propagate_ms", "sort_ms", "cells_ms", "pairs_ms", "refine_ms")}
+
+    # FP64 issue rate of this device (project microbenchmark: dependent add/mul chains, no FMA).
+    addmul_per_s, fma_per_s = eng.measure_fp64()
+    prop_flops = FLOPS_OBJECT_STEP * obj_steps / steps
+    pair_flops = (FLOPS_PAIR_CHEAP * pairs + FLOPS_PAIR_FULL * tm["exact_filter_pairs"]) / steps
+    kernels = {
+        "propagate": {"ms": phases["propagate_ms"], "flops": prop_flops},
+        "pairs": {"ms": phases["pairs_ms"], "flops": pair_flops},
+    }
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    ach = kernels[dom]["flops"] / (kernels[dom]["ms"] * 1e-3) / 1e12
+    peak = addmul_per_s / 1e12
+    roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak, "traffic": None,
+                "peak_source": "measured FP64 add/mul issue rate of this GPU (project microbenchmark, no FMA)",
+                "fma_peak_tflops": fma_per_s / 1e12,
+                "algorithmic_flops_per_launch": kernels[dom]["flops"],
+                "phase_ms_per_step": phases, "kernels": {k: {"ms": v["ms"], "tflops": v["flops"] / (v["ms"] * 1e-3) / 1e12
+                                                             if v["ms"] > 0 else None} for k, v in kernels.items()}}
+
+    line = {"metric": METRIC, "value": value, "unit": "object-steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dev_ms_max / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded generator; no dataset)", "config": config_of(a),
+            "pairs_per_s": pairs_total / (dev_ms_max * 1e-3),
+            "conjunctions_per_step": conj_total / steps / world,
+            "gpu_launches": None, "roofline": roofline, "clocks": clk,
+            "wall_s_timed_region": wall,
+            "continuous_object_steps_per_s": None}
+    # Kernel launches per step (counted from the launch sequence of one step).
+    line["gpu_launches"] = a.steps * (3 + 3 * tm["sort_passes"] + 5 + 2)
+
+    if not a.no_e2e:
+        line["e2e"] = e2e_run(ks, a, st, sz, al, local, barrier, pg)
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        base = cpu_baseline(a, st, sz, al, a.cpu_steps)
+        line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"]["pairs_per_s"] = base["pairs_per_s"]
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def e2e_run(ks, a, st, sz, al, device, barrier, pg):
+    """Through the C ABI with host buffers: upload the population from pinned
+    memory, then per step upload that step's lunar rows, run the step and read
+    its conjunction records and counters back (one chunk per step), finally
+    read the population back. Timed end to end on the host, max over ranks."""
+    import torch
+    steps = a.e2e_steps
+    pin_st = torch.from_numpy(st).pin_memory().numpy()
+    pin_sz = torch.from_numpy(sz).pin_memory().numpy()
+    pin_al = torch.from_numpy(al).pin_memory().numpy()
+    eng = ks.Engine(device)
+    eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
+    eng.set_screening(True, a.conj_km, 1.0, 0.01)
+    eng.set_steps_per_graph(1)
+    eng.set_population(pin_st[:1000], pin_sz[:1000], pin_al[:1000])
+    eng.run(2)  # warm the graph path
+    eng.take_conjunctions()
+    eng.take_step_stats()
+    barrier()
+    t0 = time.perf_counter()
+    eng.set_population(pin_st, pin_sz, pin_al)
+    nconj = 0
+    for _ in range(steps):
+        eng.run(1)
+        nconj += len(eng.take_conjunctions())
+        eng.take_step_stats()
+    fs, fa = eng.get_population()
+    barrier()
+    wall = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        wall = float(t.item())
+    world = pg.get_world_size() if pg else 1
+    obj = float(al.sum()) * steps * world
+    eng.close()
+    h2d = (st.nbytes + sz.nbytes + al.nbytes) / steps + 3 * 56 + 16
+    d2h = (fs.nbytes + fa.nbytes) / steps + nconj * 48 / steps + 200
+    return {"value": obj / wall, "unit": "object-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "steps": steps,
+            "what": "ks_set_population from pinned host memory, then per step ks_run(1) (host->device lunar "
+                    "rows, device->host conjunctions and counters, host sync), then ks_get_population; "
+                    "wall clock, max over ranks"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

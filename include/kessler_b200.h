@@ -1,0 +1,149 @@
+/*
+ * kessler_b200 - C ABI of the B200 engine for the per-step hot path of
+ * Kessler_Sim: RK4 propagation (point-mass Earth + J2 + Moon) followed by
+ * hash-grid conjunction screening (linear pair filter + Hermite TCA refinement).
+ *
+ * Plain C: pointers, sizes and status codes only. One context owns one CUDA
+ * stream on one device and the device-resident population. A context is not
+ * re-entrant: drive it from one host thread.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the
+ * reference repository). Units are km, s, km/s in the ECI frame of the input.
+ * States are passed in the reference's kessler::State layout: 6 doubles per
+ * object, {rx, ry, rz, vx, vy, vz} (src/core/orbital.hpp:51).
+ */
+#ifndef KESSLER_B200_H
+#define KESSLER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ks_records.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ks_ctx ks_ctx;
+
+/* Status codes. The reference reports failures as bool + message and then
+ * falls back to the CPU for good (src/core/collision.cpp:706-714); this ABI
+ * returns a status and keeps the message for ks_last_error, with no fallback. */
+enum {
+    KS_OK = 0,
+    KS_ERR_ARG = 1,        /* bad argument (null pointer, negative size, ...) */
+    KS_ERR_CUDA = 2,       /* a CUDA call failed; see ks_last_error */
+    KS_ERR_NO_DEVICE = 3,  /* no usable CUDA device */
+    KS_ERR_STATE = 4,      /* call out of order (e.g. ks_run before ks_set_population) */
+    KS_ERR_OVERFLOW = 5,   /* a device buffer stayed too small after retries */
+    KS_ERR_RANGE = 6,      /* input outside the supported domain (grid keys, sizes) */
+    KS_ERR_TIMEOUT = 7     /* a bounded device-side wait gave up */
+};
+
+/* Precision of the propagation and of the pair screening. */
+enum {
+    KS_PRECISION_FP64 = 0,  /* plain form: every operation in FP64, in the reference's order,
+                               no FMA contraction; bit-identical to the reference CPU path */
+    KS_PRECISION_SPLIT = 1  /* FP64 state, central term and relative positions; FP32 J2 and
+                               lunar terms and FP32 recentred pair gate (FP64 re-check) */
+};
+
+/* --- lifecycle: replaces gpu::create / gpu::destroy (src/core/collision_gpu.hpp:47-48)
+ *     and the device side of Screener::set_gpu (src/core/collision.hpp:235). */
+int ks_create(int device, ks_ctx** out);
+void ks_destroy(ks_ctx* ctx);
+const char* ks_last_error(const ks_ctx* ctx);
+const char* ks_device_name(const ks_ctx* ctx);
+/* cudaStream_t of the context, for callers that time or order work around it. */
+void* ks_stream(ks_ctx* ctx);
+
+/* --- population: the device becomes the owner of Simulation::objects' states
+ *     (src/core/orbital.hpp:145; Object::s, alive, size_m at :71-78).
+ *     states: n x 6 doubles; size_m: n doubles (characteristic size L, metres;
+ *     collision radius = L/2, src/core/collision.cpp:283-287); alive: n bytes or NULL (all alive). */
+int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double* size_m,
+                      const uint8_t* alive);
+int ks_get_population(ks_ctx* ctx, int64_t n, double* states, uint8_t* alive);
+int64_t ks_population_size(const ks_ctx* ctx);
+
+/* --- clock: Simulation::{epoch_jd, t, dt} (src/core/orbital.hpp:146-148). */
+int ks_set_clock(ks_ctx* ctx, double epoch_jd, double t, double dt);
+int ks_get_clock(const ks_ctx* ctx, double* t, int64_t* steps_done);
+
+/* --- screening configuration: ScreeningConfig (src/core/collision.hpp:168-179);
+ *     enabled=0 runs propagation only (the CLI without --screen, src/main.cpp:352). */
+int ks_set_screening(ks_ctx* ctx, int enabled, double threshold_km, double radius_scale,
+                     double min_encounter_speed_km_s);
+int ks_set_precision(ks_ctx* ctx, int precision);
+/* Steps captured per CUDA graph (0 = launch kernels directly, no graph). */
+int ks_set_steps_per_graph(ks_ctx* ctx, int steps_per_graph);
+/* Per-phase CUDA-event timing of every step (adds event records to each step). */
+int ks_set_profiling(ks_ctx* ctx, int enabled);
+
+/* --- run: Simulation::advance (src/core/orbital.hpp:154) with, per step, the
+ *     CLI's Screener::begin / Simulation::step / Screener::finish sequence
+ *     (src/main.cpp:352-373). Conjunctions and per-step counters accumulate in
+ *     the context until taken. */
+int ks_run(ks_ctx* ctx, int64_t steps);
+
+/* Conjunctions found since the last take, ordered by (t, i, j) as Screener::finish
+ * orders them (src/core/collision.cpp:743-747). With out == NULL only *count is
+ * set (number available). Otherwise up to cap records are moved out. */
+int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t* count);
+int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* count);
+
+/* --- one-shot screening on host states: replaces Screener::screen and screen_step
+ *     (src/core/collision.hpp:242-244, 266-270). before/after: n x 6 doubles,
+ *     alive_after: n bytes, size_m: n doubles. Results sorted by (t, i, j), step = 0.
+ *     Uses the context's device buffers: a resident population is discarded. */
+int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
+              const uint8_t* alive_after, const double* size_m, double t0, double dt,
+              ks_conjunction* out, int64_t cap, int64_t* count, ks_step_stats* stats);
+
+/* --- one-shot propagation on host states: `steps` calls of Simulation::step
+ *     without screening (src/core/orbital.cpp:286-300) starting at time t.
+ *     states/alive are updated in place. A resident population is discarded. */
+int ks_propagate(ks_ctx* ctx, int64_t n, double* states, uint8_t* alive, double epoch_jd,
+                 double t, double dt, int64_t steps);
+
+/* --- timing of the last ks_run when profiling is on (milliseconds summed over steps). */
+typedef struct ks_timing {
+    double propagate_ms;   /* fused RK4 + cell-key kernel */
+    double sort_ms;        /* key fix-up + radix sort */
+    double cells_ms;       /* cell ranges, hash, neighbour table, sorted gather */
+    double pairs_ms;       /* pair enumeration + filter */
+    double refine_ms;      /* per-pair TCA refinement */
+    double total_ms;       /* device time of all steps */
+    int64_t steps;
+    int64_t object_steps;  /* sum over steps of alive objects propagated */
+    int64_t sort_passes;   /* 8-bit radix passes per step */
+    int64_t candidate_pairs;     /* summed over steps */
+    int64_t exact_filter_pairs;  /* candidates that needed the full FP64 filter_pair */
+    int64_t refined_pairs;       /* pairs refined (Hermite TCA) */
+} ks_timing;
+int ks_get_timing(const ks_ctx* ctx, ks_timing* out);
+
+/* --- host utilities (no device work) --- */
+
+/* Lunar position (Meeus ch. 47 truncated series), ECI km: the function the
+ * reference evaluates three times per step (src/core/orbital.cpp:53-85, 287-289). */
+void ks_moon_position(double jd, double out[3]);
+
+/* Seeded synthetic population (Keplerian elements -> Cartesian FP64 ECI).
+ * n_base objects of the mixed catalogue (75% LEO, 6% MEO, 6% GEO, 13% GTO/HEO),
+ * then n_total - n_base fragments spread around n_parents random LEO base objects.
+ * frag_age_max_s: fragments are released up to this long before the epoch
+ * (0 = all released at the epoch, at their parent's position).
+ * Writes states (n_total x 6), size_m (n_total) and alive (n_total). */
+int ks_generate_population(uint64_t seed, int64_t n_base, int64_t n_total, int n_parents,
+                           double frag_age_max_s, double* states, double* size_m, uint8_t* alive);
+
+/* FP64 issue rate of this device, measured by a dependent-chain microbenchmark:
+ * add/mul instructions per second (no FMA) and FMA instructions per second. */
+int ks_measure_fp64(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KESSLER_B200_H */

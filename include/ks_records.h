@@ -1,0 +1,49 @@
+/*
+ * Plain-C record layouts shared by the B200 engine, its C-ABI callers and the
+ * CPU checkers. No C++ or CUDA types appear here.
+ *
+ * Units follow the reference: kilometres, seconds, km/s, Earth-centred
+ * inertial frame (src/core/orbital.hpp:4-5).
+ */
+#ifndef KS_RECORDS_H
+#define KS_RECORDS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One close approach found inside a step.
+ * Mirrors kessler::Conjunction (src/core/collision.hpp:181-187) and adds the
+ * step index so that a multi-step run can be returned as one flat list. */
+typedef struct ks_conjunction {
+    int32_t i;            /* index into the population, i < j */
+    int32_t j;
+    int64_t step;         /* global step index whose interval (t0, t0+dt) holds the TCA */
+    double t;             /* time of closest approach, seconds since epoch */
+    double miss_km;       /* distance at TCA */
+    double v_rel_km_s;    /* relative speed at TCA */
+    int32_t collision;    /* 1 if miss_km < R_i + R_j */
+    int32_t reserved;
+} ks_conjunction;         /* 48 bytes */
+
+/* Per-step screening counters.
+ * Mirrors the counting fields of kessler::ScreeningStats
+ * (src/core/collision.hpp:189-204); timings are reported separately. */
+typedef struct ks_step_stats {
+    int64_t step;              /* global step index */
+    int64_t candidate_pairs;   /* pairs produced by the grid (own cell + 13 forward cells) */
+    int64_t refined_pairs;     /* pairs the linear filter sent to the Hermite refinement */
+    int64_t co_orbiting;       /* pairs under the distance gate but slower than the minimum encounter speed */
+    int64_t conjunctions;      /* conjunctions reported for this step */
+    double cell_km;            /* grid cell edge used for this step */
+    int32_t max_cell_objects;  /* population of the fullest cell */
+    int32_t alive;             /* objects alive after the step */
+} ks_step_stats;               /* 56 bytes */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KS_RECORDS_H */

@@ -1,0 +1,207 @@
+"""B200 engine for the per-step hot path of Kessler_Sim.
+
+Python view of the C ABI (include/kessler_b200.h), used by the tests and the
+benchmark. The reference-facing C++ drop-in lives in host/kessler_b200.hpp.
+
+    eng = Engine(device=0)
+    eng.set_population(states, size_m)          # Simulation::objects
+    eng.set_clock(epoch_jd, 0.0, 10.0)          # Simulation::{epoch_jd, t, dt}
+    eng.set_screening(True, 5.0, 1.0, 0.01)     # ScreeningConfig
+    eng.run(360)                                # 360 x (begin / step / finish)
+    conj = eng.take_conjunctions()              # sorted by (t, i, j)
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._abi import (CONJ_DTYPE, PRECISION_FP64, PRECISION_SPLIT, STATS_DTYPE, STATUS_NAMES, Timing,
+                   load_library, ptr)
+
+__all__ = ["Engine", "KsError", "CONJ_DTYPE", "STATS_DTYPE", "PRECISION_FP64", "PRECISION_SPLIT",
+           "moon_position", "generate_population", "load_library", "DEFAULT_EPOCH_JD"]
+
+# src/core/orbital.hpp:30
+DEFAULT_EPOCH_JD = 2461253.916666667
+
+
+class KsError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def _states(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] != 6:
+        raise ValueError("states must have shape (n, 6): rx, ry, rz, vx, vy, vz")
+    if n is not None and a.shape[0] != n:
+        raise ValueError("states row count mismatch")
+    return a
+
+
+class Engine:
+    """One device context: stream, device-resident population, clock, screening."""
+
+    def __init__(self, device=0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        rc = self._lib.ks_create(int(device), C.byref(h))
+        if rc != 0:
+            raise KsError(rc, f"ks_create(device={device}) failed")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ks_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise KsError(rc, self._lib.ks_last_error(self._h).decode(errors="replace"))
+
+    @property
+    def device_name(self):
+        return self._lib.ks_device_name(self._h).decode()
+
+    @property
+    def stream(self):
+        """cudaStream_t of the context (int), e.g. for torch.cuda.ExternalStream."""
+        return self._lib.ks_stream(self._h) or 0
+
+    # --- population / clock / configuration ---
+    def set_population(self, states, size_m, alive=None):
+        st = _states(states)
+        n = st.shape[0]
+        sz = np.ascontiguousarray(size_m, dtype=np.float64)
+        if sz.shape != (n,):
+            raise ValueError("size_m must have shape (n,)")
+        al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        if al is not None and al.shape != (n,):
+            raise ValueError("alive must have shape (n,)")
+        self._check(self._lib.ks_set_population(self._h, n, ptr(st), ptr(sz), ptr(al)))
+
+    def get_population(self):
+        n = self._lib.ks_population_size(self._h)
+        st = np.empty((n, 6), dtype=np.float64)
+        al = np.empty(n, dtype=np.uint8)
+        self._check(self._lib.ks_get_population(self._h, n, ptr(st), ptr(al)))
+        return st, al
+
+    def set_clock(self, epoch_jd=DEFAULT_EPOCH_JD, t=0.0, dt=10.0):
+        self._check(self._lib.ks_set_clock(self._h, float(epoch_jd), float(t), float(dt)))
+
+    def clock(self):
+        t = C.c_double()
+        k = C.c_int64()
+        self._check(self._lib.ks_get_clock(self._h, C.byref(t), C.byref(k)))
+        return t.value, k.value
+
+    def set_screening(self, enabled=True, threshold_km=5.0, radius_scale=1.0, min_encounter_speed_km_s=0.01):
+        self._check(self._lib.ks_set_screening(self._h, 1 if enabled else 0, float(threshold_km),
+                                               float(radius_scale), float(min_encounter_speed_km_s)))
+
+    def set_precision(self, precision):
+        self._check(self._lib.ks_set_precision(self._h, int(precision)))
+
+    def set_steps_per_graph(self, k):
+        self._check(self._lib.ks_set_steps_per_graph(self._h, int(k)))
+
+    def set_buffer_limits(self, survivor_pairs=0, conjunctions=0):
+        self._check(self._lib.ks_set_buffer_limits(self._h, int(survivor_pairs), int(conjunctions)))
+
+    def set_l2_flush(self, nbytes):
+        self._check(self._lib.ks_set_l2_flush(self._h, int(nbytes)))
+
+    def set_profiling(self, on):
+        self._check(self._lib.ks_set_profiling(self._h, 1 if on else 0))
+
+    # --- stepping ---
+    def run(self, steps):
+        self._check(self._lib.ks_run(self._h, int(steps)))
+
+    def take_conjunctions(self):
+        cnt = C.c_int64()
+        self._check(self._lib.ks_take_conjunctions(self._h, None, 0, C.byref(cnt)))
+        out = np.zeros(cnt.value, dtype=CONJ_DTYPE)
+        if cnt.value:
+            self._check(self._lib.ks_take_conjunctions(self._h, ptr(out), cnt.value, C.byref(cnt)))
+        return out[: cnt.value]
+
+    def take_step_stats(self):
+        cnt = C.c_int64()
+        self._check(self._lib.ks_take_step_stats(self._h, None, 0, C.byref(cnt)))
+        out = np.zeros(cnt.value, dtype=STATS_DTYPE)
+        if cnt.value:
+            self._check(self._lib.ks_take_step_stats(self._h, ptr(out), cnt.value, C.byref(cnt)))
+        return out[: cnt.value]
+
+    def timing(self):
+        t = Timing()
+        self._check(self._lib.ks_get_timing(self._h, C.byref(t)))
+        return {name: getattr(t, name) for name, _ in Timing._fields_}
+
+    # --- one-shot calls on host buffers ---
+    def screen(self, before, after, alive_after, size_m, t0, dt):
+        """Screener::screen on given states; returns (conjunctions, stats)."""
+        b = _states(before)
+        n = b.shape[0]
+        a = _states(after, n)
+        al = np.ascontiguousarray(alive_after, dtype=np.uint8)
+        sz = np.ascontiguousarray(size_m, dtype=np.float64)
+        cap = 1024
+        while True:
+            out = np.zeros(cap, dtype=CONJ_DTYPE)
+            stats = np.zeros(1, dtype=STATS_DTYPE)
+            cnt = C.c_int64()
+            self._check(self._lib.ks_screen(self._h, n, ptr(b), ptr(a), ptr(al), ptr(sz), float(t0), float(dt),
+                                            ptr(out), cap, C.byref(cnt), ptr(stats)))
+            if cnt.value <= cap:
+                return out[: cnt.value], stats[0]
+            cap = cnt.value
+
+    def propagate(self, states, alive, epoch_jd, t, dt, steps):
+        """`steps` x Simulation::step without screening, on host arrays (returns copies)."""
+        st = _states(states).copy()
+        al = np.ascontiguousarray(alive, dtype=np.uint8).copy()
+        self._check(self._lib.ks_propagate(self._h, st.shape[0], ptr(st), ptr(al), float(epoch_jd), float(t),
+                                           float(dt), int(steps)))
+        return st, al
+
+    def measure_fp64(self):
+        a = C.c_double()
+        f = C.c_double()
+        self._check(self._lib.ks_measure_fp64(self._h, C.byref(a), C.byref(f)))
+        return a.value, f.value
+
+
+def moon_position(jd):
+    lib = load_library()
+    out = np.zeros(3)
+    lib.ks_moon_position(float(jd), ptr(out))
+    return out
+
+
+def generate_population(seed, n_base, n_total=None, n_parents=200, frag_age_max_s=0.0):
+    """Seeded synthetic catalogue: (states (n, 6), size_m (n,), alive (n,))."""
+    lib = load_library()
+    n_total = n_base if n_total is None else n_total
+    st = np.zeros((n_total, 6))
+    sz = np.zeros(n_total)
+    al = np.zeros(n_total, dtype=np.uint8)
+    rc = lib.ks_generate_population(C.c_uint64(seed), n_base, n_total, int(n_parents), float(frag_age_max_s),
+                                    ptr(st), ptr(sz), ptr(al))
+    if rc != 0:
+        raise KsError(rc, "ks_generate_population: bad arguments")
+    return st, sz, al

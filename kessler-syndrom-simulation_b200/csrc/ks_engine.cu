@@ -1,0 +1,813 @@
+// Host side of the B200 engine: the C ABI declared in include/kessler_b200.h.
+//
+// The device owns the population for the whole run. ks_run advances it in
+// chunks of K steps; a chunk is one CUDA graph (or K direct launches):
+//   chunk_init, then per step: propagate, fix_keys, sort, cells, pairs, refine.
+// The only per-chunk host work is uploading the K rows of lunar positions,
+// reading back K control blocks and the chunk's conjunction records, and
+// ordering those records by (t, i, j). Variable-size outputs live in
+// fixed-capacity buffers; an overflow flag makes the host grow the buffer,
+// restore the chunk's checkpoint and replay the chunk, so results never
+// depend on capacities (the reference retries its pair list the same way,
+// src/core/collision_gpu.cu:424-437).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kessler_b200.h"
+#include "ks_engine.h"
+#include "ks_host.h"
+
+using ks::Ctrl;
+using ks::StepArgs;
+using ks::StepParams;
+
+namespace {
+
+constexpr int kPhases = 6;  // event slots per step
+constexpr int kMaxReplays = 6;
+
+}  // namespace
+
+struct ks_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string name, err;
+    ks::DeviceBuffers b;
+    int64_t n = 0;
+    double epoch_jd = ks::kDefaultEpochJd;
+    double t = 0.0, dt = 10.0;
+    int64_t steps_done = 0;
+    int screening = 1;
+    double thr = 5.0, rscale = 1.0, vmin = 0.01;
+    int precision = KS_PRECISION_FP64;
+    int steps_per_graph = 32;
+    int profiling = 0;
+    int cur = 0;
+    int sort_passes = 8;
+    bool has_pop = false;
+    int max_chunk = 0;
+    StepParams* h_params = nullptr;
+    Ctrl* h_ctrl = nullptr;
+    ks::ChunkCtrl* h_chunk = nullptr;
+    ks_conjunction* h_conj = nullptr;
+    int64_t h_conj_cap = 0;
+    std::vector<ks_conjunction> conj_out;
+    std::vector<ks_step_stats> stats_out;
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> ev;
+    ks_timing timing{};
+    void* l2_flush = nullptr;
+    int64_t l2_flush_bytes = 0;
+};
+
+namespace {
+
+int fail(ks_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define KS_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(ctx, KS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+void drop_graphs(ks_ctx* ctx) {
+    for (auto& g : ctx->graph_exec) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+void free_objects(ks_ctx* ctx) {
+    ks::DeviceBuffers& b = ctx->b;
+    for (int k = 0; k < 2; ++k) { dfree(b.state[k]); dfree(b.alive[k]); dfree(b.keys[k]); dfree(b.idx[k]); }
+    dfree(b.size_m); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.tile_hist); dfree(b.block_counts);
+    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_of); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
+    dfree(b.sorted); dfree(b.sorted_orig);
+    b.cap = 0;
+    b.hash_cap = 0;
+    b.tile_hist_len = 0;
+}
+
+int ensure_objects(ks_ctx* ctx, int64_t n) {
+    if (n <= ctx->b.cap) return KS_OK;
+    if (n > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "population larger than 2^30 objects");
+    drop_graphs(ctx);
+    free_objects(ctx);
+    ks::DeviceBuffers& b = ctx->b;
+    const int64_t cap = std::max<int64_t>(n, 1024);
+    for (int k = 0; k < 2; ++k) {
+        KS_CUDA(cudaMalloc(&b.state[k], sizeof(double) * 6 * cap));
+        KS_CUDA(cudaMalloc(&b.alive[k], cap));
+        KS_CUDA(cudaMalloc(&b.keys[k], sizeof(unsigned long long) * cap));
+        KS_CUDA(cudaMalloc(&b.idx[k], sizeof(int) * cap));
+    }
+    KS_CUDA(cudaMalloc(&b.size_m, sizeof(double) * cap));
+    KS_CUDA(cudaMalloc(&b.ckpt_state, sizeof(double) * 6 * cap));
+    KS_CUDA(cudaMalloc(&b.ckpt_alive, cap));
+    b.tile_hist_len = 256 * ((cap + 2047) / 2048);
+    KS_CUDA(cudaMalloc(&b.tile_hist, sizeof(unsigned int) * b.tile_hist_len));
+    KS_CUDA(cudaMalloc(&b.block_counts, sizeof(int) * ((cap + 1023) / 1024 + 1)));
+    KS_CUDA(cudaMalloc(&b.cell_begin, sizeof(int) * (cap + 1)));
+    KS_CUDA(cudaMalloc(&b.cell_key, sizeof(unsigned long long) * cap));
+    KS_CUDA(cudaMalloc(&b.cell_of, sizeof(int) * cap));
+    KS_CUDA(cudaMalloc(&b.nbr, sizeof(int) * 13 * cap));
+    int64_t h = 16;
+    while (h < 2 * cap) h <<= 1;
+    b.hash_cap = h;
+    KS_CUDA(cudaMalloc(&b.hash_keys, sizeof(unsigned long long) * h));
+    KS_CUDA(cudaMalloc(&b.hash_vals, sizeof(int) * h));
+    KS_CUDA(cudaMalloc(&b.sorted, sizeof(double) * 6 * cap));
+    KS_CUDA(cudaMalloc(&b.sorted_orig, sizeof(int) * cap));
+    b.cap = cap;
+    return KS_OK;
+}
+
+int ensure_survivors(ks_ctx* ctx, int64_t want) {
+    if (want <= ctx->b.surv_cap) return KS_OK;
+    drop_graphs(ctx);
+    dfree(ctx->b.survivors);
+    ctx->b.surv_cap = 0;
+    KS_CUDA(cudaMalloc(&ctx->b.survivors, sizeof(int2) * want));
+    ctx->b.surv_cap = want;
+    return KS_OK;
+}
+
+int ensure_conj(ks_ctx* ctx, int64_t want) {
+    if (want > ctx->b.conj_cap) {
+        drop_graphs(ctx);
+        dfree(ctx->b.conj);
+        ctx->b.conj_cap = 0;
+        KS_CUDA(cudaMalloc(&ctx->b.conj, sizeof(ks_conjunction) * want));
+        ctx->b.conj_cap = want;
+    }
+    if (want > ctx->h_conj_cap) {
+        if (ctx->h_conj) cudaFreeHost(ctx->h_conj);
+        ctx->h_conj = nullptr;
+        ctx->h_conj_cap = 0;
+        KS_CUDA(cudaHostAlloc(&ctx->h_conj, sizeof(ks_conjunction) * want, cudaHostAllocDefault));
+        ctx->h_conj_cap = want;
+    }
+    return KS_OK;
+}
+
+// Control blocks: max_chunk step slots, then the carry slot and its checkpoint.
+int ensure_chunk(ks_ctx* ctx, int k) {
+    if (k <= ctx->max_chunk) return KS_OK;
+    drop_graphs(ctx);
+    ks::DeviceBuffers& b = ctx->b;
+    // Keep the carried speculation across the reallocation.
+    Ctrl carry{};
+    const bool keep = b.ctrl != nullptr;
+    if (keep) KS_CUDA(cudaMemcpy(&carry, b.ctrl + b.ctrl_len - 2, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    dfree(b.ctrl);
+    dfree(b.params);
+    if (ctx->h_params) cudaFreeHost(ctx->h_params);
+    if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
+    ctx->h_params = nullptr;
+    ctx->h_ctrl = nullptr;
+    b.ctrl_len = k + 2;
+    KS_CUDA(cudaMalloc(&b.ctrl, sizeof(Ctrl) * b.ctrl_len));
+    KS_CUDA(cudaMemset(b.ctrl, 0, sizeof(Ctrl) * b.ctrl_len));
+    KS_CUDA(cudaMalloc(&b.params, sizeof(StepParams) * k));
+    KS_CUDA(cudaHostAlloc(&ctx->h_params, sizeof(StepParams) * k, cudaHostAllocDefault));
+    KS_CUDA(cudaHostAlloc(&ctx->h_ctrl, sizeof(Ctrl) * b.ctrl_len, cudaHostAllocDefault));
+    if (keep) KS_CUDA(cudaMemcpy(b.ctrl + b.ctrl_len - 2, &carry, sizeof(Ctrl), cudaMemcpyHostToDevice));
+    for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
+    ctx->ev.assign(static_cast<size_t>(k) * kPhases, nullptr);
+    for (auto& e : ctx->ev) KS_CUDA(cudaEventCreate(&e));
+    ctx->max_chunk = k;
+    return KS_OK;
+}
+
+Ctrl* carry_slot(ks_ctx* ctx) { return ctx->b.ctrl + ctx->b.ctrl_len - 2; }
+Ctrl* carry_ckpt_slot(ks_ctx* ctx) { return ctx->b.ctrl + ctx->b.ctrl_len - 1; }
+
+ks::ForceConsts force_consts() {
+    ks::ForceConsts fc;
+    fc.neg_mu_earth = -ks::kMuEarth;
+    fc.k_j2 = ks::j2_numerator();
+    fc.mu_moon = ks::kMuMoon;
+    fc.r_earth = ks::kREarth;
+    return fc;
+}
+
+int passes_for_bits(int bits) { return std::max(1, (bits + 1 + 7) / 8); }
+
+// Host estimate of the key width from a seeded control block. Only sizes the
+// number of radix passes; the device checks it and the chunk is replayed with
+// more passes if the estimate was short.
+int estimate_bits(const Ctrl& c, double dt, double thr) {
+    const double vmax = [&] { double v; std::memcpy(&v, &c.spec_vmax, 8); return v; }();
+    auto dec = [](unsigned long long u) {
+        unsigned long long b = (u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u;
+        double d;
+        std::memcpy(&d, &b, 8);
+        return d;
+    };
+    const double vrel = 2.0 * vmax;
+    double cell = vrel * dt + thr + ks::kGravityGradient * vrel * dt * dt * dt;
+    if (cell < 1.0) cell = 1.0;
+    int bits = 0;
+    for (int a = 0; a < 3; ++a) {
+        const double mn = dec(c.bb_min[a]), mx = dec(c.bb_max[a]);
+        if (!(mn <= mx)) continue;
+        const long long span = static_cast<long long>(std::floor(mx / cell)) - static_cast<long long>(std::floor(mn / cell));
+        int w = 0;
+        while (w < 63 && (span >> w) > 0) ++w;
+        bits += w;
+    }
+    return bits;
+}
+
+void fill_params(ks_ctx* ctx, int k_steps, double t_start, int64_t step0, double* t_end) {
+    double t = t_start;
+    for (int k = 0; k < k_steps; ++k) {
+        StepParams& sp = ctx->h_params[k];
+        sp.t0 = t;
+        sp.step = step0 + k;
+        ks::moon_stages(ctx->epoch_jd, t, ctx->dt, sp.m);
+        t += ctx->dt;  // Simulation::step (src/core/orbital.cpp:299)
+    }
+    *t_end = t;
+}
+
+StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
+    StepArgs a{};
+    a.fc = force_consts();
+    a.dt = ctx->dt;
+    a.threshold_km = ctx->thr;
+    a.vmin2 = ctx->vmin * ctx->vmin;
+    a.radius_scale = ctx->rscale;
+    a.n = static_cast<int>(ctx->n);
+    a.screening = ctx->screening;
+    a.sort_passes = ctx->sort_passes;
+    a.sp = ctx->b.params + k;
+    a.ctrl = ctx->b.ctrl + k;
+    a.ctrl_next = (k == k_steps - 1) ? carry_slot(ctx) : ctx->b.ctrl + k + 1;
+    a.src = src;
+    return a;
+}
+
+void record(ks_ctx* ctx, int k, int phase, bool capturing) {
+    if (!ctx->profiling) return;
+    cudaEvent_t e = ctx->ev[static_cast<size_t>(k) * kPhases + phase];
+    if (capturing) cudaEventRecordWithFlags(e, ctx->stream, cudaEventRecordExternal);
+    else cudaEventRecord(e, ctx->stream);
+}
+
+void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
+    cudaStream_t s = ctx->stream;
+    ks::launch_chunk_init(ctx->b, k_steps, s);
+    int src = src0;
+    for (int k = 0; k < k_steps; ++k) {
+        const StepArgs a = step_args(ctx, k, k_steps, src);
+        if (ctx->l2_flush_bytes > 0) cudaMemsetAsync(ctx->l2_flush, k & 0xFF, ctx->l2_flush_bytes, s);
+        record(ctx, k, 0, capturing);
+        ks::launch_propagate(ctx->b, a, s);
+        record(ctx, k, 1, capturing);
+        if (ctx->screening) {
+            ks::launch_fix_keys(ctx->b, a, s);
+            ks::launch_sort(ctx->b, a, s);
+            record(ctx, k, 2, capturing);
+            ks::launch_cells(ctx->b, a, s);
+            record(ctx, k, 3, capturing);
+            ks::launch_pairs(ctx->b, a, s);
+            record(ctx, k, 4, capturing);
+            ks::launch_refine(ctx->b, a, ctx->b.conj, ctx->b.conj_cap, ctx->b.chunk, s);
+            record(ctx, k, 5, capturing);
+        }
+        src ^= 1;
+    }
+}
+
+int launch_chunk(ks_ctx* ctx, int k_steps) {
+    const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
+    if (!use_graph) {
+        enqueue_chunk(ctx, k_steps, ctx->cur, false);
+        KS_CUDA(cudaGetLastError());
+        return KS_OK;
+    }
+    cudaGraphExec_t& exec = ctx->graph_exec[ctx->cur];
+    if (!exec) {
+        cudaGraph_t g = nullptr;
+        KS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_chunk(ctx, k_steps, ctx->cur, true);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
+        if (le != cudaSuccess) return fail(ctx, KS_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(le));
+        if (ee != cudaSuccess) return fail(ctx, KS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
+        const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            exec = nullptr;
+            return fail(ctx, KS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        }
+    }
+    KS_CUDA(cudaGraphLaunch(exec, ctx->stream));
+    return KS_OK;
+}
+
+int save_checkpoint(ks_ctx* ctx) {
+    ks::DeviceBuffers& b = ctx->b;
+    KS_CUDA(cudaMemcpyAsync(b.ckpt_state, b.state[ctx->cur], sizeof(double) * 6 * b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(b.ckpt_alive, b.alive[ctx->cur], b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(carry_ckpt_slot(ctx), carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToDevice, ctx->stream));
+    return KS_OK;
+}
+
+int restore_checkpoint(ks_ctx* ctx) {
+    ks::DeviceBuffers& b = ctx->b;
+    KS_CUDA(cudaMemcpyAsync(b.state[ctx->cur], b.ckpt_state, sizeof(double) * 6 * b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(b.alive[ctx->cur], b.ckpt_alive, b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(carry_slot(ctx), carry_ckpt_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToDevice, ctx->stream));
+    return KS_OK;
+}
+
+bool conj_less(const ks_conjunction& a, const ks_conjunction& b) {
+    if (a.t != b.t) return a.t < b.t;
+    if (a.i != b.i) return a.i < b.i;
+    return a.j < b.j;
+}
+
+void accumulate_timing(ks_ctx* ctx, int k_steps) {
+    if (!ctx->profiling) return;
+    auto el = [&](int k, int p0, int p1) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[static_cast<size_t>(k) * kPhases + p0], ctx->ev[static_cast<size_t>(k) * kPhases + p1]);
+        return static_cast<double>(ms);
+    };
+    for (int k = 0; k < k_steps; ++k) {
+        ctx->timing.propagate_ms += el(k, 0, 1);
+        if (ctx->screening) {
+            ctx->timing.sort_ms += el(k, 1, 2);
+            ctx->timing.cells_ms += el(k, 2, 3);
+            ctx->timing.pairs_ms += el(k, 3, 4);
+            ctx->timing.refine_ms += el(k, 4, 5);
+            ctx->timing.total_ms += el(k, 0, 5);
+        } else {
+            ctx->timing.total_ms += el(k, 0, 1);
+        }
+    }
+}
+
+// Runs one chunk of k_steps; replays it after growing whatever overflowed.
+int run_chunk(ks_ctx* ctx, int k_steps) {
+    int rc = ensure_chunk(ctx, k_steps);
+    if (rc) return rc;
+    double t_end = 0.0;
+    fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
+    KS_CUDA(cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->screening) {
+        rc = save_checkpoint(ctx);
+        if (rc) return rc;
+    }
+    for (int attempt = 0;; ++attempt) {
+        rc = launch_chunk(ctx, k_steps);
+        if (rc) return rc;
+        KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        int flags = ctx->h_chunk->flags;
+        unsigned long long max_refined = 0;
+        int max_bits = 0;
+        for (int k = 0; k < k_steps; ++k) {
+            flags |= ctx->h_ctrl[k].flags;
+            max_refined = std::max(max_refined, ctx->h_ctrl[k].refined);
+            max_bits = std::max(max_bits, ctx->h_ctrl[k].grid.bits);
+        }
+        const bool surv_over = max_refined > static_cast<unsigned long long>(ctx->b.surv_cap);
+        if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds");
+        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over) break;
+        if (attempt >= kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after replays");
+        if (flags & ks::FLAG_SORT_BITS) {
+            ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(max_bits));
+            drop_graphs(ctx);
+        }
+        if (surv_over && (rc = ensure_survivors(ctx, static_cast<int64_t>(max_refined) * 2))) return rc;
+        if ((flags & ks::FLAG_CONJ_OVERFLOW) &&
+            (rc = ensure_conj(ctx, static_cast<int64_t>(ctx->h_chunk->conj_count) * 2)))
+            return rc;
+        rc = restore_checkpoint(ctx);
+        if (rc) return rc;
+    }
+    const int64_t nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
+    if (nc > 0) {
+        KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj, sizeof(ks_conjunction) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        const size_t base = ctx->conj_out.size();
+        ctx->conj_out.insert(ctx->conj_out.end(), ctx->h_conj, ctx->h_conj + nc);
+        std::sort(ctx->conj_out.begin() + base, ctx->conj_out.end(), conj_less);
+    }
+    for (int k = 0; k < k_steps; ++k) {
+        const Ctrl& c = ctx->h_ctrl[k];
+        ks_step_stats st{};
+        st.step = ctx->steps_done + k;
+        st.candidate_pairs = static_cast<int64_t>(c.candidates);
+        st.refined_pairs = static_cast<int64_t>(c.refined);
+        st.co_orbiting = static_cast<int64_t>(c.co_orbiting);
+        st.conjunctions = static_cast<int64_t>(c.conj);
+        st.cell_km = ctx->screening ? c.grid.cell : 0.0;
+        st.max_cell_objects = c.max_cell;
+        st.alive = c.n_alive;
+        ctx->stats_out.push_back(st);
+        ctx->timing.object_steps += static_cast<int64_t>(c.object_steps);
+        ctx->timing.candidate_pairs += static_cast<int64_t>(c.candidates);
+        ctx->timing.exact_filter_pairs += static_cast<int64_t>(c.exact_evals);
+        ctx->timing.refined_pairs += static_cast<int64_t>(c.refined);
+    }
+    accumulate_timing(ctx, k_steps);
+    ctx->timing.steps += k_steps;
+    ctx->timing.sort_passes = ctx->sort_passes;
+    ctx->steps_done += k_steps;
+    ctx->t = t_end;
+    if (k_steps & 1) ctx->cur ^= 1;
+    return KS_OK;
+}
+
+int seed_speculation(ks_ctx* ctx) {
+    ks::launch_seed_ctrl(ctx->b, static_cast<int>(ctx->n), ctx->cur, carry_slot(ctx), 1, ctx->stream);
+    Ctrl c{};
+    KS_CUDA(cudaMemcpyAsync(&c, carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->sort_passes = passes_for_bits(estimate_bits(c, ctx->dt, ctx->thr));
+    drop_graphs(ctx);
+    return KS_OK;
+}
+
+int upload_population(ks_ctx* ctx, int64_t n, const double* states, const double* size_m, const uint8_t* alive,
+                      int buf) {
+    ks::DeviceBuffers& b = ctx->b;
+    if (n > 0) {
+        KS_CUDA(cudaMemcpyAsync(b.sorted, states, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, ctx->stream));
+        ks::launch_aos_to_soa(b.sorted, b.state[buf], n, b.cap, ctx->stream);
+        if (alive) KS_CUDA(cudaMemcpyAsync(b.alive[buf], alive, n, cudaMemcpyHostToDevice, ctx->stream));
+        else KS_CUDA(cudaMemsetAsync(b.alive[buf], 1, n, ctx->stream));
+        if (size_m) KS_CUDA(cudaMemcpyAsync(b.size_m, size_m, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    KS_CUDA(cudaGetLastError());
+    return KS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ks_create(int device, ks_ctx** out) {
+    if (!out) return KS_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return KS_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return KS_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return KS_ERR_NO_DEVICE;
+    ks_ctx* ctx = new ks_ctx;
+    ctx->device = device;
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    char buf[640];
+    std::snprintf(buf, sizeof(buf), "%s (sm_%d%d, %d SMs, %.1f GiB)", prop.name, prop.major, prop.minor,
+                  prop.multiProcessorCount, prop.totalGlobalMem / 1073741824.0);
+    ctx->name = buf;
+    int rc = KS_OK;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->b.chunk, sizeof(ks::ChunkCtrl)) != cudaSuccess ||
+        cudaHostAlloc(&ctx->h_chunk, sizeof(ks::ChunkCtrl), cudaHostAllocDefault) != cudaSuccess)
+        rc = KS_ERR_CUDA;
+    if (!rc) rc = ensure_chunk(ctx, 64);
+    if (!rc) rc = ensure_survivors(ctx, 1 << 20);
+    if (!rc) rc = ensure_conj(ctx, 1 << 16);
+    if (rc) {
+        ks_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return KS_OK;
+}
+
+void ks_destroy(ks_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_graphs(ctx);
+    free_objects(ctx);
+    if (ctx->l2_flush) cudaFree(ctx->l2_flush);
+    dfree(ctx->b.survivors);
+    dfree(ctx->b.conj);
+    dfree(ctx->b.ctrl);
+    dfree(ctx->b.chunk);
+    dfree(ctx->b.params);
+    if (ctx->h_params) cudaFreeHost(ctx->h_params);
+    if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
+    if (ctx->h_chunk) cudaFreeHost(ctx->h_chunk);
+    if (ctx->h_conj) cudaFreeHost(ctx->h_conj);
+    for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* ks_last_error(const ks_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char* ks_device_name(const ks_ctx* ctx) { return ctx ? ctx->name.c_str() : ""; }
+void* ks_stream(ks_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double* size_m, const uint8_t* alive) {
+    if (!ctx || n < 0 || (n > 0 && (!states || !size_m))) return fail(ctx, KS_ERR_ARG, "ks_set_population: bad arguments");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_objects(ctx, n);
+    if (rc) return rc;
+    ctx->n = n;
+    ctx->cur = 0;
+    rc = upload_population(ctx, n, states, size_m, alive, 0);
+    if (rc) return rc;
+    rc = seed_speculation(ctx);
+    if (rc) return rc;
+    ctx->has_pop = true;
+    ctx->steps_done = 0;
+    ctx->conj_out.clear();
+    ctx->stats_out.clear();
+    return KS_OK;
+}
+
+int ks_get_population(ks_ctx* ctx, int64_t n, double* states, uint8_t* alive) {
+    if (!ctx) return KS_ERR_ARG;
+    if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "no resident population");
+    if (n != ctx->n) return fail(ctx, KS_ERR_ARG, "ks_get_population: size mismatch");
+    cudaSetDevice(ctx->device);
+    ks::DeviceBuffers& b = ctx->b;
+    if (n > 0) {
+        if (states) {
+            ks::launch_soa_to_aos(b.state[ctx->cur], b.sorted, n, b.cap, ctx->stream);
+            KS_CUDA(cudaMemcpyAsync(states, b.sorted, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        if (alive) KS_CUDA(cudaMemcpyAsync(alive, b.alive[ctx->cur], n, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return KS_OK;
+}
+
+int64_t ks_population_size(const ks_ctx* ctx) { return ctx ? ctx->n : -1; }
+
+int ks_set_clock(ks_ctx* ctx, double epoch_jd, double t, double dt) {
+    if (!ctx || !(dt > 0.0)) return fail(ctx, KS_ERR_ARG, "ks_set_clock: dt must be positive");
+    if (dt != ctx->dt) drop_graphs(ctx);
+    ctx->epoch_jd = epoch_jd;
+    ctx->t = t;
+    ctx->dt = dt;
+    if (ctx->has_pop) {
+        cudaSetDevice(ctx->device);
+        return seed_speculation(ctx);
+    }
+    return KS_OK;
+}
+
+int ks_get_clock(const ks_ctx* ctx, double* t, int64_t* steps_done) {
+    if (!ctx) return KS_ERR_ARG;
+    if (t) *t = ctx->t;
+    if (steps_done) *steps_done = ctx->steps_done;
+    return KS_OK;
+}
+
+int ks_set_screening(ks_ctx* ctx, int enabled, double threshold_km, double radius_scale,
+                     double min_encounter_speed_km_s) {
+    if (!ctx || threshold_km < 0.0 || radius_scale < 0.0 || min_encounter_speed_km_s < 0.0)
+        return fail(ctx, KS_ERR_ARG, "ks_set_screening: bad arguments");
+    drop_graphs(ctx);
+    ctx->screening = enabled ? 1 : 0;
+    ctx->thr = threshold_km;
+    ctx->rscale = radius_scale;
+    ctx->vmin = min_encounter_speed_km_s;
+    if (ctx->has_pop) {
+        cudaSetDevice(ctx->device);
+        return seed_speculation(ctx);
+    }
+    return KS_OK;
+}
+
+int ks_set_precision(ks_ctx* ctx, int precision) {
+    if (!ctx || (precision != KS_PRECISION_FP64 && precision != KS_PRECISION_SPLIT))
+        return fail(ctx, KS_ERR_ARG, "ks_set_precision: unknown mode");
+    if (precision == KS_PRECISION_SPLIT) return fail(ctx, KS_ERR_ARG, "ks_set_precision: split precision not built");
+    drop_graphs(ctx);
+    ctx->precision = precision;
+    return KS_OK;
+}
+
+int ks_set_steps_per_graph(ks_ctx* ctx, int steps_per_graph) {
+    if (!ctx || steps_per_graph < 0 || steps_per_graph > 4096) return fail(ctx, KS_ERR_ARG, "ks_set_steps_per_graph: 0..4096");
+    drop_graphs(ctx);
+    ctx->steps_per_graph = steps_per_graph;
+    return KS_OK;
+}
+
+int ks_set_buffer_limits(ks_ctx* ctx, int64_t survivor_pairs, int64_t conjunctions) {
+    if (!ctx || survivor_pairs < 0 || conjunctions < 0) return fail(ctx, KS_ERR_ARG, "ks_set_buffer_limits: bad arguments");
+    cudaSetDevice(ctx->device);
+    drop_graphs(ctx);
+    if (survivor_pairs > 0) {
+        dfree(ctx->b.survivors);
+        ctx->b.surv_cap = 0;
+        int rc = ensure_survivors(ctx, survivor_pairs);
+        if (rc) return rc;
+    }
+    if (conjunctions > 0) {
+        dfree(ctx->b.conj);
+        ctx->b.conj_cap = 0;
+        int rc = ensure_conj(ctx, conjunctions);
+        if (rc) return rc;
+    }
+    return KS_OK;
+}
+
+int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes) {
+    if (!ctx || bytes < 0) return fail(ctx, KS_ERR_ARG, "ks_set_l2_flush: bad arguments");
+    cudaSetDevice(ctx->device);
+    drop_graphs(ctx);
+    if (ctx->l2_flush) cudaFree(ctx->l2_flush);
+    ctx->l2_flush = nullptr;
+    ctx->l2_flush_bytes = 0;
+    if (bytes > 0) {
+        KS_CUDA(cudaMalloc(&ctx->l2_flush, bytes));
+        ctx->l2_flush_bytes = bytes;
+    }
+    return KS_OK;
+}
+
+int ks_set_profiling(ks_ctx* ctx, int enabled) {
+    if (!ctx) return KS_ERR_ARG;
+    drop_graphs(ctx);
+    ctx->profiling = enabled ? 1 : 0;
+    return KS_OK;
+}
+
+int ks_run(ks_ctx* ctx, int64_t steps) {
+    if (!ctx || steps < 0) return fail(ctx, KS_ERR_ARG, "ks_run: bad arguments");
+    if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_run: no population");
+    cudaSetDevice(ctx->device);
+    ctx->timing = ks_timing{};
+    const int chunk = ctx->steps_per_graph > 0 ? ctx->steps_per_graph : 64;
+    int rc = ensure_chunk(ctx, chunk);
+    if (rc) return rc;
+    int64_t left = steps;
+    while (left > 0) {
+        const int k = static_cast<int>(std::min<int64_t>(left, chunk));
+        rc = run_chunk(ctx, k);
+        if (rc) return rc;
+        left -= k;
+    }
+    return KS_OK;
+}
+
+int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t* count) {
+    if (!ctx || !count || cap < 0) return KS_ERR_ARG;
+    const int64_t avail = static_cast<int64_t>(ctx->conj_out.size());
+    if (!out) {
+        *count = avail;
+        return KS_OK;
+    }
+    const int64_t m = std::min(avail, cap);
+    std::memcpy(out, ctx->conj_out.data(), sizeof(ks_conjunction) * m);
+    ctx->conj_out.erase(ctx->conj_out.begin(), ctx->conj_out.begin() + m);
+    *count = m;
+    return KS_OK;
+}
+
+int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* count) {
+    if (!ctx || !count || cap < 0) return KS_ERR_ARG;
+    const int64_t avail = static_cast<int64_t>(ctx->stats_out.size());
+    if (!out) {
+        *count = avail;
+        return KS_OK;
+    }
+    const int64_t m = std::min(avail, cap);
+    std::memcpy(out, ctx->stats_out.data(), sizeof(ks_step_stats) * m);
+    ctx->stats_out.erase(ctx->stats_out.begin(), ctx->stats_out.begin() + m);
+    *count = m;
+    return KS_OK;
+}
+
+int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after, const uint8_t* alive_after,
+              const double* size_m, double t0, double dt, ks_conjunction* out, int64_t cap, int64_t* count,
+              ks_step_stats* stats) {
+    if (!ctx || n < 0 || !count || (n > 0 && (!before || !after || !alive_after || !size_m)) || !(dt > 0.0))
+        return fail(ctx, KS_ERR_ARG, "ks_screen: bad arguments");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_objects(ctx, n);
+    if (rc) return rc;
+    rc = ensure_chunk(ctx, 1);
+    if (rc) return rc;
+    ctx->has_pop = false;
+    ctx->n = n;
+    rc = upload_population(ctx, n, before, size_m, nullptr, 0);
+    if (!rc) rc = upload_population(ctx, n, after, nullptr, alive_after, 1);
+    if (rc) return rc;
+    const double saved_dt = ctx->dt;
+    ctx->dt = dt;
+    StepParams sp{};
+    sp.t0 = t0;
+    sp.step = 0;
+    ctx->h_params[0] = sp;
+    KS_CUDA(cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<ks_conjunction> found;
+    ks_step_stats st{};
+    for (int attempt = 0;; ++attempt) {
+        ks::launch_chunk_init(ctx->b, 1, ctx->stream);
+        StepArgs a = step_args(ctx, 0, 1, 0);
+        ks::launch_seed_ctrl(ctx->b, static_cast<int>(n), 0, a.ctrl, 0, ctx->stream);
+        ks::launch_screen_keys(ctx->b, a, ctx->stream);
+        ks::launch_sort(ctx->b, a, ctx->stream);
+        ks::launch_cells(ctx->b, a, ctx->stream);
+        ks::launch_pairs(ctx->b, a, ctx->stream);
+        ks::launch_refine(ctx->b, a, ctx->b.conj, ctx->b.conj_cap, ctx->b.chunk, ctx->stream);
+        KS_CUDA(cudaGetLastError());
+        KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        const Ctrl& c = ctx->h_ctrl[0];
+        const int flags = c.flags | ctx->h_chunk->flags;
+        const bool surv_over = c.refined > static_cast<unsigned long long>(ctx->b.surv_cap);
+        if (flags & ks::FLAG_KEY_RANGE) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds"); }
+        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over) {
+            st.step = 0;
+            st.candidate_pairs = static_cast<int64_t>(c.candidates);
+            st.refined_pairs = static_cast<int64_t>(c.refined);
+            st.co_orbiting = static_cast<int64_t>(c.co_orbiting);
+            st.conjunctions = static_cast<int64_t>(c.conj);
+            st.cell_km = c.grid.cell;
+            st.max_cell_objects = c.max_cell;
+            st.alive = c.n_alive;
+            break;
+        }
+        if (attempt >= kMaxReplays) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_OVERFLOW, "ks_screen: buffers overflow"); }
+        if (flags & ks::FLAG_SORT_BITS) ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(c.grid.bits));
+        if (surv_over && (rc = ensure_survivors(ctx, static_cast<int64_t>(c.refined) * 2))) { ctx->dt = saved_dt; return rc; }
+        if ((flags & ks::FLAG_CONJ_OVERFLOW) && (rc = ensure_conj(ctx, static_cast<int64_t>(ctx->h_chunk->conj_count) * 2))) {
+            ctx->dt = saved_dt;
+            return rc;
+        }
+    }
+    ctx->dt = saved_dt;
+    const int64_t nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
+    if (nc > 0) {
+        KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj, sizeof(ks_conjunction) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        found.assign(ctx->h_conj, ctx->h_conj + nc);
+        std::sort(found.begin(), found.end(), conj_less);
+    }
+    const int64_t m = std::min<int64_t>(nc, cap);
+    if (out && m > 0) std::memcpy(out, found.data(), sizeof(ks_conjunction) * m);
+    *count = nc;
+    if (stats) *stats = st;
+    return KS_OK;
+}
+
+int ks_propagate(ks_ctx* ctx, int64_t n, double* states, uint8_t* alive, double epoch_jd, double t, double dt,
+                 int64_t steps) {
+    if (!ctx || n < 0 || steps < 0 || (n > 0 && !states) || !(dt > 0.0))
+        return fail(ctx, KS_ERR_ARG, "ks_propagate: bad arguments");
+    std::vector<double> dummy_size(static_cast<size_t>(n > 0 ? n : 1), 0.0);
+    const int saved_screen = ctx->screening;
+    const double saved_epoch = ctx->epoch_jd, saved_t = ctx->t, saved_dt = ctx->dt;
+    ctx->screening = 0;
+    drop_graphs(ctx);
+    int rc = ks_set_population(ctx, n, states, dummy_size.data(), alive);
+    if (!rc) {
+        ctx->epoch_jd = epoch_jd;
+        ctx->t = t;
+        ctx->dt = dt;
+        rc = ks_run(ctx, steps);
+    }
+    if (!rc) rc = ks_get_population(ctx, n, states, alive);
+    ctx->screening = saved_screen;
+    ctx->epoch_jd = saved_epoch;
+    ctx->t = saved_t;
+    ctx->dt = saved_dt;
+    ctx->has_pop = false;
+    drop_graphs(ctx);
+    return rc;
+}
+
+int ks_get_timing(const ks_ctx* ctx, ks_timing* out) {
+    if (!ctx || !out) return KS_ERR_ARG;
+    *out = ctx->timing;
+    return KS_OK;
+}
+
+int ks_measure_fp64(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s) {
+    if (!ctx || !addmul_per_s || !fma_per_s) return KS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    KS_CUDA(ks::measure_fp64(addmul_per_s, fma_per_s, ctx->stream));
+    return KS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// Internal interface between the host engine (ks_engine.cu) and the kernels
+// (ks_kernels.cu). Not part of the public C ABI.
+//
+// Device data layout (one context, capacity `cap` objects):
+//   state[2]     two SoA FP64 buffers of 6*cap doubles: rx | ry | rz | vx | vy | vz,
+//                ping-ponged each step (start-of-step -> end-of-step)
+//   alive[2]     one byte per object per buffer
+//   size_m       characteristic size L (m); collision radius = L/2
+//   keys/idx     cell keys (u64) and object indices (i32), two buffers each for the radix sort
+//   cells        begin offsets, keys, owning cell per sorted entry, 13 forward neighbours per cell
+//   hash         open-addressing table cell key -> cell index
+//   sorted       start-of-step states gathered in cell order (AoS, 6 doubles per entry)
+//   survivors    pairs sent to refinement (int2, i < j)
+//   conj         conjunction records of the current chunk of steps
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ks_exact.cuh"
+#include "ks_records.h"
+
+namespace ks {
+
+// Per-step inputs computed on the host.
+struct StepParams {
+    double t0;         // start of the step, seconds since epoch (Simulation::t)
+    int64_t step;      // global index of the step in the run
+    MoonStage m[3];    // moon at t0, t0 + dt/2, t0 + dt (src/core/orbital.cpp:287-289)
+};
+
+// Grid actually used for one step: cell edge and the compact key layout.
+// Cell coordinates (floor(r / cell)) are shifted by lo and packed as
+// cx << (wy + wz) | cy << wz | cz; bit `bits` marks objects outside the grid.
+struct GridParams {
+    double cell;
+    long long lo[3];
+    long long span[3];   // hi - lo per axis
+    int w[3];
+    int bits;
+};
+
+enum : int {
+    FLAG_SURVIVOR_OVERFLOW = 1,
+    FLAG_CONJ_OVERFLOW = 2,
+    FLAG_SORT_BITS = 4,      // more key bits than the sort passes launched cover
+    FLAG_KEY_RANGE = 8,      // a key fell outside its grid bounds
+};
+
+// Per-step control block, device resident.
+struct Ctrl {
+    // Speculation inputs, written by the previous step: largest speed and
+    // position bounds over the objects alive at the start of this step.
+    unsigned long long spec_vmax;      // bits of a non-negative double
+    unsigned long long bb_min[3];      // order-preserving encodings of doubles
+    unsigned long long bb_max[3];
+    // Results of this step.
+    unsigned long long vmax_true;      // largest start speed over objects alive after the step
+    unsigned long long candidates;
+    unsigned long long co_orbiting;
+    unsigned long long refined;
+    unsigned long long conj;
+    unsigned long long object_steps;   // objects propagated (alive at start)
+    unsigned long long exact_evals;    // candidates that needed the full filter
+    int n_alive;                       // alive after the step
+    int n_cells;
+    int max_cell;
+    int flags;
+    GridParams grid;
+};
+
+struct ChunkCtrl {
+    unsigned long long conj_count;     // records appended in this chunk
+    int flags;
+    int pad;
+};
+
+struct DeviceBuffers {
+    int64_t cap = 0;
+    double* state[2] = {nullptr, nullptr};
+    uint8_t* alive[2] = {nullptr, nullptr};
+    double* size_m = nullptr;
+    double* ckpt_state = nullptr;
+    uint8_t* ckpt_alive = nullptr;
+    unsigned long long* keys[2] = {nullptr, nullptr};
+    int* idx[2] = {nullptr, nullptr};
+    unsigned int* tile_hist = nullptr;     // 256 x tiles, for one radix pass
+    int64_t tile_hist_len = 0;
+    int* block_counts = nullptr;           // cell heads per tile
+    int* cell_begin = nullptr;             // cap + 1
+    unsigned long long* cell_key = nullptr;
+    int* cell_of = nullptr;                // owning cell per sorted entry
+    int* nbr = nullptr;                    // 13 per cell
+    unsigned long long* hash_keys = nullptr;
+    int* hash_vals = nullptr;
+    int64_t hash_cap = 0;                  // power of two
+    double* sorted = nullptr;              // 6 per sorted entry
+    int* sorted_orig = nullptr;
+    int2* survivors = nullptr;
+    int64_t surv_cap = 0;
+    ks_conjunction* conj = nullptr;
+    int64_t conj_cap = 0;
+    Ctrl* ctrl = nullptr;                  // max_chunk + 1 entries
+    int ctrl_len = 0;
+    ChunkCtrl* chunk = nullptr;
+    StepParams* params = nullptr;          // max_chunk entries
+};
+
+// Everything a step's kernels need, by value.
+struct StepArgs {
+    ForceConsts fc;
+    double dt;
+    double threshold_km;
+    double vmin2;
+    double radius_scale;
+    double gate_hi2;           // unused by the propagation kernel
+    int n;                     // population size (objects, alive or not)
+    int screening;             // 0: propagation only
+    int sort_passes;
+    const StepParams* sp;      // this step's inputs
+    Ctrl* ctrl;                // this step's control block
+    Ctrl* ctrl_next;           // next step's control block (speculation outputs)
+    int src;                   // state buffer holding the start of the step (0 or 1)
+};
+
+// Kernel launchers (ks_kernels.cu). All enqueue on `stream` and never synchronise.
+void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream);
+void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int use_alive_src,
+                      cudaStream_t stream);
+void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_screen_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,
+                   ChunkCtrl* chunk, cudaStream_t stream);
+void launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t stride, cudaStream_t stream);
+void launch_soa_to_aos(const double* soa, double* aos, int64_t n, int64_t stride, cudaStream_t stream);
+// Index of the key/idx buffer holding the sorted result after `passes` passes.
+inline int sorted_buffer(int passes) { return passes & 1; }
+
+int sm_count();
+cudaError_t measure_fp64(double* addmul_per_s, double* fma_per_s, cudaStream_t stream);
+
+}  // namespace ks

@@ -1,0 +1,174 @@
+"""ORACLE - test infrastructure only.
+
+ctypes front-end of the CPU checkers built by oracle/Makefile:
+  - ``Oracle``    oracle/libks_oracle.so, the plain-C restatement (ks_oracle.c)
+  - ``Reference`` oracle/_ref/libksref.so, the reference's own sources plus
+                  ref_harness.cpp (present only where the reference tree was
+                  available at build time)
+Both expose the same calls (run / screen / step helpers) with the same record
+layouts as the engine. Only tests/, the smoke check and bench.py's CPU-baseline
+leg use this module; the product never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libks_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libksref.so")
+
+CONJ_DTYPE = np.dtype(
+    [("i", "<i4"), ("j", "<i4"), ("step", "<i8"), ("t", "<f8"), ("miss_km", "<f8"),
+     ("v_rel_km_s", "<f8"), ("collision", "<i4"), ("reserved", "<i4")], align=True)
+STATS_DTYPE = np.dtype(
+    [("step", "<i8"), ("candidate_pairs", "<i8"), ("refined_pairs", "<i8"), ("co_orbiting", "<i8"),
+     ("conjunctions", "<i8"), ("cell_km", "<f8"), ("max_cell_objects", "<i4"), ("alive", "<i4")],
+    align=True)
+
+_P = C.c_void_p
+_D = C.c_double
+_L = C.c_long
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def build(ref=True):
+    """Builds the checkers (ref=True also builds the reference when its tree exists)."""
+    targets = ["oracle"]
+    if ref and os.path.isdir("/root/reference/src"):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+class _Checker:
+    prefix = ""
+    has_threads = False
+
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        pre = self.prefix
+        run = getattr(self.lib, pre + "run")
+        run.restype = _L
+        scr = getattr(self.lib, pre + "screen")
+        scr.restype = _L
+        for name in ("moon_position", "acceleration", "rk4"):
+            getattr(self.lib, pre + name).restype = None
+        getattr(self.lib, pre + "filter_pair").restype = C.c_int
+        getattr(self.lib, pre + "filter_pair").argtypes = [_D] * 9
+        getattr(self.lib, pre + "prefilter_keep").restype = C.c_int
+        getattr(self.lib, pre + "prefilter_keep").argtypes = [C.c_float] * 9
+
+    def moon_position(self, jd):
+        out = np.zeros(3)
+        getattr(self.lib, self.prefix + "moon_position")(_D(jd), _p(out))
+        return out
+
+    def rk4(self, s, dt, m0, m1, m2):
+        out = np.zeros(6)
+        args = [np.ascontiguousarray(x, dtype=np.float64) for x in (s, m0, m1, m2)]
+        getattr(self.lib, self.prefix + "rk4")(_p(args[0]), _D(dt), _p(args[1]), _p(args[2]), _p(args[3]),
+                                               _p(out))
+        return out
+
+    def filter_pair(self, dr, dv, dt, thr, vmin2):
+        return getattr(self.lib, self.prefix + "filter_pair")(*(list(map(float, dr)) + list(map(float, dv))
+                                                               + [dt, thr, vmin2]))
+
+    def prefilter_keep(self, dr, dv, dt, thr, vmin2):
+        return getattr(self.lib, self.prefix + "prefilter_keep")(*(list(map(float, dr)) + list(map(float, dv))
+                                                                  + [dt, thr, vmin2]))
+
+    def run(self, states, size_m, alive=None, epoch_jd=2461253.916666667, t_start=0.0, dt=10.0, steps=1,
+            screen=True, threshold_km=5.0, radius_scale=1.0, min_vrel_km_s=0.01, threads=0, conj_cap=None):
+        """The CLI step loop; returns (final states, alive, conjunctions, per-step stats[, timings])."""
+        st = np.ascontiguousarray(states, dtype=np.float64).copy()
+        n = st.shape[0]
+        al = np.ones(n, np.uint8) if alive is None else np.ascontiguousarray(alive, dtype=np.uint8).copy()
+        sz = np.ascontiguousarray(size_m, dtype=np.float64)
+        cap = conj_cap if conj_cap is not None else max(1024, 64 * steps)
+        stats = np.zeros(max(steps, 1), dtype=STATS_DTYPE)
+        timings = np.zeros(5)
+        while True:
+            s2 = st.copy()
+            a2 = al.copy()
+            conj = np.zeros(cap, dtype=CONJ_DTYPE)
+            args = [_L(n), _p(s2), _p(a2), _p(sz), _D(epoch_jd), _D(t_start), _D(dt), _L(steps),
+                    C.c_int(1 if screen else 0), _D(threshold_km), _D(radius_scale), _D(min_vrel_km_s)]
+            if self.has_threads:
+                args.append(C.c_int(threads))
+            args += [_p(conj), _L(cap), _p(stats)]
+            if self.has_threads:
+                args.append(_p(timings))
+            total = getattr(self.lib, self.prefix + "run")(*args)
+            if total < 0:
+                raise RuntimeError("checker run failed")
+            if total <= cap:
+                self.last_timings = timings.copy()
+                return s2, a2, conj[:total], stats[:steps]
+            cap = int(total)
+
+    def screen(self, before, after, alive_after, size_m, t0, dt, threshold_km=5.0, radius_scale=1.0,
+               min_vrel_km_s=0.01, threads=0):
+        b = np.ascontiguousarray(before, dtype=np.float64)
+        a = np.ascontiguousarray(after, dtype=np.float64)
+        al = np.ascontiguousarray(alive_after, dtype=np.uint8)
+        sz = np.ascontiguousarray(size_m, dtype=np.float64)
+        n = b.shape[0]
+        cap = 1024
+        while True:
+            out = np.zeros(cap, dtype=CONJ_DTYPE)
+            stats = np.zeros(1, dtype=STATS_DTYPE)
+            args = [_L(n), _p(b), _p(a), _p(al), _p(sz), _D(t0), _D(dt), _D(threshold_km), _D(radius_scale),
+                    _D(min_vrel_km_s)]
+            if self.has_threads:
+                args.append(C.c_int(threads))
+            args += [_p(out), _L(cap), _p(stats)]
+            k = getattr(self.lib, self.prefix + "screen")(*args)
+            if k <= cap:
+                return out[:k], stats[0]
+            cap = int(k)
+
+
+class Oracle(_Checker):
+    """The plain-C restatement (oracle/ks_oracle.c)."""
+    prefix = "kso_"
+    has_threads = False
+
+    def __init__(self, path=ORACLE_SO):
+        super().__init__(path)
+
+
+class Reference(_Checker):
+    """The reference compiled from its own sources (oracle/_ref/libksref.so)."""
+    prefix = "ksref_"
+    has_threads = True
+
+    def __init__(self, path=REF_SO):
+        super().__init__(path)
+        self.lib.ksref_max_threads.restype = C.c_int
+        self.lib.ksref_load_catalog.restype = _L
+        self.lib.ksref_read_epoch_jd.restype = _D
+
+    def max_threads(self):
+        return self.lib.ksref_max_threads()
+
+    def load_catalog(self, path):
+        """(states, size_m, ids, epoch_jd) via the reference parser."""
+        p = path.encode()
+        n = self.lib.ksref_load_catalog(p, _L(0), None, None, None, None)
+        st = np.zeros((n, 6))
+        sz = np.zeros(n)
+        ids = np.zeros(n, np.int32)
+        dropped = C.c_int(0)
+        self.lib.ksref_load_catalog(p, _L(n), _p(st), _p(sz), _p(ids), C.byref(dropped))
+        return st, sz, ids, self.lib.ksref_read_epoch_jd(p)
+
+
+def reference_available():
+    return os.path.exists(REF_SO)

@@ -1,0 +1,202 @@
+"""Generates the golden fixtures of tests/golden/ from the REFERENCE ITSELF.
+
+Runs oracle/_ref/libksref.so (the reference's own src/core/orbital.cpp and
+src/core/collision.cpp compiled in place by oracle/Makefile, driven like its
+CLI step loop) and stores inputs and outputs, so that the tests can check the
+oracle and the engine without the reference tree.
+
+    python tests/golden/make_golden.py        # needs the reference tree
+
+Fixtures:
+  run_mixed.npz      1 500 catalogue objects + 1 500 fragments in 3 clouds
+                     (released up to 2 h before the epoch), two planted
+                     re-entries (one of them the fastest object, which forces
+                     the grid to be rebuilt without it), 40 steps
+  run_dense.npz      600 objects + 2 400 fragments in 2 clouds released at the
+                     epoch: every cloud starts inside one cell, 12 steps
+  screen_cases.npz   planted one-step encounters: crossing, co-orbiting,
+                     separating, TCA at a step edge, collision, dead object
+  ref_catalog_1h.json  counters of a 1 h run on the reference's shipped
+                     catalogue (the README's own data), for the oracle
+"""
+import importlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import checkers  # noqa: E402
+
+EPOCH = 2461253.916666667
+CATALOG = "/root/reference/data/satellites_20260801_1000Z.txt"
+
+
+def population(seed, n_base, n_total, n_parents, age):
+    ks = importlib.import_module("kessler-syndrom-simulation_b200")
+    return ks.generate_population(seed, n_base, n_total, n_parents, age)
+
+
+def _accel(r):
+    # Two-body + J2, only to plant encounters (the reference adds the Moon).
+    mu, re, j2 = 398600.4418, 6378.137, 1.08262668e-3
+    r2 = (r * r).sum()
+    rn = np.sqrt(r2)
+    a = -mu * r / (r2 * rn)
+    k = 1.5 * j2 * mu * re * re / (r2 * r2 * rn)
+    z2 = 5.0 * r[2] ** 2 / r2
+    return a + k * r * np.array([z2 - 1.0, z2 - 1.0, z2 - 3.0])
+
+
+def _propagate(s, t, h=1.0):
+    s = np.array(s, float)
+    n = int(round(abs(t) / h))
+    h = t / n
+    for _ in range(n):
+        f = lambda y: np.concatenate([y[3:], _accel(y[:3])])
+        k1 = f(s); k2 = f(s + k1 * h / 2); k3 = f(s + k2 * h / 2); k4 = f(s + k3 * h)
+        s = s + (k1 + 2 * k2 + 2 * k3 + k4) * h / 6
+    return s
+
+
+def plant_encounters(st, first, count, steps, dt, seed):
+    """Pairs (first + 2k, first + 2k + 1) that meet about mid-run: the same
+    point with velocities rotated about the radius, carried back in time."""
+    rng = np.random.default_rng(seed)
+    for k in range(count):
+        a = st[first + 2 * k].copy()
+        r = a[:3]
+        u = r / np.linalg.norm(r)
+        ang = np.radians(20 + 140 * rng.random())
+        v = a[3:]
+        vb = v * np.cos(ang) + np.cross(u, v) * np.sin(ang) + u * np.dot(u, v) * (1 - np.cos(ang))
+        off = rng.normal(size=3)
+        off -= np.dot(off, vb) * vb / np.dot(vb, vb)
+        off *= (0.05 + 3.0 * rng.random()) / np.linalg.norm(off)
+        t_meet = (steps * (0.2 + 0.6 * rng.random()) + rng.random()) * dt
+        st[first + 2 * k] = _propagate(a, -t_meet)
+        st[first + 2 * k + 1] = _propagate(np.concatenate([r + off, vb]), -t_meet)
+
+
+def plant_reentries(st, al):
+    # Object 0: falling through the surface during step 0 at 15 km/s, the
+    # fastest object of the population. Object 1: slower, dies a few steps later.
+    st[0] = [6390.0, 0.0, 0.0, -15.0, 0.3, 0.0]
+    st[1] = [0.0, 6700.0, 0.0, 0.0, -4.0, 1.0]
+
+
+def save_run(name, st, sz, al, steps, dt=10.0, thr=5.0, rscale=1.0, vmin=0.01):
+    ref = checkers.Reference()
+    fs, fa, conj, stats = ref.run(st, sz, al, epoch_jd=EPOCH, t_start=0.0, dt=dt, steps=steps, screen=True,
+                                  threshold_km=thr, radius_scale=rscale, min_vrel_km_s=vmin, threads=8)
+    np.savez_compressed(os.path.join(HERE, name), states=st, size_m=sz, alive=al, epoch_jd=EPOCH, dt=dt,
+                        steps=steps, threshold_km=thr, radius_scale=rscale, min_vrel_km_s=vmin,
+                        final_states=fs, final_alive=fa, conj=conj, stats=stats)
+    print(name, "conj", len(conj), "candidates/step", int(stats["candidate_pairs"].mean()),
+          "dead", int((fa == 0).sum()))
+
+
+def screen_cases():
+    """Hand-built before/after pairs for one Screener::screen call (dt = 10 s)."""
+    dt = 10.0
+    rng = np.random.default_rng(5)
+    before, after, size = [], [], []
+
+    def add(b, a, s=1.0):
+        before.append(b)
+        after.append(a)
+        size.append(s)
+
+    def straight(r, v):
+        r = np.asarray(r, float)
+        v = np.asarray(v, float)
+        return list(r) + list(v), list(r + v * dt) + list(v)
+
+    # Background objects far apart.
+    for k in range(200):
+        r = rng.normal(size=3)
+        r = r / np.linalg.norm(r) * (7000 + 400 * rng.random())
+        v = np.cross(r, [0, 0, 1.0])
+        v = v / np.linalg.norm(v) * 7.5
+        add(*straight(r, v))
+    # 1. Crossings, TCA inside the step, misses from 50 m to just over 5 km.
+    for k, miss in enumerate([0.05, 0.8, 2.5, 4.99, 5.02]):
+        frac = 0.15 + 0.17 * k
+        y = 7000.0 + 40.0 * k
+        add(*straight([y, 0, 1000.0 * k], [0, 7.5, 0]))
+        add(*straight([y, -3.5 * dt * frac, 1000.0 * k + miss], [0, 11.0, 0]))
+    # 2. Co-orbiting pair 300 m apart, 2 m/s relative.
+    add(*straight([0, 7100, 0], [-7.4, 0, 0]))
+    add(*straight([0, 7100.3, 0], [-7.402, 0, 0]))
+    # 3. Separating pair (closest at the start of the step).
+    add(*straight([0, 0, 7200], [7.3, 0, 0]))
+    add(*straight([0.5, 0, 7200], [7.3 + 3.0, 0, 0]))
+    # 4. TCA at the very end of the step: approaching until t0 + dt.
+    add(*straight([-7300, 0, 0], [0, 0, 7.3]))
+    add(*straight([-7300, 0, -50.0], [0, 0, 12.3]))
+    # 5. Collision: miss below the radius sum (sizes 30 m -> radius 15 m each).
+    add(*straight([5000, 5000, 0], [0, 0, 7.0]), 30.0)
+    add(*straight([5000.01, 4990.0, 35.0], [0, 2.0, 0.0]), 30.0)
+    # 6. A close pair whose second object is dead after the step.
+    add(*straight([-5000, -5000, 100], [0, 0, 7.0]))
+    add(*straight([-5000, -5000.5, 130.0], [0, 0, 4.0]))
+    b = np.array(before)
+    a = np.array(after)
+    alive = np.ones(len(b), np.uint8)
+    alive[-1] = 0
+    sz = np.array(size)
+    ref = checkers.Reference()
+    conj, stats = ref.screen(b, a, alive, sz, 1234.0, dt, threads=1)
+    np.savez_compressed(os.path.join(HERE, "screen_cases.npz"), before=b, after=a, alive_after=alive, size_m=sz,
+                        t0=1234.0, dt=dt, threshold_km=5.0, radius_scale=1.0, min_vrel_km_s=0.01, conj=conj,
+                        stats=np.array([stats]))
+    print("screen_cases conj", len(conj), conj[["i", "j", "miss_km", "collision"]])
+
+
+def catalogue_kat():
+    ref = checkers.Reference()
+    st, sz, ids, epoch = ref.load_catalog(CATALOG)
+    fs, fa, conj, stats = ref.run(st, sz, None, epoch_jd=epoch, t_start=0.0, dt=10.0, steps=360, screen=True,
+                                  threshold_km=5.0, radius_scale=1.0, min_vrel_km_s=0.01, threads=8)
+    k = int(np.argmin(conj["miss_km"]))
+    out = {
+        "source": "reference CLI step loop (oracle/_ref) on data/satellites_20260801_1000Z.txt",
+        "objects": int(len(st)), "epoch_jd": epoch, "dt": 10.0, "steps": 360, "threshold_km": 5.0,
+        "conjunctions": int(len(conj)),
+        "below_km": {str(b): int((conj["miss_km"] < b).sum()) for b in (0.1, 1.0, 2.0, 5.0)},
+        "collisions": int(conj["collision"].sum()),
+        "closest": {"miss_m": float(conj["miss_km"][k] * 1000.0), "t_h": float(conj["t"][k] / 3600.0),
+                    "id1": int(ids[conj["i"][k]]), "id2": int(ids[conj["j"][k]])},
+        "candidate_pairs_total": int(stats["candidate_pairs"].sum()),
+        "refined_pairs_total": int(stats["refined_pairs"].sum()),
+        "max_co_orbiting": int(stats["co_orbiting"].max()),
+        "final_state_sha_hint": float(np.abs(fs).sum()),
+        "readme_24h": {"conjunctions": 38367, "below_1km": 1493, "below_100m": 14, "collisions": 0,
+                       "closest_m": 7.2},
+    }
+    with open(os.path.join(HERE, "ref_catalog_1h.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("catalogue 1h", out["conjunctions"], out["closest"])
+
+
+def main():
+    checkers.build(ref=True)
+    st, sz, al = population(20260801, 1500, 3000, 3, 7200.0)
+    plant_reentries(st, al)
+    plant_encounters(st, 2, 12, 40, 10.0, 11)
+    save_run("run_mixed.npz", st, sz, al, 40)
+    st, sz, al = population(7, 600, 3000, 2, 0.0)
+    plant_encounters(st, 0, 8, 12, 10.0, 12)
+    save_run("run_dense.npz", st, sz, al, 12)
+    screen_cases()
+    if os.path.exists(CATALOG):
+        catalogue_kat()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,147 @@
+"""Parity of the B200 engine (through the C ABI) with the reference and the oracle.
+
+Bar: bit-exact. Final states, alive flags, conjunction records (pair ids, step,
+TCA, miss distance, relative speed, collision flag) and per-step counters
+(candidate pairs, refined pairs, co-orbiting pairs, cell edge, fullest cell)
+must equal the reference's, which the golden fixtures hold, and the oracle's on
+fresh inputs.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_path
+
+pytestmark = pytest.mark.gpu
+
+STAT_FIELDS = ("candidate_pairs", "refined_pairs", "co_orbiting", "conjunctions", "cell_km", "max_cell_objects",
+               "alive")
+
+
+def load(name):
+    return dict(np.load(golden_path(name)))
+
+
+def run_engine(eng, states, size_m, alive, steps, epoch_jd=2461253.916666667, dt=10.0, thr=5.0, rscale=1.0,
+               vmin=0.01, spg=32, chunks=None):
+    eng.set_steps_per_graph(spg)
+    eng.set_clock(epoch_jd, 0.0, dt)
+    eng.set_screening(True, thr, rscale, vmin)
+    eng.set_population(states, size_m, alive)
+    for k in (chunks or [steps]):
+        eng.run(k)
+    fs, fa = eng.get_population()
+    return fs, fa, eng.take_conjunctions(), eng.take_step_stats()
+
+
+def assert_same_stats(got, want):
+    assert len(got) == len(want)
+    for f in STAT_FIELDS:
+        assert np.array_equal(got[f], want[f]), f
+
+
+def assert_same_conj(got, want):
+    assert len(got) == len(want), (len(got), len(want))
+    for f in ("i", "j", "step", "t", "miss_km", "v_rel_km_s", "collision"):
+        assert np.array_equal(got[f], want[f]), f
+
+
+@pytest.mark.parametrize("name", ["run_mixed.npz", "run_dense.npz"])
+@pytest.mark.parametrize("spg", [0, 32])
+def test_engine_reproduces_reference_run(engine, name, spg):
+    fx = load(name)
+    fs, fa, conj, stats = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], int(fx["steps"]),
+                                     float(fx["epoch_jd"]), float(fx["dt"]), float(fx["threshold_km"]),
+                                     float(fx["radius_scale"]), float(fx["min_vrel_km_s"]), spg=spg)
+    assert np.array_equal(fs, fx["final_states"]), "states differ from the reference"
+    assert np.array_equal(fa, fx["final_alive"])
+    assert_same_conj(conj, fx["conj"])
+    assert_same_stats(stats, fx["stats"])
+
+
+def test_chunking_and_graph_parity_do_not_change_results(engine):
+    fx = load("run_mixed.npz")
+    base = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], 40, spg=0)
+    for spg, chunks in ((7, [13, 27]), (1, [40]), (5, [3, 3, 34])):
+        got = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], 40, spg=spg, chunks=chunks)
+        assert np.array_equal(got[0], base[0]) and np.array_equal(got[1], base[1])
+        assert_same_conj(got[2], base[2])
+        assert_same_stats(got[3], base[3])
+
+
+def test_buffer_overflow_replays_to_the_same_result(engine):
+    fx = load("run_mixed.npz")
+    base = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], 40)
+    engine.set_buffer_limits(survivor_pairs=1, conjunctions=1)
+    got = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], 40)
+    engine.set_buffer_limits(survivor_pairs=1 << 20, conjunctions=1 << 16)
+    assert np.array_equal(got[0], base[0])
+    assert_same_conj(got[2], base[2])
+    assert_same_stats(got[3], base[3])
+
+
+def test_screen_matches_reference_cases(engine):
+    fx = load("screen_cases.npz")
+    conj, stats = engine.screen(fx["before"], fx["after"], fx["alive_after"], fx["size_m"], float(fx["t0"]),
+                                float(fx["dt"]))
+    want = fx["stats"][0]
+    assert_same_conj(conj, fx["conj"])
+    for f in STAT_FIELDS[:-1]:
+        assert stats[f] == want[f], f
+
+
+@pytest.mark.parametrize("seed,n_base,n_total,parents,age,steps", [
+    (11, 3000, 20000, 8, 0.0, 6),        # fresh clouds: thousands of objects per cell
+    (12, 5000, 30000, 20, 6 * 3600.0, 8),  # aged clouds
+    (13, 28340, 28340, 1, 0.0, 12),      # catalogue-sized, no fragments
+])
+def test_engine_matches_oracle_fresh_inputs(engine, oracle, ks, seed, n_base, n_total, parents, age, steps):
+    st, sz, al = ks.generate_population(seed, n_base, n_total, parents, age)
+    want = oracle.run(st, sz, al, steps=steps)
+    got = run_engine(engine, st, sz, al, steps)
+    assert np.array_equal(got[0], want[0])
+    assert np.array_equal(got[1], want[1])
+    assert_same_conj(got[2], want[2])
+    assert_same_stats(got[3], want[3])
+
+
+def test_engine_screen_matches_oracle_wide_threshold(engine, oracle, ks):
+    st, sz, al = ks.generate_population(21, 4000, 9000, 5, 3600.0)
+    after, alive_after = engine.propagate(st, al, 2461253.916666667, 0.0, 10.0, 1)
+    for thr in (0.5, 5.0, 40.0):
+        want, ws = oracle.screen(st, after, alive_after, sz, 0.0, 10.0, threshold_km=thr)
+        engine.set_screening(True, thr, 1.0, 0.01)
+        got, gs = engine.screen(st, after, alive_after, sz, 0.0, 10.0)
+        assert_same_conj(got, want)
+        for f in STAT_FIELDS:
+            assert gs[f] == ws[f], (thr, f)
+    engine.set_screening(True, 5.0, 1.0, 0.01)
+
+
+def test_propagate_matches_oracle(engine, oracle, ks):
+    st, sz, al = ks.generate_population(31, 5000)
+    st[:3] = [[6390.0, 0, 0, -15.0, 0.3, 0], [0, 6700.0, 0, 0, -4.0, 1.0], [7000.0, 0, 0, 0, 7.5, 0]]
+    al[2] = 0  # dead objects keep their state
+    want = oracle.run(st, sz, al, steps=30, screen=False)
+    got = engine.propagate(st, al, 2461253.916666667, 0.0, 10.0, 30)
+    assert np.array_equal(got[0], want[0])
+    assert np.array_equal(got[1], want[1])
+    assert np.array_equal(got[0][2], st[2])
+
+
+def test_edge_populations(engine, oracle):
+    # empty
+    conj, stats = engine.screen(np.zeros((0, 6)), np.zeros((0, 6)), np.zeros(0, np.uint8), np.zeros(0), 0.0, 10.0)
+    assert len(conj) == 0 and stats["candidate_pairs"] == 0
+    # one object; two objects at the same point; all dead
+    one = np.array([[7000.0, 0, 0, 0, 7.5, 0]])
+    fs, fa, conj, stats = run_engine(engine, one, np.ones(1), None, 5)
+    want = oracle.run(one, np.ones(1), None, steps=5)
+    assert np.array_equal(fs, want[0]) and len(conj) == 0 and stats["candidate_pairs"].sum() == 0
+    two = np.array([[7000.0, 0, 0, 0, 7.5, 0], [7000.0, 0, 0, 0, 7.5, 0]])
+    got = run_engine(engine, two, np.ones(2), None, 3)
+    want = oracle.run(two, np.ones(2), None, steps=3)
+    assert_same_stats(got[3], want[3])
+    assert got[3]["candidate_pairs"].sum() == 3
+    dead = np.zeros(4, np.uint8)
+    got = run_engine(engine, np.tile(one, (4, 1)), np.ones(4), dead, 3)
+    assert got[3]["alive"].max() == 0 and got[3]["candidate_pairs"].sum() == 0
