@@ -850,6 +850,7 @@ void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t str
 
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     const int n = a.n;
+    if (n <= 0) return;  // nothing alive: the cell build sees n_alive == 0
     const int ntiles = (n + kSortTile - 1) / kSortTile;
     for (int pass = 0; pass < a.sort_passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
@@ -864,7 +865,7 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
 
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     const int sb = sorted_buffer(a.sort_passes);
-    const int ntiles = (a.n + kCellTile - 1) / kCellTile;
+    const int ntiles = a.n > 0 ? (a.n + kCellTile - 1) / kCellTile : 1;
     k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, reinterpret_cast<unsigned int*>(b.block_counts));
     k_scan_exclusive<<<1, 1024, 0, stream>>>(reinterpret_cast<unsigned int*>(b.block_counts), ntiles);
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
