@@ -121,6 +121,9 @@ class Engine:
     def set_buffer_limits(self, survivor_pairs=0, conjunctions=0):
         self._check(self._lib.ks_set_buffer_limits(self._h, int(survivor_pairs), int(conjunctions)))
 
+    def set_tuning(self, key, value):
+        self._check(self._lib.ks_set_tuning(self._h, key.encode(), int(value)))
+
     def set_l2_flush(self, nbytes):
         self._check(self._lib.ks_set_l2_flush(self._h, int(nbytes)))
 

@@ -56,6 +56,7 @@ SIGNATURES = {
     "ks_set_profiling": (C.c_int, [_P, C.c_int]),
     "ks_set_buffer_limits": (C.c_int, [_P, _I64, _I64]),
     "ks_set_l2_flush": (C.c_int, [_P, _I64]),
+    "ks_set_tuning": (C.c_int, [_P, C.c_char_p, _I64]),
     "ks_run": (C.c_int, [_P, _I64]),
     "ks_take_conjunctions": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),

@@ -60,6 +60,7 @@ struct ks_ctx {
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> ev;
     ks_timing timing{};
+    ks::Tuning tune;
     void* l2_flush = nullptr;
     int64_t l2_flush_bytes = 0;
 };
@@ -93,12 +94,13 @@ void drop_graphs(ks_ctx* ctx) {
 void free_objects(ks_ctx* ctx) {
     ks::DeviceBuffers& b = ctx->b;
     for (int k = 0; k < 2; ++k) { dfree(b.state[k]); dfree(b.alive[k]); dfree(b.keys[k]); dfree(b.idx[k]); }
-    dfree(b.size_m); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.tile_hist); dfree(b.block_counts);
+    dfree(b.size_m); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
+    dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr); dfree(b.scan_part); dfree(b.item_count);
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_of); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted_orig);
     b.cap = 0;
     b.hash_cap = 0;
-    b.tile_hist_len = 0;
+    b.sort_status_len = 0;
 }
 
 int ensure_objects(ks_ctx* ctx, int64_t n) {
@@ -117,8 +119,12 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.size_m, sizeof(double) * cap));
     KS_CUDA(cudaMalloc(&b.ckpt_state, sizeof(double) * 6 * cap));
     KS_CUDA(cudaMalloc(&b.ckpt_alive, cap));
-    b.tile_hist_len = 256 * ((cap + 2047) / 2048);
-    KS_CUDA(cudaMalloc(&b.tile_hist, sizeof(unsigned int) * b.tile_hist_len));
+    b.sort_status_len = 8 * 256 * ((cap + 2047) / 2048);
+    KS_CUDA(cudaMalloc(&b.sort_hist, sizeof(unsigned int) * 8 * 256));
+    KS_CUDA(cudaMalloc(&b.sort_status, sizeof(unsigned int) * b.sort_status_len));
+    KS_CUDA(cudaMalloc(&b.sort_ctr, sizeof(unsigned int) * 8));
+    KS_CUDA(cudaMalloc(&b.scan_part, sizeof(unsigned int) * ((cap + 4095) / 4096 + 1)));
+    KS_CUDA(cudaMalloc(&b.item_count, sizeof(unsigned int) * (cap + 1)));
     KS_CUDA(cudaMalloc(&b.block_counts, sizeof(int) * ((cap + 1023) / 1024 + 1)));
     KS_CUDA(cudaMalloc(&b.cell_begin, sizeof(int) * (cap + 1)));
     KS_CUDA(cudaMalloc(&b.cell_key, sizeof(unsigned long long) * cap));
@@ -142,6 +148,16 @@ int ensure_survivors(ks_ctx* ctx, int64_t want) {
     ctx->b.surv_cap = 0;
     KS_CUDA(cudaMalloc(&ctx->b.survivors, sizeof(int2) * want));
     ctx->b.surv_cap = want;
+    return KS_OK;
+}
+
+int ensure_items(ks_ctx* ctx, int64_t want) {
+    if (want <= ctx->b.items_cap) return KS_OK;
+    drop_graphs(ctx);
+    dfree(ctx->b.items);
+    ctx->b.items_cap = 0;
+    KS_CUDA(cudaMalloc(&ctx->b.items, sizeof(int4) * want));
+    ctx->b.items_cap = want;
     return KS_OK;
 }
 
@@ -246,6 +262,7 @@ void fill_params(ks_ctx* ctx, int k_steps, double t_start, int64_t step0, double
 
 StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     StepArgs a{};
+    a.tune = ctx->tune;
     a.fc = force_consts();
     a.dt = ctx->dt;
     a.threshold_km = ctx->thr;
@@ -382,21 +399,25 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
         int flags = ctx->h_chunk->flags;
         unsigned long long max_refined = 0;
-        int max_bits = 0;
+        int max_bits = 0, max_items = 0;
         for (int k = 0; k < k_steps; ++k) {
             flags |= ctx->h_ctrl[k].flags;
             max_refined = std::max(max_refined, ctx->h_ctrl[k].refined);
             max_bits = std::max(max_bits, ctx->h_ctrl[k].grid.bits);
+            max_items = std::max(max_items, ctx->h_ctrl[k].n_items);
         }
         const bool surv_over = max_refined > static_cast<unsigned long long>(ctx->b.surv_cap);
+        const bool items_over = max_items > ctx->b.items_cap;
         if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds");
-        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over) break;
+        if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) break;
         if (attempt >= kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after replays");
         if (flags & ks::FLAG_SORT_BITS) {
             ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(max_bits));
             drop_graphs(ctx);
         }
         if (surv_over && (rc = ensure_survivors(ctx, static_cast<int64_t>(max_refined) * 2))) return rc;
+        if (items_over && (rc = ensure_items(ctx, static_cast<int64_t>(max_items) * 3 / 2 + 1024))) return rc;
         if ((flags & ks::FLAG_CONJ_OVERFLOW) &&
             (rc = ensure_conj(ctx, static_cast<int64_t>(ctx->h_chunk->conj_count) * 2)))
             return rc;
@@ -487,6 +508,7 @@ int ks_create(int device, ks_ctx** out) {
         rc = KS_ERR_CUDA;
     if (!rc) rc = ensure_chunk(ctx, 64);
     if (!rc) rc = ensure_survivors(ctx, 1 << 20);
+    if (!rc) rc = ensure_items(ctx, 1 << 18);
     if (!rc) rc = ensure_conj(ctx, 1 << 16);
     if (rc) {
         ks_destroy(ctx);
@@ -504,6 +526,7 @@ void ks_destroy(ks_ctx* ctx) {
     free_objects(ctx);
     if (ctx->l2_flush) cudaFree(ctx->l2_flush);
     dfree(ctx->b.survivors);
+    dfree(ctx->b.items);
     dfree(ctx->b.conj);
     dfree(ctx->b.ctrl);
     dfree(ctx->b.chunk);
@@ -629,6 +652,16 @@ int ks_set_buffer_limits(ks_ctx* ctx, int64_t survivor_pairs, int64_t conjunctio
     return KS_OK;
 }
 
+int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
+    if (!ctx || !key) return KS_ERR_ARG;
+    const std::string k(key);
+    if (k == "pair_variant" && (value == 0 || value == 1)) ctx->tune.pair_variant = static_cast<int>(value);
+    else if (k == "pair_blocks_per_sm" && value >= 0 && value <= 32) ctx->tune.pair_blocks_per_sm = static_cast<int>(value);
+    else return fail(ctx, KS_ERR_ARG, "ks_set_tuning: unknown key or value out of range: " + k);
+    drop_graphs(ctx);
+    return KS_OK;
+}
+
 int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes) {
     if (!ctx || bytes < 0) return fail(ctx, KS_ERR_ARG, "ks_set_l2_flush: bad arguments");
     cudaSetDevice(ctx->device);
@@ -736,8 +769,10 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         const Ctrl& c = ctx->h_ctrl[0];
         const int flags = c.flags | ctx->h_chunk->flags;
         const bool surv_over = c.refined > static_cast<unsigned long long>(ctx->b.surv_cap);
+        const bool items_over = c.n_items > ctx->b.items_cap;
         if (flags & ks::FLAG_KEY_RANGE) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds"); }
-        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over) {
+        if (flags & ks::FLAG_TIMEOUT) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up"); }
+        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) {
             st.step = 0;
             st.candidate_pairs = static_cast<int64_t>(c.candidates);
             st.refined_pairs = static_cast<int64_t>(c.refined);
@@ -751,6 +786,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         if (attempt >= kMaxReplays) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_OVERFLOW, "ks_screen: buffers overflow"); }
         if (flags & ks::FLAG_SORT_BITS) ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(c.grid.bits));
         if (surv_over && (rc = ensure_survivors(ctx, static_cast<int64_t>(c.refined) * 2))) { ctx->dt = saved_dt; return rc; }
+        if (items_over && (rc = ensure_items(ctx, static_cast<int64_t>(c.n_items) * 3 / 2 + 1024))) { ctx->dt = saved_dt; return rc; }
         if ((flags & ks::FLAG_CONJ_OVERFLOW) && (rc = ensure_conj(ctx, static_cast<int64_t>(ctx->h_chunk->conj_count) * 2))) {
             ctx->dt = saved_dt;
             return rc;

@@ -10,6 +10,9 @@
 //   cells        begin offsets, keys, owning cell per sorted entry, 13 forward neighbours per cell
 //   hash         open-addressing table cell key -> cell index
 //   sorted       start-of-step states gathered in cell order (AoS, 6 doubles per entry)
+//   items        pair work list: (cell, row block, first column block, column blocks);
+//                a cell's columns are its own objects then its 13 forward
+//                neighbours' objects, in blocks of 32
 //   survivors    pairs sent to refinement (int2, i < j)
 //   conj         conjunction records of the current chunk of steps
 #pragma once
@@ -45,7 +48,11 @@ enum : int {
     FLAG_CONJ_OVERFLOW = 2,
     FLAG_SORT_BITS = 4,      // more key bits than the sort passes launched cover
     FLAG_KEY_RANGE = 8,      // a key fell outside its grid bounds
+    FLAG_ITEMS_OVERFLOW = 16,  // pair work list longer than its buffer
+    FLAG_TIMEOUT = 32,       // a bounded device-side wait gave up
 };
+
+constexpr int kColBlocksPerItem = 16;  // column blocks of 32 per pair work item
 
 // Per-step control block, device resident.
 struct Ctrl {
@@ -64,6 +71,7 @@ struct Ctrl {
     unsigned long long exact_evals;    // candidates that needed the full filter
     int n_alive;                       // alive after the step
     int n_cells;
+    int n_items;                       // pair work items
     int max_cell;
     int flags;
     GridParams grid;
@@ -84,13 +92,19 @@ struct DeviceBuffers {
     uint8_t* ckpt_alive = nullptr;
     unsigned long long* keys[2] = {nullptr, nullptr};
     int* idx[2] = {nullptr, nullptr};
-    unsigned int* tile_hist = nullptr;     // 256 x tiles, for one radix pass
-    int64_t tile_hist_len = 0;
+    unsigned int* sort_hist = nullptr;     // 8 passes x 256 digits (global offsets)
+    unsigned int* sort_status = nullptr;   // look-back words: passes x tiles x 256
+    int64_t sort_status_len = 0;
+    unsigned int* sort_ctr = nullptr;      // tile tickets, one per pass
+    unsigned int* scan_part = nullptr;     // partial sums of the device-wide scans
     int* block_counts = nullptr;           // cell heads per tile
     int* cell_begin = nullptr;             // cap + 1
     unsigned long long* cell_key = nullptr;
     int* cell_of = nullptr;                // owning cell per sorted entry
     int* nbr = nullptr;                    // 13 per cell
+    unsigned int* item_count = nullptr;    // work items per cell, then their offsets
+    int4* items = nullptr;
+    int64_t items_cap = 0;
     unsigned long long* hash_keys = nullptr;
     int* hash_vals = nullptr;
     int64_t hash_cap = 0;                  // power of two
@@ -106,8 +120,15 @@ struct DeviceBuffers {
     StepParams* params = nullptr;          // max_chunk entries
 };
 
+// Launch-shape knobs (set through ks_set_tuning; 0 = default).
+struct Tuning {
+    int pair_variant = 1;         // 0: two columns per lane, 1: one column per lane
+    int pair_blocks_per_sm = 0;   // resident blocks of the pair kernel
+};
+
 // Everything a step's kernels need, by value.
 struct StepArgs {
+    Tuning tune;
     ForceConsts fc;
     double dt;
     double threshold_km;

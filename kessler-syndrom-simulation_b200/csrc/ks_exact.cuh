@@ -50,30 +50,33 @@ __device__ __forceinline__ void accel_exact(const ForceConsts& fc, double rx, do
 }
 
 // rk4(s, dt, rm0, rm1, rm2) (src/core/orbital.cpp:107-118). s is updated in place.
+// The stage derivatives are folded into `acc` as they come, which keeps the
+// reference's summation order ((k1 + 2 k2) + 2 k3) + k4 with fewer live registers.
 __device__ __forceinline__ void rk4_exact(const ForceConsts& fc, double dt, const MoonStage& m0,
                                           const MoonStage& m1, const MoonStage& m2, double s[6]) {
     const double h2 = xdiv(dt, 2.0);
-    double k1[6], k2[6], k3[6], k4[6], y[3];
-    k1[0] = s[3]; k1[1] = s[4]; k1[2] = s[5];
-    accel_exact(fc, s[0], s[1], s[2], m0, k1[3], k1[4], k1[5]);
+    double k[6], acc[6], y[3];
+    k[0] = s[3]; k[1] = s[4]; k[2] = s[5];
+    accel_exact(fc, s[0], s[1], s[2], m0, k[3], k[4], k[5]);
+    for (int q = 0; q < 6; ++q) acc[q] = k[q];
 
-    for (int q = 0; q < 3; ++q) y[q] = xadd(s[q], xmul(k1[q], h2));
-    for (int q = 0; q < 3; ++q) k2[q] = xadd(s[3 + q], xmul(k1[3 + q], h2));
-    accel_exact(fc, y[0], y[1], y[2], m1, k2[3], k2[4], k2[5]);
+    for (int q = 0; q < 3; ++q) y[q] = xadd(s[q], xmul(k[q], h2));
+    for (int q = 0; q < 3; ++q) k[q] = xadd(s[3 + q], xmul(k[3 + q], h2));
+    accel_exact(fc, y[0], y[1], y[2], m1, k[3], k[4], k[5]);
+    for (int q = 0; q < 6; ++q) acc[q] = xadd(acc[q], xmul(k[q], 2.0));
 
-    for (int q = 0; q < 3; ++q) y[q] = xadd(s[q], xmul(k2[q], h2));
-    for (int q = 0; q < 3; ++q) k3[q] = xadd(s[3 + q], xmul(k2[3 + q], h2));
-    accel_exact(fc, y[0], y[1], y[2], m1, k3[3], k3[4], k3[5]);
+    for (int q = 0; q < 3; ++q) y[q] = xadd(s[q], xmul(k[q], h2));
+    for (int q = 0; q < 3; ++q) k[q] = xadd(s[3 + q], xmul(k[3 + q], h2));
+    accel_exact(fc, y[0], y[1], y[2], m1, k[3], k[4], k[5]);
+    for (int q = 0; q < 6; ++q) acc[q] = xadd(acc[q], xmul(k[q], 2.0));
 
-    for (int q = 0; q < 3; ++q) y[q] = xadd(s[q], xmul(k3[q], dt));
-    for (int q = 0; q < 3; ++q) k4[q] = xadd(s[3 + q], xmul(k3[3 + q], dt));
-    accel_exact(fc, y[0], y[1], y[2], m2, k4[3], k4[4], k4[5]);
+    for (int q = 0; q < 3; ++q) y[q] = xadd(s[q], xmul(k[q], dt));
+    for (int q = 0; q < 3; ++q) k[q] = xadd(s[3 + q], xmul(k[3 + q], dt));
+    accel_exact(fc, y[0], y[1], y[2], m2, k[3], k[4], k[5]);
+    for (int q = 0; q < 6; ++q) acc[q] = xadd(acc[q], k[q]);
 
     const double h6 = xdiv(dt, 6.0);
-    for (int q = 0; q < 6; ++q) {
-        const double sum = xadd(xadd(xadd(k1[q], xmul(k2[q], 2.0)), xmul(k3[q], 2.0)), k4[q]);
-        s[q] = xadd(s[q], xmul(sum, h6));
-    }
+    for (int q = 0; q < 6; ++q) s[q] = xadd(s[q], xmul(acc[q], h6));
 }
 
 enum : int { FILTER_REJECT = 0, FILTER_REFINE = 1, FILTER_CO_ORBITING = 2 };

@@ -29,6 +29,7 @@ constexpr int kSortTile = 2048;            // keys per radix tile (256 threads x
 constexpr int kSortItems = kSortTile / kBlock;
 constexpr int kWarps = kBlock / 32;
 constexpr int kCellTile = 1024;            // sorted entries per cell-build tile
+constexpr int kPropBlock = 128;            // propagation: 168 registers, 3 blocks per SM
 
 // Forward neighbour offsets (src/core/collision_filter.hpp:137-140): with the
 // pairs inside a cell they visit every pair of neighbouring cells once.
@@ -163,15 +164,16 @@ __device__ void flush_spec(SpecAccum& s, Ctrl* cur, Ctrl* next, bool screening) 
         sh_bad[warp] = bd;
     }
     __syncthreads();
+    const int nwarps = blockDim.x >> 5;
     if (threadIdx.x == 0) {
-        for (int w = 1; w < kWarps; ++w) {
+        for (int w = 1; w < nwarps; ++w) {
             vals[0] = max(vals[0], sh[w][0]);
             vals[1] = max(vals[1], sh[w][1]);
             for (int a = 0; a < 3; ++a) { vals[2 + a] = min(vals[2 + a], sh[w][2 + a]); vals[5 + a] = max(vals[5 + a], sh[w][5 + a]); }
             vals[8] += sh[w][8];
         }
         int alive = 0, bad = 0;
-        for (int w = 0; w < kWarps; ++w) { alive += sh_alive[w]; bad |= sh_bad[w]; }
+        for (int w = 0; w < nwarps; ++w) { alive += sh_alive[w]; bad |= sh_bad[w]; }
         atomicAdd(&cur->n_alive, alive);
         atomicAdd(&cur->object_steps, vals[8]);
         if (screening) {
@@ -244,7 +246,7 @@ __global__ void k_seed_ctrl(const double* __restrict__ st, int64_t stride, const
 // Propagation
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBlock) k_propagate_exact(StepArgs a, const double* __restrict__ in,
+__global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, const double* __restrict__ in,
                                                             double* __restrict__ out,
                                                             const uint8_t* __restrict__ alive_in,
                                                             uint8_t* __restrict__ alive_out,
@@ -359,83 +361,193 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
 }
 
 // ---------------------------------------------------------------------------
-// Radix sort (LSD, 8-bit digits, stable)
+// Device-wide exclusive scan of u32 counters (length read from device memory)
 // ---------------------------------------------------------------------------
 
-// Per-tile digit counts, stored digit-major: hist[d * ntiles + tile].
-__global__ void __launch_bounds__(kBlock) k_sort_hist(const unsigned long long* __restrict__ keys, int n,
-                                                      int shift, unsigned int* __restrict__ hist, int ntiles,
-                                                      Ctrl* ctrl, int check_bits) {
-    __shared__ unsigned int h[256];
-    h[threadIdx.x] = 0;
-    __syncthreads();
-    const int base = blockIdx.x * kSortTile;
-    for (int j = 0; j < kSortItems; ++j) {
-        const int p = base + j * kBlock + threadIdx.x;
-        const bool valid = p < n;
-        const unsigned d = valid ? static_cast<unsigned>((keys[p] >> shift) & 0xFF) : 256u + (threadIdx.x & 31);
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        if (valid && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
-    }
-    __syncthreads();
-    hist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
-    if (check_bits && blockIdx.x == 0 && threadIdx.x == 0 && ctrl->grid.bits + 1 > check_bits)
-        atomicOr(&ctrl->flags, FLAG_SORT_BITS);
-}
+constexpr int kScanTile = 4096;  // 256 threads x 16
 
-// Exclusive scan of `len` counters in place, one block.
-__global__ void __launch_bounds__(1024) k_scan_exclusive(unsigned int* __restrict__ v, int len) {
-    __shared__ unsigned int warp_tot[32];
-    const int per = (len + blockDim.x - 1) / blockDim.x;
-    const int b0 = threadIdx.x * per;
-    const int b1 = min(len, b0 + per);
-    unsigned int sum = 0;
-    for (int k = b0; k < b1; ++k) sum += v[k];
-    // Block-wide exclusive scan of the per-thread sums.
+__device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int v, unsigned int* total) {
+    __shared__ unsigned int wsum[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned int incl = sum;
+    unsigned int incl = v;
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
-    if (lane == 31) warp_tot[warp] = incl;
+    if (lane == 31) wsum[warp] = incl;
     __syncthreads();
-    if (warp == 0) {
-        unsigned int t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned int y = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= o) t += y;
-        }
-        warp_tot[lane] = t;  // inclusive over warps
+    unsigned int off = 0, tot = 0;
+    for (int w = 0; w < kWarps; ++w) {
+        if (w < warp) off += wsum[w];
+        tot += wsum[w];
     }
     __syncthreads();
-    unsigned int run = incl - sum + (warp > 0 ? warp_tot[warp - 1] : 0);
-    for (int k = b0; k < b1; ++k) {
-        const unsigned int c = v[k];
-        v[k] = run;
-        run += c;
+    *total = tot;
+    return off + incl - v;
+}
+
+// Per-tile sums of v[0..len).
+__global__ void __launch_bounds__(kBlock) k_scan_partials(const unsigned int* __restrict__ v, const int* len_ptr,
+                                                          int len_fixed, unsigned int* __restrict__ part) {
+    const int len = len_ptr ? *len_ptr : len_fixed;
+    const int base = blockIdx.x * kScanTile;
+    unsigned int s = 0;
+    if (base < len)
+        for (int j = threadIdx.x; j < kScanTile; j += kBlock) {
+            const int p = base + j;
+            if (p < len) s += v[p];
+        }
+    s = warp_sum(s);
+    __shared__ unsigned int sh[kWarps];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = 0;
+        for (int w = 0; w < kWarps; ++w) t += sh[w];
+        part[blockIdx.x] = t;
     }
 }
 
-// Stable scatter of one tile: ranks inside each warp with __match_any_sync,
-// orders the tile by digit in shared memory, then writes runs of equal digits
-// to consecutive global addresses.
-__global__ void __launch_bounds__(kBlock) k_sort_scatter(const unsigned long long* __restrict__ keys_in,
-                                                         const int* __restrict__ idx_in,
-                                                         unsigned long long* __restrict__ keys_out,
-                                                         int* __restrict__ idx_out, int n, int shift,
-                                                         const unsigned int* __restrict__ hist, int ntiles) {
+// Exclusive scan in place, one block, coalesced rounds of 1024 entries.
+// Optionally stores the grand total.
+__global__ void __launch_bounds__(1024) k_scan_small(unsigned int* __restrict__ v, int len,
+                                                     unsigned int* __restrict__ total) {
+    __shared__ unsigned int wsum[32];
+    __shared__ unsigned int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = 0; r < len; r += 1024) {
+        const int p = r + threadIdx.x;
+        const unsigned int x = p < len ? v[p] : 0u;
+        unsigned int incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned int t = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            wsum[lane] = t;
+        }
+        __syncthreads();
+        const unsigned int c = carry;
+        if (p < len) v[p] = c + incl - x + (warp > 0 ? wsum[warp - 1] : 0u);
+        __syncthreads();
+        if (threadIdx.x == 0) carry = c + wsum[31];
+        __syncthreads();
+    }
+    if (total && threadIdx.x == 0) *total = carry;
+}
+
+// out[p] = exclusive prefix of v at p (in place allowed), tile offsets from part.
+__global__ void __launch_bounds__(kBlock) k_scan_apply(unsigned int* __restrict__ v, const int* len_ptr, int len_fixed,
+                                                       const unsigned int* __restrict__ part) {
+    const int len = len_ptr ? *len_ptr : len_fixed;
+    const int base = blockIdx.x * kScanTile;
+    if (base >= len) return;
+    constexpr int kPer = kScanTile / kBlock;
+    const int p0 = base + threadIdx.x * kPer;
+    unsigned int x[kPer];
+    unsigned int s = 0;
+    for (int j = 0; j < kPer; ++j) {
+        x[j] = (p0 + j < len) ? v[p0 + j] : 0u;
+        s += x[j];
+    }
+    unsigned int tot;
+    unsigned int run = part[blockIdx.x] + block_exclusive_scan(s, &tot);
+    for (int j = 0; j < kPer; ++j) {
+        if (p0 + j < len) v[p0 + j] = run;
+        run += x[j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort: LSD, 8-bit digits, one pass per digit with decoupled look-back
+// (each tile publishes its digit counts, then sums its predecessors' counts).
+// ---------------------------------------------------------------------------
+
+constexpr unsigned int kStatAgg = 1u << 30;   // tile's own count is published
+constexpr unsigned int kStatInc = 2u << 30;   // count includes all previous tiles
+constexpr unsigned int kStatMask = (1u << 30) - 1;
+constexpr int kLookbackLimit = 1 << 22;       // polls before a wait gives up
+
+__device__ __forceinline__ unsigned int ld_relaxed(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Digit histograms of every pass in one read of the keys.
+__global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long long* __restrict__ keys, int n,
+                                                         int passes, unsigned int* __restrict__ hist, Ctrl* ctrl) {
+    __shared__ unsigned int h[8][256];
+    for (int p = 0; p < 8; ++p) h[p][threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+    const int lane = threadIdx.x & 31;
+    for (int j = 0; j < kSortItems; ++j) {
+        const int p = base + j * kBlock + threadIdx.x;
+        const bool valid = p < n;
+        const unsigned long long k = valid ? keys[p] : 0ull;
+        for (int pass = 0; pass < passes; ++pass) {
+            const unsigned d = valid ? static_cast<unsigned>((k >> (8 * pass)) & 0xFF) : 256u + lane;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[pass][d], __popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int pass = 0; pass < passes; ++pass) {
+        const unsigned int c = h[pass][threadIdx.x];
+        if (c) atomicAdd(&hist[pass * 256 + threadIdx.x], c);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ctrl->grid.bits + 1 > 8 * passes)
+        atomicOr(&ctrl->flags, FLAG_SORT_BITS);
+}
+
+// Exclusive scan over the 256 digits of each pass.
+__global__ void __launch_bounds__(kBlock) k_sort_digit_scan(unsigned int* __restrict__ hist, int passes) {
+    for (int pass = 0; pass < passes; ++pass) {
+        const unsigned int c = hist[pass * 256 + threadIdx.x];
+        unsigned int tot;
+        const unsigned int e = block_exclusive_scan(c, &tot);
+        hist[pass * 256 + threadIdx.x] = e;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long long* __restrict__ keys_in,
+                                                          const int* __restrict__ idx_in,
+                                                          unsigned long long* __restrict__ keys_out,
+                                                          int* __restrict__ idx_out, int n, int shift,
+                                                          const unsigned int* __restrict__ digit_base,
+                                                          unsigned int* __restrict__ status,
+                                                          unsigned int* __restrict__ ticket, Ctrl* ctrl) {
     __shared__ unsigned int wcnt[kWarps][256];
     __shared__ int gbase[256];
     __shared__ unsigned long long skeys[kSortTile];
     __shared__ int sidx[kSortTile];
+    __shared__ int tile_sh;
+    __shared__ int timed_out;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tile0 = blockIdx.x * kSortTile;
-    const int count = min(kSortTile, n - tile0);
+    if (threadIdx.x == 0) {
+        tile_sh = static_cast<int>(atomicAdd(ticket, 1u));  // tiles start in ticket order
+        timed_out = 0;
+    }
     for (int w = 0; w < kWarps; ++w) wcnt[w][threadIdx.x] = 0;
     __syncthreads();
+    const int tile = tile_sh;
+    const int tile0 = tile * kSortTile;
+    const int count = min(kSortTile, n - tile0);
 
-    // Each warp owns kSortTile / kWarps consecutive keys, read 32 at a time.
     constexpr int kPerWarp = kSortTile / kWarps;
     constexpr int kRounds = kPerWarp / 32;
     unsigned long long k[kRounds];
@@ -443,8 +555,8 @@ __global__ void __launch_bounds__(kBlock) k_sort_scatter(const unsigned long lon
     unsigned d[kRounds];
     for (int r = 0; r < kRounds; ++r) {
         const int l = warp * kPerWarp + r * 32 + lane;
-        const int p = tile0 + l;
         const bool valid = l < count;
+        const int p = tile0 + l;
         k[r] = valid ? keys_in[p] : 0ull;
         id[r] = valid ? (idx_in ? idx_in[p] : p) : 0;
         d[r] = valid ? static_cast<unsigned>((k[r] >> shift) & 0xFF) : 256u + lane;
@@ -453,31 +565,46 @@ __global__ void __launch_bounds__(kBlock) k_sort_scatter(const unsigned long lon
         __syncwarp();
     }
     __syncthreads();
-    {
-        // Thread t owns digit t: tile total, then exclusive scan across digits.
-        const int t = threadIdx.x;
-        unsigned int tot = 0;
-        for (int w = 0; w < kWarps; ++w) tot += wcnt[w][t];
-        __shared__ unsigned int wsum[kWarps];
-        unsigned int incl = tot;
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+    // Thread t owns digit t.
+    const int t = threadIdx.x;
+    unsigned int tot = 0;
+    for (int w = 0; w < kWarps; ++w) tot += wcnt[w][t];
+    unsigned int* my = status + static_cast<int64_t>(tile) * 256 + t;
+    st_relaxed(my, (tile == 0 ? kStatInc : kStatAgg) | tot);
+    unsigned int excl = 0;
+    if (tile > 0) {
+        int j = tile - 1;
+        int polls = 0;
+        while (true) {
+            const unsigned int v = ld_relaxed(status + static_cast<int64_t>(j) * 256 + t);
+            const unsigned int flag = v & ~kStatMask;
+            if (flag == 0) {
+                if (++polls > kLookbackLimit) {
+                    timed_out = 1;
+                    break;
+                }
+                continue;
+            }
+            excl += v & kStatMask;
+            if (flag == kStatInc) break;
+            --j;
         }
-        if (lane == 31) wsum[warp] = incl;
-        __syncthreads();
-        unsigned int off = 0;
-        for (int w = 0; w < warp; ++w) off += wsum[w];
-        const unsigned int start = off + incl - tot;
-        gbase[t] = static_cast<int>(hist[t * ntiles + blockIdx.x]) - static_cast<int>(start);
-        unsigned int run = start;
-        for (int w = 0; w < kWarps; ++w) {
-            const unsigned int c = wcnt[w][t];
-            wcnt[w][t] = run;
-            run += c;
-        }
+        st_relaxed(my, kStatInc | (excl + tot));
+    }
+    unsigned int unused;
+    const unsigned int start = block_exclusive_scan(tot, &unused);
+    gbase[t] = static_cast<int>(digit_base[t] + excl) - static_cast<int>(start);
+    unsigned int run = start;
+    for (int w = 0; w < kWarps; ++w) {
+        const unsigned int c = wcnt[w][t];
+        wcnt[w][t] = run;
+        run += c;
     }
     __syncthreads();
+    if (timed_out) {
+        if (threadIdx.x == 0) atomicOr(&ctrl->flags, FLAG_TIMEOUT);
+        return;  // results of this step are discarded by the host
+    }
     for (int r = 0; r < kRounds; ++r) {
         const bool valid = (warp * kPerWarp + r * 32 + lane) < count;
         const unsigned peers = __match_any_sync(0xffffffffu, d[r]);
@@ -493,10 +620,11 @@ __global__ void __launch_bounds__(kBlock) k_sort_scatter(const unsigned long lon
     __syncthreads();
     for (int l = threadIdx.x; l < count; l += kBlock) {
         const unsigned long long kk = skeys[l];
-        const unsigned dd = static_cast<unsigned>((kk >> shift) & 0xFF);
-        const int dst = gbase[dd] + l;
-        keys_out[dst] = kk;
-        idx_out[dst] = sidx[l];
+        const int dst = gbase[static_cast<unsigned>((kk >> shift) & 0xFF)] + l;
+        if (dst >= 0 && dst < n) {
+            keys_out[dst] = kk;
+            idx_out[dst] = sidx[l];
+        }
     }
 }
 
@@ -541,27 +669,17 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         if (blockIdx.x == 0 && threadIdx.x == 0) { ctrl->n_cells = 0; cell_begin[0] = 0; }
         return;
     }
+    if (blockIdx.x * kCellTile >= m) return;
     const int p0 = blockIdx.x * kCellTile + threadIdx.x * kPer;
     int heads[kPer];
-    int local = 0;
+    unsigned int local = 0;
     for (int j = 0; j < kPer; ++j) {
         const int p = p0 + j;
         heads[j] = (p < m && (p == 0 || keys[p] != keys[p - 1])) ? 1 : 0;
         local += heads[j];
     }
-    // Block exclusive scan of `local`.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = local;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    __shared__ int wsum[kWarps];
-    if (lane == 31) wsum[warp] = incl;
-    __syncthreads();
-    int off = static_cast<int>(offsets[blockIdx.x]);
-    for (int w = 0; w < warp; ++w) off += wsum[w];
-    int run = off + incl - local;  // heads before this thread's first entry
+    unsigned int unused;
+    int run = static_cast<int>(offsets[blockIdx.x] + block_exclusive_scan(local, &unused));
     for (int j = 0; j < kPer; ++j) {
         const int p = p0 + j;
         if (p >= m) break;
@@ -581,7 +699,10 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         cell_of[p] = cid;
         const int o = idx[p];
         sorted_orig[p] = o;
-        for (int q = 0; q < 6; ++q) sorted[6 * static_cast<int64_t>(p) + q] = before[q * stride + o];
+        double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
+        dst[0] = make_double2(before[o], before[stride + o]);
+        dst[1] = make_double2(before[2 * stride + o], before[3 * stride + o]);
+        dst[2] = make_double2(before[4 * stride + o], before[5 * stride + o]);
         if (p == m - 1) {
             ctrl->n_cells = cid + 1;
             cell_begin[cid + 1] = m;
@@ -589,21 +710,33 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
     }
 }
 
+__device__ __forceinline__ unsigned int cell_items(int k, int L) {
+    const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
+    unsigned int items = 0;
+    for (int a = 0; a < ta; ++a) items += static_cast<unsigned int>((tc - a + kColBlocksPerItem - 1) / kColBlocksPerItem);
+    return items;
+}
+
+// Per cell: the 13 forward neighbours, the candidate-pair count
+// k(k-1)/2 + k * (neighbour objects) and the number of pair work items.
 __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                        const unsigned long long* __restrict__ cell_key_in,
                                                        const unsigned long long* __restrict__ hk,
                                                        const int* __restrict__ hv, unsigned long long hmask,
-                                                       int* __restrict__ nbr) {
+                                                       int* __restrict__ nbr, unsigned int* __restrict__ item_count) {
     const int nc = ctrl->n_cells;
     const GridParams g = ctrl->grid;
     const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
     int biggest = 0;
+    unsigned long long cand = 0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-        biggest = max(biggest, cell_begin[c + 1] - cell_begin[c]);
+        const int k = cell_begin[c + 1] - cell_begin[c];
+        biggest = max(biggest, k);
         const unsigned long long key = cell_key_in[c];
         const long long cz = static_cast<long long>(key & mz);
         const long long cy = static_cast<long long>((key >> g.w[2]) & my);
         const long long cx = static_cast<long long>(key >> (g.w[1] + g.w[2]));
+        int others = 0;
         for (int o = 0; o < 13; ++o) {
             const long long x = cx + c_forward[o][0], y = cy + c_forward[o][1], z = cz + c_forward[o][2];
             int found = -1;
@@ -614,14 +747,56 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const int* __
                 found = hash_find(hk, hv, hmask, nk);
             }
             nbr[13 * static_cast<int64_t>(c) + o] = found;
+            if (found >= 0) others += cell_begin[found + 1] - cell_begin[found];
         }
+        cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * others;
+        item_count[c] = cell_items(k, k + others);
     }
     biggest = warp_max(biggest);
-    if ((threadIdx.x & 31) == 0 && biggest > 0) atomicMax(&ctrl->max_cell, biggest);
+    cand = warp_sum(cand);
+    if ((threadIdx.x & 31) == 0) {
+        if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
+        if (cand) atomicAdd(&ctrl->candidates, cand);
+    }
+}
+
+// Writes each cell's work items at its scanned offset.
+__global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
+                                                        const int* __restrict__ nbr,
+                                                        const unsigned int* __restrict__ item_off,
+                                                        int4* __restrict__ items, int64_t items_cap) {
+    const int nc = ctrl->n_cells;
+    bool over = false;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        const int k = cell_begin[c + 1] - cell_begin[c];
+        int L = k;
+        for (int o = 0; o < 13; ++o) {
+            const int f = nbr[13 * static_cast<int64_t>(c) + o];
+            if (f >= 0) L += cell_begin[f + 1] - cell_begin[f];
+        }
+        const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
+        int64_t w = item_off[c];
+        for (int a = 0; a < ta; ++a)
+            for (int cb = a; cb < tc; cb += kColBlocksPerItem) {
+                if (w < items_cap) items[w] = make_int4(c, a, cb, min(kColBlocksPerItem, tc - cb));
+                else over = true;
+                ++w;
+            }
+    }
+    if (over) atomicOr(&ctrl->flags, FLAG_ITEMS_OVERFLOW);
 }
 
 // ---------------------------------------------------------------------------
-// Pairs
+// Pairs: one warp per work item. Lanes hold consecutive columns of the cell's
+// column list (its own objects, then those of its 13 forward neighbours); the
+// warp loops over up to 32 rows of the cell, broadcast from shared memory.
+// Inside the cell only pairs with column > row are visited, so every candidate
+// pair of the reference (src/core/collision.cpp:522-538) is seen exactly once.
+//
+// The row loop is branch-free: each lane evaluates a conservative distance
+// gate (no division, no square root) and records in a 32-bit mask the rows
+// that the gate cannot reject. Only those pairs then run the exact
+// filter_pair, after the loop.
 // ---------------------------------------------------------------------------
 
 struct SortedState {
@@ -634,78 +809,153 @@ __device__ __forceinline__ SortedState load_sorted(const double* __restrict__ so
     return SortedState{a.x, a.y, b.x, b.y, c.x, c.y};
 }
 
-__global__ void __launch_bounds__(kBlock) k_pairs_exact(StepArgs a, const double* __restrict__ sorted,
-                                                        const int* __restrict__ orig,
-                                                        const int* __restrict__ cell_of,
-                                                        const int* __restrict__ cell_begin,
-                                                        const int* __restrict__ nbr, int2* __restrict__ surv,
-                                                        int64_t surv_cap) {
-    const int m = a.ctrl->n_alive;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long cand = 0, co = 0, full = 0;
-    if (p < m) {
-        // Conservative distance gate bound: |dv| <= 2 * max speed.
-        const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
-        const double dt3 = a.dt * a.dt * a.dt;
-        const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
-        const double gate_hi2 = gate_hi * gate_hi;
-        const SortedState me = load_sorted(sorted, p);
-        const int my_orig = orig[p];
-        auto visit = [&](int q) {
-            ++cand;
-            const SortedState o = load_sorted(sorted, q);
-            const double rx = xsub(o.rx, me.rx), ry = xsub(o.ry, me.ry), rz = xsub(o.rz, me.rz);
-            const double vx = xsub(o.vx, me.vx), vy = xsub(o.vy, me.vy), vz = xsub(o.vz, me.vz);
-            const double r2 = xdot3(rx, ry, rz);
-            const double dv2 = xdot3(vx, vy, vz);
-            const double rv = xadd(xadd(xmul(rx, vx), xmul(ry, vy)), xmul(rz, vz));
-            if (certainly_far(r2, dv2, rv, gate_hi2)) return;
-            ++full;
-            const int res = filter_pair_exact(rx, ry, rz, vx, vy, vz, a.dt, a.threshold_km, a.vmin2);
-            if (res == FILTER_CO_ORBITING) ++co;
-            const bool keep = res == FILTER_REFINE;
-            const unsigned act = __activemask();
-            const unsigned bal = __ballot_sync(act, keep);
-            if (bal) {
-                const int leader = __ffs(bal) - 1;
-                unsigned long long base = 0;
-                if ((threadIdx.x & 31) == leader) base = atomicAdd(&a.ctrl->refined, static_cast<unsigned long long>(__popc(bal)));
-                base = __shfl_sync(act, base, leader);
-                if (keep) {
-                    const unsigned long long pos = base + __popc(bal & lanemask_lt());
-                    const int oq = orig[q];
-                    if (pos < static_cast<unsigned long long>(surv_cap))
-                        surv[pos] = make_int2(min(my_orig, oq), max(my_orig, oq));
-                }
-            }
-        };
-        const int c = cell_of[p];
-        const int b = cell_begin[c];
-        const int k = cell_begin[c + 1] - b;
-        const int u = p - b;
-        // Pairs inside the cell, balanced: object u meets the (k-1)/2 objects
-        // after it (cyclically), plus the opposite one when k is even and u < k/2.
-        const int half = (k - 1) / 2;
-        for (int mm = 1; mm <= half; ++mm) {
-            int q = u + mm;
-            if (q >= k) q -= k;
-            visit(b + q);
+// 1 if the pair may pass the distance gate of filter_pair. With
+// P = |dr|^2 |dv|^2 and m = min(dr.dv, 0), P - m^2 is |dv|^2 times the
+// smallest squared distance of the linear relative motion over t >= 0; the
+// gate can reject only if that exceeds |dv|^2 gate_hi^2. The 1e-12 P margin
+// covers the rounding of P - m^2 (contraction is allowed here).
+__device__ __forceinline__ unsigned gate_open(const SortedState& c, double2 ra, double2 rb, double2 rc,
+                                              double gate_hi2) {
+    const double rx = c.rx - ra.x, ry = c.ry - ra.y, rz = c.rz - rb.x;
+    const double vx = c.vx - rb.y, vy = c.vy - rc.x, vz = c.vz - rc.y;
+    const double r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    const double dv2 = fma(vx, vx, fma(vy, vy, vz * vz));
+    const double m = fmin(fma(rx, vx, fma(ry, vy, rz * vz)), 0.0);
+    const double P = r2 * dv2;
+    return fma(-m, m, P) <= fma(dv2, gate_hi2, 1e-12 * P) ? 1u : 0u;
+}
+
+struct PairCounters {
+    unsigned long long co = 0, full = 0;
+};
+
+// Exact filter for the rows flagged in `need` against this lane's column;
+// pairs sent to refinement are appended with one atomic per warp and row.
+__device__ __forceinline__ void exact_rows(unsigned need, const SortedState& col, int col_orig,
+                                           const double2 (*rows)[3], const int* rorig, const StepArgs& a,
+                                           int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc) {
+    const int lane = threadIdx.x & 31;
+    unsigned todo = __reduce_or_sync(0xffffffffu, need);
+    while (todo) {
+        const int r = __ffs(todo) - 1;
+        todo &= todo - 1;
+        int res = FILTER_REJECT;
+        if ((need >> r) & 1u) {
+            const double2 ra = rows[r][0], rb = rows[r][1], rc = rows[r][2];
+            ++pc.full;
+            res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
+                                    xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
+            if (res == FILTER_CO_ORBITING) ++pc.co;
         }
-        if ((k & 1) == 0 && u < k / 2) visit(b + u + k / 2);
-        for (int o = 0; o < 13; ++o) {
-            const int nc = nbr[13 * static_cast<int64_t>(c) + o];
-            if (nc < 0) continue;
-            const int q1 = cell_begin[nc + 1];
-            for (int q = cell_begin[nc]; q < q1; ++q) visit(q);
+        const bool keep = res == FILTER_REFINE;
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (bal) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(&a.ctrl->refined, static_cast<unsigned long long>(__popc(bal)));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep) {
+                const unsigned long long pos = base + __popc(bal & lanemask_lt());
+                const int ro = rorig[r];
+                if (pos < static_cast<unsigned long long>(surv_cap))
+                    surv[pos] = make_int2(min(ro, col_orig), max(ro, col_orig));
+            }
         }
     }
-    cand = warp_sum(cand);
-    co = warp_sum(co);
-    full = warp_sum(full);
-    if ((threadIdx.x & 31) == 0) {
-        if (cand) atomicAdd(&a.ctrl->candidates, cand);
-        if (co) atomicAdd(&a.ctrl->co_orbiting, co);
-        if (full) atomicAdd(&a.ctrl->exact_evals, full);
+}
+
+template <int kCols>
+__global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double* __restrict__ sorted,
+                                                        const int* __restrict__ orig,
+                                                        const int* __restrict__ cell_begin,
+                                                        const int* __restrict__ nbr, const int4* __restrict__ items,
+                                                        int64_t items_cap, int2* __restrict__ surv, int64_t surv_cap) {
+    __shared__ double2 rows[kWarps][32][3];
+    __shared__ int rorig[kWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
+    const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
+    const double dt3 = a.dt * a.dt * a.dt;
+    const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
+    const double gate_hi2 = gate_hi * gate_hi;
+    PairCounters pc;
+    const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
+    for (int it = gw; it < n_items; it += nw) {
+        const int4 item = items[it];
+        const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
+        const int b0 = cell_begin[c];
+        const int k = cell_begin[c + 1] - b0;
+        // Column segments: lane 0 = the cell itself, lanes 1..13 = forward neighbours.
+        int seg_begin = 0, seg_len = 0;
+        if (lane == 0) {
+            seg_begin = b0;
+            seg_len = k;
+        } else if (lane <= 13) {
+            const int f = nbr[13 * static_cast<int64_t>(c) + lane - 1];
+            if (f >= 0) {
+                seg_begin = cell_begin[f];
+                seg_len = cell_begin[f + 1] - seg_begin;
+            }
+        }
+        int seg_start = seg_len;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, seg_start, o);
+            if (lane >= o) seg_start += y;
+        }
+        const int L = __shfl_sync(0xffffffffu, seg_start, 31);
+        seg_start -= seg_len;  // exclusive
+        const int r0 = 32 * ra;
+        const int nr = min(32, k - r0);
+        const unsigned nrmask = nr >= 32 ? 0xffffffffu : ((1u << nr) - 1u);
+        __syncwarp();
+        if (lane < nr) {
+            const double2* s = reinterpret_cast<const double2*>(sorted + 6 * static_cast<int64_t>(b0 + r0 + lane));
+            rows[warp][lane][0] = s[0];
+            rows[warp][lane][1] = s[1];
+            rows[warp][lane][2] = s[2];
+            rorig[warp][lane] = orig[b0 + r0 + lane];
+        }
+        __syncwarp();
+        for (int cb = cb0; cb < cb0 + ncb; cb += kCols) {
+            SortedState col[kCols];
+            int corig[kCols];
+            unsigned valid[kCols];
+            for (int h = 0; h < kCols; ++h) {
+                const int p = 32 * (cb + h) + lane;
+                const bool ok = (cb + h < cb0 + ncb) && p < L;
+                int sgi = 0;
+                for (int o = 1; o < 14; ++o) {
+                    const int st = __shfl_sync(0xffffffffu, seg_start, o);
+                    const int ln = __shfl_sync(0xffffffffu, seg_len, o);
+                    if (ln > 0 && st <= p) sgi = o;
+                }
+                const int sb = __shfl_sync(0xffffffffu, seg_begin, sgi);
+                const int ss = __shfl_sync(0xffffffffu, seg_start, sgi);
+                const int q = ok ? sb + (p - ss) : b0;
+                col[h] = load_sorted(sorted, q);
+                corig[h] = orig[q];
+                // The block that starts at the row block's own columns keeps only column > row.
+                valid[h] = ok ? (cb + h == ra ? ((1u << lane) - 1u) : 0xffffffffu) & nrmask : 0u;
+            }
+            unsigned need[kCols];
+            for (int h = 0; h < kCols; ++h) need[h] = 0u;
+#pragma unroll 4
+            for (int r = 0; r < nr; ++r) {
+                const double2 ra2 = rows[warp][r][0], rb2 = rows[warp][r][1], rc2 = rows[warp][r][2];
+                for (int h = 0; h < kCols; ++h) need[h] |= gate_open(col[h], ra2, rb2, rc2, gate_hi2) << r;
+            }
+            for (int h = 0; h < kCols; ++h) {
+                need[h] &= valid[h];
+                if (__any_sync(0xffffffffu, need[h] != 0u))
+                    exact_rows(need[h], col[h], corig[h], rows[warp], rorig[warp], a, surv, surv_cap, pc);
+            }
+        }
+        __syncwarp();
+    }
+    pc.co = warp_sum(pc.co);
+    pc.full = warp_sum(pc.full);
+    if (lane == 0) {
+        if (pc.co) atomicAdd(&a.ctrl->co_orbiting, pc.co);
+        if (pc.full) atomicAdd(&a.ctrl->exact_evals, pc.full);
     }
 }
 
@@ -806,6 +1056,13 @@ __global__ void __launch_bounds__(256) k_fp64_fma(double* out, int iters, double
 
 int g_sm_count = 0;
 
+int grid_for_block(int64_t n, int per_sm_blocks, int block) {
+    const int sms = sm_count();
+    const int64_t want = (n + block - 1) / block;
+    const int64_t cap = static_cast<int64_t>(sms) * per_sm_blocks;
+    return static_cast<int>(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
 int grid_for(int64_t n, int per_sm_blocks) {
     const int sms = sm_count();
     const int64_t want = (n + kBlock - 1) / kBlock;
@@ -836,7 +1093,7 @@ void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int 
 }
 
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
-    k_propagate_exact<<<grid_for(a.n, 4), kBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
+    k_propagate_exact<<<grid_for_block(a.n, 3, kPropBlock), kPropBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
                                                                 b.alive[a.src], b.alive[1 - a.src], b.keys[0], b.cap);
 }
 
@@ -852,35 +1109,53 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     const int n = a.n;
     if (n <= 0) return;  // nothing alive: the cell build sees n_alive == 0
     const int ntiles = (n + kSortTile - 1) / kSortTile;
-    for (int pass = 0; pass < a.sort_passes; ++pass) {
+    const int passes = a.sort_passes;
+    cudaMemsetAsync(b.sort_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
+    cudaMemsetAsync(b.sort_ctr, 0, sizeof(unsigned int) * 8, stream);
+    cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
+    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, passes, b.sort_hist, a.ctrl);
+    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.sort_hist, passes);
+    for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
-        const int shift = 8 * pass;
-        k_sort_hist<<<ntiles, kBlock, 0, stream>>>(b.keys[in], n, shift, b.tile_hist, ntiles, a.ctrl,
-                                                  pass == 0 ? 8 * a.sort_passes : 0);
-        k_scan_exclusive<<<1, 1024, 0, stream>>>(b.tile_hist, 256 * ntiles);
-        k_sort_scatter<<<ntiles, kBlock, 0, stream>>>(b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb],
-                                                     b.idx[outb], n, shift, b.tile_hist, ntiles);
+        k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
+            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, 8 * pass,
+            b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass, b.sort_ctr + pass,
+            a.ctrl);
     }
 }
 
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     const int sb = sorted_buffer(a.sort_passes);
     const int ntiles = a.n > 0 ? (a.n + kCellTile - 1) / kCellTile : 1;
-    k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, reinterpret_cast<unsigned int*>(b.block_counts));
-    k_scan_exclusive<<<1, 1024, 0, stream>>>(reinterpret_cast<unsigned int*>(b.block_counts), ntiles);
+    unsigned int* bc = reinterpret_cast<unsigned int*>(b.block_counts);
+    k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, bc);
+    k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr);
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
-    k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], reinterpret_cast<const unsigned int*>(b.block_counts),
-                                               a.ctrl, b.cell_begin, b.cell_key, b.cell_of, b.hash_keys, b.hash_vals,
+    k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], bc, a.ctrl, b.cell_begin, b.cell_key,
+                                               b.cell_of, b.hash_keys, b.hash_vals,
                                                static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src], b.cap,
                                                b.sorted, b.sorted_orig);
     k_neighbours<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.cell_key, b.hash_keys, b.hash_vals,
-                                                          static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
+                                                          static_cast<unsigned long long>(b.hash_cap - 1), b.nbr,
+                                                          b.item_count);
+    // Offsets of each cell's work items, and their total.
+    const int st = static_cast<int>((b.cap + kScanTile - 1) / kScanTile);
+    k_scan_partials<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
+    k_scan_small<<<1, 1024, 0, stream>>>(b.scan_part, st, reinterpret_cast<unsigned int*>(&a.ctrl->n_items));
+    k_scan_apply<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
+    k_items_write<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.item_count, b.items,
+                                                           b.items_cap);
 }
 
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
-    const int blocks = (a.n + kBlock - 1) / kBlock;
-    k_pairs_exact<<<blocks > 0 ? blocks : 1, kBlock, 0, stream>>>(a, b.sorted, b.sorted_orig, b.cell_of, b.cell_begin,
-                                                                  b.nbr, b.survivors, b.surv_cap);
+    // Default: the resident block count of each variant.
+    const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : (a.tune.pair_variant == 1 ? 3 : 2);
+    if (a.tune.pair_variant == 1)
+        k_pairs_tiles<1><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted_orig, b.cell_begin, b.nbr,
+                                                                 b.items, b.items_cap, b.survivors, b.surv_cap);
+    else
+        k_pairs_tiles<2><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted_orig, b.cell_begin, b.nbr,
+                                                                 b.items, b.items_cap, b.survivors, b.surv_cap);
 }
 
 void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,

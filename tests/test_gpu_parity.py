@@ -68,6 +68,21 @@ def test_chunking_and_graph_parity_do_not_change_results(engine):
         assert_same_stats(got[3], base[3])
 
 
+@pytest.mark.parametrize("variant,bps", [(0, 0), (0, 1), (1, 5)])
+def test_tuning_knobs_do_not_change_results(engine, variant, bps):
+    fx = load("run_dense.npz")
+    engine.set_tuning("pair_variant", variant)
+    engine.set_tuning("pair_blocks_per_sm", bps)
+    try:
+        fs, fa, conj, stats = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], int(fx["steps"]))
+    finally:
+        engine.set_tuning("pair_variant", 1)
+        engine.set_tuning("pair_blocks_per_sm", 0)
+    assert np.array_equal(fs, fx["final_states"])
+    assert_same_conj(conj, fx["conj"])
+    assert_same_stats(stats, fx["stats"])
+
+
 def test_buffer_overflow_replays_to_the_same_result(engine):
     fx = load("run_mixed.npz")
     base = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], 40)
