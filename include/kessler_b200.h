@@ -100,6 +100,26 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
               const uint8_t* alive_after, const double* size_m, double t0, double dt,
               ks_conjunction* out, int64_t cap, int64_t* count, ks_step_stats* stats);
 
+/* --- allocation-free one-shot screening. No counterpart in the reference: it
+ *     exists for callers that must not allocate GPU memory at call time, such as
+ *     an application whose device memory is already handed to its own pool, or
+ *     a time-critical loop that cannot afford cudaMalloc / cudaFree, which
+ *     synchronise the device. Same inputs, outputs and results as ks_screen
+ *     (thresholds passed explicitly, no context), on device buffers carved from
+ *     one fixed array in the library's device image (about 11 MB, held by every
+ *     GPU that loads the library until exit). Limits: n <= 16384 objects,
+ *     <= 131072 pairs sent to refinement, <= 32768 conjunctions; beyond them it
+ *     returns KS_ERR_RANGE / KS_ERR_OVERFLOW and writes no records. cap must
+ *     hold every conjunction found (*count is set either way). stream is a
+ *     cudaStream_t or NULL. error (optional, error_len bytes) receives a message.
+ *     The first call on each device looks up the array's device address, so
+ *     make that first call before any stream capture. Calls share the array:
+ *     calls that overlap on the GPU (other threads, other streams) race. */
+int ks_screen_noalloc(int64_t n, const double* before, const double* after, const uint8_t* alive_after,
+                      const double* size_m, double t0, double dt, double threshold_km, double radius_scale,
+                      double min_encounter_speed_km_s, ks_conjunction* out, int64_t cap, int64_t* count,
+                      ks_step_stats* stats, void* stream, char* error, int64_t error_len);
+
 /* --- one-shot propagation on host states: `steps` calls of Simulation::step
  *     without screening (src/core/orbital.cpp:286-300) starting at time t.
  *     states/alive are updated in place. A resident population is discarded. */

@@ -62,6 +62,8 @@ SIGNATURES = {
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_screen": (C.c_int, [_P, _I64, _P, _P, _P, _P, _D, _D, _P, _I64, C.POINTER(_I64), _P]),
     "ks_propagate": (C.c_int, [_P, _I64, _P, _P, _D, _D, _D, _I64]),
+    "ks_screen_noalloc": (C.c_int, [_I64, _P, _P, _P, _P, _D, _D, _D, _D, _D, _P, _I64, C.POINTER(_I64), _P, _P,
+                                    C.c_char_p, _I64]),
     "ks_get_timing": (C.c_int, [_P, C.POINTER(Timing)]),
     "ks_moon_position": (None, [_D, _P]),
     "ks_generate_population": (C.c_int, [C.c_uint64, _I64, _I64, C.c_int, _D, _P, _P, _P]),
