@@ -38,13 +38,13 @@ FLUSH_BYTES = 256 * 1024 * 1024
 #   object-step: acceleration x 4 (33 mul + 21 add/sub + 5 div + 3 sqrt each)
 #                + 78 RK4 combination ops = 294 mul/add + 20 div + 12 sqrt
 #   candidate pair: 6 subtractions for dr, dv, then |dr|^2, |dv|^2, dr.dv (15)
-#                   and the distance-gate comparison (4) = 25 ops; a pair that
+#                   and the division-free distance gate (4) = 25 ops (FP64 in
+#                   the plain path, FP32 in the split path); a pair that
 #                   reaches the full filter adds its ts, p, |p|, gate and
 #                   convexity terms: 30 mul/add + 1 div + 3 sqrt
 FLOPS_OBJECT_STEP = 294 + 20 + 12
 FLOPS_PAIR_CHEAP = 25
 FLOPS_PAIR_FULL = 34
-FLOPS_REFINE = 2 * 62 * 28 + 60
 
 
 def parse():
@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=360)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split"],
+                    help="path reported as the headline value (the other one is reported beside it)")
     ap.add_argument("--objects", type=int, default=1_000_000)
     ap.add_argument("--base", type=int, default=28_340)
     ap.add_argument("--parents", type=int, default=200)
@@ -65,6 +66,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=8, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-error-study", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=60)
     return ap.parse_args()
 
@@ -195,6 +197,114 @@ def run_reference_arm(a):
     return 0
 
 
+def timed_run(ks, eng, a, st, sz, al, precision, barrier):
+    """W untimed warm-up steps, then K timed steps; per-step device time from
+    CUDA events on the engine's stream, L2 flushed before each step outside
+    the events."""
+    eng.set_precision(precision)
+    eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
+    eng.set_screening(True, a.conj_km, 1.0, 0.01)
+    eng.set_steps_per_graph(a.steps_per_graph)
+    eng.set_l2_flush(FLUSH_BYTES)
+    eng.set_profiling(True)
+    eng.set_population(st, sz, al)
+    eng.run(a.warmup)
+    eng.take_conjunctions()
+    eng.take_step_stats()
+    barrier()
+    w0 = time.perf_counter()
+    eng.run(a.steps)
+    barrier()
+    wall = time.perf_counter() - w0
+    return eng.timing(), eng.take_conjunctions(), eng.take_step_stats(), wall
+
+
+def max_over_ranks(pg, x):
+    if not pg:
+        return x
+    import torch
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, x):
+    if not pg:
+        return x
+    import torch
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def roofline_of(tm, a, fp64_rate, fp32_rate, split):
+    """Dominant kernel of the step and its achieved rate against the measured
+    issue rate of the pipe that bounds it (algorithmic operations per launch
+    divided by the launch's average CUDA-event duration)."""
+    steps = max(1, tm["steps"])
+    phases = {k: tm[k] / steps for k in ("propagate_ms", "sort_ms", "cells_ms", "pairs_ms", "refine_ms")}
+    prop_ops = FLOPS_OBJECT_STEP * tm["object_steps"] / steps
+    pair_ops = FLOPS_PAIR_CHEAP * tm["candidate_pairs"] / steps
+    kernels = {
+        "propagate": {"ms": phases["propagate_ms"], "ops": prop_ops, "pipe": "fp64", "peak": fp64_rate},
+        "pairs": {"ms": phases["pairs_ms"], "ops": pair_ops, "pipe": "fp32" if split else "fp64",
+                  "peak": fp32_rate if split else fp64_rate},
+    }
+    for k in kernels.values():
+        k["tflops"] = k["ops"] / (k["ms"] * 1e-3) / 1e12 if k["ms"] > 0 else None
+        k["frac"] = (k["tflops"] * 1e12 / k["peak"]) if k["tflops"] else None
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    d = kernels[dom]
+    return {"bound": d["pipe"], "kernel": dom, "achieved": d["tflops"], "peak": d["peak"] / 1e12,
+            "unit": "TFLOP/s", "frac": d["frac"], "traffic": traffic_of(dom, split),
+            "peak_source": "measured on this GPU by the project microbenchmark (dependent add/mul chains, no FMA); "
+                           "MEASURED_PEAKS.json has no FP64/FP32 SIMT figure",
+            "algorithmic_ops_per_launch": d["ops"], "phase_ms_per_step": phases,
+            "kernels": {k: {"ms": v["ms"], "pipe": v["pipe"], "tflops": v["tflops"], "frac": v["frac"]}
+                        for k, v in kernels.items()}}
+
+
+def traffic_of(kernel, split):
+    """DRAM bytes per launch of the kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
+    key = f"{kernel}_{'split' if split else 'fp64'}"
+    try:
+        for line in open(path):
+            f = line.split()
+            if len(f) >= 2 and f[0] == key:
+                return float(f[1])
+    except OSError:
+        pass
+    return None
+
+
+def launches_per_step(sort_passes):
+    # propagate, fix_keys, sort (upsweep, digit scan, one kernel per pass),
+    # cells (count, scan, write, neighbours, 3 scan kernels, items), pairs, refine
+    return 1 + 1 + (2 + sort_passes) + 8 + 1 + 1
+
+
+def error_study(ks, eng, a, st, al):
+    """Split vs FP64 propagation of the whole population: position and velocity
+    differences at 1, 6 and 24 h (the FP64 path is bit-identical to the reference)."""
+    out = {}
+    s64, s32, a64, a32, t = st, st, al, al, 0.0
+    for hours in (1, 6, 24):
+        steps = int(round((hours * 3600.0 - t) / a.dt))
+        eng.set_precision(ks.PRECISION_FP64)
+        s64, a64 = eng.propagate(s64, a64, ks.DEFAULT_EPOCH_JD, t, a.dt, steps)
+        eng.set_precision(ks.PRECISION_SPLIT)
+        s32, a32 = eng.propagate(s32, a32, ks.DEFAULT_EPOCH_JD, t, a.dt, steps)
+        t = hours * 3600.0
+        live = (a64 == 1) & (a32 == 1)
+        dr = np.linalg.norm(s32[live, :3] - s64[live, :3], axis=1) * 1e3
+        dv = np.linalg.norm(s32[live, 3:] - s64[live, 3:], axis=1) * 1e6
+        out[f"{hours}h"] = {"max_pos_m": float(dr.max()), "p99_pos_m": float(np.percentile(dr, 99)),
+                            "median_pos_m": float(np.median(dr)), "max_vel_mm_s": float(dv.max()),
+                            "alive_mismatch": int(((a64 == 1) != (a32 == 1)).sum())}
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -212,86 +322,63 @@ def main():
     ks = importlib.import_module("kessler-syndrom-simulation_b200")
     st, sz, al = ks.generate_population(a.seed + rank, a.base, a.objects, a.parents, a.frag_age_s)
 
-    eng = ks.Engine(local)
-    eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
-    eng.set_screening(True, a.conj_km, 1.0, 0.01)
-    eng.set_precision(ks.PRECISION_FP64 if a.precision == "fp64" else ks.PRECISION_SPLIT)
-    eng.set_steps_per_graph(a.steps_per_graph)
-    eng.set_l2_flush(FLUSH_BYTES)
-    eng.set_profiling(True)
-    eng.set_population(st, sz, al)
-    eng.run(a.warmup)
-    eng.take_conjunctions()
-    eng.take_step_stats()
-
     def barrier():
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
 
-    barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    w0 = time.perf_counter()
-    eng.run(a.steps)
-    barrier()
-    wall = time.perf_counter() - w0
-    clk = clocks.stop()
-    tm = eng.timing()
-    conj = eng.take_conjunctions()
-    stats = eng.take_step_stats()
+    eng = ks.Engine(local)
+    fp64_rate, fp32_rate = eng.measure_fp64()[0], measure_fp32(eng)
+    head = ks.PRECISION_SPLIT if a.precision == "split" else ks.PRECISION_FP64
+    other = ks.PRECISION_FP64 if head == ks.PRECISION_SPLIT else ks.PRECISION_SPLIT
+    runs = {}
+    clk = None
+    for prec in (other, head):  # headline last, with clocks sampled
+        if prec == head:
+            clocks = ClockSampler(local)
+            clocks.start()
+        runs[prec] = timed_run(ks, eng, a, st, sz, al, prec, barrier)
+        if prec == head:
+            clk = clocks.stop()
 
-    dev_ms = tm["total_ms"]
-    obj_steps = tm["object_steps"]
-    pairs = tm["candidate_pairs"]
-    if pg:
-        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms_max = float(t.item())
-        c = torch.tensor([obj_steps, pairs, len(conj)], device="cuda", dtype=torch.float64)
-        pg.all_reduce(c, op=pg.ReduceOp.SUM)
-        obj_total, pairs_total, conj_total = (float(x) for x in c.tolist())
-    else:
-        dev_ms_max, obj_total, pairs_total, conj_total = dev_ms, float(obj_steps), float(pairs), float(len(conj))
+    def summary(prec):
+        tm, conj, stats, wall = runs[prec]
+        dev_ms = max_over_ranks(pg, tm["total_ms"])
+        obj = sum_over_ranks(pg, float(tm["object_steps"]))
+        pairs = sum_over_ranks(pg, float(tm["candidate_pairs"]))
+        steps = max(1, tm["steps"])
+        return {"value": obj / (dev_ms * 1e-3), "ms_per_step": dev_ms / steps, "pairs_per_s": pairs / (dev_ms * 1e-3),
+                "conjunctions_per_step": len(conj) / steps, "refined_pairs_per_step": tm["refined_pairs"] / steps,
+                "exact_filter_pairs_per_step": tm["exact_filter_pairs"] / steps,
+                "roofline": roofline_of(tm, a, fp64_rate, fp32_rate, prec == ks.PRECISION_SPLIT),
+                "wall_s_timed_region": wall, "sort_passes": tm["sort_passes"]}
 
-    value = obj_total / (dev_ms_max * 1e-3)
-    steps = max(1, tm["steps"])
-    phases = {k: tm[k] / steps for k in ("propagate_ms", "sort_ms", "cells_ms", "pairs_ms", "refine_ms")}
-
-    # FP64 issue rate of this device (project microbenchmark: dependent add/mul chains, no FMA).
-    addmul_per_s, fma_per_s = eng.measure_fp64()
-    prop_flops = FLOPS_OBJECT_STEP * obj_steps / steps
-    pair_flops = (FLOPS_PAIR_CHEAP * pairs + FLOPS_PAIR_FULL * tm["exact_filter_pairs"]) / steps
-    kernels = {
-        "propagate": {"ms": phases["propagate_ms"], "flops": prop_flops},
-        "pairs": {"ms": phases["pairs_ms"], "flops": pair_flops},
-    }
-    dom = max(kernels, key=lambda k: kernels[k]["ms"])
-    ach = kernels[dom]["flops"] / (kernels[dom]["ms"] * 1e-3) / 1e12
-    peak = addmul_per_s / 1e12
-    roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": ach / peak, "traffic": None,
-                "peak_source": "measured FP64 add/mul issue rate of this GPU (project microbenchmark, no FMA)",
-                "fma_peak_tflops": fma_per_s / 1e12,
-                "algorithmic_flops_per_launch": kernels[dom]["flops"],
-                "phase_ms_per_step": phases, "kernels": {k: {"ms": v["ms"], "tflops": v["flops"] / (v["ms"] * 1e-3) / 1e12
-                                                             if v["ms"] > 0 else None} for k, v in kernels.items()}}
-
-    line = {"metric": METRIC, "value": value, "unit": "object-steps/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": dev_ms_max / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+f32",
+    main_s, other_s = summary(head), summary(other)
+    c_head, c_other = runs[head][1], runs[other][1]
+    kh = set(zip(c_head["i"].tolist(), c_head["j"].tolist(), c_head["step"].tolist()))
+    ko = set(zip(c_other["i"].tolist(), c_other["j"].tolist(), c_other["step"].tolist()))
+    split_set, fp64_set = (kh, ko) if head == ks.PRECISION_SPLIT else (ko, kh)
+    tm_head = runs[head][0]
+    line = {"metric": METRIC, "value": main_s["value"], "unit": "object-steps/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": main_s["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32 (split)" if head == ks.PRECISION_SPLIT else "f64",
             "data": "synthetic (seeded generator; no dataset)", "config": config_of(a),
-            "pairs_per_s": pairs_total / (dev_ms_max * 1e-3),
-            "conjunctions_per_step": conj_total / steps / world,
-            "gpu_launches": None, "roofline": roofline, "clocks": clk,
-            "wall_s_timed_region": wall,
-            "continuous_object_steps_per_s": None}
-    # Kernel launches per step (counted from the launch sequence of one step).
-    line["gpu_launches"] = a.steps * (3 + 3 * tm["sort_passes"] + 5 + 2)
-
+            "pairs_per_s": main_s["pairs_per_s"], "conjunctions_per_step": main_s["conjunctions_per_step"],
+            "gpu_launches": a.steps * launches_per_step(tm_head["sort_passes"]) +
+                            -(-a.steps // max(1, a.steps_per_graph)),
+            "roofline": main_s["roofline"], "clocks": clk,
+            "fp64" if head == ks.PRECISION_SPLIT else "split": other_s,
+            "conjunction_sets": {"split_only": len(split_set - fp64_set), "fp64_only": len(fp64_set - split_set),
+                                 "common": len(split_set & fp64_set),
+                                 "over": f"the {a.steps} timed steps, pairs matched by (i, j, step)"},
+            "refined_pairs_per_step": main_s["refined_pairs_per_step"],
+            "wall_s_timed_region": main_s["wall_s_timed_region"]}
+    if not a.no_error_study:
+        line["split_error_vs_fp64"] = error_study(ks, eng, a, st, al)
     if not a.no_e2e:
-        line["e2e"] = e2e_run(ks, a, st, sz, al, local, barrier, pg)
+        line["e2e"] = e2e_run(ks, a, st, sz, al, local, barrier, pg, head)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         base = cpu_baseline(a, st, sz, al, a.cpu_steps)
         line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -304,7 +391,11 @@ def main():
     return 0
 
 
-def e2e_run(ks, a, st, sz, al, device, barrier, pg):
+def measure_fp32(eng):
+    return eng.measure_fp32()[0]
+
+
+def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     """Through the C ABI with host buffers: upload the population from pinned
     memory, then per step upload that step's lunar rows, run the step and read
     its conjunction records and counters back (one chunk per step), finally
@@ -315,6 +406,7 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg):
     pin_sz = torch.from_numpy(sz).pin_memory().numpy()
     pin_al = torch.from_numpy(al).pin_memory().numpy()
     eng = ks.Engine(device)
+    eng.set_precision(precision)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
     eng.set_screening(True, a.conj_km, 1.0, 0.01)
     eng.set_steps_per_graph(1)

@@ -161,6 +161,8 @@ int ks_generate_population(uint64_t seed, int64_t n_base, int64_t n_total, int n
 /* FP64 issue rate of this device, measured by a dependent-chain microbenchmark:
  * add/mul instructions per second (no FMA) and FMA instructions per second. */
 int ks_measure_fp64(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s);
+/* The same for FP32 (add/mul without contraction, and FMA). */
+int ks_measure_fp32(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s);
 
 #ifdef __cplusplus
 }

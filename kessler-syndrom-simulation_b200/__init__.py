@@ -183,9 +183,17 @@ class Engine:
         return st, al
 
     def measure_fp64(self):
+        """(add/mul, FMA) FP64 instructions per second of this device."""
         a = C.c_double()
         f = C.c_double()
         self._check(self._lib.ks_measure_fp64(self._h, C.byref(a), C.byref(f)))
+        return a.value, f.value
+
+    def measure_fp32(self):
+        """(add/mul, FMA) FP32 instructions per second of this device."""
+        a = C.c_double()
+        f = C.c_double()
+        self._check(self._lib.ks_measure_fp32(self._h, C.byref(a), C.byref(f)))
         return a.value, f.value
 
 

@@ -97,7 +97,7 @@ void free_objects(ks_ctx* ctx) {
     dfree(b.size_m); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr); dfree(b.scan_part); dfree(b.item_count);
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_of); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
-    dfree(b.sorted); dfree(b.sorted_orig);
+    dfree(b.sorted); dfree(b.sorted32); dfree(b.sorted_orig);
     b.cap = 0;
     b.hash_cap = 0;
     b.sort_status_len = 0;
@@ -136,6 +136,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.hash_keys, sizeof(unsigned long long) * h));
     KS_CUDA(cudaMalloc(&b.hash_vals, sizeof(int) * h));
     KS_CUDA(cudaMalloc(&b.sorted, sizeof(double) * 6 * cap));
+    KS_CUDA(cudaMalloc(&b.sorted32, sizeof(float4) * 2 * cap));
     KS_CUDA(cudaMalloc(&b.sorted_orig, sizeof(int) * cap));
     b.cap = cap;
     return KS_OK;
@@ -270,6 +271,7 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     a.radius_scale = ctx->rscale;
     a.n = static_cast<int>(ctx->n);
     a.screening = ctx->screening;
+    a.precision = ctx->precision;
     a.sort_passes = ctx->sort_passes;
     a.sp = ctx->b.params + k;
     a.ctrl = ctx->b.ctrl + k;
@@ -620,7 +622,6 @@ int ks_set_screening(ks_ctx* ctx, int enabled, double threshold_km, double radiu
 int ks_set_precision(ks_ctx* ctx, int precision) {
     if (!ctx || (precision != KS_PRECISION_FP64 && precision != KS_PRECISION_SPLIT))
         return fail(ctx, KS_ERR_ARG, "ks_set_precision: unknown mode");
-    if (precision == KS_PRECISION_SPLIT) return fail(ctx, KS_ERR_ARG, "ks_set_precision: split precision not built");
     drop_graphs(ctx);
     ctx->precision = precision;
     return KS_OK;
@@ -843,6 +844,13 @@ int ks_measure_fp64(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s) {
     if (!ctx || !addmul_per_s || !fma_per_s) return KS_ERR_ARG;
     cudaSetDevice(ctx->device);
     KS_CUDA(ks::measure_fp64(addmul_per_s, fma_per_s, ctx->stream));
+    return KS_OK;
+}
+
+int ks_measure_fp32(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s) {
+    if (!ctx || !addmul_per_s || !fma_per_s) return KS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    KS_CUDA(ks::measure_fp32(addmul_per_s, fma_per_s, ctx->stream));
     return KS_OK;
 }
 

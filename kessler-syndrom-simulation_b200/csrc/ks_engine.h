@@ -109,6 +109,7 @@ struct DeviceBuffers {
     int* hash_vals = nullptr;
     int64_t hash_cap = 0;                  // power of two
     double* sorted = nullptr;              // 6 per sorted entry
+    float4* sorted32 = nullptr;            // split precision: cell-relative position, velocity
     int* sorted_orig = nullptr;
     int2* survivors = nullptr;
     int64_t surv_cap = 0;
@@ -137,6 +138,7 @@ struct StepArgs {
     double gate_hi2;           // unused by the propagation kernel
     int n;                     // population size (objects, alive or not)
     int screening;             // 0: propagation only
+    int precision;             // KS_PRECISION_FP64 or KS_PRECISION_SPLIT
     int sort_passes;
     const StepParams* sp;      // this step's inputs
     Ctrl* ctrl;                // this step's control block
@@ -163,5 +165,6 @@ inline int sorted_buffer(int passes) { return passes & 1; }
 
 int sm_count();
 cudaError_t measure_fp64(double* addmul_per_s, double* fma_per_s, cudaStream_t stream);
+cudaError_t measure_fp32(double* addmul_per_s, double* fma_per_s, cudaStream_t stream);
 
 }  // namespace ks
