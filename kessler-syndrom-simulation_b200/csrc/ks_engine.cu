@@ -226,7 +226,7 @@ int passes_for_bits(int bits) { return std::max(1, (bits + 1 + 7) / 8); }
 // Host estimate of the key width from a seeded control block. Only sizes the
 // number of radix passes; the device checks it and the chunk is replayed with
 // more passes if the estimate was short.
-int estimate_bits(const Ctrl& c, double dt, double thr) {
+int estimate_bits(const Ctrl& c, double dt, double thr, int sub) {
     const double vmax = [&] { double v; std::memcpy(&v, &c.spec_vmax, 8); return v; }();
     auto dec = [](unsigned long long u) {
         unsigned long long b = (u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u;
@@ -246,7 +246,7 @@ int estimate_bits(const Ctrl& c, double dt, double thr) {
         while (w < 63 && (span >> w) > 0) ++w;
         bits += w;
     }
-    return bits;
+    return bits + 3 * sub;
 }
 
 void fill_params(ks_ctx* ctx, int k_steps, double t_start, int64_t step0, double* t_end) {
@@ -465,7 +465,7 @@ int seed_speculation(ks_ctx* ctx) {
     Ctrl c{};
     KS_CUDA(cudaMemcpyAsync(&c, carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA(cudaStreamSynchronize(ctx->stream));
-    ctx->sort_passes = passes_for_bits(estimate_bits(c, ctx->dt, ctx->thr));
+    ctx->sort_passes = passes_for_bits(estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits));
     drop_graphs(ctx);
     return KS_OK;
 }
@@ -658,6 +658,13 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     const std::string k(key);
     if (k == "pair_variant" && (value == 0 || value == 1)) ctx->tune.pair_variant = static_cast<int>(value);
     else if (k == "pair_blocks_per_sm" && value >= 0 && value <= 32) ctx->tune.pair_blocks_per_sm = static_cast<int>(value);
+    else if (k == "subcell_bits" && value >= 0 && value <= 3) {
+        ctx->tune.subcell_bits = static_cast<int>(value);
+        if (ctx->has_pop) {
+            drop_graphs(ctx);
+            return seed_speculation(ctx);
+        }
+    } else if (k == "box_min_rows" && value >= 0 && value <= 33) ctx->tune.box_min_rows = static_cast<int>(value);
     else return fail(ctx, KS_ERR_ARG, "ks_set_tuning: unknown key or value out of range: " + k);
     drop_graphs(ctx);
     return KS_OK;

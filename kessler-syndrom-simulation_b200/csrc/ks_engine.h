@@ -34,13 +34,17 @@ struct StepParams {
 
 // Grid actually used for one step: cell edge and the compact key layout.
 // Cell coordinates (floor(r / cell)) are shifted by lo and packed as
-// cx << (wy + wz) | cy << wz | cz; bit `bits` marks objects outside the grid.
+// cx << (wy + wz) | cy << wz | cz; below them, 3 * sub bits order the objects
+// of a cell by the Morton code of their 2^sub x 2^sub x 2^sub sub-cell (any
+// order inside a cell gives the same pairs); bit `bits` marks objects outside
+// the grid.
 struct GridParams {
     double cell;
     long long lo[3];
     long long span[3];   // hi - lo per axis
     int w[3];
-    int bits;
+    int sub;             // sub-cell bits per axis
+    int bits;            // wx + wy + wz + 3 * sub
 };
 
 enum : int {
@@ -72,6 +76,7 @@ struct Ctrl {
     int n_alive;                       // alive after the step
     int n_cells;
     int n_items;                       // pair work items
+    unsigned int item_ticket;          // next pair work item to hand out
     int max_cell;
     int flags;
     GridParams grid;
@@ -125,6 +130,8 @@ struct DeviceBuffers {
 struct Tuning {
     int pair_variant = 1;         // 0: two columns per lane, 1: one column per lane
     int pair_blocks_per_sm = 0;   // resident blocks of the pair kernel
+    int subcell_bits = 1;         // Morton order inside cells, bits per axis (0..3)
+    int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
 };
 
 // Everything a step's kernels need, by value.

@@ -51,7 +51,7 @@ __device__ __forceinline__ double dec_double(unsigned long long u) {
 // Cell edge (src/core/collision.cpp:339-356) from the largest start speed, and
 // the compact key layout over the position bounds.
 __device__ void make_grid(double vmax, const unsigned long long* bb_min, const unsigned long long* bb_max,
-                          double dt, double threshold_km, GridParams& g) {
+                          double dt, double threshold_km, int sub, GridParams& g) {
     const double vrel = xmul(2.0, vmax);
     const double c = xadd(xadd(xmul(vrel, dt), threshold_km),
                           xmul(xmul(xmul(xmul(kGravityGradient, vrel), dt), dt), dt));
@@ -69,18 +69,37 @@ __device__ void make_grid(double vmax, const unsigned long long* bb_min, const u
         g.w[a] = span > 0 ? 64 - __clzll(span) : 0;
         bits += g.w[a];
     }
-    g.bits = bits;
+    g.sub = sub;
+    g.bits = bits + 3 * sub;
 }
 
-// Compact key of a start-of-step position; sets *bad if outside the bounds.
+__device__ __forceinline__ unsigned sub_coord(double q, double fq, int sub) {
+    const int s = static_cast<int>((q - fq) * static_cast<double>(1 << sub));
+    return static_cast<unsigned>(min(max(s, 0), (1 << sub) - 1));
+}
+
+// Key of a start-of-step position: compact cell coordinates (floor(r / cell),
+// the reference's cell, src/core/collision.cpp:393-395) above the Morton code
+// of the sub-cell; sets *bad if the cell lies outside the bounds.
 __device__ __forceinline__ unsigned long long cell_key(const GridParams& g, double x, double y, double z,
                                                        int* bad) {
-    const long long cx = static_cast<long long>(floor(xdiv(x, g.cell))) - g.lo[0];
-    const long long cy = static_cast<long long>(floor(xdiv(y, g.cell))) - g.lo[1];
-    const long long cz = static_cast<long long>(floor(xdiv(z, g.cell))) - g.lo[2];
+    const double qx = xdiv(x, g.cell), qy = xdiv(y, g.cell), qz = xdiv(z, g.cell);
+    const double fx = floor(qx), fy = floor(qy), fz = floor(qz);
+    const long long cx = static_cast<long long>(fx) - g.lo[0];
+    const long long cy = static_cast<long long>(fy) - g.lo[1];
+    const long long cz = static_cast<long long>(fz) - g.lo[2];
     if (cx < 0 || cx > g.span[0] || cy < 0 || cy > g.span[1] || cz < 0 || cz > g.span[2]) *bad = 1;
-    return (static_cast<unsigned long long>(cx) << (g.w[1] + g.w[2])) |
-           (static_cast<unsigned long long>(cy) << g.w[2]) | static_cast<unsigned long long>(cz);
+    const unsigned long long cell = (static_cast<unsigned long long>(cx) << (g.w[1] + g.w[2])) |
+                                    (static_cast<unsigned long long>(cy) << g.w[2]) |
+                                    static_cast<unsigned long long>(cz);
+    unsigned long long morton = 0;
+    if (g.sub > 0) {
+        const unsigned sx = sub_coord(qx, fx, g.sub), sy = sub_coord(qy, fy, g.sub), sz = sub_coord(qz, fz, g.sub);
+        for (int b = 0; b < g.sub; ++b)
+            morton |= static_cast<unsigned long long>(((sx >> b) & 1u) << (3 * b + 2) | ((sy >> b) & 1u) << (3 * b + 1) |
+                                                      ((sz >> b) & 1u) << (3 * b));
+    }
+    return (cell << (3 * g.sub)) | morton;
 }
 
 __device__ __forceinline__ unsigned long long dead_key(const GridParams& g) { return 1ull << g.bits; }
@@ -200,6 +219,8 @@ __device__ void ctrl_reset(Ctrl& c) {
     c.vmax_true = 0ull;
     c.candidates = c.co_orbiting = c.refined = c.conj = c.object_steps = c.exact_evals = 0ull;
     c.n_alive = c.n_cells = c.max_cell = c.flags = 0;
+    c.n_items = 0;
+    c.item_ticket = 0u;
     c.grid = GridParams{};
 }
 
@@ -259,7 +280,7 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
     if (threadIdx.x == 0) {
         if (a.screening)
             make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
-                      a.ctrl->bb_max, a.dt, a.threshold_km, g);
+                      a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, g);
         for (int q = 0; q < 3; ++q) moon[q] = a.sp->m[q];
         if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
     }
@@ -318,7 +339,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
     if (threadIdx.x == 0) {
         if (a.screening)
             make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
-                      a.ctrl->bb_max, a.dt, a.threshold_km, g);
+                      a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, g);
         for (int q = 0; q < 3; ++q) moon[q] = to_f32(a.sp->m[q]);
         if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
     }
@@ -373,7 +394,7 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
     __shared__ GridParams g;
     if (threadIdx.x == 0) {
         make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
-                  a.ctrl->bb_max, a.dt, a.threshold_km, g);
+                  a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, g);
         if (blockIdx.x == 0) {
             a.ctrl->grid = g;
             a.ctrl->vmax_true = a.ctrl->spec_vmax;
@@ -409,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
     __shared__ GridParams g;
     if (threadIdx.x == 0) {
         make_grid(__longlong_as_double(static_cast<long long>(vt)), a.ctrl->bb_min, a.ctrl->bb_max, a.dt,
-                  a.threshold_km, g);
+                  a.threshold_km, a.tune.subcell_bits, g);
         if (blockIdx.x == 0) a.ctrl->grid = g;
     }
     __syncthreads();
@@ -696,11 +717,12 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
 __global__ void __launch_bounds__(kBlock) k_cell_count(const unsigned long long* __restrict__ keys,
                                                        const Ctrl* __restrict__ ctrl, unsigned int* __restrict__ counts) {
     const int m = ctrl->n_alive;
+    const int shift = 3 * ctrl->grid.sub;
     const int base = blockIdx.x * kCellTile;
     int c = 0;
     for (int j = threadIdx.x; j < kCellTile; j += kBlock) {
         const int p = base + j;
-        if (p < m && (p == 0 || keys[p] != keys[p - 1])) ++c;
+        if (p < m && (p == 0 || (keys[p] >> shift) != (keys[p - 1] >> shift))) ++c;
     }
     c = warp_sum(c);
     __shared__ int sh[kWarps];
@@ -732,11 +754,12 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
     }
     if (blockIdx.x * kCellTile >= m) return;
     const int p0 = blockIdx.x * kCellTile + threadIdx.x * kPer;
+    const int sh = 3 * ctrl->grid.sub;
     int heads[kPer];
     unsigned int local = 0;
     for (int j = 0; j < kPer; ++j) {
         const int p = p0 + j;
-        heads[j] = (p < m && (p == 0 || keys[p] != keys[p - 1])) ? 1 : 0;
+        heads[j] = (p < m && (p == 0 || (keys[p] >> sh) != (keys[p - 1] >> sh))) ? 1 : 0;
         local += heads[j];
     }
     unsigned int unused;
@@ -746,7 +769,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         if (p >= m) break;
         run += heads[j];
         const int cid = run - 1;
-        const unsigned long long key = keys[p];
+        const unsigned long long key = keys[p] >> sh;  // cell part
         if (heads[j]) {
             cell_begin[cid] = p;
             cell_key_out[cid] = key;
@@ -870,8 +893,10 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
 //
 // The row loop is branch-free: each lane evaluates a conservative distance
 // gate (no division, no square root) and records in a 32-bit mask the rows
-// that the gate cannot reject. Only those pairs then run the exact
-// filter_pair, after the loop.
+// that the gate cannot reject. Those pairs then pass a conservative
+// convexity test (a pair that is separating, not slow and convex over the
+// step is rejected by filter_pair whatever its distance); only the rest run
+// the exact filter_pair in FP64.
 // ---------------------------------------------------------------------------
 
 struct SortedState {
@@ -900,42 +925,127 @@ __device__ __forceinline__ unsigned gate_open(const SortedState& c, double2 ra, 
     return fma(-m, m, P) <= fma(dv2, gate_hi2, 1e-12 * P) ? 1u : 0u;
 }
 
+// True only if filter_pair certainly returns FILTER_REJECT through its
+// convexity clause or its distance gate, never FILTER_CO_ORBITING: the pair is
+// faster than the minimum encounter speed, separating (dr.dv >= 0) and
+// convex over the step (|dv|^2 > G |dr|^2). FP64 inputs are the filter's own
+// dr, dv; the margins cover the contraction of the three sums.
+__device__ __forceinline__ bool certainly_convex_reject(double rx, double ry, double rz, double vx, double vy,
+                                                        double vz, double vmin2) {
+    const double r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    const double dv2 = fma(vx, vx, fma(vy, vy, vz * vz));
+    const double rv = fma(rx, vx, fma(ry, vy, rz * vz));
+    return dv2 > vmin2 * (1.0 + 1e-12) && rv > 0.0 && rv * rv > 1e-28 * (r2 * dv2) &&
+           dv2 > kGravityGradient * r2 * (1.0 + 1e-12);
+}
+
 struct PairCounters {
     unsigned long long co = 0, full = 0;
 };
 
-// Exact filter for the rows flagged in `need` against this lane's column;
-// pairs sent to refinement are appended with one atomic per warp and row.
+// Next work item for this warp (one atomic per item).
+__device__ __forceinline__ int next_item(Ctrl* ctrl) {
+    unsigned int t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(&ctrl->item_ticket, 1u);
+    return static_cast<int>(__shfl_sync(0xffffffffu, t, 0));
+}
+
+// Appends the pairs flagged `keep` (one atomic per warp).
+__device__ __forceinline__ void append_pairs(bool keep, int row_orig, int col_orig, Ctrl* ctrl,
+                                             int2* __restrict__ surv, int64_t surv_cap) {
+    const int lane = threadIdx.x & 31;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (!bal) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&ctrl->refined, static_cast<unsigned long long>(__popc(bal)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (keep) {
+        const unsigned long long pos = base + __popc(bal & lanemask_lt());
+        if (pos < static_cast<unsigned long long>(surv_cap))
+            surv[pos] = make_int2(min(row_orig, col_orig), max(row_orig, col_orig));
+    }
+}
+
+// Exact filter for the rows flagged in `need` against this lane's column.
 __device__ __forceinline__ void exact_rows(unsigned need, const SortedState& col, int col_orig,
                                            const double2 (*rows)[3], const int* rorig, const StepArgs& a,
                                            int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc) {
-    const int lane = threadIdx.x & 31;
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
     while (todo) {
         const int r = __ffs(todo) - 1;
         todo &= todo - 1;
-        int res = FILTER_REJECT;
-        if ((need >> r) & 1u) {
+        bool mine = (need >> r) & 1u;
+        double rx = 0, ry = 0, rz = 0, vx = 0, vy = 0, vz = 0;
+        if (mine) {
             const double2 ra = rows[r][0], rb = rows[r][1], rc = rows[r][2];
+            rx = xsub(col.rx, ra.x); ry = xsub(col.ry, ra.y); rz = xsub(col.rz, rb.x);
+            vx = xsub(col.vx, rb.y); vy = xsub(col.vy, rc.x); vz = xsub(col.vz, rc.y);
+            mine = !certainly_convex_reject(rx, ry, rz, vx, vy, vz, a.vmin2);
+        }
+        if (!__any_sync(0xffffffffu, mine)) continue;
+        int res = FILTER_REJECT;
+        if (mine) {
             ++pc.full;
-            res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
-                                    xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
+            res = filter_pair_exact(rx, ry, rz, vx, vy, vz, a.dt, a.threshold_km, a.vmin2);
             if (res == FILTER_CO_ORBITING) ++pc.co;
         }
-        const bool keep = res == FILTER_REFINE;
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (bal) {
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(&a.ctrl->refined, static_cast<unsigned long long>(__popc(bal)));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (keep) {
-                const unsigned long long pos = base + __popc(bal & lanemask_lt());
-                const int ro = rorig[r];
-                if (pos < static_cast<unsigned long long>(surv_cap))
-                    surv[pos] = make_int2(min(ro, col_orig), max(ro, col_orig));
-            }
+        append_pairs(res == FILTER_REFINE, rorig[r], col_orig, a.ctrl, surv, surv_cap);
+    }
+}
+
+// Per-warp table of the item's non-empty column segments (the cell itself and
+// its forward neighbours), for a binary search from column index to object.
+struct SegTable {
+    int start[16];   // first column index of the segment
+    int begin[16];   // first sorted position of the segment's cell
+    int id[16];      // 0 = the cell itself, 1 + o = forward neighbour o
+};
+
+// Builds the table for cell c; returns the column-list length L and the
+// number of segments.
+__device__ __forceinline__ int build_segments(SegTable& t, int c, int b0, int k, const int* __restrict__ cell_begin,
+                                              const int* __restrict__ nbr, int* nseg_out) {
+    const int lane = threadIdx.x & 31;
+    int seg_begin = 0, seg_len = 0;
+    if (lane == 0) {
+        seg_begin = b0;
+        seg_len = k;
+    } else if (lane <= 13) {
+        const int f = nbr[13 * static_cast<int64_t>(c) + lane - 1];
+        if (f >= 0) {
+            seg_begin = cell_begin[f];
+            seg_len = cell_begin[f + 1] - seg_begin;
         }
     }
+    int incl = seg_len;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const unsigned nz = __ballot_sync(0xffffffffu, seg_len > 0);
+    if (seg_len > 0) {
+        const int j = __popc(nz & lanemask_lt());
+        t.start[j] = incl - seg_len;
+        t.begin[j] = seg_begin;
+        t.id[j] = lane;
+    }
+    __syncwarp();
+    *nseg_out = __popc(nz);
+    return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+// Column index p -> sorted position and segment id (4 halvings cover 16 segments).
+__device__ __forceinline__ int locate(const SegTable& t, int nseg, int p, int* sid) {
+    int lo = 0, hi = nseg - 1;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+        const int mid = (lo + hi + 1) >> 1;
+        const bool ge = t.start[mid] <= p;
+        lo = ge ? mid : lo;
+        hi = ge ? hi : mid - 1;
+    }
+    *sid = t.id[lo];
+    return t.begin[lo] + (p - t.start[lo]);
 }
 
 template <int kCols>
@@ -946,6 +1056,7 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
                                                         int64_t items_cap, int2* __restrict__ surv, int64_t surv_cap) {
     __shared__ double2 rows[kWarps][32][3];
     __shared__ int rorig[kWarps][32];
+    __shared__ SegTable segs[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
@@ -953,35 +1064,18 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
     const double gate_hi2 = gate_hi * gate_hi;
     PairCounters pc;
-    const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
-    for (int it = gw; it < n_items; it += nw) {
+    // Items are handed out dynamically: their costs differ by orders of magnitude.
+    for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
         const int4 item = items[it];
         const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
-        // Column segments: lane 0 = the cell itself, lanes 1..13 = forward neighbours.
-        int seg_begin = 0, seg_len = 0;
-        if (lane == 0) {
-            seg_begin = b0;
-            seg_len = k;
-        } else if (lane <= 13) {
-            const int f = nbr[13 * static_cast<int64_t>(c) + lane - 1];
-            if (f >= 0) {
-                seg_begin = cell_begin[f];
-                seg_len = cell_begin[f + 1] - seg_begin;
-            }
-        }
-        int seg_start = seg_len;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, seg_start, o);
-            if (lane >= o) seg_start += y;
-        }
-        const int L = __shfl_sync(0xffffffffu, seg_start, 31);
-        seg_start -= seg_len;  // exclusive
+        __syncwarp();
+        int nseg;
+        const int L = build_segments(segs[warp], c, b0, k, cell_begin, nbr, &nseg);
         const int r0 = 32 * ra;
         const int nr = min(32, k - r0);
         const unsigned nrmask = nr >= 32 ? 0xffffffffu : ((1u << nr) - 1u);
-        __syncwarp();
         if (lane < nr) {
             const double2* s = reinterpret_cast<const double2*>(sorted + 6 * static_cast<int64_t>(b0 + r0 + lane));
             rows[warp][lane][0] = s[0];
@@ -997,15 +1091,8 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
             for (int h = 0; h < kCols; ++h) {
                 const int p = 32 * (cb + h) + lane;
                 const bool ok = (cb + h < cb0 + ncb) && p < L;
-                int sgi = 0;
-                for (int o = 1; o < 14; ++o) {
-                    const int st = __shfl_sync(0xffffffffu, seg_start, o);
-                    const int ln = __shfl_sync(0xffffffffu, seg_len, o);
-                    if (ln > 0 && st <= p) sgi = o;
-                }
-                const int sb = __shfl_sync(0xffffffffu, seg_begin, sgi);
-                const int ss = __shfl_sync(0xffffffffu, seg_start, sgi);
-                const int q = ok ? sb + (p - ss) : b0;
+                int sid;
+                const int q = ok ? locate(segs[warp], nseg, p, &sid) : b0;
                 col[h] = load_sorted(sorted, q);
                 corig[h] = orig[q];
                 // The block that starts at the row block's own columns keeps only column > row.
@@ -1024,7 +1111,6 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
                     exact_rows(need[h], col[h], corig[h], rows[warp], rorig[warp], a, surv, surv_cap, pc);
             }
         }
-        __syncwarp();
     }
     pc.co = warp_sum(pc.co);
     pc.full = warp_sum(pc.full);
@@ -1034,112 +1120,189 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
     }
 }
 
+// ---------------------------------------------------------------------------
 // Split-precision pair kernel: same work items and the same exact decision
-// (filter_pair on the FP64 states) for the pairs the FP32 gate cannot reject.
-// Rows and columns are FP32 records relative to their own cell's corner; a
-// column from forward neighbour o is moved into the row cell's frame by
-// c_forward[o] cell edges.
-template <int kCols>
-__global__ void __launch_bounds__(kBlock) k_pairs_tiles_f32(StepArgs a, const double* __restrict__ sorted,
-                                                            const float4* __restrict__ sorted32,
-                                                            const int* __restrict__ orig,
-                                                            const int* __restrict__ cell_begin,
-                                                            const int* __restrict__ nbr,
-                                                            const int4* __restrict__ items, int64_t items_cap,
-                                                            int2* __restrict__ surv, int64_t surv_cap) {
+// (filter_pair on the FP64 states) for the pairs the FP32 tests cannot
+// reject. Rows and columns are FP32 records relative to their own cell's
+// corner; a column from forward neighbour o is moved into the row cell's
+// frame by c_forward[o] cell edges. Tiles whose row block and column block
+// are provably apart over the whole step (position and velocity boxes) are
+// skipped before the row loop.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float warp_min_f(float v) {
+    float r;
+    asm("redux.sync.min.f32 %0, %1, 0xffffffff;" : "=f"(r) : "f"(v));
+    return r;
+}
+__device__ __forceinline__ float warp_max_f(float v) {
+    float r;
+    asm("redux.sync.max.f32 %0, %1, 0xffffffff;" : "=f"(r) : "f"(v));
+    return r;
+}
+
+struct Box {
+    float pmin[3], pmax[3], vmin[3], vmax[3];
+};
+
+__device__ __forceinline__ Box warp_box(float4 p, float4 v) {
+    Box b;
+    b.pmin[0] = warp_min_f(p.x); b.pmin[1] = warp_min_f(p.y); b.pmin[2] = warp_min_f(p.z);
+    b.pmax[0] = warp_max_f(p.x); b.pmax[1] = warp_max_f(p.y); b.pmax[2] = warp_max_f(p.z);
+    b.vmin[0] = warp_min_f(v.x); b.vmin[1] = warp_min_f(v.y); b.vmin[2] = warp_min_f(v.z);
+    b.vmax[0] = warp_max_f(v.x); b.vmax[1] = warp_max_f(v.y); b.vmax[2] = warp_max_f(v.z);
+    return b;
+}
+
+// True if every pair (row in box a, column in box b) stays farther apart than
+// gate over [0, dt]: box distance minus dt times the largest relative speed.
+// gate already carries the FP32 record errors; the factor covers the FP32
+// rounding of this test.
+__device__ __forceinline__ bool boxes_apart(const Box& a, const Box& b, float dt, float gate) {
+    float d2 = 0.f, w2 = 0.f;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const float gap = fmaxf(0.f, fmaxf(b.pmin[q] - a.pmax[q], a.pmin[q] - b.pmax[q]));
+        d2 = fmaf(gap, gap, d2);
+        const float w = fmaxf(fabsf(b.vmax[q] - a.vmin[q]), fabsf(b.vmin[q] - a.vmax[q]));
+        w2 = fmaf(w, w, w2);
+    }
+    return sqrtf(d2) * (1.0f - 1e-5f) - dt * sqrtf(w2) * (1.0f + 1e-5f) > gate;
+}
+
+// FP32 version of certainly_convex_reject for FP32 records whose dr, dv carry
+// absolute errors up to e_r, e_v (kF32PosErrKm, kF32VelErrKmS); vmin2e is
+// (vmin + e_v)^2. Margins as derived in the comments below.
+__device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, float rz, float vx, float vy,
+                                                            float vz, float vmin2e) {
+    constexpr float er = kF32PosErrKm, ev = kF32VelErrKmS;
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    const float dv2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
+    const float rv = fmaf(rx, vx, fmaf(ry, vy, rz * vz));
+    // |dv| >= |dv'| - ev > vmin.
+    const bool fast = dv2 > 1.0001f * vmin2e + 1e-12f;
+    // rv >= rv' - (|dr'| ev + |dv'| er + er ev + 2e-7 |dr'||dv'|); squared bound.
+    const bool separating =
+        rv > 0.f && rv * rv > 4.01f * (r2 * (ev * ev) + dv2 * (er * er) + (er * ev) * (er * ev) + 4e-14f * r2 * dv2);
+    // dv2 >= dv2'(1 - ev - 1e-6) - ev - ev^2 and r2 <= r2'(1 + er + 1e-6) + er + er^2 (|x| <= (x^2 + 1) / 2).
+    const bool convex = dv2 * 0.99999f - 6.1e-6f > static_cast<float>(kGravityGradient) * 1.0011f * r2 + 1.1e-9f;
+    return fast && separating && convex;
+}
+
+__device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ sorted,
+                                               const int* __restrict__ orig, const float4 (*rows32)[2],
+                                               const double2 (*rows)[3], const int* rorig, float vmin2e,
+                                               const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
+                                               PairCounters& pc) {
+    unsigned todo = __reduce_or_sync(0xffffffffu, need);
+    // FP32 convexity pass: drop rows no lane still needs.
+    unsigned still = 0u;
+    {
+        unsigned t = todo;
+        while (t) {
+            const int r = __ffs(t) - 1;
+            t &= t - 1;
+            if ((need >> r) & 1u) {
+                const float4 rp = rows32[r][0], rv = rows32[r][1];
+                if (!certainly_convex_reject_f32(cp.x - rp.x, cp.y - rp.y, cp.z - rp.z, cv.x - rv.x, cv.y - rv.y,
+                                                 cv.z - rv.z, vmin2e))
+                    still |= 1u << r;
+            }
+        }
+    }
+    todo = __reduce_or_sync(0xffffffffu, still);
+    if (!todo) return;
+    const SortedState col = load_sorted(sorted, q);
+    const int col_orig = orig[q];
+    while (todo) {
+        const int r = __ffs(todo) - 1;
+        todo &= todo - 1;
+        int res = FILTER_REJECT;
+        if ((still >> r) & 1u) {
+            const double2 ra = rows[r][0], rb = rows[r][1], rc = rows[r][2];
+            ++pc.full;
+            res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
+                                    xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
+            if (res == FILTER_CO_ORBITING) ++pc.co;
+        }
+        append_pairs(res == FILTER_REFINE, rorig[r], col_orig, a.ctrl, surv, surv_cap);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 3) k_pairs_split(StepArgs a, const double* __restrict__ sorted,
+                                                        const float4* __restrict__ sorted32,
+                                                        const int* __restrict__ orig,
+                                                        const int* __restrict__ cell_begin,
+                                                        const int* __restrict__ nbr, const int4* __restrict__ items,
+                                                        int64_t items_cap, int2* __restrict__ surv, int64_t surv_cap) {
     __shared__ float4 rows32[kWarps][32][2];
     __shared__ double2 rows[kWarps][32][3];
     __shared__ int rorig[kWarps][32];
+    __shared__ SegTable segs[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
-    const float gate_f = static_cast<float>((gate_hi + kF32PosErrKm + kF32VelErrKmS * a.dt) * (1.0 + 1e-6));
+    const double gate_e = (gate_hi + kF32PosErrKm + kF32VelErrKmS * a.dt) * (1.0 + 1e-6);
+    const float gate_f = static_cast<float>(gate_e);
     const float gate2 = gate_f * gate_f;
+    const float dt_f = static_cast<float>(a.dt);
     const float cell_f = static_cast<float>(a.ctrl->grid.cell);
+    const double vme = sqrt(a.vmin2) + kF32VelErrKmS;
+    const float vmin2e = static_cast<float>(vme * vme * (1.0 + 1e-6));
+    const int box_rows = a.tune.box_min_rows;
     PairCounters pc;
-    const int gw = blockIdx.x * kWarps + warp, nw = gridDim.x * kWarps;
-    for (int it = gw; it < n_items; it += nw) {
+    // Items are handed out dynamically: their costs differ by orders of magnitude.
+    for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
         const int4 item = items[it];
         const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
-        int seg_begin = 0, seg_len = 0;
-        if (lane == 0) {
-            seg_begin = b0;
-            seg_len = k;
-        } else if (lane <= 13) {
-            const int f = nbr[13 * static_cast<int64_t>(c) + lane - 1];
-            if (f >= 0) {
-                seg_begin = cell_begin[f];
-                seg_len = cell_begin[f + 1] - seg_begin;
-            }
-        }
-        int seg_start = seg_len;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, seg_start, o);
-            if (lane >= o) seg_start += y;
-        }
-        const int L = __shfl_sync(0xffffffffu, seg_start, 31);
-        seg_start -= seg_len;
+        __syncwarp();
+        int nseg;
+        const int L = build_segments(segs[warp], c, b0, k, cell_begin, nbr, &nseg);
         const int r0 = 32 * ra;
         const int nr = min(32, k - r0);
         const unsigned nrmask = nr >= 32 ? 0xffffffffu : ((1u << nr) - 1u);
-        __syncwarp();
+        const int rl = b0 + r0 + (lane < nr ? lane : 0);
+        const float4 my_rp = sorted32[2 * static_cast<int64_t>(rl)];
+        const float4 my_rv = sorted32[2 * static_cast<int64_t>(rl) + 1];
         if (lane < nr) {
-            const int rp = b0 + r0 + lane;
-            rows32[warp][lane][0] = sorted32[2 * static_cast<int64_t>(rp)];
-            rows32[warp][lane][1] = sorted32[2 * static_cast<int64_t>(rp) + 1];
-            const double2* s = reinterpret_cast<const double2*>(sorted + 6 * static_cast<int64_t>(rp));
+            rows32[warp][lane][0] = my_rp;
+            rows32[warp][lane][1] = my_rv;
+            const double2* s = reinterpret_cast<const double2*>(sorted + 6 * static_cast<int64_t>(rl));
             rows[warp][lane][0] = s[0];
             rows[warp][lane][1] = s[1];
             rows[warp][lane][2] = s[2];
-            rorig[warp][lane] = orig[rp];
+            rorig[warp][lane] = orig[rl];
         }
+        const bool use_box = box_rows > 0 && nr >= box_rows;
+        Box rbox;
+        if (use_box) rbox = warp_box(my_rp, my_rv);
         __syncwarp();
-        for (int cb = cb0; cb < cb0 + ncb; cb += kCols) {
-            float4 cp[kCols], cv[kCols];
-            int cq[kCols];
-            unsigned valid[kCols];
-            for (int h = 0; h < kCols; ++h) {
-                const int p = 32 * (cb + h) + lane;
-                const bool ok = (cb + h < cb0 + ncb) && p < L;
-                int sgi = 0;
-                for (int o = 1; o < 14; ++o) {
-                    const int st = __shfl_sync(0xffffffffu, seg_start, o);
-                    const int ln = __shfl_sync(0xffffffffu, seg_len, o);
-                    if (ln > 0 && st <= p) sgi = o;
-                }
-                const int sb = __shfl_sync(0xffffffffu, seg_begin, sgi);
-                const int ss = __shfl_sync(0xffffffffu, seg_start, sgi);
-                const int q = ok ? sb + (p - ss) : b0;
-                cq[h] = q;
-                cp[h] = sorted32[2 * static_cast<int64_t>(q)];
-                cv[h] = sorted32[2 * static_cast<int64_t>(q) + 1];
-                if (sgi > 0) {
-                    cp[h].x = fmaf(static_cast<float>(c_forward[sgi - 1][0]), cell_f, cp[h].x);
-                    cp[h].y = fmaf(static_cast<float>(c_forward[sgi - 1][1]), cell_f, cp[h].y);
-                    cp[h].z = fmaf(static_cast<float>(c_forward[sgi - 1][2]), cell_f, cp[h].z);
-                }
-                valid[h] = ok ? (cb + h == ra ? ((1u << lane) - 1u) : 0xffffffffu) & nrmask : 0u;
+        for (int cb = cb0; cb < cb0 + ncb; ++cb) {
+            const int p = 32 * cb + lane;
+            const bool ok = p < L;
+            int sid = 0;
+            const int q = ok ? locate(segs[warp], nseg, p, &sid) : b0;
+            float4 cp = sorted32[2 * static_cast<int64_t>(q)];
+            const float4 cv = sorted32[2 * static_cast<int64_t>(q) + 1];
+            if (sid > 0) {
+                cp.x = fmaf(static_cast<float>(c_forward[sid - 1][0]), cell_f, cp.x);
+                cp.y = fmaf(static_cast<float>(c_forward[sid - 1][1]), cell_f, cp.y);
+                cp.z = fmaf(static_cast<float>(c_forward[sid - 1][2]), cell_f, cp.z);
             }
-            unsigned need[kCols];
-            for (int h = 0; h < kCols; ++h) need[h] = 0u;
+            if (use_box && boxes_apart(rbox, warp_box(cp, cv), dt_f, gate_f)) continue;
+            const unsigned valid = ok ? (cb == ra ? ((1u << lane) - 1u) : 0xffffffffu) & nrmask : 0u;
+            unsigned need = 0u;
 #pragma unroll 4
-            for (int r = 0; r < nr; ++r) {
-                const float4 rp = rows32[warp][r][0], rv = rows32[warp][r][1];
-                for (int h = 0; h < kCols; ++h) need[h] |= gate_open_f32(cp[h], cv[h], rp, rv, gate2) << r;
-            }
-            for (int h = 0; h < kCols; ++h) {
-                need[h] &= valid[h];
-                if (__any_sync(0xffffffffu, need[h] != 0u)) {
-                    const SortedState col = load_sorted(sorted, cq[h]);
-                    exact_rows(need[h], col, orig[cq[h]], rows[warp], rorig[warp], a, surv, surv_cap, pc);
-                }
-            }
+            for (int r = 0; r < nr; ++r) need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
+            need &= valid;
+            if (__any_sync(0xffffffffu, need != 0u))
+                exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, a, surv,
+                               surv_cap, pc);
         }
-        __syncwarp();
     }
     pc.co = warp_sum(pc.co);
     pc.full = warp_sum(pc.full);
@@ -1368,19 +1531,14 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 }
 
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
-    // Default: the resident block count of each variant.
-    const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : (a.tune.pair_variant == 1 ? 3 : 2);
+    // Default: the resident block count of each kernel.
     if (a.precision == KS_PRECISION_SPLIT) {
-        if (a.tune.pair_variant == 1)
-            k_pairs_tiles_f32<1><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
-                                                                         b.cell_begin, b.nbr, b.items, b.items_cap,
-                                                                         b.survivors, b.surv_cap);
-        else
-            k_pairs_tiles_f32<2><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
-                                                                         b.cell_begin, b.nbr, b.items, b.items_cap,
-                                                                         b.survivors, b.surv_cap);
+        const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 3;
+        k_pairs_split<<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig, b.cell_begin,
+                                                              b.nbr, b.items, b.items_cap, b.survivors, b.surv_cap);
         return;
     }
+    const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : (a.tune.pair_variant == 1 ? 3 : 2);
     if (a.tune.pair_variant == 1)
         k_pairs_tiles<1><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted_orig, b.cell_begin, b.nbr,
                                                                  b.items, b.items_cap, b.survivors, b.surv_cap);

@@ -239,7 +239,7 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
             while (w < 63 && (span >> w) > 0) ++w;
             bits += w;
         }
-        a.sort_passes = std::max(1, (bits + 1 + 7) / 8);
+        a.sort_passes = std::max(1, (bits + 3 * a.tune.subcell_bits + 1 + 7) / 8);
     }
     for (int attempt = 0;; ++attempt) {
         if (attempt > 0) {

@@ -88,3 +88,33 @@ def test_split_propagation_error_budget(engine, ks):
     print("split vs FP64 position error [m] max/median, velocity error max [mm/s]:", err)
     assert err[1][0] < 0.05
     assert err[24][0] < 1.0
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("sub,box", [(0, 8), (2, 0), (3, 1), (1, 33)])
+def test_grid_order_and_pruning_knobs_do_not_change_results(engine, ks, prec, sub, box):
+    """Morton order inside cells and tile pruning only change the amount of
+    work: conjunctions and counters stay those of the default settings."""
+    st, sz, al = ks.generate_population(71, 3000, 20000, 10, 1800.0)
+
+    def run():
+        engine.set_precision(prec)
+        engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
+        engine.set_screening(True, 5.0, 1.0, 0.01)
+        engine.set_population(st, sz, al)
+        engine.run(8)
+        return engine.get_population(), engine.take_conjunctions(), engine.take_step_stats()
+
+    base = run()
+    engine.set_tuning("subcell_bits", sub)
+    engine.set_tuning("box_min_rows", box)
+    try:
+        got = run()
+    finally:
+        engine.set_tuning("subcell_bits", 1)
+        engine.set_tuning("box_min_rows", 8)
+        engine.set_precision(ks.PRECISION_FP64)
+    assert np.array_equal(got[0][0], base[0][0])
+    same_conj(got[1], base[1])
+    for f in STAT_FIELDS:
+        assert np.array_equal(got[2][f], base[2][f]), f
