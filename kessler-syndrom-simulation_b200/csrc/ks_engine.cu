@@ -96,7 +96,7 @@ void free_objects(ks_ctx* ctx) {
     for (int k = 0; k < 2; ++k) { dfree(b.state[k]); dfree(b.alive[k]); dfree(b.keys[k]); dfree(b.idx[k]); }
     dfree(b.size_m); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr); dfree(b.scan_part); dfree(b.item_count);
-    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_of); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
+    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_len); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted32); dfree(b.sorted_orig);
     b.cap = 0;
     b.hash_cap = 0;
@@ -128,7 +128,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.block_counts, sizeof(int) * ((cap + 1023) / 1024 + 1)));
     KS_CUDA(cudaMalloc(&b.cell_begin, sizeof(int) * (cap + 1)));
     KS_CUDA(cudaMalloc(&b.cell_key, sizeof(unsigned long long) * cap));
-    KS_CUDA(cudaMalloc(&b.cell_of, sizeof(int) * cap));
+    KS_CUDA(cudaMalloc(&b.cell_len, sizeof(int) * cap));
     KS_CUDA(cudaMalloc(&b.nbr, sizeof(int) * 13 * cap));
     int64_t h = 16;
     while (h < 2 * cap) h <<= 1;
@@ -474,8 +474,7 @@ int upload_population(ks_ctx* ctx, int64_t n, const double* states, const double
                       int buf) {
     ks::DeviceBuffers& b = ctx->b;
     if (n > 0) {
-        KS_CUDA(cudaMemcpyAsync(b.sorted, states, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, ctx->stream));
-        ks::launch_aos_to_soa(b.sorted, b.state[buf], n, b.cap, ctx->stream);
+        KS_CUDA(cudaMemcpyAsync(b.state[buf], states, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, ctx->stream));
         if (alive) KS_CUDA(cudaMemcpyAsync(b.alive[buf], alive, n, cudaMemcpyHostToDevice, ctx->stream));
         else KS_CUDA(cudaMemsetAsync(b.alive[buf], 1, n, ctx->stream));
         if (size_m) KS_CUDA(cudaMemcpyAsync(b.size_m, size_m, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
@@ -571,10 +570,8 @@ int ks_get_population(ks_ctx* ctx, int64_t n, double* states, uint8_t* alive) {
     cudaSetDevice(ctx->device);
     ks::DeviceBuffers& b = ctx->b;
     if (n > 0) {
-        if (states) {
-            ks::launch_soa_to_aos(b.state[ctx->cur], b.sorted, n, b.cap, ctx->stream);
-            KS_CUDA(cudaMemcpyAsync(states, b.sorted, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, ctx->stream));
-        }
+        if (states)
+            KS_CUDA(cudaMemcpyAsync(states, b.state[ctx->cur], sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, ctx->stream));
         if (alive) KS_CUDA(cudaMemcpyAsync(alive, b.alive[ctx->cur], n, cudaMemcpyDeviceToHost, ctx->stream));
     }
     KS_CUDA(cudaStreamSynchronize(ctx->stream));

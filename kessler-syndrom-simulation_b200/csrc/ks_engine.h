@@ -2,12 +2,13 @@
 // (ks_kernels.cu). Not part of the public C ABI.
 //
 // Device data layout (one context, capacity `cap` objects):
-//   state[2]     two SoA FP64 buffers of 6*cap doubles: rx | ry | rz | vx | vy | vz,
-//                ping-ponged each step (start-of-step -> end-of-step)
+//   state[2]     two FP64 buffers of cap states, 6 contiguous doubles each
+//                {rx, ry, rz, vx, vy, vz} (the reference's State), ping-ponged
+//                each step (start-of-step -> end-of-step)
 //   alive[2]     one byte per object per buffer
 //   size_m       characteristic size L (m); collision radius = L/2
 //   keys/idx     cell keys (u64) and object indices (i32), two buffers each for the radix sort
-//   cells        begin offsets, keys, owning cell per sorted entry, 13 forward neighbours per cell
+//   cells        begin offsets, keys, column-list lengths, 13 forward neighbours per cell
 //   hash         open-addressing table cell key -> cell index
 //   sorted       start-of-step states gathered in cell order (AoS, 6 doubles per entry)
 //   items        pair work list: (cell, row block, first column block, column blocks);
@@ -105,7 +106,7 @@ struct DeviceBuffers {
     int* block_counts = nullptr;           // cell heads per tile
     int* cell_begin = nullptr;             // cap + 1
     unsigned long long* cell_key = nullptr;
-    int* cell_of = nullptr;                // owning cell per sorted entry
+    int* cell_len = nullptr;               // per cell: length of its column list
     int* nbr = nullptr;                    // 13 per cell
     unsigned int* item_count = nullptr;    // work items per cell, then their offsets
     int4* items = nullptr;
@@ -165,8 +166,6 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,
                    ChunkCtrl* chunk, cudaStream_t stream);
-void launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t stride, cudaStream_t stream);
-void launch_soa_to_aos(const double* soa, double* aos, int64_t n, int64_t stride, cudaStream_t stream);
 // Index of the key/idx buffer holding the sorted result after `passes` passes.
 inline int sorted_buffer(int passes) { return passes & 1; }
 

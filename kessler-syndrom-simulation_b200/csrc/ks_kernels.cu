@@ -152,6 +152,20 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
+// Object states are stored as the reference's State: 6 contiguous doubles
+// {rx, ry, rz, vx, vy, vz} (src/core/orbital.hpp:51), read as three 16-byte words.
+__device__ __forceinline__ void ld6(const double* __restrict__ base, int64_t i, double s[6]) {
+    const double2* p = reinterpret_cast<const double2*>(base + 6 * i);
+    const double2 a = p[0], b = p[1], c = p[2];
+    s[0] = a.x; s[1] = a.y; s[2] = b.x; s[3] = b.y; s[4] = c.x; s[5] = c.y;
+}
+__device__ __forceinline__ void st6(double* __restrict__ base, int64_t i, const double s[6]) {
+    double2* p = reinterpret_cast<double2*>(base + 6 * i);
+    p[0] = make_double2(s[0], s[1]);
+    p[1] = make_double2(s[2], s[3]);
+    p[2] = make_double2(s[4], s[5]);
+}
+
 // Reduces per-thread speculation values over the block and applies them with
 // one atomic per quantity per block.
 struct SpecAccum {
@@ -245,16 +259,16 @@ __global__ void k_ctrl_reset(Ctrl* c) {
 }
 
 // Speed and position bounds over alive objects of one state buffer.
-__global__ void k_seed_ctrl(const double* __restrict__ st, int64_t stride, const uint8_t* __restrict__ alive,
-                            int n, Ctrl* target) {
+__global__ void k_seed_ctrl(const double* __restrict__ st, const uint8_t* __restrict__ alive, int n, Ctrl* target) {
     SpecAccum s;
     s.init();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (!alive[i]) continue;
-        const double vx = st[3 * stride + i], vy = st[4 * stride + i], vz = st[5 * stride + i];
-        s.vnext = fmax(s.vnext, xsqrt(xdot3(vx, vy, vz)));
+        double x[6];
+        ld6(st, i, x);
+        s.vnext = fmax(s.vnext, xsqrt(xdot3(x[3], x[4], x[5])));
         for (int a = 0; a < 3; ++a) {
-            const unsigned long long e = enc_double(st[a * stride + i]);
+            const unsigned long long e = enc_double(x[a]);
             s.mn[a] = min(s.mn[a], e);
             s.mx[a] = max(s.mx[a], e);
         }
@@ -273,8 +287,7 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
                                                             double* __restrict__ out,
                                                             const uint8_t* __restrict__ alive_in,
                                                             uint8_t* __restrict__ alive_out,
-                                                            unsigned long long* __restrict__ keys,
-                                                            int64_t stride) {
+                                                            unsigned long long* __restrict__ keys) {
     __shared__ GridParams g;
     __shared__ MoonStage moon[3];
     if (threadIdx.x == 0) {
@@ -290,9 +303,9 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
     acc.init();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         double s[6];
-        for (int q = 0; q < 6; ++q) s[q] = in[q * stride + i];
+        ld6(in, i, s);
         if (!alive_in[i]) {
-            for (int q = 0; q < 6; ++q) out[q * stride + i] = s[q];
+            st6(out, i, s);
             alive_out[i] = 0;
             if (a.screening) keys[i] = dead_key(g);
             continue;
@@ -305,7 +318,7 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
             vb = xsqrt(xdot3(s[3], s[4], s[5]));
         }
         rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
-        for (int q = 0; q < 6; ++q) out[q * stride + i] = s[q];
+        st6(out, i, s);
         // Re-entry (src/core/orbital.cpp:297).
         const bool alive = !(xsqrt(xdot3(s[0], s[1], s[2])) < fc.r_earth);
         alive_out[i] = alive ? 1 : 0;
@@ -332,8 +345,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
                                                                    double* __restrict__ out,
                                                                    const uint8_t* __restrict__ alive_in,
                                                                    uint8_t* __restrict__ alive_out,
-                                                                   unsigned long long* __restrict__ keys,
-                                                                   int64_t stride) {
+                                                                   unsigned long long* __restrict__ keys) {
     __shared__ GridParams g;
     __shared__ MoonStageF moon[3];
     if (threadIdx.x == 0) {
@@ -350,9 +362,9 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
     acc.init();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         double s[6];
-        for (int q = 0; q < 6; ++q) s[q] = in[q * stride + i];
+        ld6(in, i, s);
         if (!alive_in[i]) {
-            for (int q = 0; q < 6; ++q) out[q * stride + i] = s[q];
+            st6(out, i, s);
             alive_out[i] = 0;
             if (a.screening) keys[i] = dead_key(g);
             continue;
@@ -365,7 +377,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
             vb = xsqrt(xdot3(s[3], s[4], s[5]));
         }
         rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
-        for (int q = 0; q < 6; ++q) out[q * stride + i] = s[q];
+        st6(out, i, s);
         const bool alive = !(fma(s[0], s[0], fma(s[1], s[1], s[2] * s[2])) < re2);
         alive_out[i] = alive ? 1 : 0;
         if (alive) {
@@ -390,7 +402,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
 // bounds of exactly these objects, so the speculation is the true grid.
 __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double* __restrict__ before,
                                                         const uint8_t* __restrict__ alive_after,
-                                                        unsigned long long* __restrict__ keys, int64_t stride) {
+                                                        unsigned long long* __restrict__ keys) {
     __shared__ GridParams g;
     if (threadIdx.x == 0) {
         make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
@@ -404,7 +416,8 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
     int bad = 0, alive = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         if (alive_after[i]) {
-            keys[i] = cell_key(g, before[i], before[stride + i], before[2 * stride + i], &bad);
+            keys[i] = cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
+                               before[6 * static_cast<int64_t>(i) + 2], &bad);
             ++alive;
         } else {
             keys[i] = dead_key(g);
@@ -424,7 +437,7 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
 // the keys with it. Otherwise every block returns at once.
 __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* __restrict__ before,
                                                      const uint8_t* __restrict__ alive_after,
-                                                     unsigned long long* __restrict__ keys, int64_t stride) {
+                                                     unsigned long long* __restrict__ keys) {
     const unsigned long long vt = a.ctrl->vmax_true;
     if (vt == a.ctrl->spec_vmax) return;
     __shared__ GridParams g;
@@ -436,7 +449,8 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
     __syncthreads();
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
-        keys[i] = alive_after[i] ? cell_key(g, before[i], before[stride + i], before[2 * stride + i], &bad)
+        keys[i] = alive_after[i] ? cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
+                                            before[6 * static_cast<int64_t>(i) + 2], &bad)
                                  : dead_key(g);
     bad = warp_max(bad);
     if ((threadIdx.x & 31) == 0 && bad) atomicOr(&a.ctrl->flags, FLAG_KEY_RANGE);
@@ -741,10 +755,9 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                                                        const unsigned int* __restrict__ offsets, Ctrl* ctrl,
                                                        int* __restrict__ cell_begin,
                                                        unsigned long long* __restrict__ cell_key_out,
-                                                       int* __restrict__ cell_of,
                                                        unsigned long long* __restrict__ hk, int* __restrict__ hv,
                                                        unsigned long long hmask, const double* __restrict__ before,
-                                                       int64_t stride, double* __restrict__ sorted,
+                                                       double* __restrict__ sorted,
                                                        int* __restrict__ sorted_orig, float4* __restrict__ sorted32) {
     constexpr int kPer = kCellTile / kBlock;  // consecutive entries per thread
     const int m = ctrl->n_alive;
@@ -780,11 +793,11 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                 h = (h + 1) & hmask;
             }
         }
-        cell_of[p] = cid;
         const int o = idx[p];
         sorted_orig[p] = o;
-        const double x = before[o], y = before[stride + o], z = before[2 * stride + o];
-        const double vx = before[3 * stride + o], vy = before[4 * stride + o], vz = before[5 * stride + o];
+        double st[6];
+        ld6(before, o, st);
+        const double x = st[0], y = st[1], z = st[2], vx = st[3], vy = st[4], vz = st[5];
         double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
         dst[0] = make_double2(x, y);
         dst[1] = make_double2(z, vx);
@@ -808,78 +821,107 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
     }
 }
 
-__device__ __forceinline__ unsigned int cell_items(int k, int L) {
-    const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-    unsigned int items = 0;
-    for (int a = 0; a < ta; ++a) items += static_cast<unsigned int>((tc - a + kColBlocksPerItem - 1) / kColBlocksPerItem);
-    return items;
-}
-
-// Per cell: the 13 forward neighbours, the candidate-pair count
-// k(k-1)/2 + k * (neighbour objects) and the number of pair work items.
-__global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const int* __restrict__ cell_begin,
-                                                       const unsigned long long* __restrict__ cell_key_in,
+// Thread per (cell, forward neighbour): the neighbour's cell index or -1.
+__global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigned long long* __restrict__ cell_key_in,
                                                        const unsigned long long* __restrict__ hk,
                                                        const int* __restrict__ hv, unsigned long long hmask,
-                                                       int* __restrict__ nbr, unsigned int* __restrict__ item_count) {
+                                                       int* __restrict__ nbr) {
     const int nc = ctrl->n_cells;
     const GridParams g = ctrl->grid;
     const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
-    int biggest = 0;
-    unsigned long long cand = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-        const int k = cell_begin[c + 1] - cell_begin[c];
-        biggest = max(biggest, k);
+    const int64_t total = 13 * static_cast<int64_t>(nc);
+    for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(t / 13), o = static_cast<int>(t % 13);
         const unsigned long long key = cell_key_in[c];
-        const long long cz = static_cast<long long>(key & mz);
-        const long long cy = static_cast<long long>((key >> g.w[2]) & my);
-        const long long cx = static_cast<long long>(key >> (g.w[1] + g.w[2]));
-        int others = 0;
-        for (int o = 0; o < 13; ++o) {
-            const long long x = cx + c_forward[o][0], y = cy + c_forward[o][1], z = cz + c_forward[o][2];
-            int found = -1;
-            if (x >= 0 && x <= g.span[0] && y >= 0 && y <= g.span[1] && z >= 0 && z <= g.span[2]) {
-                const unsigned long long nk = (static_cast<unsigned long long>(x) << (g.w[1] + g.w[2])) |
-                                              (static_cast<unsigned long long>(y) << g.w[2]) |
-                                              static_cast<unsigned long long>(z);
-                found = hash_find(hk, hv, hmask, nk);
-            }
-            nbr[13 * static_cast<int64_t>(c) + o] = found;
-            if (found >= 0) others += cell_begin[found + 1] - cell_begin[found];
+        const long long x = static_cast<long long>(key >> (g.w[1] + g.w[2])) + c_forward[o][0];
+        const long long y = static_cast<long long>((key >> g.w[2]) & my) + c_forward[o][1];
+        const long long z = static_cast<long long>(key & mz) + c_forward[o][2];
+        int found = -1;
+        if (x >= 0 && x <= g.span[0] && y >= 0 && y <= g.span[1] && z >= 0 && z <= g.span[2]) {
+            const unsigned long long nk = (static_cast<unsigned long long>(x) << (g.w[1] + g.w[2])) |
+                                          (static_cast<unsigned long long>(y) << g.w[2]) |
+                                          static_cast<unsigned long long>(z);
+            found = hash_find(hk, hv, hmask, nk);
         }
-        cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * others;
-        item_count[c] = cell_items(k, k + others);
-    }
-    biggest = warp_max(biggest);
-    cand = warp_sum(cand);
-    if ((threadIdx.x & 31) == 0) {
-        if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
-        if (cand) atomicAdd(&ctrl->candidates, cand);
+        nbr[t] = found;
     }
 }
 
-// Writes each cell's work items at its scanned offset.
-__global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
+// Number of work items of row block a: its column blocks a .. tc-1 in groups.
+__device__ __forceinline__ unsigned int row_block_items(int a, int tc) {
+    return static_cast<unsigned int>((tc - a + kColBlocksPerItem - 1) / kColBlocksPerItem);
+}
+
+// Warp per cell: the length L of the cell's column list (own objects plus the
+// forward neighbours'), the candidate-pair count k(k-1)/2 + k(L-k) (the pairs
+// the reference visits, src/core/collision.cpp:522-538) and the work items.
+__global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr,
+                                                        unsigned int* __restrict__ item_count,
+                                                        int* __restrict__ cell_len) {
+    const int nc = ctrl->n_cells;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long cand = 0;
+    int biggest = 0;
+    for (int c = gw; c < nc; c += nw) {
+        const int b0 = cell_begin[c];
+        const int k = cell_begin[c + 1] - b0;
+        int other = 0;
+        if (lane < 13) {
+            const int f = nbr[13 * static_cast<int64_t>(c) + lane];
+            if (f >= 0) other = cell_begin[f + 1] - cell_begin[f];
+        }
+        other = warp_sum(other);
+        const int L = k + other;
+        const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
+        unsigned int items = 0;
+        for (int a = lane; a < ta; a += 32) items += row_block_items(a, tc);
+        items = warp_sum(items);
+        if (lane == 0) {
+            item_count[c] = items;
+            cell_len[c] = L;
+            cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
+            biggest = max(biggest, k);
+        }
+    }
+    if (lane == 0) {
+        if (cand) atomicAdd(&ctrl->candidates, cand);
+        if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
+    }
+}
+
+// Warp per cell: writes the cell's work items at its scanned offset, row
+// blocks spread over the lanes.
+__global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
+                                                        const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ item_off,
                                                         int4* __restrict__ items, int64_t items_cap) {
     const int nc = ctrl->n_cells;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     bool over = false;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    for (int c = gw; c < nc; c += nw) {
         const int k = cell_begin[c + 1] - cell_begin[c];
-        int L = k;
-        for (int o = 0; o < 13; ++o) {
-            const int f = nbr[13 * static_cast<int64_t>(c) + o];
-            if (f >= 0) L += cell_begin[f + 1] - cell_begin[f];
-        }
+        const int L = cell_len[c];
         const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-        int64_t w = item_off[c];
-        for (int a = 0; a < ta; ++a)
-            for (int cb = a; cb < tc; cb += kColBlocksPerItem) {
+        int64_t base = item_off[c];
+        for (int a0 = 0; a0 < ta; a0 += 32) {
+            const int a = a0 + lane;
+            const unsigned int mine = a < ta ? row_block_items(a, tc) : 0u;
+            unsigned int incl = mine;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            int64_t w = base + (incl - mine);
+            for (int cb = a; a < ta && cb < tc; cb += kColBlocksPerItem, ++w) {
                 if (w < items_cap) items[w] = make_int4(c, a, cb, min(kColBlocksPerItem, tc - cb));
                 else over = true;
-                ++w;
             }
+            base += __shfl_sync(0xffffffffu, incl, 31);
+        }
     }
     if (over) atomicOr(&ctrl->flags, FLAG_ITEMS_OVERFLOW);
 }
@@ -1317,7 +1359,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_split(StepArgs a, const dou
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const double* __restrict__ before,
-                                                         const double* __restrict__ after, int64_t stride,
+                                                         const double* __restrict__ after,
                                                          const double* __restrict__ size_m,
                                                          const int2* __restrict__ surv, int64_t surv_cap,
                                                          ks_conjunction* __restrict__ out, int64_t cap,
@@ -1327,12 +1369,17 @@ __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const doubl
     const double s_hi = xsub(1.0, 1e-9);
     for (unsigned long long w = blockIdx.x * blockDim.x + threadIdx.x; w < ns; w += gridDim.x * blockDim.x) {
         const int i = surv[w].x, j = surv[w].y;
+        double bi[6], bj[6], ai[6], aj[6];
+        ld6(before, i, bi);
+        ld6(before, j, bj);
+        ld6(after, i, ai);
+        ld6(after, j, aj);
         Hermite h;
         for (int q = 0; q < 3; ++q) {
-            h.p0[q] = xsub(before[q * stride + j], before[q * stride + i]);
-            h.m0[q] = xmul(xsub(before[(3 + q) * stride + j], before[(3 + q) * stride + i]), a.dt);
-            h.p1[q] = xsub(after[q * stride + j], after[q * stride + i]);
-            h.m1[q] = xmul(xsub(after[(3 + q) * stride + j], after[(3 + q) * stride + i]), a.dt);
+            h.p0[q] = xsub(bj[q], bi[q]);
+            h.m0[q] = xmul(xsub(bj[3 + q], bi[3 + q]), a.dt);
+            h.p1[q] = xsub(aj[q], ai[q]);
+            h.m1[q] = xmul(xsub(aj[3 + q], ai[3 + q]), a.dt);
         }
         const double s = closest_approach_exact(h);
         if (s <= 1e-9 || s >= s_hi) continue;
@@ -1356,26 +1403,6 @@ __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const doubl
         const unsigned long long slot = atomicAdd(&chunk->conj_count, 1ull);
         if (slot < static_cast<unsigned long long>(cap)) out[slot] = c;
         else atomicOr(&chunk->flags, FLAG_CONJ_OVERFLOW);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Layout conversion
-// ---------------------------------------------------------------------------
-
-__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int64_t n, int64_t stride) {
-    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < 6 * n;
-         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t i = e / 6, q = e % 6;
-        soa[q * stride + i] = aos[e];
-    }
-}
-
-__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int64_t n, int64_t stride) {
-    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < 6 * n;
-         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t i = e / 6, q = e % 6;
-        aos[e] = soa[q * stride + i];
     }
 }
 
@@ -1465,26 +1492,26 @@ void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream)
 
 void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int use_alive_src, cudaStream_t stream) {
     k_ctrl_reset<<<1, 32, 0, stream>>>(target);
-    k_seed_ctrl<<<grid_for(n, 4), kBlock, 0, stream>>>(b.state[src], b.cap,
-                                                        use_alive_src ? b.alive[src] : b.alive[1 - src], n, target);
+    k_seed_ctrl<<<grid_for(n, 4), kBlock, 0, stream>>>(b.state[src], use_alive_src ? b.alive[src] : b.alive[1 - src],
+                                                        n, target);
 }
 
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     if (a.precision == KS_PRECISION_SPLIT) {
         k_propagate_split<<<grid_for_block(a.n, 4, kPropBlock), kPropBlock, 0, stream>>>(
-            a, b.state[a.src], b.state[1 - a.src], b.alive[a.src], b.alive[1 - a.src], b.keys[0], b.cap);
+            a, b.state[a.src], b.state[1 - a.src], b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
         return;
     }
     k_propagate_exact<<<grid_for_block(a.n, 3, kPropBlock), kPropBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
-                                                                b.alive[a.src], b.alive[1 - a.src], b.keys[0], b.cap);
+                                                                b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 
 void launch_screen_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
-    k_screen_keys<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a, b.state[a.src], b.alive[1 - a.src], b.keys[0], b.cap);
+    k_screen_keys<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a, b.state[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 
 void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
-    k_fix_keys<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a, b.state[a.src], b.alive[1 - a.src], b.keys[0], b.cap);
+    k_fix_keys<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a, b.state[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
@@ -1514,20 +1541,21 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
     k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr);
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
     k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], bc, a.ctrl, b.cell_begin, b.cell_key,
-                                               b.cell_of, b.hash_keys, b.hash_vals,
-                                               static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src], b.cap,
+                                               b.hash_keys, b.hash_vals,
+                                               static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src],
                                                b.sorted, b.sorted_orig,
                                                a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr);
-    k_neighbours<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.cell_key, b.hash_keys, b.hash_vals,
-                                                          static_cast<unsigned long long>(b.hash_cap - 1), b.nbr,
-                                                          b.item_count);
+    k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
+        a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
+    k_items_count<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr,
+                                                                                      b.item_count, b.cell_len);
     // Offsets of each cell's work items, and their total.
     const int st = static_cast<int>((b.cap + kScanTile - 1) / kScanTile);
     k_scan_partials<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
     k_scan_small<<<1, 1024, 0, stream>>>(b.scan_part, st, reinterpret_cast<unsigned int*>(&a.ctrl->n_items));
     k_scan_apply<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
-    k_items_write<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.item_count, b.items,
-                                                           b.items_cap);
+    k_items_write<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
+        a.ctrl, b.cell_begin, b.cell_len, b.item_count, b.items, b.items_cap);
 }
 
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
@@ -1549,18 +1577,8 @@ void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 
 void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,
                    ChunkCtrl* chunk, cudaStream_t stream) {
-    k_refine_exact<<<sm_count() * 2, kBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src], b.cap, b.size_m,
+    k_refine_exact<<<sm_count() * 2, kBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src], b.size_m,
                                                          b.survivors, b.surv_cap, conj_out, conj_cap, chunk);
-}
-
-void launch_aos_to_soa(const double* aos, double* soa, int64_t n, int64_t stride, cudaStream_t stream) {
-    if (n <= 0) return;
-    k_aos_to_soa<<<grid_for(6 * n, 8), kBlock, 0, stream>>>(aos, soa, n, stride);
-}
-
-void launch_soa_to_aos(const double* soa, double* aos, int64_t n, int64_t stride, cudaStream_t stream) {
-    if (n <= 0) return;
-    k_soa_to_aos<<<grid_for(6 * n, 8), kBlock, 0, stream>>>(soa, aos, n, stride);
 }
 
 cudaError_t measure_fp64(double* addmul_per_s, double* fma_per_s, cudaStream_t stream) {

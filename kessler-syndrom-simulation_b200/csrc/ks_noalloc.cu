@@ -49,7 +49,7 @@ constexpr int64_t scratch_bytes() {
     b += align256(sizeof(int) * ((n + 1023) / 1024 + 1));                // block_counts
     b += align256(sizeof(int) * (n + 1));                // cell_begin
     b += align256(sizeof(unsigned long long) * n);       // cell_key
-    b += align256(sizeof(int) * n);                      // cell_of
+    b += align256(sizeof(int) * n);                      // cell_len
     b += align256(sizeof(int) * 13 * n);                 // nbr
     b += align256(sizeof(unsigned int) * (n + 1));       // item_count
     b += align256(sizeof(int4) * kNoAllocItems);         // items
@@ -107,7 +107,7 @@ ks::DeviceBuffers carve(unsigned char* base) {
     b.block_counts = take<int>(p, sizeof(int) * ((n + 1023) / 1024 + 1));
     b.cell_begin = take<int>(p, sizeof(int) * (n + 1));
     b.cell_key = take<unsigned long long>(p, sizeof(unsigned long long) * n);
-    b.cell_of = take<int>(p, sizeof(int) * n);
+    b.cell_len = take<int>(p, sizeof(int) * n);
     b.nbr = take<int>(p, sizeof(int) * 13 * n);
     b.item_count = take<unsigned int>(p, sizeof(unsigned int) * (n + 1));
     b.items = take<int4>(p, sizeof(int4) * kNoAllocItems);
@@ -180,10 +180,8 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
     ks::DeviceBuffers b = carve(base);
 
     if (n > 0) {
-        NA_CUDA(cudaMemcpyAsync(b.sorted, before, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
-        ks::launch_aos_to_soa(b.sorted, b.state[0], n, b.cap, s);
-        NA_CUDA(cudaMemcpyAsync(b.sorted, after, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
-        ks::launch_aos_to_soa(b.sorted, b.state[1], n, b.cap, s);
+        NA_CUDA(cudaMemcpyAsync(b.state[0], before, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
+        NA_CUDA(cudaMemcpyAsync(b.state[1], after, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s));
         NA_CUDA(cudaMemcpyAsync(b.alive[1], alive_after, n, cudaMemcpyHostToDevice, s));
         NA_CUDA(cudaMemcpyAsync(b.size_m, size_m, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     }
