@@ -18,11 +18,18 @@ Fixtures:
                      separating, TCA at a step edge, collision, dead object
   ref_catalog_1h.json  counters of a 1 h run on the reference's shipped
                      catalogue (the README's own data), for the oracle
+  cli_catalog.txt    a 2 500-object synthetic catalogue in the reference's
+                     pipe format (with planted encounters), and
+  cli_ref_*.csv      the conjunctions.csv / final_state.csv the reference CLI
+                     (oracle/_ref/kessler_sim) writes for it over 15 minutes
 """
 import importlib
 import json
 import os
+import shutil
+import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
@@ -184,6 +191,26 @@ def catalogue_kat():
     print("catalogue 1h", out["conjunctions"], out["closest"])
 
 
+CLI_ARGS = ["0.25", "10", "--conj-km", "5"]
+
+
+def cli_golden():
+    ks = importlib.import_module("kessler-syndrom-simulation_b200")
+    cio = importlib.import_module("kessler-syndrom-simulation_b200.catalog_io")
+    st, sz, al = ks.generate_population(99, 1500, 2500, 3, 1800.0)
+    plant_encounters(st, 0, 20, 90, 10.0, 13)
+    cat = os.path.join(HERE, "cli_catalog.txt")
+    cio.write_catalog(cat, st, ids=np.arange(100001, 100001 + len(st)), rcs=cio.rcs_class_for_size(sz))
+    exe = os.path.join(ROOT, "oracle", "_ref", "kessler_sim")
+    with tempfile.TemporaryDirectory() as tmp:
+        out = subprocess.run([exe, cat] + CLI_ARGS + ["--threads", "8"], cwd=tmp, capture_output=True, text=True,
+                             check=True)
+        shutil.copy(os.path.join(tmp, "output", "conjunctions.csv"), os.path.join(HERE, "cli_ref_conjunctions.csv"))
+        shutil.copy(os.path.join(tmp, "output", "final_state.csv"), os.path.join(HERE, "cli_ref_final_state.csv"))
+    n = sum(1 for _ in open(os.path.join(HERE, "cli_ref_conjunctions.csv"))) - 1
+    print("cli golden: conjunctions", n)
+
+
 def main():
     checkers.build(ref=True)
     st, sz, al = population(20260801, 1500, 3000, 3, 7200.0)
@@ -194,6 +221,7 @@ def main():
     plant_encounters(st, 0, 8, 12, 10.0, 12)
     save_run("run_dense.npz", st, sz, al, 12)
     screen_cases()
+    cli_golden()
     if os.path.exists(CATALOG):
         catalogue_kat()
 
