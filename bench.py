@@ -219,22 +219,29 @@ def timed_run(ks, eng, a, st, sz, al, precision, barrier):
     return eng.timing(), eng.take_conjunctions(), eng.take_step_stats(), wall
 
 
-def max_over_ranks(pg, x):
+def _reduce(pg, x, op):
     if not pg:
         return x
     import torch
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    pg.all_reduce(t, op=op(pg))
     return float(t.item())
+
+
+def max_over_ranks(pg, x):
+    """Max over ranks (the slowest rank's device time bounds the job)."""
+    return _reduce(pg, x, lambda d: d.ReduceOp.MAX)
 
 
 def sum_over_ranks(pg, x):
-    if not pg:
-        return x
-    import torch
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    """Sum over ranks (whole-job work: every rank runs its own realisation)."""
+    return _reduce(pg, x, lambda d: d.ReduceOp.SUM)
+
+
+def realisation_seed(seed, rank):
+    """Seed of the population a rank simulates (independent realisations)."""
+    return seed + rank
 
 
 def roofline_of(tm, a, fp64_rate, fp32_rate, split):
@@ -320,7 +327,7 @@ def main():
                                 device_id=torch.device("cuda", local))
         pg = dist
     ks = importlib.import_module("kessler-syndrom-simulation_b200")
-    st, sz, al = ks.generate_population(a.seed + rank, a.base, a.objects, a.parents, a.frag_age_s)
+    st, sz, al = ks.generate_population(realisation_seed(a.seed, rank), a.base, a.objects, a.parents, a.frag_age_s)
 
     def barrier():
         torch.cuda.synchronize()
@@ -425,10 +432,7 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     fs, fa = eng.get_population()
     barrier()
     wall = time.perf_counter() - t0
-    if pg:
-        t = torch.tensor([wall], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        wall = float(t.item())
+    wall = max_over_ranks(pg, wall)
     world = pg.get_world_size() if pg else 1
     obj = float(al.sum()) * steps * world
     eng.close()
