@@ -63,6 +63,17 @@ void* ks_stream(ks_ctx* ctx);
  *     collision radius = L/2, src/core/collision.cpp:283-287); alive: n bytes or NULL (all alive). */
 int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double* size_m,
                       const uint8_t* alive);
+/* A batch of independent realisations (Monte Carlo runs) resident together:
+ * realisation r owns objects offsets[r] .. offsets[r+1]-1 of the arrays
+ * (offsets has realisations + 1 entries, offsets[0] = 0, at most 65535
+ * realisations). Every kernel of a step covers all realisations; objects of
+ * different realisations never share a cell, so each realisation's
+ * conjunctions are those of a run on its objects alone. Conjunction indices
+ * are batch-wide, with the realisation in ks_conjunction.realisation; step
+ * counters are sums over realisations. Replaces one Simulation per
+ * realisation (src/core/orbital.hpp:144-163). */
+int ks_set_population_batch(ks_ctx* ctx, int32_t realisations, const int64_t* offsets, const double* states,
+                            const double* size_m, const uint8_t* alive);
 int ks_get_population(ks_ctx* ctx, int64_t n, double* states, uint8_t* alive);
 int64_t ks_population_size(const ks_ctx* ctx);
 

@@ -18,14 +18,14 @@ extern "C" {
  * Mirrors kessler::Conjunction (src/core/collision.hpp:181-187) and adds the
  * step index so that a multi-step run can be returned as one flat list. */
 typedef struct ks_conjunction {
-    int32_t i;            /* index into the population, i < j */
+    int32_t i;            /* index into the population, i < j (whole batch for a batched population) */
     int32_t j;
     int64_t step;         /* global step index whose interval (t0, t0+dt) holds the TCA */
     double t;             /* time of closest approach, seconds since epoch */
     double miss_km;       /* distance at TCA */
     double v_rel_km_s;    /* relative speed at TCA */
     int32_t collision;    /* 1 if miss_km < R_i + R_j */
-    int32_t reserved;
+    int32_t realisation;  /* realisation both objects belong to (0 for a single population) */
 } ks_conjunction;         /* 48 bytes */
 
 /* Per-step screening counters.

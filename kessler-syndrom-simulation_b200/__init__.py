@@ -92,6 +92,14 @@ class Engine:
             raise ValueError("alive must have shape (n,)")
         self._check(self._lib.ks_set_population(self._h, n, ptr(st), ptr(sz), ptr(al)))
 
+    def set_population_batch(self, offsets, states, size_m, alive=None):
+        """Independent realisations: realisation r owns rows offsets[r]:offsets[r+1]."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        st = _states(states, int(off[-1]))
+        sz = np.ascontiguousarray(size_m, dtype=np.float64)
+        al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        self._check(self._lib.ks_set_population_batch(self._h, len(off) - 1, ptr(off), ptr(st), ptr(sz), ptr(al)))
+
     def get_population(self):
         n = self._lib.ks_population_size(self._h)
         st = np.empty((n, 6), dtype=np.float64)

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libkessler_b200.so")
 
 CONJ_DTYPE = np.dtype(
     [("i", "<i4"), ("j", "<i4"), ("step", "<i8"), ("t", "<f8"), ("miss_km", "<f8"),
-     ("v_rel_km_s", "<f8"), ("collision", "<i4"), ("reserved", "<i4")], align=True)
+     ("v_rel_km_s", "<f8"), ("collision", "<i4"), ("realisation", "<i4")], align=True)
 STATS_DTYPE = np.dtype(
     [("step", "<i8"), ("candidate_pairs", "<i8"), ("refined_pairs", "<i8"), ("co_orbiting", "<i8"),
      ("conjunctions", "<i8"), ("cell_km", "<f8"), ("max_cell_objects", "<i4"), ("alive", "<i4")],
@@ -46,6 +46,7 @@ SIGNATURES = {
     "ks_device_name": (C.c_char_p, [_P]),
     "ks_stream": (_P, [_P]),
     "ks_set_population": (C.c_int, [_P, _I64, _P, _P, _P]),
+    "ks_set_population_batch": (C.c_int, [_P, C.c_int32, _P, _P, _P, _P]),
     "ks_get_population": (C.c_int, [_P, _I64, _P, _P]),
     "ks_population_size": (_I64, [_P]),
     "ks_set_clock": (C.c_int, [_P, _D, _D, _D]),

@@ -61,6 +61,9 @@ struct ks_ctx {
     std::vector<cudaEvent_t> ev;
     ks_timing timing{};
     ks::Tuning tune;
+    int realisations = 1;
+    int rbits = 0;
+    std::vector<int64_t> offsets;  // realisation offsets (batches)
     void* l2_flush = nullptr;
     int64_t l2_flush_bytes = 0;
 };
@@ -94,7 +97,7 @@ void drop_graphs(ks_ctx* ctx) {
 void free_objects(ks_ctx* ctx) {
     ks::DeviceBuffers& b = ctx->b;
     for (int k = 0; k < 2; ++k) { dfree(b.state[k]); dfree(b.alive[k]); dfree(b.keys[k]); dfree(b.idx[k]); }
-    dfree(b.size_m); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
+    dfree(b.size_m); dfree(b.real_id); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr); dfree(b.scan_part); dfree(b.item_count);
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_len); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted32); dfree(b.sorted_orig);
@@ -117,6 +120,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
         KS_CUDA(cudaMalloc(&b.idx[k], sizeof(int) * cap));
     }
     KS_CUDA(cudaMalloc(&b.size_m, sizeof(double) * cap));
+    KS_CUDA(cudaMalloc(&b.real_id, sizeof(uint16_t) * cap));
     KS_CUDA(cudaMalloc(&b.ckpt_state, sizeof(double) * 6 * cap));
     KS_CUDA(cudaMalloc(&b.ckpt_alive, cap));
     b.sort_status_len = 8 * 256 * ((cap + 2047) / 2048);
@@ -226,7 +230,7 @@ int passes_for_bits(int bits) { return std::max(1, (bits + 1 + 7) / 8); }
 // Host estimate of the key width from a seeded control block. Only sizes the
 // number of radix passes; the device checks it and the chunk is replayed with
 // more passes if the estimate was short.
-int estimate_bits(const Ctrl& c, double dt, double thr, int sub) {
+int estimate_bits(const Ctrl& c, double dt, double thr, int sub, int rbits, double scale) {
     const double vmax = [&] { double v; std::memcpy(&v, &c.spec_vmax, 8); return v; }();
     auto dec = [](unsigned long long u) {
         unsigned long long b = (u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u;
@@ -237,7 +241,8 @@ int estimate_bits(const Ctrl& c, double dt, double thr, int sub) {
     const double vrel = 2.0 * vmax;
     double cell = vrel * dt + thr + ks::kGravityGradient * vrel * dt * dt * dt;
     if (cell < 1.0) cell = 1.0;
-    int bits = 0;
+    if (scale > 1.0) cell *= scale;
+    int bits = rbits;
     for (int a = 0; a < 3; ++a) {
         const double mn = dec(c.bb_min[a]), mx = dec(c.bb_max[a]);
         if (!(mn <= mx)) continue;
@@ -270,6 +275,8 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     a.vmin2 = ctx->vmin * ctx->vmin;
     a.radius_scale = ctx->rscale;
     a.n = static_cast<int>(ctx->n);
+    a.rbits = ctx->rbits;
+    a.real_id = ctx->rbits > 0 ? ctx->b.real_id : nullptr;
     a.screening = ctx->screening;
     a.precision = ctx->precision;
     a.sort_passes = ctx->sort_passes;
@@ -410,7 +417,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         }
         const bool surv_over = max_refined > static_cast<unsigned long long>(ctx->b.surv_cap);
         const bool items_over = max_items > ctx->b.items_cap;
-        if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds");
+        if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits");
         if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
         if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) break;
         if (attempt >= kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after replays");
@@ -465,7 +472,8 @@ int seed_speculation(ks_ctx* ctx) {
     Ctrl c{};
     KS_CUDA(cudaMemcpyAsync(&c, carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA(cudaStreamSynchronize(ctx->stream));
-    ctx->sort_passes = passes_for_bits(estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits));
+    ctx->sort_passes = passes_for_bits(
+        estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale));
     drop_graphs(ctx);
     return KS_OK;
 }
@@ -548,10 +556,47 @@ void* ks_stream(ks_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nu
 int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double* size_m, const uint8_t* alive) {
     if (!ctx || n < 0 || (n > 0 && (!states || !size_m))) return fail(ctx, KS_ERR_ARG, "ks_set_population: bad arguments");
     cudaSetDevice(ctx->device);
+    ctx->realisations = 1;
+    ctx->rbits = 0;
+    ctx->offsets.assign({0, n});
     int rc = ensure_objects(ctx, n);
     if (rc) return rc;
     ctx->n = n;
     ctx->cur = 0;
+    rc = upload_population(ctx, n, states, size_m, alive, 0);
+    if (rc) return rc;
+    rc = seed_speculation(ctx);
+    if (rc) return rc;
+    ctx->has_pop = true;
+    ctx->steps_done = 0;
+    ctx->conj_out.clear();
+    ctx->stats_out.clear();
+    return KS_OK;
+}
+
+int ks_set_population_batch(ks_ctx* ctx, int32_t realisations, const int64_t* offsets, const double* states,
+                            const double* size_m, const uint8_t* alive) {
+    if (!ctx || realisations < 1 || realisations > 65535 || !offsets || offsets[0] != 0)
+        return fail(ctx, KS_ERR_ARG, "ks_set_population_batch: bad arguments");
+    for (int r = 0; r < realisations; ++r)
+        if (offsets[r + 1] < offsets[r]) return fail(ctx, KS_ERR_ARG, "ks_set_population_batch: offsets must not decrease");
+    const int64_t n = offsets[realisations];
+    if (n > 0 && (!states || !size_m)) return fail(ctx, KS_ERR_ARG, "ks_set_population_batch: bad arguments");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_objects(ctx, n);
+    if (rc) return rc;
+    std::vector<uint16_t> rid(static_cast<size_t>(n));
+    for (int r = 0; r < realisations; ++r)
+        for (int64_t i = offsets[r]; i < offsets[r + 1]; ++i) rid[static_cast<size_t>(i)] = static_cast<uint16_t>(r);
+    if (n > 0) KS_CUDA(cudaMemcpy(ctx->b.real_id, rid.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    int rbits = 0;
+    while ((1 << rbits) < realisations) ++rbits;
+    ctx->realisations = realisations;
+    ctx->rbits = rbits;
+    ctx->offsets.assign(offsets, offsets + realisations + 1);
+    ctx->n = n;
+    ctx->cur = 0;
+    drop_graphs(ctx);
     rc = upload_population(ctx, n, states, size_m, alive, 0);
     if (rc) return rc;
     rc = seed_speculation(ctx);
@@ -662,6 +707,13 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
             return seed_speculation(ctx);
         }
     } else if (k == "box_min_rows" && value >= 0 && value <= 33) ctx->tune.box_min_rows = static_cast<int>(value);
+    else if (k == "cell_scale_permille" && value >= 1000 && value <= 4000) {
+        ctx->tune.cell_scale = static_cast<double>(value) / 1000.0;
+        if (ctx->has_pop) {
+            drop_graphs(ctx);
+            return seed_speculation(ctx);
+        }
+    }
     else return fail(ctx, KS_ERR_ARG, "ks_set_tuning: unknown key or value out of range: " + k);
     drop_graphs(ctx);
     return KS_OK;
@@ -746,6 +798,9 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
     if (rc) return rc;
     ctx->has_pop = false;
     ctx->n = n;
+    ctx->realisations = 1;
+    ctx->rbits = 0;
+    ctx->offsets.assign({0, n});
     rc = upload_population(ctx, n, before, size_m, nullptr, 0);
     if (!rc) rc = upload_population(ctx, n, after, nullptr, alive_after, 1);
     if (rc) return rc;
@@ -775,7 +830,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         const int flags = c.flags | ctx->h_chunk->flags;
         const bool surv_over = c.refined > static_cast<unsigned long long>(ctx->b.surv_cap);
         const bool items_over = c.n_items > ctx->b.items_cap;
-        if (flags & ks::FLAG_KEY_RANGE) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds"); }
+        if (flags & ks::FLAG_KEY_RANGE) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits"); }
         if (flags & ks::FLAG_TIMEOUT) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up"); }
         if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) {
             st.step = 0;

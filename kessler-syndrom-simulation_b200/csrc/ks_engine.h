@@ -44,8 +44,9 @@ struct GridParams {
     long long lo[3];
     long long span[3];   // hi - lo per axis
     int w[3];
+    int rbits;           // realisation index bits, above the cell coordinates (batches)
     int sub;             // sub-cell bits per axis
-    int bits;            // wx + wy + wz + 3 * sub
+    int bits;            // rbits + wx + wy + wz + 3 * sub
 };
 
 enum : int {
@@ -94,6 +95,7 @@ struct DeviceBuffers {
     double* state[2] = {nullptr, nullptr};
     uint8_t* alive[2] = {nullptr, nullptr};
     double* size_m = nullptr;
+    uint16_t* real_id = nullptr;           // realisation of each object (batches), else null
     double* ckpt_state = nullptr;
     uint8_t* ckpt_alive = nullptr;
     unsigned long long* keys[2] = {nullptr, nullptr};
@@ -133,6 +135,7 @@ struct Tuning {
     int pair_blocks_per_sm = 0;   // resident blocks of the pair kernel
     int subcell_bits = 1;         // Morton order inside cells, bits per axis (0..3)
     int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
+    double cell_scale = 1.0;      // cell edge = reference edge x this (>= 1; changes only candidate counts)
 };
 
 // Everything a step's kernels need, by value.
@@ -145,6 +148,8 @@ struct StepArgs {
     double radius_scale;
     double gate_hi2;           // unused by the propagation kernel
     int n;                     // population size (objects, alive or not)
+    int rbits;                 // realisation bits of the keys (0: one population)
+    const uint16_t* real_id;   // realisation of each object, or null
     int screening;             // 0: propagation only
     int precision;             // KS_PRECISION_FP64 or KS_PRECISION_SPLIT
     int sort_passes;

@@ -51,11 +51,12 @@ __device__ __forceinline__ double dec_double(unsigned long long u) {
 // Cell edge (src/core/collision.cpp:339-356) from the largest start speed, and
 // the compact key layout over the position bounds.
 __device__ void make_grid(double vmax, const unsigned long long* bb_min, const unsigned long long* bb_max,
-                          double dt, double threshold_km, int sub, GridParams& g) {
+                          double dt, double threshold_km, int sub, int rbits, double scale, GridParams& g) {
     const double vrel = xmul(2.0, vmax);
     const double c = xadd(xadd(xmul(vrel, dt), threshold_km),
                           xmul(xmul(xmul(xmul(kGravityGradient, vrel), dt), dt), dt));
     g.cell = c > 1.0 ? c : 1.0;
+    if (scale > 1.0) g.cell = xmul(g.cell, scale);
     int bits = 0;
     for (int a = 0; a < 3; ++a) {
         const double mn = dec_double(bb_min[a]), mx = dec_double(bb_max[a]);
@@ -70,7 +71,8 @@ __device__ void make_grid(double vmax, const unsigned long long* bb_min, const u
         bits += g.w[a];
     }
     g.sub = sub;
-    g.bits = bits + 3 * sub;
+    g.rbits = rbits;
+    g.bits = rbits + bits + 3 * sub;
 }
 
 __device__ __forceinline__ unsigned sub_coord(double q, double fq, int sub) {
@@ -78,18 +80,19 @@ __device__ __forceinline__ unsigned sub_coord(double q, double fq, int sub) {
     return static_cast<unsigned>(min(max(s, 0), (1 << sub) - 1));
 }
 
-// Key of a start-of-step position: compact cell coordinates (floor(r / cell),
-// the reference's cell, src/core/collision.cpp:393-395) above the Morton code
-// of the sub-cell; sets *bad if the cell lies outside the bounds.
+// Key of a start-of-step position: realisation index, then compact cell
+// coordinates (floor(r / cell), the reference's cell, src/core/collision.cpp:393-395),
+// then the Morton code of the sub-cell; sets *bad if the cell lies outside the bounds.
 __device__ __forceinline__ unsigned long long cell_key(const GridParams& g, double x, double y, double z,
-                                                       int* bad) {
+                                                       unsigned rid, int* bad) {
     const double qx = xdiv(x, g.cell), qy = xdiv(y, g.cell), qz = xdiv(z, g.cell);
     const double fx = floor(qx), fy = floor(qy), fz = floor(qz);
     const long long cx = static_cast<long long>(fx) - g.lo[0];
     const long long cy = static_cast<long long>(fy) - g.lo[1];
     const long long cz = static_cast<long long>(fz) - g.lo[2];
-    if (cx < 0 || cx > g.span[0] || cy < 0 || cy > g.span[1] || cz < 0 || cz > g.span[2]) *bad = 1;
-    const unsigned long long cell = (static_cast<unsigned long long>(cx) << (g.w[1] + g.w[2])) |
+    if (cx < 0 || cx > g.span[0] || cy < 0 || cy > g.span[1] || cz < 0 || cz > g.span[2] || g.bits > 62) *bad = 1;
+    const unsigned long long cell = (static_cast<unsigned long long>(rid) << (g.w[0] + g.w[1] + g.w[2])) |
+                                    (static_cast<unsigned long long>(cx) << (g.w[1] + g.w[2])) |
                                     (static_cast<unsigned long long>(cy) << g.w[2]) |
                                     static_cast<unsigned long long>(cz);
     unsigned long long morton = 0;
@@ -102,7 +105,7 @@ __device__ __forceinline__ unsigned long long cell_key(const GridParams& g, doub
     return (cell << (3 * g.sub)) | morton;
 }
 
-__device__ __forceinline__ unsigned long long dead_key(const GridParams& g) { return 1ull << g.bits; }
+__device__ __forceinline__ unsigned long long dead_key(const GridParams& g) { return 1ull << min(g.bits, 63); }
 
 __device__ __forceinline__ unsigned long long hash_slot(unsigned long long k, unsigned long long mask) {
     // 64-bit finaliser (Stafford's mix 13); spreads neighbouring keys.
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
     if (threadIdx.x == 0) {
         if (a.screening)
             make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
-                      a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, g);
+                      a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
         for (int q = 0; q < 3; ++q) moon[q] = a.sp->m[q];
         if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
     }
@@ -314,7 +317,7 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
         unsigned long long key = 0ull;
         double vb = 0.0;
         if (a.screening) {
-            key = cell_key(g, s[0], s[1], s[2], &acc.bad);
+            key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
             vb = xsqrt(xdot3(s[3], s[4], s[5]));
         }
         rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
     if (threadIdx.x == 0) {
         if (a.screening)
             make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
-                      a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, g);
+                      a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
         for (int q = 0; q < 3; ++q) moon[q] = to_f32(a.sp->m[q]);
         if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
     }
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
         unsigned long long key = 0ull;
         double vb = 0.0;
         if (a.screening) {
-            key = cell_key(g, s[0], s[1], s[2], &acc.bad);
+            key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
             vb = xsqrt(xdot3(s[3], s[4], s[5]));
         }
         rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
@@ -406,7 +409,7 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
     __shared__ GridParams g;
     if (threadIdx.x == 0) {
         make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
-                  a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, g);
+                  a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
         if (blockIdx.x == 0) {
             a.ctrl->grid = g;
             a.ctrl->vmax_true = a.ctrl->spec_vmax;
@@ -417,7 +420,7 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         if (alive_after[i]) {
             keys[i] = cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
-                               before[6 * static_cast<int64_t>(i) + 2], &bad);
+                               before[6 * static_cast<int64_t>(i) + 2], a.real_id ? a.real_id[i] : 0u, &bad);
             ++alive;
         } else {
             keys[i] = dead_key(g);
@@ -443,14 +446,14 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
     __shared__ GridParams g;
     if (threadIdx.x == 0) {
         make_grid(__longlong_as_double(static_cast<long long>(vt)), a.ctrl->bb_min, a.ctrl->bb_max, a.dt,
-                  a.threshold_km, a.tune.subcell_bits, g);
+                  a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
         if (blockIdx.x == 0) a.ctrl->grid = g;
     }
     __syncthreads();
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
         keys[i] = alive_after[i] ? cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
-                                            before[6 * static_cast<int64_t>(i) + 2], &bad)
+                                            before[6 * static_cast<int64_t>(i) + 2], a.real_id ? a.real_id[i] : 0u, &bad)
                                  : dead_key(g);
     bad = warp_max(bad);
     if ((threadIdx.x & 31) == 0 && bad) atomicOr(&a.ctrl->flags, FLAG_KEY_RANGE);
@@ -806,7 +809,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
             // Position relative to the corner of the object's own cell, velocity, in FP32.
             const GridParams& g = ctrl->grid;
             const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
-            const double cx = static_cast<double>(static_cast<long long>(key >> (g.w[1] + g.w[2])) + g.lo[0]) * g.cell;
+            const unsigned long long mx = (1ull << g.w[0]) - 1;
+            const double cx = static_cast<double>(static_cast<long long>((key >> (g.w[1] + g.w[2])) & mx) + g.lo[0]) * g.cell;
             const double cy = static_cast<double>(static_cast<long long>((key >> g.w[2]) & my) + g.lo[1]) * g.cell;
             const double cz = static_cast<double>(static_cast<long long>(key & mz) + g.lo[2]) * g.cell;
             sorted32[2 * static_cast<int64_t>(p)] =
@@ -834,12 +838,14 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
          t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int c = static_cast<int>(t / 13), o = static_cast<int>(t % 13);
         const unsigned long long key = cell_key_in[c];
-        const long long x = static_cast<long long>(key >> (g.w[1] + g.w[2])) + c_forward[o][0];
+        const unsigned long long rid = key >> (g.w[0] + g.w[1] + g.w[2]);
+        const long long x = static_cast<long long>((key >> (g.w[1] + g.w[2])) & ((1ull << g.w[0]) - 1)) + c_forward[o][0];
         const long long y = static_cast<long long>((key >> g.w[2]) & my) + c_forward[o][1];
         const long long z = static_cast<long long>(key & mz) + c_forward[o][2];
         int found = -1;
         if (x >= 0 && x <= g.span[0] && y >= 0 && y <= g.span[1] && z >= 0 && z <= g.span[2]) {
-            const unsigned long long nk = (static_cast<unsigned long long>(x) << (g.w[1] + g.w[2])) |
+            const unsigned long long nk = (rid << (g.w[0] + g.w[1] + g.w[2])) |
+                                          (static_cast<unsigned long long>(x) << (g.w[1] + g.w[2])) |
                                           (static_cast<unsigned long long>(y) << g.w[2]) |
                                           static_cast<unsigned long long>(z);
             found = hash_find(hk, hv, hmask, nk);
@@ -1398,7 +1404,7 @@ __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const doubl
         const double ri = xmul(xmul(xmul(0.5, size_m[i]), 1e-3), a.radius_scale);
         const double rj = xmul(xmul(xmul(0.5, size_m[j]), 1e-3), a.radius_scale);
         c.collision = miss < xadd(ri, rj) ? 1 : 0;
-        c.reserved = 0;
+        c.realisation = a.real_id ? a.real_id[i] : 0;
         atomicAdd(&a.ctrl->conj, 1ull);
         const unsigned long long slot = atomicAdd(&chunk->conj_count, 1ull);
         if (slot < static_cast<unsigned long long>(cap)) out[slot] = c;

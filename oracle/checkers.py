@@ -21,7 +21,7 @@ REF_SO = os.path.join(HERE, "_ref", "libksref.so")
 
 CONJ_DTYPE = np.dtype(
     [("i", "<i4"), ("j", "<i4"), ("step", "<i8"), ("t", "<f8"), ("miss_km", "<f8"),
-     ("v_rel_km_s", "<f8"), ("collision", "<i4"), ("reserved", "<i4")], align=True)
+     ("v_rel_km_s", "<f8"), ("collision", "<i4"), ("realisation", "<i4")], align=True)
 STATS_DTYPE = np.dtype(
     [("step", "<i8"), ("candidate_pairs", "<i8"), ("refined_pairs", "<i8"), ("co_orbiting", "<i8"),
      ("conjunctions", "<i8"), ("cell_km", "<f8"), ("max_cell_objects", "<i4"), ("alive", "<i4")],

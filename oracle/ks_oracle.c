@@ -256,7 +256,7 @@ static int kso_refine_pair(const double* before, const double* after, const doub
     out->v_rel_km_s = kso_norm3(v) / dt;
     out->collision = miss < kso_collision_radius_km(size_m[i], radius_scale) +
                                 kso_collision_radius_km(size_m[j], radius_scale);
-    out->reserved = 0;
+    out->realisation = 0;
     return 1;
 }
 
