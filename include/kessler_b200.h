@@ -103,6 +103,42 @@ int ks_run(ks_ctx* ctx, int64_t steps);
 int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t* count);
 int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* count);
 
+/* --- fragmentation: Fragmentation (src/core/breakup.hpp:100-153), the CLI's
+ *     --breakup / --impact (src/main.cpp:28-36, 343-346, 401-407).
+ * With on != 0, every collision a step reports is fragmented by the NASA
+ * Standard Breakup Model before the next step, as the reference's loop does
+ * after Screener::finish: parents destroyed (or the target eroded below the
+ * catastrophic threshold), fragments appended after the population and carried
+ * to the end of the step. A run of steps ends its chunk at each step that holds
+ * a collision. Fragments and events equal the reference's for the same seed
+ * (same draws, same arithmetic). lc_m: smallest fragment followed;
+ * catastrophic_j_per_g: specific-energy threshold; realisation r of a batch
+ * draws from its own stream seeded seed + r. BreakupConfig (breakup.hpp:75-79). */
+int ks_set_breakup(ks_ctx* ctx, int on, double lc_m, double catastrophic_j_per_g, uint64_t seed);
+/* Masses (kg) of the population's objects, 0 = unknown (fragmentation then
+ * uses 100 kg): the output of assign_masses (src/core/breakup.cpp:104-111). */
+int ks_set_masses(ks_ctx* ctx, int64_t n, const double* mass_kg);
+/* Forced impact of a fictitious projectile on object `target`, now:
+ * Fragmentation::impact (src/core/breakup.cpp:340-360). */
+int ks_impact(ks_ctx* ctx, int64_t target, double projectile_mass_kg, double v_rel_km_s);
+/* One forced impact on a lone object, on the host, no context or device: the
+ * SBM with a fresh stream seeded `seed` (Fragmentation::impact on a one-object
+ * Simulation at time t). Writes up to cap fragments at their birth state
+ * (6 doubles each) with size, mass and area-to-mass; target_after receives the
+ * target's [alive, mass_kg] afterwards. Returns the number of fragments, or -1. */
+int64_t ks_sbm_impact(uint64_t seed, double lc_m, double catastrophic_j_per_g, const double* state,
+                      double target_mass_kg, double target_size_m, double projectile_mass_kg, double v_rel_km_s,
+                      double t, ks_breakup_event* event, double* frag_states, double* frag_size, double* frag_mass,
+                      double* frag_area_to_mass, int64_t cap, double* target_after);
+/* Fragmentation events since the last take, in the order they happened
+ * (same conventions as ks_take_conjunctions). */
+int ks_take_breakups(ks_ctx* ctx, ks_breakup_event* out, int64_t cap, int64_t* count);
+/* Per-object properties (any pointer may be NULL): size (m), mass (kg, 0 =
+ * unknown), area-to-mass ratio (m^2/kg, fragments only), originating event
+ * (-1 for the initial population) and realisation. n = ks_population_size. */
+int ks_get_objects(ks_ctx* ctx, int64_t n, double* size_m, double* mass_kg, double* area_to_mass, int32_t* event,
+                   int32_t* realisation);
+
 /* --- one-shot screening on host states: replaces Screener::screen and screen_step
  *     (src/core/collision.hpp:242-244, 266-270). before/after: n x 6 doubles,
  *     alive_after: n bytes, size_m: n doubles. Results sorted by (t, i, j), step = 0.

@@ -42,6 +42,30 @@ typedef struct ks_step_stats {
     int32_t alive;             /* objects alive after the step */
 } ks_step_stats;               /* 56 bytes */
 
+/* One fragmentation (collision or forced impact).
+ * Mirrors kessler::BreakupEvent (src/core/breakup.hpp:81-98); names are left
+ * to the caller (a fragment is "FRAG <id>-<k>" for the k-th fragment of event
+ * <id>, a forced impact's projectile "PROJECTILE"). */
+typedef struct ks_breakup_event {
+    int64_t step;                /* step whose interval holds the event (the next step for a forced impact) */
+    double t;                    /* seconds since epoch */
+    int32_t id;                  /* event number within its realisation, from 0 */
+    int32_t realisation;
+    int64_t target, projectile;  /* object indices; -1 for a forced impact's fictitious projectile */
+    int32_t catastrophic;
+    int32_t fragments;           /* fragments added: objects first_fragment .. first_fragment + fragments - 1 */
+    int32_t escaped;             /* fragments on hyperbolic trajectories, dropped */
+    int32_t pad;
+    int64_t first_fragment;
+    double v_rel_km_s;
+    double energy_j_per_g;
+    double target_mass_kg, projectile_mass_kg;
+    double sbm_mass_kg;          /* M of the number law */
+    double expected_fragments;   /* N(> L_c) of the law */
+    double fragments_mass_kg;
+    double position[3];          /* target position at the event, km */
+} ks_breakup_event;              /* 144 bytes */
+
 #ifdef __cplusplus
 }
 #endif

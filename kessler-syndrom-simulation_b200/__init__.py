@@ -14,11 +14,11 @@ import ctypes as C
 
 import numpy as np
 
-from ._abi import (CONJ_DTYPE, PRECISION_FP64, PRECISION_SPLIT, STATS_DTYPE, STATUS_NAMES, Timing,
+from ._abi import (BREAKUP_DTYPE, CONJ_DTYPE, PRECISION_FP64, PRECISION_SPLIT, STATS_DTYPE, STATUS_NAMES, Timing,
                    load_library, ptr)
 
-__all__ = ["Engine", "KsError", "CONJ_DTYPE", "STATS_DTYPE", "PRECISION_FP64", "PRECISION_SPLIT",
-           "moon_position", "generate_population", "load_library", "DEFAULT_EPOCH_JD"]
+__all__ = ["Engine", "KsError", "BREAKUP_DTYPE", "CONJ_DTYPE", "STATS_DTYPE", "PRECISION_FP64", "PRECISION_SPLIT",
+           "moon_position", "generate_population", "sbm_impact", "load_library", "DEFAULT_EPOCH_JD"]
 
 # src/core/orbital.hpp:30
 DEFAULT_EPOCH_JD = 2461253.916666667
@@ -158,6 +158,35 @@ class Engine:
             self._check(self._lib.ks_take_step_stats(self._h, ptr(out), cnt.value, C.byref(cnt)))
         return out[: cnt.value]
 
+    # --- fragmentation (NASA SBM) ---
+    def set_breakup(self, on=True, lc_m=0.10, catastrophic_j_per_g=40.0, seed=1):
+        self._check(self._lib.ks_set_breakup(self._h, 1 if on else 0, float(lc_m), float(catastrophic_j_per_g),
+                                             int(seed)))
+
+    def set_masses(self, mass_kg):
+        m = np.ascontiguousarray(mass_kg, dtype=np.float64)
+        self._check(self._lib.ks_set_masses(self._h, len(m), ptr(m)))
+
+    def impact(self, target, projectile_mass_kg=10.0, v_rel_km_s=10.0):
+        self._check(self._lib.ks_impact(self._h, int(target), float(projectile_mass_kg), float(v_rel_km_s)))
+
+    def take_breakups(self):
+        cnt = C.c_int64()
+        self._check(self._lib.ks_take_breakups(self._h, None, 0, C.byref(cnt)))
+        out = np.zeros(cnt.value, dtype=BREAKUP_DTYPE)
+        if cnt.value:
+            self._check(self._lib.ks_take_breakups(self._h, ptr(out), cnt.value, C.byref(cnt)))
+        return out[: cnt.value]
+
+    def objects(self):
+        """Per-object size_m, mass_kg, area_to_mass, event (-1: initial population) and realisation."""
+        n = self._lib.ks_population_size(self._h)
+        out = {"size_m": np.empty(n), "mass_kg": np.empty(n), "area_to_mass": np.empty(n),
+               "event": np.empty(n, np.int32), "realisation": np.empty(n, np.int32)}
+        self._check(self._lib.ks_get_objects(self._h, n, ptr(out["size_m"]), ptr(out["mass_kg"]),
+                                             ptr(out["area_to_mass"]), ptr(out["event"]), ptr(out["realisation"])))
+        return out
+
     def timing(self):
         t = Timing()
         self._check(self._lib.ks_get_timing(self._h, C.byref(t)))
@@ -210,6 +239,28 @@ def moon_position(jd):
     out = np.zeros(3)
     lib.ks_moon_position(float(jd), ptr(out))
     return out
+
+
+def sbm_impact(state, target_mass_kg, target_size_m, projectile_mass_kg=10.0, v_rel_km_s=10.0, t=0.0, seed=1,
+               lc_m=0.10, catastrophic_j_per_g=40.0):
+    """NASA SBM forced impact on one object, on the host (no device).
+
+    Returns (event record, fragment birth states (m, 6), sizes, masses, area-to-mass, [target alive, mass])."""
+    lib = load_library()
+    st = np.ascontiguousarray(state, dtype=np.float64).reshape(6)
+    ev = np.zeros(1, dtype=BREAKUP_DTYPE)
+    after = np.zeros(2)
+    cap = 1024
+    while True:
+        fs, fz, fm, fa = np.zeros((cap, 6)), np.zeros(cap), np.zeros(cap), np.zeros(cap)
+        m = lib.ks_sbm_impact(int(seed), float(lc_m), float(catastrophic_j_per_g), ptr(st), float(target_mass_kg),
+                              float(target_size_m), float(projectile_mass_kg), float(v_rel_km_s), float(t), ptr(ev),
+                              ptr(fs), ptr(fz), ptr(fm), ptr(fa), cap, ptr(after))
+        if m < 0:
+            raise KsError(1, "ks_sbm_impact: bad arguments")
+        if m <= cap:
+            return ev[0], fs[:m], fz[:m], fm[:m], fa[:m], after
+        cap = int(m)
 
 
 def generate_population(seed, n_base, n_total=None, n_parents=200, frag_age_max_s=0.0):

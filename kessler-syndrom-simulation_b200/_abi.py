@@ -18,7 +18,13 @@ STATS_DTYPE = np.dtype(
     [("step", "<i8"), ("candidate_pairs", "<i8"), ("refined_pairs", "<i8"), ("co_orbiting", "<i8"),
      ("conjunctions", "<i8"), ("cell_km", "<f8"), ("max_cell_objects", "<i4"), ("alive", "<i4")],
     align=True)
-assert CONJ_DTYPE.itemsize == 48 and STATS_DTYPE.itemsize == 56
+BREAKUP_DTYPE = np.dtype(
+    [("step", "<i8"), ("t", "<f8"), ("id", "<i4"), ("realisation", "<i4"), ("target", "<i8"), ("projectile", "<i8"),
+     ("catastrophic", "<i4"), ("fragments", "<i4"), ("escaped", "<i4"), ("pad", "<i4"), ("first_fragment", "<i8"),
+     ("v_rel_km_s", "<f8"), ("energy_j_per_g", "<f8"), ("target_mass_kg", "<f8"), ("projectile_mass_kg", "<f8"),
+     ("sbm_mass_kg", "<f8"), ("expected_fragments", "<f8"), ("fragments_mass_kg", "<f8"), ("position", "<f8", (3,))],
+    align=True)
+assert CONJ_DTYPE.itemsize == 48 and STATS_DTYPE.itemsize == 56 and BREAKUP_DTYPE.itemsize == 144
 
 
 class Timing(C.Structure):
@@ -61,6 +67,12 @@ SIGNATURES = {
     "ks_run": (C.c_int, [_P, _I64]),
     "ks_take_conjunctions": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
+    "ks_set_breakup": (C.c_int, [_P, C.c_int, _D, _D, C.c_uint64]),
+    "ks_set_masses": (C.c_int, [_P, _I64, _P]),
+    "ks_impact": (C.c_int, [_P, _I64, _D, _D]),
+    "ks_take_breakups": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
+    "ks_sbm_impact": (_I64, [C.c_uint64, _D, _D, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P, _P, _I64, _P]),
+    "ks_get_objects": (C.c_int, [_P, _I64, _P, _P, _P, _P, _P]),
     "ks_screen": (C.c_int, [_P, _I64, _P, _P, _P, _P, _D, _D, _P, _I64, C.POINTER(_I64), _P]),
     "ks_propagate": (C.c_int, [_P, _I64, _P, _P, _D, _D, _D, _I64]),
     "ks_screen_noalloc": (C.c_int, [_I64, _P, _P, _P, _P, _D, _D, _D, _D, _D, _P, _I64, C.POINTER(_I64), _P, _P,

@@ -17,16 +17,18 @@ def rcs_class_for_size(size_m):
     return np.where(s < 0.4, "SMALL", np.where(s < 1.8, "MEDIUM", "LARGE"))
 
 
-def write_catalog(path, states, ids=None, names=None, rcs=None, epoch_iso="2026-08-01T10:00:00+00:00"):
+def write_catalog(path, states, ids=None, names=None, rcs=None, epoch_iso="2026-08-01T10:00:00+00:00", types=None):
     """Writes states (n, 6) as a catalogue the reference CLI can read.
 
     Values are written with 17 significant digits, so they read back bit for bit.
+    types: object types (PAYLOAD, DEBRIS, ROCKET BODY, UNKNOWN); DEBRIS by default.
     """
     st = np.asarray(states, dtype=np.float64)
     n = st.shape[0]
     ids = np.arange(1, n + 1) if ids is None else np.asarray(ids)
     names = [f"OBJ {int(i)}" for i in ids] if names is None else list(names)
     rcs = ["MEDIUM"] * n if rcs is None else list(rcs)
+    types = ["DEBRIS"] * n if types is None else list(types)
     with open(path, "w") as f:
         f.write("# Synthetic catalogue, seeded, states at one common epoch\n")
         f.write(f"# Reference date (epoch commun) : {epoch_iso}\n")
@@ -36,7 +38,7 @@ def write_catalog(path, states, ids=None, names=None, rcs=None, epoch_iso="2026-
             x = st[k]
             alt = float(np.linalg.norm(x[:3])) - 6378.137
             vals = " | ".join(f"{v:.17g}" for v in x)
-            f.write(f"{int(ids[k])} | {names[k]} | DEBRIS | 2026-000A | XX | {rcs[k]} | 0 | "
+            f.write(f"{int(ids[k])} | {names[k]} | {types[k]} | 2026-000A | XX | {rcs[k]} | 0 | "
                     f"2026-08-01T10:00:00 | 0 | 0 | {alt:.3f} | {vals}\n")
 
 

@@ -14,10 +14,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <set>
 #include <string>
 #include <vector>
 
 #include "kessler_b200.h"
+#include "ks_breakup.h"
 #include "ks_engine.h"
 #include "ks_host.h"
 
@@ -66,6 +68,22 @@ struct ks_ctx {
     std::vector<int64_t> offsets;  // realisation offsets (batches)
     void* l2_flush = nullptr;
     int64_t l2_flush_bytes = 0;
+
+    // Fragmentation (NASA SBM) on the host, between steps. Per-object
+    // properties the device does not need are mirrored here, built on first
+    // use; one random stream and event counter per realisation.
+    struct Breakup {
+        bool on = false;
+        ks::SbmParams params;
+        uint64_t seed = 1;
+        std::vector<ks::SbmRng> rng;
+        std::vector<int32_t> next_event;
+        std::vector<double> size_m, mass_kg, area_to_mass;
+        std::vector<int32_t> event;
+        std::vector<uint16_t> rid;
+        bool mirrors = false;
+        std::vector<ks_breakup_event> out;
+    } bk;
 };
 
 namespace {
@@ -389,7 +407,13 @@ void accumulate_timing(ks_ctx* ctx, int k_steps) {
     }
 }
 
+int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_conjunction>& hits);
+
 // Runs one chunk of k_steps; replays it after growing whatever overflowed.
+// With fragmentation on, a chunk ends at the first step that holds a
+// collision (the chunk is replayed up to that step), and the collisions are
+// fragmented before the next step, as the reference's loop does after each
+// step (src/main.cpp:401-407).
 int run_chunk(ks_ctx* ctx, int k_steps) {
     int rc = ensure_chunk(ctx, k_steps);
     if (rc) return rc;
@@ -432,14 +456,44 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
             return rc;
         rc = restore_checkpoint(ctx);
         if (rc) return rc;
+        continue;
     }
-    const int64_t nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
-    if (nc > 0) {
-        KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj, sizeof(ks_conjunction) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    int64_t nc = 0;
+    for (int cut = 0;; ++cut) {
+        nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
+        if (nc > 0) {
+            KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj, sizeof(ks_conjunction) * nc, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+            KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        if (!ctx->bk.on || nc == 0) break;
+        int64_t first_hit = -1;
+        for (int64_t q = 0; q < nc; ++q)
+            if (ctx->h_conj[q].collision && (first_hit < 0 || ctx->h_conj[q].step < first_hit)) first_hit = ctx->h_conj[q].step;
+        if (first_hit < 0 || first_hit - ctx->steps_done >= k_steps - 1) break;
+        if (cut > 0) return fail(ctx, KS_ERR_STATE, "replay to the first collision step did not end there");
+        // Replay the chunk up to the step of the first collision (same inputs, same results).
+        k_steps = static_cast<int>(first_hit - ctx->steps_done) + 1;
+        fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
+        rc = restore_checkpoint(ctx);
+        if (rc) return rc;
+        rc = launch_chunk(ctx, k_steps);
+        if (rc) return rc;
+        KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_chunk->flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_TIMEOUT | ks::FLAG_KEY_RANGE))
+            return fail(ctx, KS_ERR_STATE, "replay to the first collision step overflowed");
+    }
+    std::vector<ks_conjunction> hits;
+    const double t_last = ctx->h_params[k_steps - 1].t0;
+    if (nc > 0) {
         const size_t base = ctx->conj_out.size();
         ctx->conj_out.insert(ctx->conj_out.end(), ctx->h_conj, ctx->h_conj + nc);
         std::sort(ctx->conj_out.begin() + base, ctx->conj_out.end(), conj_less);
+        if (ctx->bk.on)
+            for (size_t q = base; q < ctx->conj_out.size(); ++q)
+                if (ctx->conj_out[q].collision) hits.push_back(ctx->conj_out[q]);
     }
     for (int k = 0; k < k_steps; ++k) {
         const Ctrl& c = ctx->h_ctrl[k];
@@ -464,6 +518,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     ctx->steps_done += k_steps;
     ctx->t = t_end;
     if (k_steps & 1) ctx->cur ^= 1;
+    if (!hits.empty()) return apply_collisions(ctx, ctx->steps_done - 1, t_last, hits);
     return KS_OK;
 }
 
@@ -489,6 +544,214 @@ int upload_population(ks_ctx* ctx, int64_t n, const double* states, const double
     }
     KS_CUDA(cudaGetLastError());
     return KS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Fragmentation between steps (NASA SBM on the host, fragments' sub-step on
+// the device)
+// ---------------------------------------------------------------------------
+
+void reset_breakup_run(ks_ctx* ctx) {
+    ks_ctx::Breakup& k = ctx->bk;
+    k.rng.clear();
+    k.next_event.clear();
+    k.out.clear();
+    k.mirrors = false;
+    k.size_m.clear();
+    k.mass_kg.clear();
+    k.area_to_mass.clear();
+    k.event.clear();
+    k.rid.clear();
+}
+
+// Host copies of the per-object properties fragmentation reads.
+int ensure_mirrors(ks_ctx* ctx) {
+    ks_ctx::Breakup& k = ctx->bk;
+    if (k.mirrors) return KS_OK;
+    const size_t n = static_cast<size_t>(ctx->n);
+    k.size_m.assign(n, 0.0);
+    k.mass_kg.assign(n, 0.0);
+    k.area_to_mass.assign(n, 0.0);
+    k.event.assign(n, -1);
+    k.rid.assign(n, 0);
+    if (n > 0) {
+        KS_CUDA(cudaMemcpyAsync(k.size_m.data(), ctx->b.size_m, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        if (ctx->rbits > 0)
+            KS_CUDA(cudaMemcpyAsync(k.rid.data(), ctx->b.real_id, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    k.mirrors = true;
+    return KS_OK;
+}
+
+// One random stream per realisation, seeded seed + realisation.
+void ensure_streams(ks_ctx* ctx) {
+    ks_ctx::Breakup& k = ctx->bk;
+    while (static_cast<int>(k.rng.size()) < ctx->realisations) {
+        k.rng.emplace_back(k.seed + static_cast<uint64_t>(k.rng.size()));
+        k.next_event.push_back(0);
+    }
+}
+
+// Grows the object arrays to hold `want` objects, keeping the current states,
+// alive flags, sizes and realisation ids.
+int grow_objects(ks_ctx* ctx, int64_t want) {
+    ks::DeviceBuffers& b = ctx->b;
+    if (want <= b.cap) return KS_OK;
+    const int64_t n = ctx->n;
+    const int64_t cap = std::max<int64_t>(want, b.cap + b.cap / 2 + 1024);
+    double *st = nullptr, *sz = nullptr;
+    uint8_t* al = nullptr;
+    uint16_t* rid = nullptr;
+    if (n > 0) {
+        KS_CUDA(cudaMalloc(&st, sizeof(double) * 6 * n));
+        KS_CUDA(cudaMalloc(&sz, sizeof(double) * n));
+        KS_CUDA(cudaMalloc(&al, n));
+        KS_CUDA(cudaMalloc(&rid, sizeof(uint16_t) * n));
+        KS_CUDA(cudaMemcpyAsync(st, b.state[ctx->cur], sizeof(double) * 6 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(sz, b.size_m, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(al, b.alive[ctx->cur], n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(rid, b.real_id, sizeof(uint16_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    int rc = ensure_objects(ctx, cap);
+    if (!rc && n > 0) {
+        KS_CUDA(cudaMemcpyAsync(b.state[ctx->cur], st, sizeof(double) * 6 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.size_m, sz, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.alive[ctx->cur], al, n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.real_id, rid, sizeof(uint16_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    dfree(st);
+    dfree(sz);
+    dfree(al);
+    dfree(rid);
+    return rc;
+}
+
+struct NewFragments {
+    std::vector<ks::SbmFragment> rows;
+    std::vector<uint16_t> rid;
+    std::vector<int32_t> event;
+    struct Span {
+        int64_t first;
+        int count;
+        double remaining_s;  // time from the event to the end of its step
+        double jd0;          // Julian date of the event
+    };
+    std::vector<Span> spans;
+    std::vector<int64_t> killed;
+};
+
+// Appends the fragments after the population, carries those born inside a
+// step to its end (on the device), and removes the destroyed parents.
+int commit_fragments(ks_ctx* ctx, const NewFragments& nf) {
+    ks::DeviceBuffers& b = ctx->b;
+    const int64_t n0 = ctx->n;
+    const int64_t m = static_cast<int64_t>(nf.rows.size());
+    int rc = grow_objects(ctx, n0 + m);
+    if (rc) return rc;
+    if (m > 0) {
+        std::vector<double> st(static_cast<size_t>(6 * m)), sz(static_cast<size_t>(m));
+        std::vector<uint8_t> al(static_cast<size_t>(m), 1);
+        for (int64_t q = 0; q < m; ++q) {
+            const ks::SbmFragment& f = nf.rows[static_cast<size_t>(q)];
+            std::copy(f.s, f.s + 6, &st[static_cast<size_t>(6 * q)]);
+            sz[static_cast<size_t>(q)] = f.size_m;
+        }
+        for (const NewFragments::Span& sp : nf.spans) {
+            if (sp.remaining_s > 0) continue;
+            // Born at the end of the interval: alive unless below the surface
+            // (src/core/breakup.cpp:305-306).
+            for (int q = 0; q < sp.count; ++q) {
+                const double* r = &st[static_cast<size_t>(6 * (sp.first - n0 + q))];
+                al[static_cast<size_t>(sp.first - n0 + q)] =
+                    std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) >= ks::kREarth ? 1 : 0;
+            }
+        }
+        double* dst = b.state[ctx->cur] + 6 * n0;
+        KS_CUDA(cudaMemcpyAsync(dst, st.data(), sizeof(double) * 6 * m, cudaMemcpyHostToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.size_m + n0, sz.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.alive[ctx->cur] + n0, al.data(), m, cudaMemcpyHostToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.real_id + n0, nf.rid.data(), sizeof(uint16_t) * m, cudaMemcpyHostToDevice, ctx->stream));
+        const ks::ForceConsts fc = force_consts();
+        for (const NewFragments::Span& sp : nf.spans) {
+            if (sp.remaining_s <= 0 || sp.count == 0) continue;
+            ks::MoonStage ms[3];
+            ks::moon_stages_from(sp.jd0, sp.remaining_s, ms);
+            ks::launch_advance_rows(fc, sp.remaining_s, ms, b.state[ctx->cur], b.alive[ctx->cur], sp.first, sp.count,
+                                    ctx->stream);
+        }
+        KS_CUDA(cudaGetLastError());
+    }
+    for (int64_t idx : nf.killed) KS_CUDA(cudaMemsetAsync(b.alive[ctx->cur] + idx, 0, 1, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ks_ctx::Breakup& k = ctx->bk;
+    for (int64_t q = 0; q < m; ++q) {
+        const ks::SbmFragment& f = nf.rows[static_cast<size_t>(q)];
+        k.size_m.push_back(f.size_m);
+        k.mass_kg.push_back(f.mass_kg);
+        k.area_to_mass.push_back(f.area_to_mass);
+        k.event.push_back(nf.event[static_cast<size_t>(q)]);
+        k.rid.push_back(nf.rid[static_cast<size_t>(q)]);
+    }
+    ctx->n = n0 + m;
+    return seed_speculation(ctx);
+}
+
+// Fragments the collisions of the step that started at t0 (src/core/breakup.cpp:316-338):
+// in (t, i, j) order, skipping pairs with a parent destroyed earlier in the
+// step; parents are interpolated to the collision instant.
+int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_conjunction>& hits) {
+    int rc = ensure_mirrors(ctx);
+    if (rc) return rc;
+    ensure_streams(ctx);
+    ks_ctx::Breakup& k = ctx->bk;
+    const double dt = ctx->dt;
+    const double* before = ctx->b.state[ctx->cur ^ 1];
+    const double* after = ctx->b.state[ctx->cur];
+    std::set<int64_t> dead;
+    NewFragments nf;
+    for (const ks_conjunction& c : hits) {
+        if (dead.count(c.i) || dead.count(c.j)) continue;
+        double rows[4][6];
+        KS_CUDA(cudaMemcpyAsync(rows[0], before + 6 * static_cast<int64_t>(c.i), 48, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(rows[1], after + 6 * static_cast<int64_t>(c.i), 48, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(rows[2], before + 6 * static_cast<int64_t>(c.j), 48, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(rows[3], after + 6 * static_cast<int64_t>(c.j), 48, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        const double s = (c.t - t0) / dt;
+        auto parent = [&](int64_t idx, const double* b0, const double* b1) {
+            ks::SbmParent p;
+            p.index = idx;
+            ks::interpolate_state(b0, b1, dt, s, p.s);
+            p.mass_kg = ks::sbm_mass_or_default(k.mass_kg[static_cast<size_t>(idx)]);
+            p.size_m = k.size_m[static_cast<size_t>(idx)];
+            return p;
+        };
+        const ks::SbmParent pa = parent(c.i, rows[0], rows[1]), pb = parent(c.j, rows[2], rows[3]);
+        const bool a_heavier = pa.mass_kg >= pb.mass_kg;
+        const ks::SbmParent& tgt = a_heavier ? pa : pb;
+        const ks::SbmParent& prj = a_heavier ? pb : pa;
+        const int r = k.rid[static_cast<size_t>(c.i)];
+        ks_breakup_event ev{};
+        ev.step = step;
+        ev.id = k.next_event[static_cast<size_t>(r)]++;
+        ev.realisation = r;
+        ev.target = tgt.index;
+        ev.projectile = prj.index;
+        ev.first_fragment = ctx->n + static_cast<int64_t>(nf.rows.size());
+        ks::SbmOutcome oc;
+        ks::sbm_fragment(k.rng[static_cast<size_t>(r)], k.params, tgt, prj, c.t, ev, nf.rows, oc);
+        if (oc.kill_projectile) { dead.insert(prj.index); nf.killed.push_back(prj.index); }
+        if (oc.kill_target) { dead.insert(tgt.index); nf.killed.push_back(tgt.index); }
+        if (oc.reduce_target) k.mass_kg[static_cast<size_t>(tgt.index)] = oc.target_mass_after;
+        nf.spans.push_back({ev.first_fragment, ev.fragments, t0 + dt - c.t, ctx->epoch_jd + c.t / 86400.0});
+        nf.rid.resize(nf.rows.size(), static_cast<uint16_t>(r));
+        nf.event.resize(nf.rows.size(), ev.id);
+        k.out.push_back(ev);
+    }
+    return commit_fragments(ctx, nf);
 }
 
 }  // namespace
@@ -559,6 +822,7 @@ int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double
     ctx->realisations = 1;
     ctx->rbits = 0;
     ctx->offsets.assign({0, n});
+    reset_breakup_run(ctx);
     int rc = ensure_objects(ctx, n);
     if (rc) return rc;
     ctx->n = n;
@@ -594,6 +858,7 @@ int ks_set_population_batch(ks_ctx* ctx, int32_t realisations, const int64_t* of
     ctx->realisations = realisations;
     ctx->rbits = rbits;
     ctx->offsets.assign(offsets, offsets + realisations + 1);
+    reset_breakup_run(ctx);
     ctx->n = n;
     ctx->cur = 0;
     drop_graphs(ctx);
@@ -748,12 +1013,12 @@ int ks_run(ks_ctx* ctx, int64_t steps) {
     const int chunk = ctx->steps_per_graph > 0 ? ctx->steps_per_graph : 64;
     int rc = ensure_chunk(ctx, chunk);
     if (rc) return rc;
-    int64_t left = steps;
-    while (left > 0) {
-        const int k = static_cast<int>(std::min<int64_t>(left, chunk));
+    const int64_t end = ctx->steps_done + steps;
+    while (ctx->steps_done < end) {
+        // A chunk may end early, at a step that holds a collision to fragment.
+        const int k = static_cast<int>(std::min<int64_t>(end - ctx->steps_done, chunk));
         rc = run_chunk(ctx, k);
         if (rc) return rc;
-        left -= k;
     }
     return KS_OK;
 }
@@ -786,6 +1051,129 @@ int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* co
     return KS_OK;
 }
 
+int ks_set_breakup(ks_ctx* ctx, int on, double lc_m, double catastrophic_j_per_g, uint64_t seed) {
+    if (!ctx || !(lc_m > 0.0) || !(catastrophic_j_per_g > 0.0)) return fail(ctx, KS_ERR_ARG, "ks_set_breakup: bad arguments");
+    ctx->bk.on = on != 0;
+    ctx->bk.params.lc_m = lc_m;
+    ctx->bk.params.catastrophic_j_per_g = catastrophic_j_per_g;
+    ctx->bk.seed = seed;
+    ctx->bk.rng.clear();
+    ctx->bk.next_event.clear();
+    return KS_OK;
+}
+
+int ks_set_masses(ks_ctx* ctx, int64_t n, const double* mass_kg) {
+    if (!ctx || !ctx->has_pop || n != ctx->n || (n > 0 && !mass_kg))
+        return fail(ctx, KS_ERR_ARG, "ks_set_masses: needs one mass per object of the population");
+    cudaSetDevice(ctx->device);
+    const int rc = ensure_mirrors(ctx);
+    if (rc) return rc;
+    std::copy(mass_kg, mass_kg + n, ctx->bk.mass_kg.begin());
+    return KS_OK;
+}
+
+int ks_impact(ks_ctx* ctx, int64_t target, double projectile_mass_kg, double v_rel_km_s) {
+    if (!ctx || !ctx->has_pop || target < 0 || target >= ctx->n || !(projectile_mass_kg > 0.0) || !(v_rel_km_s >= 0.0))
+        return fail(ctx, KS_ERR_ARG, "ks_impact: bad arguments");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_mirrors(ctx);
+    if (rc) return rc;
+    ensure_streams(ctx);
+    ks_ctx::Breakup& k = ctx->bk;
+    double s[6];
+    KS_CUDA(cudaMemcpyAsync(s, ctx->b.state[ctx->cur] + 6 * target, 48, cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int r = k.rid[static_cast<size_t>(target)];
+    ks::SbmParent tgt, prj;
+    ks::sbm_impact_parents(k.rng[static_cast<size_t>(r)], target, s, k.mass_kg[static_cast<size_t>(target)],
+                           k.size_m[static_cast<size_t>(target)], projectile_mass_kg, v_rel_km_s, tgt, prj);
+    ks_breakup_event ev{};
+    ev.step = ctx->steps_done;
+    ev.id = k.next_event[static_cast<size_t>(r)]++;
+    ev.realisation = r;
+    ev.target = tgt.index;
+    ev.projectile = prj.index;
+    ev.first_fragment = ctx->n;
+    NewFragments nf;
+    ks::SbmOutcome oc;
+    ks::sbm_fragment(k.rng[static_cast<size_t>(r)], k.params, tgt, prj, ctx->t, ev, nf.rows, oc);
+    if (oc.kill_projectile) nf.killed.push_back(prj.index);
+    if (oc.kill_target) nf.killed.push_back(tgt.index);
+    if (oc.reduce_target) k.mass_kg[static_cast<size_t>(tgt.index)] = oc.target_mass_after;
+    nf.spans.push_back({ev.first_fragment, ev.fragments, 0.0, ctx->epoch_jd + ctx->t / 86400.0});
+    nf.rid.assign(nf.rows.size(), static_cast<uint16_t>(r));
+    nf.event.assign(nf.rows.size(), ev.id);
+    k.out.push_back(ev);
+    return commit_fragments(ctx, nf);
+}
+
+int64_t ks_sbm_impact(uint64_t seed, double lc_m, double catastrophic_j_per_g, const double* state,
+                      double target_mass_kg, double target_size_m, double projectile_mass_kg, double v_rel_km_s,
+                      double t, ks_breakup_event* event, double* frag_states, double* frag_size, double* frag_mass,
+                      double* frag_area_to_mass, int64_t cap, double* target_after) {
+    if (!state || !event || cap < 0 || !(lc_m > 0.0) || !(projectile_mass_kg > 0.0)) return -1;
+    ks::SbmRng rng(seed);
+    ks::SbmParams p;
+    p.lc_m = lc_m;
+    p.catastrophic_j_per_g = catastrophic_j_per_g;
+    ks::SbmParent tgt, prj;
+    ks::sbm_impact_parents(rng, 0, state, target_mass_kg, target_size_m, projectile_mass_kg, v_rel_km_s, tgt, prj);
+    ks_breakup_event ev{};
+    ev.target = tgt.index;
+    ev.projectile = prj.index;
+    ev.first_fragment = 1;
+    std::vector<ks::SbmFragment> rows;
+    ks::SbmOutcome oc;
+    ks::sbm_fragment(rng, p, tgt, prj, t, ev, rows, oc);
+    *event = ev;
+    const int64_t m = static_cast<int64_t>(rows.size());
+    for (int64_t k = 0; k < m && k < cap; ++k) {
+        const ks::SbmFragment& f = rows[static_cast<size_t>(k)];
+        if (frag_states) std::copy(f.s, f.s + 6, frag_states + 6 * k);
+        if (frag_size) frag_size[k] = f.size_m;
+        if (frag_mass) frag_mass[k] = f.mass_kg;
+        if (frag_area_to_mass) frag_area_to_mass[k] = f.area_to_mass;
+    }
+    if (target_after) {
+        const bool killed = (oc.kill_target && tgt.index == 0) || (oc.kill_projectile && prj.index == 0);
+        target_after[0] = killed ? 0.0 : 1.0;
+        target_after[1] = oc.reduce_target && tgt.index == 0 ? oc.target_mass_after : target_mass_kg;
+    }
+    return m;
+}
+
+int ks_take_breakups(ks_ctx* ctx, ks_breakup_event* out, int64_t cap, int64_t* count) {
+    if (!ctx || !count || cap < 0) return KS_ERR_ARG;
+    std::vector<ks_breakup_event>& v = ctx->bk.out;
+    if (!out) {
+        *count = static_cast<int64_t>(v.size());
+        return KS_OK;
+    }
+    const int64_t m = std::min(static_cast<int64_t>(v.size()), cap);
+    std::memcpy(out, v.data(), sizeof(ks_breakup_event) * m);
+    v.erase(v.begin(), v.begin() + m);
+    *count = m;
+    return KS_OK;
+}
+
+int ks_get_objects(ks_ctx* ctx, int64_t n, double* size_m, double* mass_kg, double* area_to_mass, int32_t* event,
+                   int32_t* realisation) {
+    if (!ctx || !ctx->has_pop || n != ctx->n) return fail(ctx, KS_ERR_ARG, "ks_get_objects: n must be the population size");
+    cudaSetDevice(ctx->device);
+    const int rc = ensure_mirrors(ctx);
+    if (rc) return rc;
+    const ks_ctx::Breakup& k = ctx->bk;
+    for (int64_t i = 0; i < n; ++i) {
+        const size_t q = static_cast<size_t>(i);
+        if (size_m) size_m[i] = k.size_m[q];
+        if (mass_kg) mass_kg[i] = k.mass_kg[q];
+        if (area_to_mass) area_to_mass[i] = k.area_to_mass[q];
+        if (event) event[i] = k.event[q];
+        if (realisation) realisation[i] = k.rid[q];
+    }
+    return KS_OK;
+}
+
 int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after, const uint8_t* alive_after,
               const double* size_m, double t0, double dt, ks_conjunction* out, int64_t cap, int64_t* count,
               ks_step_stats* stats) {
@@ -801,6 +1189,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
     ctx->realisations = 1;
     ctx->rbits = 0;
     ctx->offsets.assign({0, n});
+    reset_breakup_run(ctx);
     rc = upload_population(ctx, n, before, size_m, nullptr, 0);
     if (!rc) rc = upload_population(ctx, n, after, nullptr, alive_after, 1);
     if (rc) return rc;

@@ -165,6 +165,9 @@ void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int 
                       cudaStream_t stream);
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_screen_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+// One RK4 step of dt over rows [first, first + count) (fragments born inside a step).
+void launch_advance_rows(const ForceConsts& fc, double dt, const MoonStage m[3], double* state, uint8_t* alive,
+                         int64_t first, int count, cudaStream_t stream);
 void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);

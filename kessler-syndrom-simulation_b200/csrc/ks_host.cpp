@@ -67,21 +67,29 @@ void moon_position(double jd, double out[3]) {
     out[2] = ye * std::sin(eps) + ze * std::cos(eps);
 }
 
+void moon_stage_at(double jd, MoonStage& out) {
+    double p[3];
+    moon_position(jd, p);
+    const double mn = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    const double s = kMuMoon / (mn * mn * mn);
+    out.mx = p[0];
+    out.my = p[1];
+    out.mz = p[2];
+    out.ix = p[0] * s;
+    out.iy = p[1] * s;
+    out.iz = p[2] * s;
+}
+
 void moon_stages(double epoch_jd, double t, double dt, MoonStage out[3]) {
     const double jd[3] = {epoch_jd + t / 86400.0, epoch_jd + (t + dt / 2) / 86400.0,
                           epoch_jd + (t + dt) / 86400.0};
-    for (int k = 0; k < 3; ++k) {
-        double p[3];
-        moon_position(jd[k], p);
-        const double mn = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
-        const double s = kMuMoon / (mn * mn * mn);
-        out[k].mx = p[0];
-        out[k].my = p[1];
-        out[k].mz = p[2];
-        out[k].ix = p[0] * s;
-        out[k].iy = p[1] * s;
-        out[k].iz = p[2] * s;
-    }
+    for (int k = 0; k < 3; ++k) moon_stage_at(jd[k], out[k]);
+}
+
+void moon_stages_from(double jd0, double span_s, MoonStage out[3]) {
+    moon_stage_at(jd0, out[0]);
+    moon_stage_at(jd0 + span_s / 2 / 86400.0, out[1]);
+    moon_stage_at(jd0 + span_s / 86400.0, out[2]);
 }
 
 // ---------------------------------------------------------------------------

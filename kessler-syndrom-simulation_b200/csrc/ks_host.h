@@ -29,4 +29,11 @@ void moon_position(double jd, double out[3]);
 // each with its indirect term rm * (MU_MOON / |rm|^3) (src/core/orbital.cpp:103).
 void moon_stages(double epoch_jd, double t, double dt, MoonStage out[3]);
 
+// One lunar stage at Julian date jd (position and indirect term).
+void moon_stage_at(double jd, MoonStage& out);
+
+// The stages of a sub-step of span_s seconds from Julian date jd0, with the
+// Julian dates formed as src/core/breakup.cpp:211-214 forms them for fragments.
+void moon_stages_from(double jd0, double span_s, MoonStage out[3]);
+
 }  // namespace ks

@@ -342,6 +342,23 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
     flush_spec(acc, a.ctrl, a.ctrl_next, a.screening != 0);
 }
 
+// One RK4 step of dt over rows [first, first + count) with given lunar stages,
+// for fragments born inside a step: their state is carried from the event to
+// the end of the step (src/core/breakup.cpp:304-306), and a fragment that ends
+// below the surface is not alive.
+__global__ void __launch_bounds__(kPropBlock) k_advance_rows(ForceConsts fc, double dt, MoonStage m0, MoonStage m1,
+                                                              MoonStage m2, double* __restrict__ state,
+                                                              uint8_t* __restrict__ alive, int64_t first, int count) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t i = first + k;
+    double s[6];
+    ld6(state, i, s);
+    rk4_exact(fc, dt, m0, m1, m2, s);
+    st6(state, i, s);
+    alive[i] = xsqrt(xdot3(s[0], s[1], s[2])) >= fc.r_earth ? 1 : 0;
+}
+
 // Split-precision propagation (FP32 J2 and lunar terms, FP64 state and central
 // term); keys and speculation exactly as in k_propagate_exact.
 __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, const double* __restrict__ in,
@@ -1510,6 +1527,13 @@ void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t st
     }
     k_propagate_exact<<<grid_for_block(a.n, 3, kPropBlock), kPropBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
                                                                 b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
+}
+
+void launch_advance_rows(const ForceConsts& fc, double dt, const MoonStage m[3], double* state, uint8_t* alive,
+                         int64_t first, int count, cudaStream_t stream) {
+    if (count <= 0) return;
+    k_advance_rows<<<(count + kPropBlock - 1) / kPropBlock, kPropBlock, 0, stream>>>(fc, dt, m[0], m[1], m[2], state,
+                                                                                     alive, first, count);
 }
 
 void launch_screen_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {

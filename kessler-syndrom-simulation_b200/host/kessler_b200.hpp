@@ -245,6 +245,34 @@ public:
         ks_get_clock(ctx_.get(), &t, &k);
         return t;
     }
+    int64_t size() const { return ks_population_size(ctx_.get()); }
+
+    // Fragmentation (BreakupConfig / Fragmentation, src/core/breakup.hpp:75-153).
+    void set_breakup(bool on, double lc_m = 0.10, double catastrophic_j_per_g = 40.0, uint64_t seed = 1) {
+        check(ctx_.get(), ks_set_breakup(ctx_.get(), on ? 1 : 0, lc_m, catastrophic_j_per_g, seed), "ks_set_breakup");
+    }
+    void set_masses(const std::vector<double>& mass_kg) {
+        check(ctx_.get(), ks_set_masses(ctx_.get(), static_cast<int64_t>(mass_kg.size()), mass_kg.data()),
+              "ks_set_masses");
+    }
+    void impact(int64_t target, double projectile_mass_kg, double v_rel_km_s) {
+        check(ctx_.get(), ks_impact(ctx_.get(), target, projectile_mass_kg, v_rel_km_s), "ks_impact");
+    }
+    std::vector<ks_breakup_event> take_breakups() {
+        int64_t n = 0;
+        check(ctx_.get(), ks_take_breakups(ctx_.get(), nullptr, 0, &n), "ks_take_breakups");
+        std::vector<ks_breakup_event> out(static_cast<size_t>(n));
+        if (n) check(ctx_.get(), ks_take_breakups(ctx_.get(), out.data(), n, &n), "ks_take_breakups");
+        out.resize(static_cast<size_t>(n));
+        return out;
+    }
+    // Per-object originating event (-1 for the initial population).
+    std::vector<int32_t> events_of_objects() {
+        const int64_t n = size();
+        std::vector<int32_t> ev(static_cast<size_t>(n));
+        check(ctx_.get(), ks_get_objects(ctx_.get(), n, nullptr, nullptr, nullptr, ev.data(), nullptr), "ks_get_objects");
+        return ev;
+    }
 
 private:
     Context ctx_;

@@ -22,6 +22,12 @@ REF_SO = os.path.join(HERE, "_ref", "libksref.so")
 CONJ_DTYPE = np.dtype(
     [("i", "<i4"), ("j", "<i4"), ("step", "<i8"), ("t", "<f8"), ("miss_km", "<f8"),
      ("v_rel_km_s", "<f8"), ("collision", "<i4"), ("realisation", "<i4")], align=True)
+BREAKUP_DTYPE = np.dtype(
+    [("step", "<i8"), ("t", "<f8"), ("id", "<i4"), ("realisation", "<i4"), ("target", "<i8"), ("projectile", "<i8"),
+     ("catastrophic", "<i4"), ("fragments", "<i4"), ("escaped", "<i4"), ("pad", "<i4"), ("first_fragment", "<i8"),
+     ("v_rel_km_s", "<f8"), ("energy_j_per_g", "<f8"), ("target_mass_kg", "<f8"), ("projectile_mass_kg", "<f8"),
+     ("sbm_mass_kg", "<f8"), ("expected_fragments", "<f8"), ("fragments_mass_kg", "<f8"), ("position", "<f8", (3,))],
+    align=True)
 STATS_DTYPE = np.dtype(
     [("step", "<i8"), ("candidate_pairs", "<i8"), ("refined_pairs", "<i8"), ("co_orbiting", "<i8"),
      ("conjunctions", "<i8"), ("cell_km", "<f8"), ("max_cell_objects", "<i4"), ("alive", "<i4")],
@@ -157,6 +163,62 @@ class Reference(_Checker):
 
     def max_threads(self):
         return self.lib.ksref_max_threads()
+
+    def impact(self, state, mass_kg, size_m, projectile_mass_kg, v_rel_km_s, t=0.0, seed=1, lc_m=0.10,
+               catastrophic_j_per_g=40.0, epoch_jd=2461253.916666667):
+        """Fragmentation::impact on a one-object simulation: (event, states, sizes, masses, a2m, [alive, mass])."""
+        f = self.lib.ksref_impact
+        f.restype = _L
+        st = np.ascontiguousarray(state, dtype=np.float64).reshape(6)
+        ev = np.zeros(1, dtype=BREAKUP_DTYPE)
+        after = np.zeros(2)
+        cap = 1024
+        while True:
+            fs, fz, fm, fa = np.zeros((cap, 6)), np.zeros(cap), np.zeros(cap), np.zeros(cap)
+            m = f(C.c_uint64(seed), _D(lc_m), _D(catastrophic_j_per_g), _p(st), _D(mass_kg), _D(size_m),
+                  _D(projectile_mass_kg), _D(v_rel_km_s), _D(epoch_jd), _D(t), _p(ev), _p(fs), _p(fz), _p(fm),
+                  _p(fa), _L(cap), _p(after))
+            if m <= cap:
+                return ev[0], fs[:m], fz[:m], fm[:m], fa[:m], after
+            cap = int(m)
+
+    def run_breakup(self, states, size_m, mass_kg=None, alive=None, epoch_jd=2461253.916666667, dt=10.0, steps=1,
+                    threshold_km=5.0, radius_scale=1.0, min_vrel_km_s=0.01, threads=0, lc_m=0.10,
+                    catastrophic_j_per_g=40.0, seed=1, impact=None):
+        """The CLI loop with --breakup; impact = (index, mass_kg, v_rel_km_s, step) or None.
+
+        Returns dict: states, alive, size_m, mass_kg, area_to_mass, event, conj, events, stats."""
+        f = self.lib.ksref_run_breakup
+        f.restype = C.c_int
+        st = np.ascontiguousarray(states, dtype=np.float64)
+        n = st.shape[0]
+        al = np.ones(n, np.uint8) if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        sz = np.ascontiguousarray(size_m, dtype=np.float64)
+        ms = np.zeros(n) if mass_kg is None else np.ascontiguousarray(mass_kg, dtype=np.float64)
+        ii, im, iv, istep = impact if impact is not None else (-1, 0.0, 0.0, 0)
+        obj_cap, conj_cap, ev_cap = 2 * n + 1024, 4096, 256
+        while True:
+            out = {"states": np.zeros((obj_cap, 6)), "alive": np.zeros(obj_cap, np.uint8),
+                   "size_m": np.zeros(obj_cap), "mass_kg": np.zeros(obj_cap), "area_to_mass": np.zeros(obj_cap),
+                   "event": np.zeros(obj_cap, np.int32), "conj": np.zeros(conj_cap, dtype=CONJ_DTYPE),
+                   "events": np.zeros(ev_cap, dtype=BREAKUP_DTYPE), "stats": np.zeros(max(steps, 1), STATS_DTYPE)}
+            counts = np.zeros(3, np.int64)
+            rc = f(_L(n), _p(st), _p(al), _p(sz), _p(ms), _D(epoch_jd), _D(dt), _L(steps), _D(threshold_km),
+                   _D(radius_scale), _D(min_vrel_km_s), C.c_int(threads), _D(lc_m), _D(catastrophic_j_per_g),
+                   C.c_uint64(seed), _L(ii), _D(im), _D(iv), _L(istep), _L(obj_cap), _p(out["states"]),
+                   _p(out["alive"]), _p(out["size_m"]), _p(out["mass_kg"]), _p(out["area_to_mass"]),
+                   _p(out["event"]), _p(out["conj"]), _L(conj_cap), _p(out["events"]), _L(ev_cap),
+                   _p(out["stats"]), _p(counts))
+            if rc == 0:
+                m, nc, ne = (int(x) for x in counts)
+                for k in ("states", "alive", "size_m", "mass_kg", "area_to_mass", "event"):
+                    out[k] = out[k][:m]
+                out["conj"] = out["conj"][:nc]
+                out["events"] = out["events"][:ne]
+                out["stats"] = out["stats"][:steps]
+                return out
+            obj_cap, conj_cap, ev_cap = max(obj_cap, int(counts[0])), max(conj_cap, int(counts[1])), \
+                max(ev_cap, int(counts[2]))
 
     def load_catalog(self, path):
         """(states, size_m, ids, epoch_jd) via the reference parser."""

@@ -7,8 +7,10 @@
 // baseline leg load it.
 //
 // It drives the reference exactly the way its CLI step loop does
-// (src/main.cpp:346-407, screening on, no breakup): copy `before`,
-// Screener::begin, Simulation::step, Screener::finish, collect conjunctions.
+// (src/main.cpp:346-407): copy `before`, Screener::begin, Simulation::step,
+// Screener::finish, collect conjunctions, and (ksref_run_breakup) hand them to
+// Fragmentation::apply, with an optional forced impact (Fragmentation::impact)
+// at the start of one step.
 // Object sizes are set directly (Object::size_m) because the catalogue text
 // format only carries radar-cross-section classes (src/core/orbital.cpp:162).
 
@@ -18,6 +20,7 @@
 #include <cstring>
 #include <vector>
 
+#include "core/breakup.hpp"
 #include "core/collision.hpp"
 #include "core/collision_filter.hpp"
 #include "core/orbital.hpp"
@@ -138,6 +141,164 @@ long ksref_screen(long n, const double* before, const double* after, const uint8
                                st.cell_km, st.max_cell_objects, static_cast<int32_t>(alive)};
     }
     return nf;
+}
+
+namespace {
+
+ks_breakup_event to_record(const BreakupEvent& ev, long step, long first_fragment) {
+    ks_breakup_event r{};
+    r.step = step;
+    r.t = ev.t;
+    r.id = ev.id;
+    r.realisation = 0;
+    r.target = ev.target;
+    r.projectile = ev.projectile;
+    r.catastrophic = ev.catastrophic ? 1 : 0;
+    r.fragments = ev.fragments;
+    r.escaped = ev.escaped;
+    r.first_fragment = first_fragment;
+    r.v_rel_km_s = ev.v_rel_km_s;
+    r.energy_j_per_g = ev.energy_j_per_g;
+    r.target_mass_kg = ev.target_mass_kg;
+    r.projectile_mass_kg = ev.projectile_mass_kg;
+    r.sbm_mass_kg = ev.sbm_mass_kg;
+    r.expected_fragments = ev.expected_fragments;
+    r.fragments_mass_kg = ev.fragments_mass_kg;
+    r.position[0] = ev.position.x;
+    r.position[1] = ev.position.y;
+    r.position[2] = ev.position.z;
+    return r;
+}
+
+}  // namespace
+
+// Fragmentation::impact on a one-object simulation at time t. Writes up to cap
+// fragments (birth states, sizes, masses, area-to-mass); returns the number of
+// fragments created. target_after: [alive, mass_kg] of the target afterwards.
+long ksref_impact(uint64_t seed, double lc_m, double catastrophic_j_per_g, const double* state, double mass_kg,
+                  double size_m, double projectile_mass_kg, double v_rel_km_s, double epoch_jd, double t,
+                  ks_breakup_event* event, double* frag_states, double* frag_size, double* frag_mass,
+                  double* frag_a2m, long cap, double* target_after) {
+    Simulation sim;
+    sim.epoch_jd = epoch_jd;
+    sim.t = t;
+    Object o;
+    o.s = State{{state[0], state[1], state[2]}, {state[3], state[4], state[5]}};
+    o.mass_kg = mass_kg;
+    o.size_m = size_m;
+    sim.objects.push_back(o);
+    BreakupConfig cfg;
+    cfg.lc_m = lc_m;
+    cfg.catastrophic_j_per_g = catastrophic_j_per_g;
+    cfg.seed = seed;
+    Fragmentation frag(cfg);
+    const BreakupEvent ev = frag.impact(sim, 0, projectile_mass_kg, v_rel_km_s);
+    *event = to_record(ev, 0, 1);
+    const long m = static_cast<long>(sim.objects.size()) - 1;
+    for (long k = 0; k < m && k < cap; ++k) {
+        const Object& f = sim.objects[static_cast<size_t>(k + 1)];
+        double* s = frag_states + 6 * k;
+        s[0] = f.s.r.x; s[1] = f.s.r.y; s[2] = f.s.r.z;
+        s[3] = f.s.v.x; s[4] = f.s.v.y; s[5] = f.s.v.z;
+        frag_size[k] = f.size_m;
+        frag_mass[k] = f.mass_kg;
+        frag_a2m[k] = f.area_to_mass;
+    }
+    target_after[0] = sim.objects[0].alive ? 1.0 : 0.0;
+    target_after[1] = sim.objects[0].mass_kg;
+    return m;
+}
+
+// The CLI step loop with --breakup (src/main.cpp:343-407): screening every
+// step, Fragmentation::apply on its conjunctions, and a forced impact on object
+// impact_index (if >= 0) at the start of step impact_step.
+//   in:  n objects (states n x 6, alive, size_m, mass_kg; 0 = unknown mass)
+//   out: up to obj_cap objects (initial ones then fragments): states, alive,
+//        size, mass, area-to-mass, originating event; conjunctions, events,
+//        per-step counters (steps entries).
+// counts: [objects, conjunctions, events]. Returns 0, or 1 if a capacity was
+// too small (counts then hold the sizes needed).
+int ksref_run_breakup(long n, const double* states, const uint8_t* alive, const double* size_m, const double* mass_kg,
+                      double epoch_jd, double dt, long steps, double threshold_km, double radius_scale,
+                      double min_encounter_speed_km_s, int threads, double lc_m, double catastrophic_j_per_g,
+                      uint64_t seed, long impact_index, double impact_mass_kg, double impact_vrel_km_s,
+                      long impact_step, long obj_cap, double* out_states, uint8_t* out_alive, double* out_size,
+                      double* out_mass, double* out_a2m, int32_t* out_event, ks_conjunction* conj, long conj_cap,
+                      ks_breakup_event* events, long ev_cap, ks_step_stats* stats, long* counts) {
+    set_threads(threads);
+    Simulation sim;
+    sim.objects.resize(n);
+    for (long i = 0; i < n; ++i) {
+        const double* s = states + 6 * i;
+        Object& o = sim.objects[i];
+        o.id = static_cast<int>(i);
+        o.s = State{{s[0], s[1], s[2]}, {s[3], s[4], s[5]}};
+        o.alive = alive[i] != 0;
+        o.size_m = size_m[i];
+        o.mass_kg = mass_kg ? mass_kg[i] : 0.0;
+    }
+    sim.epoch_jd = epoch_jd;
+    sim.dt = dt;
+    ScreeningConfig cfg;
+    cfg.threshold_km = threshold_km;
+    cfg.radius_scale = radius_scale;
+    cfg.min_encounter_speed_km_s = min_encounter_speed_km_s;
+    Screener screener(cfg);
+    BreakupConfig bcfg;
+    bcfg.lc_m = lc_m;
+    bcfg.catastrophic_j_per_g = catastrophic_j_per_g;
+    bcfg.seed = seed;
+    Fragmentation frag(bcfg);
+    std::vector<State> before;
+    std::vector<ks_breakup_event> evs;
+    long n_conj = 0, next_first = n;
+    auto record = [&](const BreakupEvent& ev, long step) {
+        evs.push_back(to_record(ev, step, next_first));
+        next_first += ev.fragments;
+    };
+    for (long step = 0; step < steps; ++step) {
+        if (impact_index >= 0 && step == impact_step)
+            record(frag.impact(sim, static_cast<int>(impact_index), impact_mass_kg, impact_vrel_km_s), step);
+        const int nobj = static_cast<int>(sim.objects.size());
+        before.resize(nobj);
+        for (int i = 0; i < nobj; ++i) before[i] = sim.objects[i].s;
+        screener.begin(before, sim.objects, sim.dt);
+        const double t0 = sim.t;
+        sim.step();
+        ScreeningStats st;
+        std::vector<Conjunction> found = screener.finish(before, sim.objects, t0, sim.dt, &st);
+        for (const Conjunction& c : found) {
+            if (n_conj < conj_cap)
+                conj[n_conj] = ks_conjunction{c.i, c.j, step, c.t, c.miss_km, c.v_rel_km_s, c.collision ? 1 : 0, 0};
+            ++n_conj;
+        }
+        if (stats) {
+            long alive_n = 0;
+            for (const Object& o : sim.objects) alive_n += o.alive ? 1 : 0;
+            stats[step] = ks_step_stats{step, st.candidate_pairs, st.refined_pairs, st.co_orbiting,
+                                        static_cast<int64_t>(found.size()), st.cell_km, st.max_cell_objects,
+                                        static_cast<int32_t>(alive_n)};
+        }
+        for (const BreakupEvent& ev : frag.apply(sim, before, t0, sim.dt, found)) record(ev, step);
+    }
+    const long m = static_cast<long>(sim.objects.size());
+    counts[0] = m;
+    counts[1] = n_conj;
+    counts[2] = static_cast<long>(evs.size());
+    if (m > obj_cap || n_conj > conj_cap || counts[2] > ev_cap) return 1;
+    for (long i = 0; i < m; ++i) {
+        const Object& o = sim.objects[static_cast<size_t>(i)];
+        double* s = out_states + 6 * i;
+        s[0] = o.s.r.x; s[1] = o.s.r.y; s[2] = o.s.r.z;
+        s[3] = o.s.v.x; s[4] = o.s.v.y; s[5] = o.s.v.z;
+        out_alive[i] = o.alive ? 1 : 0;
+        out_size[i] = o.size_m;
+        out_mass[i] = o.mass_kg;
+        out_a2m[i] = o.area_to_mass;
+        out_event[i] = o.event;
+    }
+    std::copy(evs.begin(), evs.end(), events);
+    return 0;
 }
 
 // The CLI step loop (src/main.cpp:346-407), screening optional, no breakup.

@@ -22,6 +22,12 @@ Fixtures:
                      pipe format (with planted encounters), and
   cli_ref_*.csv      the conjunctions.csv / final_state.csv the reference CLI
                      (oracle/_ref/kessler_sim) writes for it over 15 minutes
+  run_breakup.npz    the CLI loop with --breakup through the reference's
+                     Fragmentation (planted collisions, a forced impact),
+                     every object's final state and properties, events
+  cli_breakup_*      a 2 000-object catalogue of mixed object types and the
+                     four files the reference CLI writes for it with --breakup
+                     and --impact over 1.2 h
 """
 import importlib
 import json
@@ -106,6 +112,27 @@ def save_run(name, st, sz, al, steps, dt=10.0, thr=5.0, rscale=1.0, vmin=0.01):
                         final_states=fs, final_alive=fa, conj=conj, stats=stats)
     print(name, "conj", len(conj), "candidates/step", int(stats["candidate_pairs"].mean()),
           "dead", int((fa == 0).sum()))
+
+
+def breakup_run(name="run_breakup.npz", steps=40, rscale=300.0, lc=0.1, seed=7):
+    """The CLI loop with --breakup: planted encounters that end in collisions,
+    a forced impact at step 3, the fragments screened from the next step on."""
+    st, sz, al = population(4242, 1500, 2500, 3, 1800.0)
+    plant_encounters(st, 100, 16, steps, 10.0, 17)
+    rng = np.random.default_rng(9)
+    mass = np.where(rng.random(len(sz)) < 0.5, 0.0, rng.uniform(1.0, 2000.0, len(sz)))
+    mass[116], mass[117] = 0.5, 2000.0  # a cratering (non-catastrophic) collision
+    impact = (50, 300.0, 10.0, 3)
+    ref = checkers.Reference()
+    out = ref.run_breakup(st, sz, mass, al, epoch_jd=EPOCH, dt=10.0, steps=steps, threshold_km=5.0,
+                          radius_scale=rscale, min_vrel_km_s=0.01, threads=8, lc_m=lc, seed=seed, impact=impact)
+    np.savez_compressed(os.path.join(HERE, name), states=st, size_m=sz, alive=al, mass_kg=mass, epoch_jd=EPOCH,
+                        dt=10.0, steps=steps, threshold_km=5.0, radius_scale=rscale, min_vrel_km_s=0.01, lc_m=lc,
+                        seed=seed, impact=np.array(impact), **{"out_" + k: v for k, v in out.items()})
+    ev = out["events"]
+    print(name, "objects", len(out["size_m"]), "events", len(ev), "catastrophic", int(ev["catastrophic"].sum()),
+          "fragments", int(ev["fragments"].sum()), "conj", len(out["conj"]), "collisions",
+          int(out["conj"]["collision"].sum()))
 
 
 def screen_cases():
@@ -211,6 +238,37 @@ def cli_golden():
     print("cli golden: conjunctions", n)
 
 
+CLI_BREAKUP_ARGS = ["1.2", "10", "--breakup", "--radius-scale", "500", "--lc", "0.1", "--seed", "3",
+                    "--impact", "100051", "--impact-mass", "500", "--impact-vrel", "10", "--impact-at", "0.05"]
+
+
+def cli_breakup_golden():
+    """The reference CLI with --breakup and --impact on a catalogue of mixed
+    object types (catalogue masses from the default mass table)."""
+    ks = importlib.import_module("kessler-syndrom-simulation_b200")
+    cio = importlib.import_module("kessler-syndrom-simulation_b200.catalog_io")
+    st, sz, al = ks.generate_population(77, 1500, 2000, 2, 3600.0)
+    plant_encounters(st, 100, 30, 432, 10.0, 29)
+    rng = np.random.default_rng(31)
+    rcs = cio.rcs_class_for_size(sz)
+    rcs[100:160] = np.where(rng.random(60) < 0.5, "LARGE", "MEDIUM")
+    types = np.where(rng.random(len(sz)) < 0.3, "PAYLOAD", np.where(rng.random(len(sz)) < 0.15, "ROCKET BODY",
+                                                                     "DEBRIS"))
+    types[50] = "PAYLOAD"
+    rcs[50] = "LARGE"
+    cat = os.path.join(HERE, "cli_breakup_catalog.txt")
+    cio.write_catalog(cat, st, ids=np.arange(100001, 100001 + len(st)), rcs=rcs, types=types)
+    exe = os.path.join(ROOT, "oracle", "_ref", "kessler_sim")
+    with tempfile.TemporaryDirectory() as tmp:
+        out = subprocess.run([exe, cat] + CLI_BREAKUP_ARGS + ["--threads", "8"], cwd=tmp, capture_output=True,
+                             text=True, check=True)
+        for name in ("conjunctions.csv", "final_state.csv", "breakups.csv", "population.csv"):
+            shutil.copy(os.path.join(tmp, "output", name), os.path.join(HERE, "cli_breakup_ref_" + name))
+    print("cli breakup golden:", open(os.path.join(HERE, "cli_breakup_ref_breakups.csv")).read().count("\n") - 1,
+          "events,", open(os.path.join(HERE, "cli_breakup_ref_conjunctions.csv")).read().count("\n") - 1,
+          "conjunctions")
+
+
 def main():
     checkers.build(ref=True)
     st, sz, al = population(20260801, 1500, 3000, 3, 7200.0)
@@ -222,6 +280,8 @@ def main():
     save_run("run_dense.npz", st, sz, al, 12)
     screen_cases()
     cli_golden()
+    cli_breakup_golden()
+    breakup_run()
     if os.path.exists(CATALOG):
         catalogue_kat()
 

@@ -60,3 +60,23 @@ def test_cli_split_precision_finds_the_same_encounters(tmp_path):
     assert [(g[1], g[2]) for g in got] == [(w[1], w[2]) for w in want]
     for g, w in zip(got, want):
         assert abs(float(g[5]) - float(w[5])) < 1e-4  # miss distance within 10 cm after 15 minutes
+
+
+BREAKUP_ARGS = ["1.2", "10", "--breakup", "--radius-scale", "500", "--lc", "0.1", "--seed", "3",
+                "--impact", "100051", "--impact-mass", "500", "--impact-vrel", "10", "--impact-at", "0.05"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spg", ["32", "5"])
+def test_cli_breakup_matches_reference_cli_files(tmp_path, spg):
+    # tests/golden/cli_breakup_ref_*.csv: the reference CLI with --breakup and a
+    # forced impact; collisions fragment objects (fragments of fragments too).
+    exe = os.path.join(PKG, "ks_sim")
+    out = subprocess.run([exe, golden_path("cli_breakup_catalog.txt")] + BREAKUP_ARGS +
+                         ["--steps-per-graph", spg, "--out", str(tmp_path)], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr
+    for name in ("breakups.csv", "population.csv", "conjunctions.csv", "final_state.csv"):
+        got = open(tmp_path / name).read()
+        want = open(golden_path("cli_breakup_ref_" + name)).read()
+        assert got == want, name
