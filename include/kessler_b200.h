@@ -90,6 +90,46 @@ int ks_set_precision(ks_ctx* ctx, int precision);
 int ks_set_steps_per_graph(ks_ctx* ctx, int steps_per_graph);
 /* Per-phase CUDA-event timing of every step (adds event records to each step). */
 int ks_set_profiling(ks_ctx* ctx, int enabled);
+/* Upper bounds (0 = none) on the survivor-pair and conjunction buffers, which
+ * otherwise grow on demand (the reference grows its pair list the same way,
+ * src/core/collision_gpu.cu:424-437). A step that needs more replays, then
+ * fails with KS_ERR_OVERFLOW. */
+int ks_set_buffer_limits(ks_ctx* ctx, int64_t survivor_pairs, int64_t conjunctions);
+/* Writes `bytes` of scratch before every step (0 = off), so that each step
+ * starts with a cold L2; for measurements. */
+int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
+
+/* Launch-shape knobs (no counterpart in the reference): "pair_variant" (0: two
+ * columns per lane, 1: one), "pair_blocks_per_sm" (0 = default),
+ * "subcell_bits" (0..3: Morton order of objects inside a cell), "box_min_rows"
+ * (split pair kernel: skip tiles whose row and column blocks are provably
+ * apart, for tiles of at least this many rows; 0 = off), "cell_scale_permille"
+ * (1000..4000: grid cell edge = the reference's edge x value/1000),
+ * "prop_block" (32..128, threads per block of the propagation kernels).
+ * Conjunctions, refined and co-orbiting counts and states never change;
+ * candidate_pairs and cell_km change with the cell edge. */
+int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value);
+
+/* Configuration chosen by ks_autotune. */
+typedef struct ks_tuning_choice {
+    int32_t steps_per_graph;
+    int32_t pair_variant, pair_blocks_per_sm, subcell_bits, box_min_rows;
+    int32_t cell_scale_permille;
+    int32_t prop_block;
+    int32_t trials;              /* configurations timed */
+    double ms_per_step_start;    /* device time per step of the starting configuration */
+    double ms_per_step_best;     /* ... and of the chosen one */
+} ks_tuning_choice;
+
+/* Autotuner (no counterpart in the reference, whose OpenMP loop has no launch
+ * shape to choose): times short runs of the resident population from a
+ * snapshot under candidate steps-per-graph, pair-kernel shapes (variant and
+ * resident blocks per SM), sub-cell order, box pruning, grid cell edge and
+ * propagation block size, by coordinate descent, and keeps the fastest. Each
+ * trial runs at least trial_steps steps (and two graphs). The population,
+ * clock, conjunctions and counters are restored afterwards, so the
+ * simulation's results are those of an untuned run; only speed changes. */
+int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out);
 
 /* --- run: Simulation::advance (src/core/orbital.hpp:154) with, per step, the
  *     CLI's Screener::begin / Simulation::step / Screener::finish sequence

@@ -15,7 +15,7 @@ import ctypes as C
 import numpy as np
 
 from ._abi import (BREAKUP_DTYPE, CONJ_DTYPE, PRECISION_FP64, PRECISION_SPLIT, STATS_DTYPE, STATUS_NAMES, Timing,
-                   load_library, ptr)
+                   TuningChoice, load_library, ptr)
 
 __all__ = ["Engine", "KsError", "BREAKUP_DTYPE", "CONJ_DTYPE", "STATS_DTYPE", "PRECISION_FP64", "PRECISION_SPLIT",
            "moon_position", "generate_population", "sbm_impact", "load_library", "DEFAULT_EPOCH_JD"]
@@ -100,6 +100,9 @@ class Engine:
         al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
         self._check(self._lib.ks_set_population_batch(self._h, len(off) - 1, ptr(off), ptr(st), ptr(sz), ptr(al)))
 
+    def population_size(self):
+        return int(self._lib.ks_population_size(self._h))
+
     def get_population(self):
         n = self._lib.ks_population_size(self._h)
         st = np.empty((n, 6), dtype=np.float64)
@@ -157,6 +160,14 @@ class Engine:
         if cnt.value:
             self._check(self._lib.ks_take_step_stats(self._h, ptr(out), cnt.value, C.byref(cnt)))
         return out[: cnt.value]
+
+    def autotune(self, trial_steps=16):
+        """Times candidate launch configurations on the resident population and keeps the fastest.
+
+        The simulation is left exactly where it was; returns the chosen configuration."""
+        ch = TuningChoice()
+        self._check(self._lib.ks_autotune(self._h, int(trial_steps), C.byref(ch)))
+        return {name: getattr(ch, name) for name, _ in TuningChoice._fields_}
 
     # --- fragmentation (NASA SBM) ---
     def set_breakup(self, on=True, lc_m=0.10, catastrophic_j_per_g=40.0, seed=1):

@@ -34,6 +34,13 @@ class Timing(C.Structure):
                 ("candidate_pairs", C.c_int64), ("exact_filter_pairs", C.c_int64), ("refined_pairs", C.c_int64)]
 
 
+class TuningChoice(C.Structure):
+    _fields_ = [("steps_per_graph", C.c_int32), ("pair_variant", C.c_int32), ("pair_blocks_per_sm", C.c_int32),
+                ("subcell_bits", C.c_int32), ("box_min_rows", C.c_int32), ("cell_scale_permille", C.c_int32),
+                ("prop_block", C.c_int32), ("trials", C.c_int32), ("ms_per_step_start", C.c_double),
+                ("ms_per_step_best", C.c_double)]
+
+
 KS_OK = 0
 STATUS_NAMES = {0: "KS_OK", 1: "KS_ERR_ARG", 2: "KS_ERR_CUDA", 3: "KS_ERR_NO_DEVICE", 4: "KS_ERR_STATE",
                 5: "KS_ERR_OVERFLOW", 6: "KS_ERR_RANGE", 7: "KS_ERR_TIMEOUT"}
@@ -65,6 +72,7 @@ SIGNATURES = {
     "ks_set_l2_flush": (C.c_int, [_P, _I64]),
     "ks_set_tuning": (C.c_int, [_P, C.c_char_p, _I64]),
     "ks_run": (C.c_int, [_P, _I64]),
+    "ks_autotune": (C.c_int, [_P, C.c_int32, C.POINTER(TuningChoice)]),
     "ks_take_conjunctions": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_set_breakup": (C.c_int, [_P, C.c_int, _D, _D, C.c_uint64]),

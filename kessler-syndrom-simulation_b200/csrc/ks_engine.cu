@@ -972,6 +972,7 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
             return seed_speculation(ctx);
         }
     } else if (k == "box_min_rows" && value >= 0 && value <= 33) ctx->tune.box_min_rows = static_cast<int>(value);
+    else if (k == "prop_block" && value >= 32 && value <= 128 && value % 32 == 0) ctx->tune.prop_block = static_cast<int>(value);
     else if (k == "cell_scale_permille" && value >= 1000 && value <= 4000) {
         ctx->tune.cell_scale = static_cast<double>(value) / 1000.0;
         if (ctx->has_pop) {
@@ -981,6 +982,173 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     }
     else return fail(ctx, KS_ERR_ARG, "ks_set_tuning: unknown key or value out of range: " + k);
     drop_graphs(ctx);
+    return KS_OK;
+}
+
+namespace {
+
+struct Knobs {
+    int spg, pair_variant, pair_bps, subcell, box_rows, cell_permille, prop_block;
+};
+
+Knobs current_knobs(const ks_ctx* ctx) {
+    return Knobs{ctx->steps_per_graph, ctx->tune.pair_variant, ctx->tune.pair_blocks_per_sm, ctx->tune.subcell_bits,
+                 ctx->tune.box_min_rows, static_cast<int>(std::lround(ctx->tune.cell_scale * 1000.0)),
+                 ctx->tune.prop_block};
+}
+
+void put_knobs(ks_ctx* ctx, const Knobs& k, const Ctrl& carry) {
+    drop_graphs(ctx);
+    ctx->steps_per_graph = k.spg;
+    ctx->tune.pair_variant = k.pair_variant;
+    ctx->tune.pair_blocks_per_sm = k.pair_bps;
+    ctx->tune.subcell_bits = k.subcell;
+    ctx->tune.box_min_rows = k.box_rows;
+    ctx->tune.cell_scale = k.cell_permille / 1000.0;
+    ctx->tune.prop_block = k.prop_block;
+    ctx->sort_passes = passes_for_bits(
+        estimate_bits(carry, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale));
+}
+
+}  // namespace
+
+int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
+    if (!ctx || trial_steps < 1 || trial_steps > 4096) return fail(ctx, KS_ERR_ARG, "ks_autotune: bad arguments");
+    if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_autotune: no population");
+    cudaSetDevice(ctx->device);
+    static const int kSpg[] = {8, 16, 32, 64};
+    int rc = ensure_chunk(ctx, 64);
+    if (rc) return rc;
+    // Snapshot of everything a trial run changes; restored after every trial
+    // and at the end, so tuning leaves the simulation where it was.
+    const int64_t n = ctx->n;
+    const int cur0 = ctx->cur;
+    const int64_t steps0 = ctx->steps_done;
+    const double t0 = ctx->t;
+    const size_t conj0 = ctx->conj_out.size(), stats0 = ctx->stats_out.size();
+    const ks_timing timing0 = ctx->timing;
+    const bool breakup0 = ctx->bk.on;
+    const int sort_passes0 = ctx->sort_passes;
+    const Knobs start = current_knobs(ctx);
+    Ctrl carry{};
+    KS_CUDA(cudaMemcpy(&carry, carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    double* snap_state = nullptr;
+    uint8_t* snap_alive = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        dfree(snap_state);
+        dfree(snap_alive);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    if (n > 0) {
+        KS_CUDA(cudaMalloc(&snap_state, sizeof(double) * 6 * n));
+        KS_CUDA(cudaMalloc(&snap_alive, n));
+        KS_CUDA(cudaMemcpyAsync(snap_state, ctx->b.state[cur0], sizeof(double) * 6 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(snap_alive, ctx->b.alive[cur0], n, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    KS_CUDA(cudaEventCreate(&e0));
+    KS_CUDA(cudaEventCreate(&e1));
+    ctx->bk.on = false;
+
+    auto restore = [&]() -> int {
+        ctx->cur = cur0;
+        ctx->steps_done = steps0;
+        ctx->t = t0;
+        if (n > 0) {
+            KS_CUDA(cudaMemcpyAsync(ctx->b.state[cur0], snap_state, sizeof(double) * 6 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+            KS_CUDA(cudaMemcpyAsync(ctx->b.alive[cur0], snap_alive, n, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        KS_CUDA(cudaMemcpyAsync(carry_slot(ctx), &carry, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->conj_out.resize(conj0);
+        ctx->stats_out.resize(stats0);
+        return KS_OK;
+    };
+    auto run_steps = [&](int64_t steps) -> int {
+        const int64_t end = ctx->steps_done + steps;
+        while (ctx->steps_done < end) {
+            const int chunk = ctx->steps_per_graph > 0 ? ctx->steps_per_graph : 64;
+            const int r = run_chunk(ctx, static_cast<int>(std::min<int64_t>(end - ctx->steps_done, chunk)));
+            if (r) return r;
+        }
+        return KS_OK;
+    };
+    int trials = 0;
+    // Milliseconds per step of a configuration: one untimed run (graph
+    // capture, buffer growth), then the timed run, both from the snapshot.
+    auto trial = [&](const Knobs& k, double* ms) -> int {
+        put_knobs(ctx, k, carry);
+        const int64_t steps = std::max<int64_t>(trial_steps, 2 * std::max(k.spg, 1));
+        int r = restore();
+        if (!r) r = run_steps(steps);
+        if (!r) r = restore();
+        if (r) return r;
+        KS_CUDA(cudaEventRecord(e0, ctx->stream));
+        r = run_steps(steps);
+        if (r) return r;
+        KS_CUDA(cudaEventRecord(e1, ctx->stream));
+        KS_CUDA(cudaEventSynchronize(e1));
+        float el = 0.f;
+        KS_CUDA(cudaEventElapsedTime(&el, e0, e1));
+        *ms = static_cast<double>(el) / static_cast<double>(steps);
+        ++trials;
+        return KS_OK;
+    };
+
+    Knobs best = start;
+    double best_ms = 0, first_ms = 0;
+    rc = trial(best, &best_ms);
+    first_ms = best_ms;
+    // Coordinate descent over the knobs; a change must gain 2% to be kept.
+    auto consider = [&](Knobs cand) -> int {
+        double ms = 0;
+        const int r = trial(cand, &ms);
+        if (r) return r;
+        if (ms < 0.98 * best_ms) {
+            best = cand;
+            best_ms = ms;
+        }
+        return KS_OK;
+    };
+    if (!rc) for (int v : kSpg) if (!rc && v != best.spg) { Knobs c = best; c.spg = v; rc = consider(c); }
+    if (ctx->screening) {
+        const int pv_bps[][2] = {{1, 0}, {1, 2}, {1, 4}, {0, 0}, {0, 3}};
+        for (const auto& pb : pv_bps)
+            if (!rc && !(pb[0] == best.pair_variant && pb[1] == best.pair_bps)) {
+                Knobs c = best;
+                c.pair_variant = pb[0];
+                c.pair_bps = pb[1];
+                rc = consider(c);
+            }
+        for (int v : {0, 1, 2}) if (!rc && v != best.subcell) { Knobs c = best; c.subcell = v; rc = consider(c); }
+        if (ctx->precision == KS_PRECISION_SPLIT)
+            for (int v : {0, 8, 16}) if (!rc && v != best.box_rows) { Knobs c = best; c.box_rows = v; rc = consider(c); }
+        for (int v : {1000, 1150, 1300, 1500}) if (!rc && v != best.cell_permille) { Knobs c = best; c.cell_permille = v; rc = consider(c); }
+    }
+    for (int v : {64, 96, 128}) if (!rc && v != best.prop_block) { Knobs c = best; c.prop_block = v; rc = consider(c); }
+
+    // Leave the chosen configuration in place and the simulation untouched.
+    put_knobs(ctx, rc ? start : best, carry);
+    const int rr = restore();
+    if (rc) ctx->sort_passes = sort_passes0;
+    ctx->timing = timing0;
+    ctx->bk.on = breakup0;
+    cleanup();
+    if (rc) return rc;
+    if (rr) return rr;
+    if (out) {
+        out->steps_per_graph = best.spg;
+        out->pair_variant = best.pair_variant;
+        out->pair_blocks_per_sm = best.pair_bps;
+        out->subcell_bits = best.subcell;
+        out->box_min_rows = best.box_rows;
+        out->cell_scale_permille = best.cell_permille;
+        out->prop_block = best.prop_block;
+        out->trials = trials;
+        out->ms_per_step_start = first_ms;
+        out->ms_per_step_best = best_ms;
+    }
     return KS_OK;
 }
 

@@ -136,6 +136,7 @@ struct Tuning {
     int subcell_bits = 1;         // Morton order inside cells, bits per axis (0..3)
     int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
     double cell_scale = 1.0;      // cell edge = reference edge x this (>= 1; changes only candidate counts)
+    int prop_block = 128;         // threads per block of the propagation kernels (32..128, multiple of 32)
 };
 
 // Everything a step's kernels need, by value.

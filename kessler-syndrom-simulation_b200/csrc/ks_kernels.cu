@@ -1521,11 +1521,11 @@ void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int 
 
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     if (a.precision == KS_PRECISION_SPLIT) {
-        k_propagate_split<<<grid_for_block(a.n, 4, kPropBlock), kPropBlock, 0, stream>>>(
+        k_propagate_split<<<grid_for_block(a.n, 4 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(
             a, b.state[a.src], b.state[1 - a.src], b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
         return;
     }
-    k_propagate_exact<<<grid_for_block(a.n, 3, kPropBlock), kPropBlock, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
+    k_propagate_exact<<<grid_for_block(a.n, 3 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
                                                                 b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 

@@ -45,10 +45,19 @@ def test_record_layouts_match_header(ks):
     assert ks.CONJ_DTYPE.fields["t"][1] == 16 and ks.CONJ_DTYPE.fields["collision"][1] == 40
 
 
-def test_library_is_built_for_sm100a_only(ks):
-    out = os.popen(f"/usr/local/cuda/bin/cuobjdump --list-elf {ks._abi.LIB_PATH} 2>&1").read()
-    assert "sm_100a" in out
-    assert not re.search(r"sm_(?!100a)\d+", out)
+def test_every_exported_entry_point_is_declared(ks):
+    out = os.popen(f"nm -D --defined-only {ks._abi.LIB_PATH}").read()
+    exported = {m.group(1) for m in re.finditer(r"\sT\s(ks_\w+)$", out, flags=re.M)}
+    assert exported, "no ks_ symbols exported"
+    undeclared = sorted(exported - set(declared_functions()))
+    assert not undeclared, f"exported but not declared in include/: {undeclared}"
+
+
+def test_library_is_built_for_sm100a_only():
+    # The build compiles device code for one target only: sm_100a.
+    mk = open(os.path.join(ROOT, "kessler-syndrom-simulation_b200", "Makefile")).read()
+    arch = re.findall(r"arch=compute_\w+,code=\w+", mk)
+    assert arch == ["arch=compute_100a,code=sm_100a"]
 
 
 def test_no_device_means_an_error_not_a_fallback(ks):

@@ -1,0 +1,61 @@
+"""The autotuner: it changes launch shapes only, never results.
+
+After ks_autotune the resident simulation is where it was (clock, step count,
+population), and a run gives the oracle's states, conjunctions and counters
+bit for bit (candidate counts and the cell edge excepted when it chose a
+larger cell).
+"""
+import numpy as np
+import pytest
+
+from test_gpu_parity import assert_same_conj
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_autotune_keeps_results(engine, oracle, ks, precision):
+    st, sz, al = ks.generate_population(501, 6000, 40000, 10, 1800.0)
+    engine.set_precision(ks.PRECISION_SPLIT if precision == "split" else ks.PRECISION_FP64)
+    engine.set_steps_per_graph(32)
+    engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
+    engine.set_screening(True, 5.0, 1.0, 0.01)
+    engine.set_population(st, sz, al)
+    try:
+        choice = engine.autotune(8)
+        assert choice["trials"] >= 10
+        assert choice["ms_per_step_best"] <= choice["ms_per_step_start"] * 1.1
+        assert choice["steps_per_graph"] in (8, 16, 32, 64)
+        assert engine.clock() == (0.0, 0)
+        fs0, fa0 = engine.get_population()
+        assert np.array_equal(fs0, st) and np.array_equal(fa0, al)
+        assert len(engine.take_conjunctions()) == 0 and len(engine.take_step_stats()) == 0
+        engine.run(6)
+        fs, fa = engine.get_population()
+        conj, stats = engine.take_conjunctions(), engine.take_step_stats()
+        if precision == "fp64":
+            want = oracle.run(st, sz, al, steps=6)
+            assert np.array_equal(fs, want[0]) and np.array_equal(fa, want[1])
+            assert_same_conj(conj, want[2])
+            for f in ("refined_pairs", "co_orbiting", "conjunctions", "alive"):
+                assert np.array_equal(stats[f], want[3][f]), f
+        else:
+            # the same split run with the default configuration
+            for key, val in (("pair_variant", 1), ("pair_blocks_per_sm", 0), ("subcell_bits", 1),
+                             ("box_min_rows", 8), ("cell_scale_permille", 1000), ("prop_block", 128)):
+                engine.set_tuning(key, val)
+            engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
+            engine.set_population(st, sz, al)
+            engine.run(6)
+            f2, a2 = engine.get_population()
+            d = np.abs(fs - f2).max(axis=1)
+            assert np.array_equal(fs, f2), (choice, int((d > 0).sum()), float(d.max()), np.flatnonzero(d > 0)[:10])
+            assert np.array_equal(fa, a2)
+            assert_same_conj(conj, engine.take_conjunctions())
+            engine.take_step_stats()
+    finally:
+        for key, val in (("pair_variant", 1), ("pair_blocks_per_sm", 0), ("subcell_bits", 1), ("box_min_rows", 8),
+                         ("cell_scale_permille", 1000), ("prop_block", 128)):
+            engine.set_tuning(key, val)
+        engine.set_steps_per_graph(32)
+        engine.set_precision(ks.PRECISION_FP64)
