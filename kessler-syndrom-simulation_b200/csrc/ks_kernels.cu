@@ -1113,8 +1113,52 @@ __device__ __forceinline__ int locate(const SegTable& t, int nseg, int p, int* s
     return t.begin[lo] + (p - t.start[lo]);
 }
 
+// Position / velocity bounding box of the 32 lanes' FP64 states.
+struct BoxD {
+    double pmin[3], pmax[3], vmin[3], vmax[3];
+};
+
+__device__ __forceinline__ double warp_min_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ BoxD warp_box_d(const SortedState& s) {
+    BoxD b;
+    const double p[3] = {s.rx, s.ry, s.rz}, v[3] = {s.vx, s.vy, s.vz};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        b.pmin[q] = warp_min_d(p[q]);
+        b.pmax[q] = warp_max_d(p[q]);
+        b.vmin[q] = warp_min_d(v[q]);
+        b.vmax[q] = warp_max_d(v[q]);
+    }
+    return b;
+}
+
+// True if the column stays farther than gate from every state of the box
+// over [0, dt]: |dr + dv t| >= |dr| - dt |dv| >= (box distance) - dt (largest
+// relative speed), so filter_pair's distance gate rejects all those pairs.
+// The factors cover the FP64 rounding of this test.
+__device__ __forceinline__ bool apart_from_box_d(const BoxD& b, const SortedState& c, double dt, double gate) {
+    const double p[3] = {c.rx, c.ry, c.rz}, v[3] = {c.vx, c.vy, c.vz};
+    double d2 = 0.0, w2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double gap = fmax(0.0, fmax(p[q] - b.pmax[q], b.pmin[q] - p[q]));
+        d2 = fma(gap, gap, d2);
+        const double w = fmax(fabs(v[q] - b.vmin[q]), fabs(v[q] - b.vmax[q]));
+        w2 = fma(w, w, w2);
+    }
+    return sqrt(d2) * (1.0 - 1e-12) - dt * sqrt(w2) * (1.0 + 1e-12) > gate;
+}
+
 template <int kCols>
-__global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double* __restrict__ sorted,
+__global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const double* __restrict__ sorted,
                                                         const int* __restrict__ orig,
                                                         const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr, const int4* __restrict__ items,
@@ -1122,12 +1166,17 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
     __shared__ double2 rows[kWarps][32][3];
     __shared__ int rorig[kWarps][32];
     __shared__ SegTable segs[kWarps];
+    // Per-warp queue of columns that survived the row-box test (sorted index, valid rows).
+    __shared__ int qidx[kWarps][64];
+    __shared__ unsigned qmask[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
     const double gate_hi2 = gate_hi * gate_hi;
+    const int box_rows = kCols == 1 ? a.tune.box_min_rows : 0;
     PairCounters pc;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
@@ -1149,6 +1198,52 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tiles(StepArgs a, const double
             rorig[warp][lane] = orig[b0 + r0 + lane];
         }
         __syncwarp();
+        if (box_rows > 0 && nr >= box_rows) {
+            // Columns tested against the rows' box, survivors compacted into full warps.
+            const BoxD rbox = warp_box_d(load_sorted(sorted, b0 + r0 + (lane < nr ? lane : 0)));
+            auto drain = [&](int count) {
+                __syncwarp();
+                const bool has = lane < count;
+                const int q = qidx[warp][has ? lane : 0];
+                const unsigned valid = has ? qmask[warp][lane] : 0u;
+                __syncwarp();
+                const SortedState col = load_sorted(sorted, q);
+                unsigned need = 0u;
+#pragma unroll 4
+                for (int r = 0; r < nr; ++r)
+                    need |= gate_open(col, rows[warp][r][0], rows[warp][r][1], rows[warp][r][2], gate_hi2) << r;
+                need &= valid;
+                if (__any_sync(0xffffffffu, need != 0u))
+                    exact_rows(need, col, orig[q], rows[warp], rorig[warp], a, surv, surv_cap, pc);
+            };
+            int queued = 0;
+            for (int cb = cb0; cb < cb0 + ncb; ++cb) {
+                const int p = 32 * cb + lane;
+                const bool ok = p < L;
+                int sid;
+                const int q = ok ? locate(segs[warp], nseg, p, &sid) : b0;
+                const unsigned valid = ok ? (cb == ra ? lanes_below : 0xffffffffu) & nrmask : 0u;
+                const bool keep = valid != 0u && !apart_from_box_d(rbox, load_sorted(sorted, q), a.dt, gate_hi);
+                const unsigned kept = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int slot = queued + __popc(kept & lanes_below);
+                    qidx[warp][slot] = q;
+                    qmask[warp][slot] = valid;
+                }
+                queued += __popc(kept);
+                if (queued >= 32) {
+                    drain(32);
+                    if (lane < queued - 32) {
+                        qidx[warp][lane] = qidx[warp][32 + lane];
+                        qmask[warp][lane] = qmask[warp][32 + lane];
+                    }
+                    queued -= 32;
+                }
+            }
+            if (queued > 0) drain(queued);
+            __syncwarp();
+            continue;
+        }
         for (int cb = cb0; cb < cb0 + ncb; cb += kCols) {
             SortedState col[kCols];
             int corig[kCols];
@@ -1304,7 +1399,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_split(StepArgs a, const dou
     __shared__ double2 rows[kWarps][32][3];
     __shared__ int rorig[kWarps][32];
     __shared__ SegTable segs[kWarps];
+    // Per-warp queue of columns that survived the row-box test, drained 32 at a time.
+    __shared__ float4 qcol[kWarps][64][2];
+    __shared__ int qidx[kWarps][64];
+    __shared__ unsigned qmask[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
@@ -1342,10 +1442,31 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_split(StepArgs a, const dou
             rows[warp][lane][2] = s[2];
             rorig[warp][lane] = orig[rl];
         }
+        // Tiles of at least box_rows rows test each column against the rows'
+        // position / velocity box first and keep only columns that could come
+        // within the gate of some row, compacted into full warps.
         const bool use_box = box_rows > 0 && nr >= box_rows;
         Box rbox;
         if (use_box) rbox = warp_box(my_rp, my_rv);
         __syncwarp();
+        // Columns held by the lanes (entry `lane` of a batch) against every row.
+        auto gate_rows = [&](float4 cp, float4 cv, int q, unsigned valid) {
+            unsigned need = 0u;
+#pragma unroll 4
+            for (int r = 0; r < nr; ++r)
+                need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
+            need &= valid;
+            if (__any_sync(0xffffffffu, need != 0u))
+                exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, a, surv,
+                               surv_cap, pc);
+        };
+        auto drain = [&](int count) {
+            __syncwarp();
+            const int e = lane < count ? lane : 0;
+            gate_rows(qcol[warp][e][0], qcol[warp][e][1], qidx[warp][e], lane < count ? qmask[warp][e] : 0u);
+            __syncwarp();
+        };
+        int queued = 0;
         for (int cb = cb0; cb < cb0 + ncb; ++cb) {
             const int p = 32 * cb + lane;
             const bool ok = p < L;
@@ -1358,16 +1479,37 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_split(StepArgs a, const dou
                 cp.y = fmaf(static_cast<float>(c_forward[sid - 1][1]), cell_f, cp.y);
                 cp.z = fmaf(static_cast<float>(c_forward[sid - 1][2]), cell_f, cp.z);
             }
-            if (use_box && boxes_apart(rbox, warp_box(cp, cv), dt_f, gate_f)) continue;
-            const unsigned valid = ok ? (cb == ra ? ((1u << lane) - 1u) : 0xffffffffu) & nrmask : 0u;
-            unsigned need = 0u;
-#pragma unroll 4
-            for (int r = 0; r < nr; ++r) need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
-            need &= valid;
-            if (__any_sync(0xffffffffu, need != 0u))
-                exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, a, surv,
-                               surv_cap, pc);
+            const unsigned valid = ok ? (cb == ra ? lanes_below : 0xffffffffu) & nrmask : 0u;
+            if (!use_box) {
+                gate_rows(cp, cv, q, valid);
+                continue;
+            }
+            Box cbox;
+            cbox.pmin[0] = cbox.pmax[0] = cp.x; cbox.pmin[1] = cbox.pmax[1] = cp.y; cbox.pmin[2] = cbox.pmax[2] = cp.z;
+            cbox.vmin[0] = cbox.vmax[0] = cv.x; cbox.vmin[1] = cbox.vmax[1] = cv.y; cbox.vmin[2] = cbox.vmax[2] = cv.z;
+            const bool keep = valid != 0u && !boxes_apart(rbox, cbox, dt_f, gate_f);
+            const unsigned kept = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int slot = queued + __popc(kept & lanes_below);
+                qcol[warp][slot][0] = cp;
+                qcol[warp][slot][1] = cv;
+                qidx[warp][slot] = q;
+                qmask[warp][slot] = valid;
+            }
+            queued += __popc(kept);
+            if (queued >= 32) {
+                drain(32);
+                if (lane < queued - 32) {
+                    qcol[warp][lane][0] = qcol[warp][32 + lane][0];
+                    qcol[warp][lane][1] = qcol[warp][32 + lane][1];
+                    qidx[warp][lane] = qidx[warp][32 + lane];
+                    qmask[warp][lane] = qmask[warp][32 + lane];
+                }
+                queued -= 32;
+            }
         }
+        if (queued > 0) drain(queued);
+        __syncwarp();
     }
     pc.co = warp_sum(pc.co);
     pc.full = warp_sum(pc.full);
