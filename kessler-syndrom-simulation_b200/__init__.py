@@ -103,10 +103,15 @@ class Engine:
     def population_size(self):
         return int(self._lib.ks_population_size(self._h))
 
-    def get_population(self):
+    def get_population(self, states=None, alive=None):
+        """(states (n, 6), alive (n,)); optional preallocated outputs (e.g. pinned host memory)."""
         n = self._lib.ks_population_size(self._h)
-        st = np.empty((n, 6), dtype=np.float64)
-        al = np.empty(n, dtype=np.uint8)
+        st = np.empty((n, 6), dtype=np.float64) if states is None else states
+        al = np.empty(n, dtype=np.uint8) if alive is None else alive
+        if st.shape != (n, 6) or st.dtype != np.float64 or not st.flags.c_contiguous:
+            raise ValueError("states must be a C-contiguous float64 array of shape (n, 6)")
+        if al.shape != (n,) or al.dtype != np.uint8:
+            raise ValueError("alive must be a uint8 array of shape (n,)")
         self._check(self._lib.ks_get_population(self._h, n, ptr(st), ptr(al)))
         return st, al
 

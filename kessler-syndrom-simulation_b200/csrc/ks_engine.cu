@@ -63,6 +63,7 @@ struct ks_ctx {
     std::vector<cudaEvent_t> ev;
     ks_timing timing{};
     ks::Tuning tune;
+    bool ckpt_states = false;  // the checkpoint holds states (chunks of more than one step)
     int realisations = 1;
     int rbits = 0;
     std::vector<int64_t> offsets;  // realisation offsets (batches)
@@ -184,13 +185,31 @@ int ensure_items(ks_ctx* ctx, int64_t want) {
     return KS_OK;
 }
 
+void free_conj(ks_ctx* ctx) {
+    ks::DeviceBuffers& b = ctx->b;
+    dfree(b.conj);
+    for (int k = 0; k < 2; ++k) { dfree(b.conj_keys[k]); dfree(b.conj_idx[k]); }
+    dfree(b.conj_status); dfree(b.conj_hist); dfree(b.conj_ctr); dfree(b.conj_sorted);
+    b.conj_cap = 0;
+}
+
 int ensure_conj(ks_ctx* ctx, int64_t want) {
     if (want > ctx->b.conj_cap) {
+        if (want > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "more than 2^30 conjunctions in one chunk");
         drop_graphs(ctx);
-        dfree(ctx->b.conj);
-        ctx->b.conj_cap = 0;
-        KS_CUDA(cudaMalloc(&ctx->b.conj, sizeof(ks_conjunction) * want));
-        ctx->b.conj_cap = want;
+        free_conj(ctx);
+        ks::DeviceBuffers& b = ctx->b;
+        const int64_t tiles = (want + 2047) / 2048;
+        KS_CUDA(cudaMalloc(&b.conj, sizeof(ks_conjunction) * want));
+        KS_CUDA(cudaMalloc(&b.conj_sorted, sizeof(ks_conjunction) * want));
+        for (int k = 0; k < 2; ++k) {
+            KS_CUDA(cudaMalloc(&b.conj_keys[k], sizeof(unsigned long long) * want));
+            KS_CUDA(cudaMalloc(&b.conj_idx[k], sizeof(int) * want));
+        }
+        KS_CUDA(cudaMalloc(&b.conj_status, sizeof(unsigned int) * 256 * 4 * tiles));
+        KS_CUDA(cudaMalloc(&b.conj_hist, sizeof(unsigned int) * 8 * 256));
+        KS_CUDA(cudaMalloc(&b.conj_ctr, sizeof(unsigned int) * 8));
+        b.conj_cap = want;
     }
     if (want > ctx->h_conj_cap) {
         if (ctx->h_conj) cudaFreeHost(ctx->h_conj);
@@ -335,6 +354,8 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
         }
         src ^= 1;
     }
+    if (ctx->screening)
+        ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, s);
 }
 
 int launch_chunk(ks_ctx* ctx, int k_steps) {
@@ -364,18 +385,26 @@ int launch_chunk(ks_ctx* ctx, int k_steps) {
     return KS_OK;
 }
 
-int save_checkpoint(ks_ctx* ctx) {
+// Start-of-chunk checkpoint for replays. A one-step chunk never overwrites
+// its input states (steps ping-pong between two buffers), so only the
+// carried control block is saved then.
+int save_checkpoint(ks_ctx* ctx, int k_steps) {
     ks::DeviceBuffers& b = ctx->b;
-    KS_CUDA(cudaMemcpyAsync(b.ckpt_state, b.state[ctx->cur], sizeof(double) * 6 * b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
-    KS_CUDA(cudaMemcpyAsync(b.ckpt_alive, b.alive[ctx->cur], b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->ckpt_states = k_steps > 1;
+    if (ctx->ckpt_states) {
+        KS_CUDA(cudaMemcpyAsync(b.ckpt_state, b.state[ctx->cur], sizeof(double) * 6 * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.ckpt_alive, b.alive[ctx->cur], ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
     KS_CUDA(cudaMemcpyAsync(carry_ckpt_slot(ctx), carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToDevice, ctx->stream));
     return KS_OK;
 }
 
 int restore_checkpoint(ks_ctx* ctx) {
     ks::DeviceBuffers& b = ctx->b;
-    KS_CUDA(cudaMemcpyAsync(b.state[ctx->cur], b.ckpt_state, sizeof(double) * 6 * b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
-    KS_CUDA(cudaMemcpyAsync(b.alive[ctx->cur], b.ckpt_alive, b.cap, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (ctx->ckpt_states) {
+        KS_CUDA(cudaMemcpyAsync(b.state[ctx->cur], b.ckpt_state, sizeof(double) * 6 * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.alive[ctx->cur], b.ckpt_alive, ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
     KS_CUDA(cudaMemcpyAsync(carry_slot(ctx), carry_ckpt_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToDevice, ctx->stream));
     return KS_OK;
 }
@@ -384,6 +413,23 @@ bool conj_less(const ks_conjunction& a, const ks_conjunction& b) {
     if (a.t != b.t) return a.t < b.t;
     if (a.i != b.i) return a.i < b.i;
     return a.j < b.j;
+}
+
+// (t, i, j) order of records the device already ordered by a key monotone in
+// t: only records that shared a key can be out of order, so an insertion
+// pass is linear in practice.
+template <typename It>
+void finish_order(It first, It last) {
+    for (It it = first; it != last; ++it) {
+        if (it == first || !conj_less(*it, *(it - 1))) continue;
+        const ks_conjunction v = *it;
+        It j = it;
+        do {
+            *j = *(j - 1);
+            --j;
+        } while (j != first && conj_less(v, *(j - 1)));
+        *j = v;
+    }
 }
 
 void accumulate_timing(ks_ctx* ctx, int k_steps) {
@@ -421,7 +467,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
     KS_CUDA(cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, ctx->stream));
     if (ctx->screening) {
-        rc = save_checkpoint(ctx);
+        rc = save_checkpoint(ctx, k_steps);
         if (rc) return rc;
     }
     for (int attempt = 0;; ++attempt) {
@@ -462,8 +508,9 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     for (int cut = 0;; ++cut) {
         nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
         if (nc > 0) {
-            KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj, sizeof(ks_conjunction) * nc, cudaMemcpyDeviceToHost,
-                                    ctx->stream));
+            // Records already ordered by TCA on the device (conj_sorted).
+            KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj_sorted, sizeof(ks_conjunction) * nc,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
             KS_CUDA(cudaStreamSynchronize(ctx->stream));
         }
         if (!ctx->bk.on || nc == 0) break;
@@ -490,7 +537,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     if (nc > 0) {
         const size_t base = ctx->conj_out.size();
         ctx->conj_out.insert(ctx->conj_out.end(), ctx->h_conj, ctx->h_conj + nc);
-        std::sort(ctx->conj_out.begin() + base, ctx->conj_out.end(), conj_less);
+        finish_order(ctx->conj_out.begin() + base, ctx->conj_out.end());
         if (ctx->bk.on)
             for (size_t q = base; q < ctx->conj_out.size(); ++q)
                 if (ctx->conj_out[q].collision) hits.push_back(ctx->conj_out[q]);
@@ -799,7 +846,7 @@ void ks_destroy(ks_ctx* ctx) {
     if (ctx->l2_flush) cudaFree(ctx->l2_flush);
     dfree(ctx->b.survivors);
     dfree(ctx->b.items);
-    dfree(ctx->b.conj);
+    free_conj(ctx);
     dfree(ctx->b.ctrl);
     dfree(ctx->b.chunk);
     dfree(ctx->b.params);
@@ -952,8 +999,7 @@ int ks_set_buffer_limits(ks_ctx* ctx, int64_t survivor_pairs, int64_t conjunctio
         if (rc) return rc;
     }
     if (conjunctions > 0) {
-        dfree(ctx->b.conj);
-        ctx->b.conj_cap = 0;
+        free_conj(ctx);
         int rc = ensure_conj(ctx, conjunctions);
         if (rc) return rc;
     }

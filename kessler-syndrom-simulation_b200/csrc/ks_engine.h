@@ -87,7 +87,7 @@ struct Ctrl {
 struct ChunkCtrl {
     unsigned long long conj_count;     // records appended in this chunk
     int flags;
-    int pad;
+    int sort_n;                        // records ordered by the chunk's conjunction sort
 };
 
 struct DeviceBuffers {
@@ -123,6 +123,15 @@ struct DeviceBuffers {
     int64_t surv_cap = 0;
     ks_conjunction* conj = nullptr;
     int64_t conj_cap = 0;
+    // Ordering of a chunk's conjunction records on the device (radix sort on a
+    // 32-bit key monotone in t): keys / indices ping-pong, look-back status,
+    // digit histograms, tile tickets, and the records in order.
+    unsigned long long* conj_keys[2] = {nullptr, nullptr};
+    int* conj_idx[2] = {nullptr, nullptr};
+    unsigned int* conj_status = nullptr;
+    unsigned int* conj_hist = nullptr;
+    unsigned int* conj_ctr = nullptr;
+    ks_conjunction* conj_sorted = nullptr;
     Ctrl* ctrl = nullptr;                  // max_chunk + 1 entries
     int ctrl_len = 0;
     ChunkCtrl* chunk = nullptr;
@@ -173,6 +182,12 @@ void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t str
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+// Orders the chunk's conjunction records by TCA into conj_sorted (records
+// whose TCAs share a 32-bit key keep their append order; the host finishes
+// the (t, i, j) order). t_start: device address of the chunk's first step
+// start time; span_s: the chunk's duration.
+void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s,
+                      cudaStream_t stream);
 void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,
                    ChunkCtrl* chunk, cudaStream_t stream);
 // Index of the key/idx buffer holding the sorted result after `passes` passes.

@@ -604,8 +604,11 @@ __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
 
 // Digit histograms of every pass in one read of the keys.
 __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long long* __restrict__ keys, int n,
-                                                         int passes, unsigned int* __restrict__ hist, Ctrl* ctrl) {
+                                                         const int* __restrict__ n_dev, int passes,
+                                                         unsigned int* __restrict__ hist, Ctrl* ctrl) {
     __shared__ unsigned int h[8][256];
+    if (n_dev) n = min(n, *n_dev);
+    if (blockIdx.x * kSortTile >= n) return;
     for (int p = 0; p < 8; ++p) h[p][threadIdx.x] = 0;
     __syncthreads();
     const int base = blockIdx.x * kSortTile;
@@ -625,7 +628,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long lon
         const unsigned int c = h[pass][threadIdx.x];
         if (c) atomicAdd(&hist[pass * 256 + threadIdx.x], c);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && ctrl->grid.bits + 1 > 8 * passes)
+    if (ctrl && blockIdx.x == 0 && threadIdx.x == 0 && ctrl->grid.bits + 1 > 8 * passes)
         atomicOr(&ctrl->flags, FLAG_SORT_BITS);
 }
 
@@ -643,10 +646,11 @@ __global__ void __launch_bounds__(kBlock) k_sort_digit_scan(unsigned int* __rest
 __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long long* __restrict__ keys_in,
                                                           const int* __restrict__ idx_in,
                                                           unsigned long long* __restrict__ keys_out,
-                                                          int* __restrict__ idx_out, int n, int shift,
+                                                          int* __restrict__ idx_out, int n,
+                                                          const int* __restrict__ n_dev, int shift,
                                                           const unsigned int* __restrict__ digit_base,
                                                           unsigned int* __restrict__ status,
-                                                          unsigned int* __restrict__ ticket, Ctrl* ctrl) {
+                                                          unsigned int* __restrict__ ticket, int* flags) {
     __shared__ unsigned int wcnt[kWarps][256];
     __shared__ int gbase[256];
     __shared__ unsigned long long skeys[kSortTile];
@@ -659,9 +663,11 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
         timed_out = 0;
     }
     for (int w = 0; w < kWarps; ++w) wcnt[w][threadIdx.x] = 0;
+    if (n_dev) n = min(n, *n_dev);
     __syncthreads();
     const int tile = tile_sh;
     const int tile0 = tile * kSortTile;
+    if (tile0 >= n) return;  // tickets are in order: no later tile waits on this one
     const int count = min(kSortTile, n - tile0);
 
     constexpr int kPerWarp = kSortTile / kWarps;
@@ -718,7 +724,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
     }
     __syncthreads();
     if (timed_out) {
-        if (threadIdx.x == 0) atomicOr(&ctrl->flags, FLAG_TIMEOUT);
+        if (threadIdx.x == 0) atomicOr(flags, FLAG_TIMEOUT);
         return;  // results of this step are discarded by the host
     }
     for (int r = 0; r < kRounds; ++r) {
@@ -802,8 +808,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         if (p >= m) break;
         run += heads[j];
         const int cid = run - 1;
-        const unsigned long long key = keys[p] >> sh;  // cell part
         if (heads[j]) {
+            const unsigned long long key = keys[p] >> sh;  // cell part
             cell_begin[cid] = p;
             cell_key_out[cid] = key;
             unsigned long long h = hash_slot(key, hmask);
@@ -813,31 +819,55 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                 h = (h + 1) & hmask;
             }
         }
-        const int o = idx[p];
-        sorted_orig[p] = o;
-        double st[6];
-        ld6(before, o, st);
-        const double x = st[0], y = st[1], z = st[2], vx = st[3], vy = st[4], vz = st[5];
+        if (p == m - 1) {
+            ctrl->n_cells = cid + 1;
+            cell_begin[cid + 1] = m;
+        }
+    }
+    // Gather of the start-of-step states in sorted order: entries strided
+    // across the block so that stores coalesce, every load of a thread's
+    // entries issued before the first store (random rows of `before`).
+    __shared__ GridParams g;
+    if (threadIdx.x == 0) g = ctrl->grid;
+    __syncthreads();
+    const int base = blockIdx.x * kCellTile + threadIdx.x;
+    int o[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int p = base + j * kBlock;
+        o[j] = p < m ? idx[p] : -1;
+    }
+    double2 st[kPer][3];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        if (o[j] < 0) continue;
+        const double2* src = reinterpret_cast<const double2*>(before + 6 * static_cast<int64_t>(o[j]));
+        st[j][0] = src[0];
+        st[j][1] = src[1];
+        st[j][2] = src[2];
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int p = base + j * kBlock;
+        if (o[j] < 0) continue;
+        sorted_orig[p] = o[j];
         double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
-        dst[0] = make_double2(x, y);
-        dst[1] = make_double2(z, vx);
-        dst[2] = make_double2(vy, vz);
+        dst[0] = st[j][0];
+        dst[1] = st[j][1];
+        dst[2] = st[j][2];
         if (sorted32) {
             // Position relative to the corner of the object's own cell, velocity, in FP32.
-            const GridParams& g = ctrl->grid;
+            const unsigned long long key = keys[p] >> sh;
             const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
             const unsigned long long mx = (1ull << g.w[0]) - 1;
             const double cx = static_cast<double>(static_cast<long long>((key >> (g.w[1] + g.w[2])) & mx) + g.lo[0]) * g.cell;
             const double cy = static_cast<double>(static_cast<long long>((key >> g.w[2]) & my) + g.lo[1]) * g.cell;
             const double cz = static_cast<double>(static_cast<long long>(key & mz) + g.lo[2]) * g.cell;
-            sorted32[2 * static_cast<int64_t>(p)] =
-                make_float4(static_cast<float>(x - cx), static_cast<float>(y - cy), static_cast<float>(z - cz), 0.0f);
-            sorted32[2 * static_cast<int64_t>(p) + 1] =
-                make_float4(static_cast<float>(vx), static_cast<float>(vy), static_cast<float>(vz), 0.0f);
-        }
-        if (p == m - 1) {
-            ctrl->n_cells = cid + 1;
-            cell_begin[cid + 1] = m;
+            sorted32[2 * static_cast<int64_t>(p)] = make_float4(static_cast<float>(st[j][0].x - cx),
+                                                                static_cast<float>(st[j][0].y - cy),
+                                                                static_cast<float>(st[j][1].x - cz), 0.0f);
+            sorted32[2 * static_cast<int64_t>(p) + 1] = make_float4(
+                static_cast<float>(st[j][1].y), static_cast<float>(st[j][2].x), static_cast<float>(st[j][2].y), 0.0f);
         }
     }
 }
@@ -1694,15 +1724,59 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     cudaMemsetAsync(b.sort_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
     cudaMemsetAsync(b.sort_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
-    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, passes, b.sort_hist, a.ctrl);
+    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, nullptr, passes, b.sort_hist, a.ctrl);
     k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.sort_hist, passes);
     for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
-            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, 8 * pass,
+            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, nullptr, 8 * pass,
             b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass, b.sort_ctr + pass,
-            a.ctrl);
+            &a.ctrl->flags);
     }
+}
+
+// Key of each of the chunk's records: floor(2^32 (t - t_start) / span),
+// clamped, a non-decreasing function of t.
+__global__ void __launch_bounds__(kBlock) k_conj_keys(const ks_conjunction* __restrict__ conj, int64_t cap,
+                                                      ChunkCtrl* chunk, const double* __restrict__ t_start,
+                                                      double span_s, unsigned long long* __restrict__ keys) {
+    const int n = static_cast<int>(min(chunk->conj_count, static_cast<unsigned long long>(cap)));
+    if (blockIdx.x == 0 && threadIdx.x == 0) chunk->sort_n = n;
+    const double t0 = *t_start;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const double f = xmul(xdiv(xsub(conj[q].t, t0), span_s), 4294967296.0);
+        const double c = fmin(fmax(floor(f), 0.0), 4294967295.0);
+        keys[q] = static_cast<unsigned long long>(c);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_conj_gather(const ks_conjunction* __restrict__ conj,
+                                                        const int* __restrict__ order, const ChunkCtrl* chunk,
+                                                        ks_conjunction* __restrict__ out) {
+    const int n = chunk->sort_n;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = conj[order[q]];
+}
+
+void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s,
+                      cudaStream_t stream) {
+    const int cap = static_cast<int>(b.conj_cap);
+    if (cap <= 0) return;
+    constexpr int kPasses = 4;
+    const int ntiles = (cap + kSortTile - 1) / kSortTile;
+    cudaMemsetAsync(b.conj_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
+    cudaMemsetAsync(b.conj_ctr, 0, sizeof(unsigned int) * 8, stream);
+    cudaMemsetAsync(b.conj_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * kPasses, stream);
+    k_conj_keys<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_cap, chunk, t_start, span_s, b.conj_keys[0]);
+    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.conj_keys[0], cap, &chunk->sort_n, kPasses, b.conj_hist, nullptr);
+    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.conj_hist, kPasses);
+    for (int pass = 0; pass < kPasses; ++pass) {
+        const int in = pass & 1, outb = 1 - in;
+        k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
+            b.conj_keys[in], pass == 0 ? nullptr : b.conj_idx[in], b.conj_keys[outb], b.conj_idx[outb], cap,
+            &chunk->sort_n, 8 * pass, b.conj_hist + 256 * pass,
+            b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass, &chunk->flags);
+    }
+    k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_idx[kPasses & 1], chunk, b.conj_sorted);
 }
 
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
