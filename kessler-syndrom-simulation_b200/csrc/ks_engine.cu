@@ -1167,7 +1167,7 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
                 c.pair_bps = pb[1];
                 rc = consider(c);
             }
-        for (int v : {0, 1, 2}) if (!rc && v != best.subcell) { Knobs c = best; c.subcell = v; rc = consider(c); }
+        for (int v : {0, 1, 2, 3}) if (!rc && v != best.subcell) { Knobs c = best; c.subcell = v; rc = consider(c); }
         for (int v : {0, 4, 8, 16}) if (!rc && v != best.box_rows) { Knobs c = best; c.box_rows = v; rc = consider(c); }
         for (int v : {1000, 1150, 1300, 1500}) if (!rc && v != best.cell_permille) { Knobs c = best; c.cell_permille = v; rc = consider(c); }
     }

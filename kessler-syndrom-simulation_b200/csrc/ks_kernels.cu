@@ -1419,7 +1419,8 @@ __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 
     }
 }
 
-__global__ void __launch_bounds__(kBlock, 3) k_pairs_split(StepArgs a, const double* __restrict__ sorted,
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, const double* __restrict__ sorted,
                                                         const float4* __restrict__ sorted32,
                                                         const int* __restrict__ orig,
                                                         const int* __restrict__ cell_begin,
@@ -1807,9 +1808,16 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     // Default: the resident block count of each kernel.
     if (a.precision == KS_PRECISION_SPLIT) {
+        // Register budget for 3 resident blocks per SM (80 registers), or for 4 (64).
         const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 3;
-        k_pairs_split<<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig, b.cell_begin,
-                                                              b.nbr, b.items, b.items_cap, b.survivors, b.surv_cap);
+        if (bps >= 4)
+            k_pairs_split<4><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
+                                                                     b.cell_begin, b.nbr, b.items, b.items_cap,
+                                                                     b.survivors, b.surv_cap);
+        else
+            k_pairs_split<3><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
+                                                                     b.cell_begin, b.nbr, b.items, b.items_cap,
+                                                                     b.survivors, b.surv_cap);
         return;
     }
     const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : (a.tune.pair_variant == 1 ? 3 : 2);
