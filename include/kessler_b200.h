@@ -105,7 +105,8 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * (split pair kernel: skip tiles whose row and column blocks are provably
  * apart, for tiles of at least this many rows; 0 = off), "cell_scale_permille"
  * (1000..4000: grid cell edge = the reference's edge x value/1000),
- * "prop_block" (32..128, threads per block of the propagation kernels).
+ * "prop_block" (32..128, threads per block of the propagation kernels),
+ * "item_col_blocks" (1..64, column blocks of 32 per pair-kernel work item).
  * Conjunctions, refined and co-orbiting counts and states never change;
  * candidate_pairs and cell_km change with the cell edge. */
 int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value);
@@ -116,6 +117,7 @@ typedef struct ks_tuning_choice {
     int32_t pair_variant, pair_blocks_per_sm, subcell_bits, box_min_rows;
     int32_t cell_scale_permille;
     int32_t prop_block;
+    int32_t item_col_blocks;
     int32_t trials;              /* configurations timed */
     double ms_per_step_start;    /* device time per step of the starting configuration */
     double ms_per_step_best;     /* ... and of the chosen one */

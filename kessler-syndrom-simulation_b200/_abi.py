@@ -37,7 +37,8 @@ class Timing(C.Structure):
 class TuningChoice(C.Structure):
     _fields_ = [("steps_per_graph", C.c_int32), ("pair_variant", C.c_int32), ("pair_blocks_per_sm", C.c_int32),
                 ("subcell_bits", C.c_int32), ("box_min_rows", C.c_int32), ("cell_scale_permille", C.c_int32),
-                ("prop_block", C.c_int32), ("trials", C.c_int32), ("ms_per_step_start", C.c_double),
+                ("prop_block", C.c_int32), ("item_col_blocks", C.c_int32), ("trials", C.c_int32),
+                ("ms_per_step_start", C.c_double),
                 ("ms_per_step_best", C.c_double)]
 
 

@@ -1019,6 +1019,7 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
         }
     } else if (k == "box_min_rows" && value >= 0 && value <= 33) ctx->tune.box_min_rows = static_cast<int>(value);
     else if (k == "prop_block" && value >= 32 && value <= 128 && value % 32 == 0) ctx->tune.prop_block = static_cast<int>(value);
+    else if (k == "item_col_blocks" && value >= 1 && value <= 64) ctx->tune.item_col_blocks = static_cast<int>(value);
     else if (k == "cell_scale_permille" && value >= 1000 && value <= 4000) {
         ctx->tune.cell_scale = static_cast<double>(value) / 1000.0;
         if (ctx->has_pop) {
@@ -1034,13 +1035,13 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
 namespace {
 
 struct Knobs {
-    int spg, pair_variant, pair_bps, subcell, box_rows, cell_permille, prop_block;
+    int spg, pair_variant, pair_bps, subcell, box_rows, cell_permille, prop_block, item_cols;
 };
 
 Knobs current_knobs(const ks_ctx* ctx) {
     return Knobs{ctx->steps_per_graph, ctx->tune.pair_variant, ctx->tune.pair_blocks_per_sm, ctx->tune.subcell_bits,
                  ctx->tune.box_min_rows, static_cast<int>(std::lround(ctx->tune.cell_scale * 1000.0)),
-                 ctx->tune.prop_block};
+                 ctx->tune.prop_block, ctx->tune.item_col_blocks};
 }
 
 void put_knobs(ks_ctx* ctx, const Knobs& k, const Ctrl& carry) {
@@ -1052,6 +1053,7 @@ void put_knobs(ks_ctx* ctx, const Knobs& k, const Ctrl& carry) {
     ctx->tune.box_min_rows = k.box_rows;
     ctx->tune.cell_scale = k.cell_permille / 1000.0;
     ctx->tune.prop_block = k.prop_block;
+    ctx->tune.item_col_blocks = k.item_cols;
     ctx->sort_passes = passes_for_bits(
         estimate_bits(carry, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale));
 }
@@ -1171,6 +1173,8 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
         for (int v : {0, 4, 8, 16}) if (!rc && v != best.box_rows) { Knobs c = best; c.box_rows = v; rc = consider(c); }
         for (int v : {1000, 1150, 1300, 1500}) if (!rc && v != best.cell_permille) { Knobs c = best; c.cell_permille = v; rc = consider(c); }
     }
+    if (ctx->screening)
+        for (int v : {4, 8, 16, 32}) if (!rc && v != best.item_cols) { Knobs c = best; c.item_cols = v; rc = consider(c); }
     for (int v : {64, 96, 128}) if (!rc && v != best.prop_block) { Knobs c = best; c.prop_block = v; rc = consider(c); }
 
     // Leave the chosen configuration in place and the simulation untouched.
@@ -1190,6 +1194,7 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
         out->box_min_rows = best.box_rows;
         out->cell_scale_permille = best.cell_permille;
         out->prop_block = best.prop_block;
+        out->item_col_blocks = best.item_cols;
         out->trials = trials;
         out->ms_per_step_start = first_ms;
         out->ms_per_step_best = best_ms;

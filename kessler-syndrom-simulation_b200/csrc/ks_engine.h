@@ -58,7 +58,6 @@ enum : int {
     FLAG_TIMEOUT = 32,       // a bounded device-side wait gave up
 };
 
-constexpr int kColBlocksPerItem = 16;  // column blocks of 32 per pair work item
 
 // Per-step control block, device resident.
 struct Ctrl {
@@ -146,6 +145,7 @@ struct Tuning {
     int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
     double cell_scale = 1.0;      // cell edge = reference edge x this (>= 1; changes only candidate counts)
     int prop_block = 128;         // threads per block of the propagation kernels (32..128, multiple of 32)
+    int item_col_blocks = 16;     // column blocks of 32 per pair work item (1..64)
 };
 
 // Everything a step's kernels need, by value.

@@ -902,8 +902,8 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
 }
 
 // Number of work items of row block a: its column blocks a .. tc-1 in groups.
-__device__ __forceinline__ unsigned int row_block_items(int a, int tc) {
-    return static_cast<unsigned int>((tc - a + kColBlocksPerItem - 1) / kColBlocksPerItem);
+__device__ __forceinline__ unsigned int row_block_items(int a, int tc, int per) {
+    return static_cast<unsigned int>((tc - a + per - 1) / per);
 }
 
 // Warp per cell: the length L of the cell's column list (own objects plus the
@@ -912,7 +912,7 @@ __device__ __forceinline__ unsigned int row_block_items(int a, int tc) {
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr,
                                                         unsigned int* __restrict__ item_count,
-                                                        int* __restrict__ cell_len) {
+                                                        int* __restrict__ cell_len, int per) {
     const int nc = ctrl->n_cells;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -930,7 +930,7 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
         const int L = k + other;
         const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
         unsigned int items = 0;
-        for (int a = lane; a < ta; a += 32) items += row_block_items(a, tc);
+        for (int a = lane; a < ta; a += 32) items += row_block_items(a, tc, per);
         items = warp_sum(items);
         if (lane == 0) {
             item_count[c] = items;
@@ -950,7 +950,7 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
 __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ item_off,
-                                                        int4* __restrict__ items, int64_t items_cap) {
+                                                        int4* __restrict__ items, int64_t items_cap, int per) {
     const int nc = ctrl->n_cells;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -962,15 +962,15 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
         int64_t base = item_off[c];
         for (int a0 = 0; a0 < ta; a0 += 32) {
             const int a = a0 + lane;
-            const unsigned int mine = a < ta ? row_block_items(a, tc) : 0u;
+            const unsigned int mine = a < ta ? row_block_items(a, tc, per) : 0u;
             unsigned int incl = mine;
             for (int o = 1; o < 32; o <<= 1) {
                 const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
             int64_t w = base + (incl - mine);
-            for (int cb = a; a < ta && cb < tc; cb += kColBlocksPerItem, ++w) {
-                if (w < items_cap) items[w] = make_int4(c, a, cb, min(kColBlocksPerItem, tc - cb));
+            for (int cb = a; a < ta && cb < tc; cb += per, ++w) {
+                if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
                 else over = true;
             }
             base += __shfl_sync(0xffffffffu, incl, 31);
@@ -1794,15 +1794,15 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
                                                a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
-    k_items_count<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr,
-                                                                                      b.item_count, b.cell_len);
+    k_items_count<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
+        a.ctrl, b.cell_begin, b.nbr, b.item_count, b.cell_len, a.tune.item_col_blocks);
     // Offsets of each cell's work items, and their total.
     const int st = static_cast<int>((b.cap + kScanTile - 1) / kScanTile);
     k_scan_partials<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
     k_scan_small<<<1, 1024, 0, stream>>>(b.scan_part, st, reinterpret_cast<unsigned int*>(&a.ctrl->n_items));
     k_scan_apply<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
     k_items_write<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
-        a.ctrl, b.cell_begin, b.cell_len, b.item_count, b.items, b.items_cap);
+        a.ctrl, b.cell_begin, b.cell_len, b.item_count, b.items, b.items_cap, a.tune.item_col_blocks);
 }
 
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
