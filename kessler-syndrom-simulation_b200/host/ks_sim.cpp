@@ -1,7 +1,11 @@
 // ks_sim: the reference CLI's screened step loop (src/main.cpp:346-407) on
 // the B200 engine, with the same inputs and the same output files.
 //
-//   ks_sim [catalogue] [duration_h] [dt_s] [options]
+//   ks_sim [catalogue] [duration_h] [dt_s] [out_every_s] [ids] [options]
+//     out_every_s          write DIR/snapshot_<k>.csv every out_every_s seconds (0 = final state only)
+//     ids                  comma-separated ids: instead of snapshots, their positions go to
+//                          DIR/trajectories.csv and the Moon's to DIR/moon.csv (every out_every_s,
+//                          default 60 s)
 //     --conj-km X          conjunction threshold, km (default 5)
 //     --radius-scale S     multiplies every collision radius (default 1)
 //     --min-vrel V         minimum encounter speed, m/s (default 10)
@@ -24,8 +28,9 @@
 // 11-16; sizes from the RCS class, src/core/orbital.cpp:136-170) and the
 // common epoch of its header (src/core/orbital.cpp:172-188). Writes
 // DIR/conjunctions.csv and DIR/final_state.csv in the reference's formats
-// (src/main.cpp:264-266, 395-400; src/core/orbital.cpp:190-197), and with
+// (src/main.cpp:264-266, 395-400; src/core/orbital.cpp:190-197), with
 // fragmentation DIR/breakups.csv and DIR/population.csv (src/main.cpp:283-333),
+// and the periodic snapshots or trajectories of src/main.cpp:185-235, 437-447,
 // so the files can be diffed against the reference's.
 #include <algorithm>
 #include <chrono>
@@ -219,6 +224,13 @@ int main(int argc, char** argv) {
     const std::string path = pos.size() > 0 ? pos[0] : "data/satellites_20260801_1000Z.txt";
     const double duration = (pos.size() > 1 ? std::atof(pos[1].c_str()) : 24.0) * 3600.0;
     const double dt = pos.size() > 2 ? std::atof(pos[2].c_str()) : 10.0;
+    const double out_every = pos.size() > 3 ? std::atof(pos[3].c_str()) : 0.0;
+    std::vector<int> track_ids;
+    if (pos.size() > 4) {
+        std::stringstream ss(pos[4]);
+        std::string tok;
+        while (std::getline(ss, tok, ',')) track_ids.push_back(std::atoi(tok.c_str()));
+    }
 
     int dropped = 0;
     const std::vector<CatalogObject> objs = load_catalog(path, &dropped);
@@ -261,6 +273,11 @@ int main(int argc, char** argv) {
         cfg.threshold_km = max_size * 1e-3 * cfg.radius_scale;
     }
     const long steps = static_cast<long>(std::ceil(duration / dt));
+    long next_out = out_every > 0 ? static_cast<long>(out_every / dt) : 0;
+    std::vector<size_t> tracked;
+    for (size_t i = 0; i < n; ++i)
+        if (std::find(track_ids.begin(), track_ids.end(), objs[i].id) != track_ids.end()) tracked.push_back(i);
+    if (!track_ids.empty() && next_out == 0) next_out = std::max(1L, static_cast<long>(60.0 / dt));
 
     // Object names and ids, extended as fragments appear (src/core/breakup.cpp:295-303).
     std::vector<int> ids(n);
@@ -285,6 +302,45 @@ int main(int argc, char** argv) {
         }
 
         std::filesystem::create_directories(out_dir);
+        if (next_out > 0 && track_ids.empty()) {
+            // Snapshots of an earlier run would mix with this one's (src/main.cpp:207-219).
+            std::error_code ec;
+            for (const auto& e : std::filesystem::directory_iterator(out_dir, ec)) {
+                const std::string fn = e.path().filename().string();
+                if (fn.rfind("snapshot_", 0) == 0 && e.path().extension() == ".csv") std::filesystem::remove(e.path(), ec);
+            }
+        }
+        std::ofstream traj, moon_out;
+        if (!track_ids.empty()) {
+            traj.open(out_dir + "/trajectories.csv");
+            traj << "t_s,id,name,x_km,y_km,z_km\n";
+            moon_out.open(out_dir + "/moon.csv");
+            moon_out << "t_s,x_km,y_km,z_km\n";
+        }
+        std::vector<double> snap_states;
+        std::vector<uint8_t> snap_alive;
+        long snap_index = 0;
+        // Positions of the tracked objects and of the Moon (src/main.cpp:222-233).
+        auto record = [&](double t, const std::vector<double>& st) {
+            for (size_t i : tracked)
+                traj << t << ',' << ids[i] << ',' << names[i] << ',' << st[6 * i] << ',' << st[6 * i + 1] << ','
+                     << st[6 * i + 2] << '\n';
+            double m[3];
+            ks_moon_position(epoch + t / 86400.0, m);
+            moon_out << t << ',' << m[0] << ',' << m[1] << ',' << m[2] << '\n';
+        };
+        auto write_states = [&](const std::string& file, double t, const std::vector<double>& st,
+                                const std::vector<uint8_t>& al) {
+            std::ofstream snap(file);
+            snap << "# t = " << t << " s apres l'epoch\nid,x_km,y_km,z_km,vx,vy,vz,alive\n";
+            snap.precision(9);
+            for (size_t i = 0; i < al.size(); ++i) {
+                snap << ids[i];
+                for (int q = 0; q < 6; ++q) snap << ',' << st[6 * i + q];
+                snap << ',' << (al[i] ? 1 : 0) << '\n';
+            }
+        };
+        if (!tracked.empty()) record(0.0, states);
         std::ofstream conj_out(out_dir + "/conjunctions.csv");
         conj_out << "t_s,id1,id2,name1,name2,miss_km,v_rel_km_s,collision\n";
         conj_out << std::setprecision(10);
@@ -372,6 +428,7 @@ int main(int argc, char** argv) {
                         k = q - done;
                         break;
                     }
+            if (next_out > 0) k = std::min(k, next_out - done % next_out);
             sim.advance(k);
             done += k;
             take_events();
@@ -394,20 +451,20 @@ int main(int argc, char** argv) {
                 last_hour = static_cast<long>(t_before[static_cast<size_t>(done)] / 3600.0);
                 log_population();
             }
+            if (next_out > 0 && done % next_out == 0) {
+                sim.get_population(snap_states, snap_alive);
+                if (!tracked.empty()) record(sim.time(), snap_states);
+                else
+                    write_states(out_dir + "/snapshot_" + std::to_string(snap_index++) + ".csv", sim.time(),
+                                 snap_states, snap_alive);
+            }
         }
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 
         std::vector<double> fs;
         std::vector<uint8_t> fa;
         sim.get_population(fs, fa);
-        std::ofstream snap(out_dir + "/final_state.csv");
-        snap << "# t = " << sim.time() << " s apres l'epoch\nid,x_km,y_km,z_km,vx,vy,vz,alive\n";
-        snap.precision(9);
-        for (size_t i = 0; i < fa.size(); ++i) {
-            snap << ids[i];
-            for (int q = 0; q < 6; ++q) snap << ',' << fs[6 * i + q];
-            snap << ',' << (fa[i] ? 1 : 0) << '\n';
-        }
+        write_states(out_dir + "/final_state.csv", sim.time(), fs, fa);
 
         std::cout << "conjunctions below " << cfg.threshold_km << " km: " << n_conj << " (collisions " << n_coll
                   << ")\n";

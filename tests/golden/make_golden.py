@@ -25,6 +25,8 @@ Fixtures:
   run_breakup.npz    the CLI loop with --breakup through the reference's
                      Fragmentation (planted collisions, a forced impact),
                      every object's final state and properties, events
+  cli_snapshot_ref.json  SHA-256 of the reference CLI's periodic snapshots and
+                     of its trajectories.csv / moon.csv for tracked ids
   cli_breakup_*      a 2 000-object catalogue of mixed object types and the
                      four files the reference CLI writes for it with --breakup
                      and --impact over 1.2 h
@@ -269,6 +271,33 @@ def cli_breakup_golden():
           "conjunctions")
 
 
+CLI_SNAPSHOT_RUNS = {
+    "snapshots": ["0.25", "10", "300", "--conj-km", "5"],
+    "tracks": ["0.25", "10", "120", "100001,100007,100050,100399", "--conj-km", "5"],
+}
+
+
+def cli_snapshot_golden():
+    """SHA-256 of the files the reference CLI writes with periodic snapshots
+    (positional out_every) and with tracked ids (trajectories.csv, moon.csv)
+    for cli_catalog.txt; the files themselves are not kept."""
+    import hashlib
+    cat = os.path.join(HERE, "cli_catalog.txt")
+    exe = os.path.join(ROOT, "oracle", "_ref", "kessler_sim")
+    out = {}
+    for name, args in CLI_SNAPSHOT_RUNS.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            subprocess.run([exe, cat] + args + ["--threads", "8"], cwd=tmp, capture_output=True, text=True,
+                           check=True)
+            files = sorted(f for f in os.listdir(os.path.join(tmp, "output"))
+                           if f.startswith(("snapshot_", "trajectories", "moon")))
+            out[name] = {"args": args, "sha256": {f: hashlib.sha256(open(os.path.join(tmp, "output", f), "rb").read())
+                                                  .hexdigest() for f in files}}
+    with open(os.path.join(HERE, "cli_snapshot_ref.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("cli snapshot golden:", {k: sorted(v["sha256"]) for k, v in out.items()})
+
+
 def main():
     checkers.build(ref=True)
     st, sz, al = population(20260801, 1500, 3000, 3, 7200.0)
@@ -281,6 +310,7 @@ def main():
     screen_cases()
     cli_golden()
     cli_breakup_golden()
+    cli_snapshot_golden()
     breakup_run()
     if os.path.exists(CATALOG):
         catalogue_kat()

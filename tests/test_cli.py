@@ -80,3 +80,21 @@ def test_cli_breakup_matches_reference_cli_files(tmp_path, spg):
         got = open(tmp_path / name).read()
         want = open(golden_path("cli_breakup_ref_" + name)).read()
         assert got == want, name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("run", ["snapshots", "tracks"])
+def test_cli_snapshots_match_reference_cli(tmp_path, run):
+    # tests/golden/cli_snapshot_ref.json: SHA-256 of the reference CLI's periodic
+    # snapshot files, or of its trajectories.csv and moon.csv for tracked ids.
+    import hashlib
+    import json
+    ref = json.load(open(golden_path("cli_snapshot_ref.json")))[run]
+    exe = os.path.join(PKG, "ks_sim")
+    out = subprocess.run([exe, golden_path("cli_catalog.txt")] + ref["args"] + ["--out", str(tmp_path)],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    got = sorted(f for f in os.listdir(tmp_path) if f.startswith(("snapshot_", "trajectories", "moon")))
+    assert got == sorted(ref["sha256"])
+    for f in got:
+        assert hashlib.sha256(open(tmp_path / f, "rb").read()).hexdigest() == ref["sha256"][f], f
