@@ -172,6 +172,18 @@ int64_t ks_sbm_impact(uint64_t seed, double lc_m, double catastrophic_j_per_g, c
                       double target_mass_kg, double target_size_m, double projectile_mass_kg, double v_rel_km_s,
                       double t, ks_breakup_event* event, double* frag_states, double* frag_size, double* frag_mass,
                       double* frag_area_to_mass, int64_t cap, double* target_after);
+/* Population file (no counterpart in the reference, whose catalogue format
+ * carries neither sizes, masses nor fragment provenance, and whose snapshots,
+ * src/core/orbital.cpp:190-197, keep only states at 9 digits): writes the
+ * resident population bit for bit - states, alive flags, sizes, masses,
+ * area-to-mass ratios, originating events, realisations - with the clock and
+ * the fragmentation configuration and random streams, so that
+ * ks_load_population resumes the run exactly (same states, conjunctions and
+ * fragments as an uninterrupted run). Conjunctions, counters and breakup
+ * events not yet taken are not saved. Little-endian binary: a "KSPOPv1"
+ * header, then the per-object arrays, then the random streams. */
+int ks_save_population(ks_ctx* ctx, const char* path);
+int ks_load_population(ks_ctx* ctx, const char* path);
 /* Fragmentation events since the last take, in the order they happened
  * (same conventions as ks_take_conjunctions). */
 int ks_take_breakups(ks_ctx* ctx, ks_breakup_event* out, int64_t cap, int64_t* count);

@@ -11,6 +11,7 @@ benchmark. The reference-facing C++ drop-in lives in host/kessler_b200.hpp.
     conj = eng.take_conjunctions()              # sorted by (t, i, j)
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -185,6 +186,13 @@ class Engine:
 
     def impact(self, target, projectile_mass_kg=10.0, v_rel_km_s=10.0):
         self._check(self._lib.ks_impact(self._h, int(target), float(projectile_mass_kg), float(v_rel_km_s)))
+
+    def save_population(self, path):
+        """Writes the resident population, clock and fragmentation streams to `path` (exact resume)."""
+        self._check(self._lib.ks_save_population(self._h, os.fspath(path).encode()))
+
+    def load_population(self, path):
+        self._check(self._lib.ks_load_population(self._h, os.fspath(path).encode()))
 
     def take_breakups(self):
         cnt = C.c_int64()

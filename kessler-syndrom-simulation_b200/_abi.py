@@ -80,6 +80,8 @@ SIGNATURES = {
     "ks_set_masses": (C.c_int, [_P, _I64, _P]),
     "ks_impact": (C.c_int, [_P, _I64, _D, _D]),
     "ks_take_breakups": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
+    "ks_save_population": (C.c_int, [_P, C.c_char_p]),
+    "ks_load_population": (C.c_int, [_P, C.c_char_p]),
     "ks_sbm_impact": (_I64, [C.c_uint64, _D, _D, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P, _P, _I64, _P]),
     "ks_get_objects": (C.c_int, [_P, _I64, _P, _P, _P, _P, _P]),
     "ks_screen": (C.c_int, [_P, _I64, _P, _P, _P, _P, _D, _D, _P, _I64, C.POINTER(_I64), _P]),

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <sstream>
 
 #include "ks_host.h"
 
@@ -54,6 +55,21 @@ double draw_log_area_to_mass(SbmRng& rng, double lam) {
 double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 }  // namespace
+
+std::string SbmRng::state() const {
+    std::ostringstream os;
+    os << engine_;
+    return os.str();
+}
+
+bool SbmRng::set_state(const std::string& text) {
+    std::istringstream is(text);
+    std::mt19937_64 e;
+    is >> e;
+    if (!is) return false;
+    engine_ = e;
+    return true;
+}
 
 double SbmRng::uniform() { return static_cast<double>(engine_() >> 11) * 0x1.0p-53; }
 

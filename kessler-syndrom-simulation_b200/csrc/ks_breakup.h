@@ -20,6 +20,7 @@
 
 #include <cstdint>
 #include <random>
+#include <string>
 #include <vector>
 
 #include "ks_records.h"
@@ -33,6 +34,8 @@ public:
     double uniform();              // [0, 1), 53 bits
     double normal();               // N(0, 1), Box-Muller on (1 - u1, u2)
     long long poisson(double mean);  // Knuth below a mean of 10, Hormann's PTRS above
+    std::string state() const;                // engine state, as the standard library prints it
+    bool set_state(const std::string& text);  // restores a printed state
 
 private:
     std::mt19937_64 engine_;

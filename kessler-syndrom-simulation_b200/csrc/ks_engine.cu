@@ -14,7 +14,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <set>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -803,6 +805,36 @@ int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_
 
 }  // namespace
 
+namespace {
+
+// Population file: header, then per-object arrays, then the fragmentation
+// streams (Mersenne Twister state as the C++ standard library prints it).
+constexpr char kPopMagic[8] = {'K', 'S', 'P', 'O', 'P', 'v', '1', '\0'};
+
+struct PopHeader {
+    char magic[8];
+    int64_t n;
+    int32_t realisations, streams;
+    double epoch_jd, t, dt;
+    int64_t steps_done;
+    int32_t breakup_on, pad;
+    double lc_m, catastrophic_j_per_g;
+    uint64_t seed;
+};
+
+template <typename T>
+bool put(std::ofstream& f, const T* p, size_t count) {
+    f.write(reinterpret_cast<const char*>(p), static_cast<std::streamsize>(sizeof(T) * count));
+    return static_cast<bool>(f);
+}
+template <typename T>
+bool get(std::ifstream& f, T* p, size_t count) {
+    f.read(reinterpret_cast<char*>(p), static_cast<std::streamsize>(sizeof(T) * count));
+    return static_cast<bool>(f);
+}
+
+}  // namespace
+
 extern "C" {
 
 int ks_create(int device, ks_ctx** out) {
@@ -1358,6 +1390,120 @@ int64_t ks_sbm_impact(uint64_t seed, double lc_m, double catastrophic_j_per_g, c
         target_after[1] = oc.reduce_target && tgt.index == 0 ? oc.target_mass_after : target_mass_kg;
     }
     return m;
+}
+
+int ks_save_population(ks_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, KS_ERR_ARG, "ks_save_population: bad arguments");
+    if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_save_population: no population");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_mirrors(ctx);
+    if (rc) return rc;
+    const size_t n = static_cast<size_t>(ctx->n);
+    std::vector<double> st(6 * n);
+    std::vector<uint8_t> al(n);
+    if (n > 0) {
+        KS_CUDA(cudaMemcpyAsync(st.data(), ctx->b.state[ctx->cur], sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(al.data(), ctx->b.alive[ctx->cur], n, cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    const ks_ctx::Breakup& k = ctx->bk;
+    PopHeader h{};
+    std::memcpy(h.magic, kPopMagic, 8);
+    h.n = ctx->n;
+    h.realisations = ctx->realisations;
+    h.streams = static_cast<int32_t>(k.rng.size());
+    h.epoch_jd = ctx->epoch_jd;
+    h.t = ctx->t;
+    h.dt = ctx->dt;
+    h.steps_done = ctx->steps_done;
+    h.breakup_on = k.on ? 1 : 0;
+    h.lc_m = k.params.lc_m;
+    h.catastrophic_j_per_g = k.params.catastrophic_j_per_g;
+    h.seed = k.seed;
+    std::ofstream f(path, std::ios::binary | std::ios::trunc);
+    bool ok = static_cast<bool>(f) && put(f, &h, 1) && put(f, st.data(), 6 * n) && put(f, al.data(), n) &&
+              put(f, k.size_m.data(), n) && put(f, k.mass_kg.data(), n) && put(f, k.area_to_mass.data(), n) &&
+              put(f, k.event.data(), n) && put(f, k.rid.data(), n);
+    for (size_t r = 0; ok && r < k.rng.size(); ++r) {
+        const std::string text = k.rng[r].state();
+        const int32_t ne = k.next_event[r];
+        const uint32_t len = static_cast<uint32_t>(text.size());
+        ok = put(f, &ne, 1) && put(f, &len, 1) && put(f, text.data(), len);
+    }
+    if (!ok) return fail(ctx, KS_ERR_ARG, std::string("ks_save_population: cannot write ") + path);
+    return KS_OK;
+}
+
+int ks_load_population(ks_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, KS_ERR_ARG, "ks_load_population: bad arguments");
+    std::ifstream f(path, std::ios::binary);
+    PopHeader h{};
+    if (!f || !get(f, &h, 1) || std::memcmp(h.magic, kPopMagic, 8) != 0)
+        return fail(ctx, KS_ERR_ARG, std::string("ks_load_population: not a population file: ") + path);
+    if (h.n < 0 || h.n > (int64_t(1) << 30) || h.realisations < 1 || h.realisations > 65535 || h.streams < 0 ||
+        h.streams > h.realisations || !(h.dt > 0.0))
+        return fail(ctx, KS_ERR_ARG, "ks_load_population: inconsistent header");
+    const size_t n = static_cast<size_t>(h.n);
+    std::vector<double> st(6 * n), size_m(n), mass(n), a2m(n);
+    std::vector<uint8_t> al(n);
+    std::vector<int32_t> ev(n);
+    std::vector<uint16_t> rid(n);
+    bool ok = get(f, st.data(), 6 * n) && get(f, al.data(), n) && get(f, size_m.data(), n) && get(f, mass.data(), n) &&
+              get(f, a2m.data(), n) && get(f, ev.data(), n) && get(f, rid.data(), n);
+    std::vector<ks::SbmRng> rngs;
+    std::vector<int32_t> next_event;
+    for (int32_t r = 0; ok && r < h.streams; ++r) {
+        int32_t ne = 0;
+        uint32_t len = 0;
+        ok = get(f, &ne, 1) && get(f, &len, 1) && len < (1u << 20);
+        std::string text(ok ? len : 0, '\0');
+        ok = ok && (len == 0 || get(f, &text[0], len));
+        ks::SbmRng g;
+        ok = ok && g.set_state(text);
+        rngs.push_back(g);
+        next_event.push_back(ne);
+    }
+    for (size_t i = 0; ok && i < n; ++i) ok = rid[i] < h.realisations;
+    if (!ok) return fail(ctx, KS_ERR_ARG, std::string("ks_load_population: truncated or corrupt file: ") + path);
+    cudaSetDevice(ctx->device);
+    int rc = ensure_objects(ctx, h.n);
+    if (rc) return rc;
+    ctx->n = h.n;
+    ctx->cur = 0;
+    ctx->realisations = h.realisations;
+    int rbits = 0;
+    while ((1 << rbits) < h.realisations) ++rbits;
+    ctx->rbits = rbits;
+    ctx->offsets.assign({0, h.n});
+    drop_graphs(ctx);
+    rc = upload_population(ctx, h.n, st.data(), size_m.data(), al.data(), 0);
+    if (rc) return rc;
+    if (n > 0) KS_CUDA(cudaMemcpyAsync(ctx->b.real_id, rid.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->epoch_jd = h.epoch_jd;
+    ctx->t = h.t;
+    ctx->dt = h.dt;
+    ctx->steps_done = h.steps_done;
+    ks_ctx::Breakup& k = ctx->bk;
+    reset_breakup_run(ctx);
+    k.on = h.breakup_on != 0;
+    k.params.lc_m = h.lc_m;
+    k.params.catastrophic_j_per_g = h.catastrophic_j_per_g;
+    k.seed = h.seed;
+    k.rng = std::move(rngs);
+    k.next_event = std::move(next_event);
+    k.size_m = std::move(size_m);
+    k.mass_kg = std::move(mass);
+    k.area_to_mass = std::move(a2m);
+    k.event = std::move(ev);
+    k.rid = std::move(rid);
+    k.mirrors = true;
+    rc = seed_speculation(ctx);
+    if (rc) return rc;
+    ctx->has_pop = true;
+    ctx->conj_out.clear();
+    ctx->stats_out.clear();
+    return KS_OK;
 }
 
 int ks_take_breakups(ks_ctx* ctx, ks_breakup_event* out, int64_t cap, int64_t* count) {

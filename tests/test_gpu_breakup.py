@@ -113,3 +113,51 @@ def test_breakup_off_leaves_collisions_alone(engine, oracle):
     assert_same_conj(conj, want[2])
     assert conj["collision"].sum() > 0 and len(engine.take_breakups()) == 0
     assert engine.get_population()[0].shape[0] == len(fx["states"])
+
+
+def test_population_file_resumes_the_run_exactly(engine, ks, tmp_path):
+    # Save after 13 steps (fragments of the forced impact and of a planted
+    # collision already in), resume in a fresh context, finish the 40 steps:
+    # the same final population, properties and later events as the reference's
+    # uninterrupted run.
+    fx = load()
+    engine.set_steps_per_graph(16)
+    engine.set_clock(float(fx["epoch_jd"]), 0.0, float(fx["dt"]))
+    engine.set_screening(True, float(fx["threshold_km"]), float(fx["radius_scale"]), float(fx["min_vrel_km_s"]))
+    engine.set_population(fx["states"], fx["size_m"], fx["alive"])
+    engine.set_masses(fx["mass_kg"])
+    engine.set_breakup(True, float(fx["lc_m"]), 40.0, int(fx["seed"]))
+    idx, mass, vrel, step = fx["impact"]
+    engine.run(int(step))
+    engine.impact(int(idx), float(mass), float(vrel))
+    engine.run(13 - int(step))
+    first = engine.take_breakups()
+    engine.take_conjunctions()
+    engine.take_step_stats()
+    path = tmp_path / "mid.kspop"
+    engine.save_population(path)
+    engine.set_breakup(False)
+    other = ks.Engine(0)
+    try:
+        other.set_steps_per_graph(7)
+        other.set_screening(True, float(fx["threshold_km"]), float(fx["radius_scale"]), float(fx["min_vrel_km_s"]))
+        other.load_population(path)
+        assert other.clock() == engine.clock()
+        other.run(int(fx["steps"]) - 13)
+        fs, fa = other.get_population()
+        props = other.objects()
+        events = np.concatenate([first, other.take_breakups()])
+    finally:
+        other.close()
+    assert np.array_equal(fs, fx["out_states"]) and np.array_equal(fa, fx["out_alive"])
+    for k in ("size_m", "mass_kg", "area_to_mass", "event"):
+        assert np.array_equal(props[k], fx["out_" + k]), k
+    for f in EVENT_FIELDS:
+        assert np.array_equal(events[f], fx["out_events"][f]), f
+
+
+def test_population_file_rejects_other_files(engine, tmp_path):
+    bad = tmp_path / "bad.kspop"
+    bad.write_bytes(b"not a population file")
+    with pytest.raises(Exception):
+        engine.load_population(bad)
