@@ -295,6 +295,36 @@ def launches_per_step(sort_passes):
     return 1 + 1 + (2 + sort_passes) + 8 + 1 + 1
 
 
+BORDER_TOL_KM = 1e-5  # 1 cm: the agreement the plain form is held to after 24 h
+
+
+def borderline_pairs(c_head, c_other, size_m, thr_km, head_is_split, tol_km=BORDER_TOL_KM, listed=20):
+    """Conjunctions of either precision whose miss distance lies within tol of the
+    threshold or of the pair's radius sum (where the two paths may decide
+    differently), counted and listed separately, with both miss distances."""
+    split_c, fp64_c = (c_head, c_other) if head_is_split else (c_other, c_head)
+
+    def near(c):
+        rsum = 0.5e-3 * (size_m[c["i"]] + size_m[c["j"]])
+        m = c["miss_km"]
+        return (np.abs(m - thr_km) < tol_km) | (np.abs(m - rsum) < tol_km)
+
+    keys = set()
+    for c in (split_c, fp64_c):
+        sel = c[near(c)]
+        keys.update(zip(sel["i"].tolist(), sel["j"].tolist(), sel["step"].tolist()))
+
+    def miss_of(c, key):
+        hit = c[(c["i"] == key[0]) & (c["j"] == key[1]) & (c["step"] == key[2])]
+        return float(hit["miss_km"][0]) if len(hit) else None
+
+    rows = [{"i": k[0], "j": k[1], "step": k[2], "miss_km_split": miss_of(split_c, k), "miss_km_fp64": miss_of(fp64_c, k),
+             "radius_sum_km": 0.5e-3 * float(size_m[k[0]] + size_m[k[1]])} for k in sorted(keys, key=lambda k: (k[2], k[0], k[1]))]
+    only = [r for r in rows if r["miss_km_split"] is None or r["miss_km_fp64"] is None]
+    return {"borderline": {"tolerance_km": tol_km, "count": len(rows), "in_one_set_only": len(only),
+                           "listed": (only + [r for r in rows if r not in only])[:listed]}}
+
+
 def error_study(ks, eng, a, st, al):
     """Split vs FP64 propagation of the whole population: position and velocity
     differences at 1, 6 and 24 h (the FP64 path is bit-identical to the reference)."""
@@ -381,9 +411,11 @@ def main():
                             -(-a.steps // max(1, a.steps_per_graph)),
             "roofline": main_s["roofline"], "clocks": clk,
             "fp64" if head == ks.PRECISION_SPLIT else "split": other_s,
-            "conjunction_sets": {"split_only": len(split_set - fp64_set), "fp64_only": len(fp64_set - split_set),
-                                 "common": len(split_set & fp64_set),
-                                 "over": f"the {a.steps} timed steps, pairs matched by (i, j, step)"},
+            "conjunction_sets": dict(
+                {"split_only": len(split_set - fp64_set), "fp64_only": len(fp64_set - split_set),
+                 "common": len(split_set & fp64_set),
+                 "over": f"the {a.steps} timed steps, pairs matched by (i, j, step)"},
+                **borderline_pairs(c_head, c_other, sz, a.conj_km, head == ks.PRECISION_SPLIT)),
             "refined_pairs_per_step": main_s["refined_pairs_per_step"],
             "wall_s_timed_region": main_s["wall_s_timed_region"]}
     if not a.no_error_study:
