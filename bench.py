@@ -301,7 +301,9 @@ BORDER_TOL_KM = 1e-5  # 1 cm: the agreement the plain form is held to after 24 h
 def borderline_pairs(c_head, c_other, size_m, thr_km, head_is_split, tol_km=BORDER_TOL_KM, listed=20):
     """Conjunctions of either precision whose miss distance lies within tol of the
     threshold or of the pair's radius sum (where the two paths may decide
-    differently), counted and listed separately, with both miss distances."""
+    differently), counted and listed separately with both miss distances; and
+    every pair found by one precision only, with its miss distance and TCA
+    fraction of the step (the refinement drops TCAs within 1e-9 of a step edge)."""
     split_c, fp64_c = (c_head, c_other) if head_is_split else (c_other, c_head)
 
     def near(c):
@@ -321,8 +323,17 @@ def borderline_pairs(c_head, c_other, size_m, thr_km, head_is_split, tol_km=BORD
     rows = [{"i": k[0], "j": k[1], "step": k[2], "miss_km_split": miss_of(split_c, k), "miss_km_fp64": miss_of(fp64_c, k),
              "radius_sum_km": 0.5e-3 * float(size_m[k[0]] + size_m[k[1]])} for k in sorted(keys, key=lambda k: (k[2], k[0], k[1]))]
     only = [r for r in rows if r["miss_km_split"] is None or r["miss_km_fp64"] is None]
+    ks_ = set(zip(split_c["i"].tolist(), split_c["j"].tolist(), split_c["step"].tolist()))
+    kf_ = set(zip(fp64_c["i"].tolist(), fp64_c["j"].tolist(), fp64_c["step"].tolist()))
+    one_set = []
+    for name, c, keys_only in (("split", split_c, ks_ - kf_), ("fp64", fp64_c, kf_ - ks_)):
+        for k in sorted(keys_only, key=lambda k: (k[2], k[0], k[1]))[:listed]:
+            hit = c[(c["i"] == k[0]) & (c["j"] == k[1]) & (c["step"] == k[2])][0]
+            one_set.append({"found_by": name, "i": k[0], "j": k[1], "step": k[2], "miss_km": float(hit["miss_km"]),
+                            "t": float(hit["t"]), "radius_sum_km": 0.5e-3 * float(size_m[k[0]] + size_m[k[1]])})
     return {"borderline": {"tolerance_km": tol_km, "count": len(rows), "in_one_set_only": len(only),
-                           "listed": (only + [r for r in rows if r not in only])[:listed]}}
+                           "listed": (only + [r for r in rows if r not in only])[:listed]},
+            "one_set_only": one_set}
 
 
 def error_study(ks, eng, a, st, al):

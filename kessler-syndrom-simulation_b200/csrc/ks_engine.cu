@@ -323,6 +323,7 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     a.ctrl = ctx->b.ctrl + k;
     a.ctrl_next = (k == k_steps - 1) ? carry_slot(ctx) : ctx->b.ctrl + k + 1;
     a.src = src;
+    a.hist = ctx->screening ? ctx->b.sort_hist : nullptr;  // the propagation counts the sort's digits
     return a;
 }
 
@@ -341,6 +342,7 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
         const StepArgs a = step_args(ctx, k, k_steps, src);
         if (ctx->l2_flush_bytes > 0) cudaMemsetAsync(ctx->l2_flush, k & 0xFF, ctx->l2_flush_bytes, s);
         record(ctx, k, 0, capturing);
+        if (a.hist) cudaMemsetAsync(a.hist, 0, sizeof(unsigned int) * 8 * 256, s);
         ks::launch_propagate(ctx->b, a, s);
         record(ctx, k, 1, capturing);
         if (ctx->screening) {
@@ -1569,6 +1571,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
     for (int attempt = 0;; ++attempt) {
         ks::launch_chunk_init(ctx->b, 1, ctx->stream);
         StepArgs a = step_args(ctx, 0, 1, 0);
+        a.hist = nullptr;  // keys come from k_screen_keys: the sort counts their digits itself
         ks::launch_seed_ctrl(ctx->b, static_cast<int>(n), 0, a.ctrl, 0, ctx->stream);
         ks::launch_screen_keys(ctx->b, a, ctx->stream);
         ks::launch_sort(ctx->b, a, ctx->stream);

@@ -56,6 +56,7 @@ enum : int {
     FLAG_KEY_RANGE = 8,      // a key fell outside its grid bounds
     FLAG_ITEMS_OVERFLOW = 16,  // pair work list longer than its buffer
     FLAG_TIMEOUT = 32,       // a bounded device-side wait gave up
+    FLAG_KEYS_REBUILT = 64,  // k_fix_keys rebuilt the keys: their digit histogram is recounted
 };
 
 
@@ -167,6 +168,7 @@ struct StepArgs {
     Ctrl* ctrl;                // this step's control block
     Ctrl* ctrl_next;           // next step's control block (speculation outputs)
     int src;                   // state buffer holding the start of the step (0 or 1)
+    unsigned int* hist;        // radix digit histogram the propagation fills with the keys it emits, or null
 };
 
 // Kernel launchers (ks_kernels.cu). All enqueue on `stream` and never synchronise.

@@ -286,6 +286,30 @@ __global__ void k_seed_ctrl(const double* __restrict__ st, const uint8_t* __rest
 // Propagation
 // ---------------------------------------------------------------------------
 
+// Radix digit histogram of the keys a block emits (all sort passes at once),
+// aggregated per warp with __match_any_sync and flushed once per block.
+__device__ __forceinline__ void hist_zero(unsigned int* sh, int passes) {
+    for (int t = threadIdx.x; t < passes * 256; t += blockDim.x) sh[t] = 0u;
+}
+// Called by all 32 lanes; `have` marks lanes holding a key. The top pass's
+// digits are nearly all equal, so that pass is aggregated over the warp; the
+// lower passes' digits are spread and go straight to shared atomics.
+__device__ __forceinline__ void warp_hist_add(unsigned int* sh, bool have, unsigned long long key, int passes,
+                                              int lane) {
+    for (int pass = 0; pass + 1 < passes; ++pass)
+        if (have) atomicAdd(&sh[pass * 256 + static_cast<unsigned>((key >> (8 * pass)) & 0xFF)], 1u);
+    const int top = passes - 1;
+    const unsigned d = have ? static_cast<unsigned>((key >> (8 * top)) & 0xFF) : 256u + lane;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (have && lane == __ffs(peers) - 1) atomicAdd(&sh[top * 256 + d], __popc(peers));
+}
+__device__ __forceinline__ void hist_flush(const unsigned int* sh, unsigned int* hist, int passes) {
+    for (int t = threadIdx.x; t < passes * 256; t += blockDim.x) {
+        const unsigned int v = sh[t];
+        if (v) atomicAdd(&hist[t], v);
+    }
+}
+
 __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, const double* __restrict__ in,
                                                             double* __restrict__ out,
                                                             const uint8_t* __restrict__ alive_in,
@@ -300,44 +324,63 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
         for (int q = 0; q < 3; ++q) moon[q] = a.sp->m[q];
         if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
     }
+    __shared__ unsigned int sh_hist[8 * 256];
+    const bool with_hist = a.screening && a.hist != nullptr;
+    if (with_hist) hist_zero(sh_hist, a.sort_passes);
     __syncthreads();
     const ForceConsts fc = a.fc;
     SpecAccum acc;
     acc.init();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        double s[6];
-        ld6(in, i, s);
-        if (!alive_in[i]) {
-            st6(out, i, s);
-            alive_out[i] = 0;
-            if (a.screening) keys[i] = dead_key(g);
-            continue;
-        }
-        acc.props += 1;
-        unsigned long long key = 0ull;
-        double vb = 0.0;
-        if (a.screening) {
-            key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
-            vb = xsqrt(xdot3(s[3], s[4], s[5]));
-        }
-        rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
-        st6(out, i, s);
-        // Re-entry (src/core/orbital.cpp:297).
-        const bool alive = !(xsqrt(xdot3(s[0], s[1], s[2])) < fc.r_earth);
-        alive_out[i] = alive ? 1 : 0;
-        if (alive) {
-            acc.alive += 1;
-            if (a.screening) {
-                acc.vtrue = fmax(acc.vtrue, vb);
-                acc.vnext = fmax(acc.vnext, xsqrt(xdot3(s[3], s[4], s[5])));
-                for (int q = 0; q < 3; ++q) {
-                    const unsigned long long e = enc_double(s[q]);
-                    acc.mn[q] = min(acc.mn[q], e);
-                    acc.mx[q] = max(acc.mx[q], e);
+    const int lane = threadIdx.x & 31;
+    // Warp-uniform loop (whole warps iterate together) so that the digit
+    // histogram can aggregate over the warp.
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += gridDim.x * blockDim.x) {
+        const int i = base + lane;
+        unsigned long long out_key = 0ull;
+        if (i < a.n) {
+            double s[6];
+            ld6(in, i, s);
+            if (!alive_in[i]) {
+                st6(out, i, s);
+                alive_out[i] = 0;
+                out_key = dead_key(g);
+            } else {
+                acc.props += 1;
+                unsigned long long key = 0ull;
+                double vb = 0.0;
+                if (a.screening) {
+                    key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
+                    vb = xsqrt(xdot3(s[3], s[4], s[5]));
                 }
+                rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
+                st6(out, i, s);
+                // Re-entry (src/core/orbital.cpp:297).
+                const bool alive = !(xsqrt(xdot3(s[0], s[1], s[2])) < fc.r_earth);
+                alive_out[i] = alive ? 1 : 0;
+                if (alive) {
+                    acc.alive += 1;
+                    if (a.screening) {
+                        acc.vtrue = fmax(acc.vtrue, vb);
+                        acc.vnext = fmax(acc.vnext, xsqrt(xdot3(s[3], s[4], s[5])));
+                        for (int q = 0; q < 3; ++q) {
+                            const unsigned long long e = enc_double(s[q]);
+                            acc.mn[q] = min(acc.mn[q], e);
+                            acc.mx[q] = max(acc.mx[q], e);
+                        }
+                    }
+                }
+                out_key = alive ? key : dead_key(g);
             }
+            if (a.screening) keys[i] = out_key;
         }
-        if (a.screening) keys[i] = alive ? key : dead_key(g);
+        if (with_hist) {
+            __syncwarp();
+            warp_hist_add(sh_hist, i < a.n, out_key, a.sort_passes, lane);
+        }
+    }
+    if (with_hist) {
+        __syncthreads();
+        hist_flush(sh_hist, a.hist, a.sort_passes);
     }
     flush_spec(acc, a.ctrl, a.ctrl_next, a.screening != 0);
 }
@@ -375,44 +418,61 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
         for (int q = 0; q < 3; ++q) moon[q] = to_f32(a.sp->m[q]);
         if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
     }
+    __shared__ unsigned int sh_hist[8 * 256];
+    const bool with_hist = a.screening && a.hist != nullptr;
+    if (with_hist) hist_zero(sh_hist, a.sort_passes);
     __syncthreads();
     const SplitConsts sc{-a.fc.neg_mu_earth, static_cast<float>(a.fc.k_j2), static_cast<float>(a.fc.mu_moon)};
     const double re2 = a.fc.r_earth * a.fc.r_earth;
     SpecAccum acc;
     acc.init();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        double s[6];
-        ld6(in, i, s);
-        if (!alive_in[i]) {
-            st6(out, i, s);
-            alive_out[i] = 0;
-            if (a.screening) keys[i] = dead_key(g);
-            continue;
-        }
-        acc.props += 1;
-        unsigned long long key = 0ull;
-        double vb = 0.0;
-        if (a.screening) {
-            key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
-            vb = xsqrt(xdot3(s[3], s[4], s[5]));
-        }
-        rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
-        st6(out, i, s);
-        const bool alive = !(fma(s[0], s[0], fma(s[1], s[1], s[2] * s[2])) < re2);
-        alive_out[i] = alive ? 1 : 0;
-        if (alive) {
-            acc.alive += 1;
-            if (a.screening) {
-                acc.vtrue = fmax(acc.vtrue, vb);
-                acc.vnext = fmax(acc.vnext, xsqrt(xdot3(s[3], s[4], s[5])));
-                for (int q = 0; q < 3; ++q) {
-                    const unsigned long long e = enc_double(s[q]);
-                    acc.mn[q] = min(acc.mn[q], e);
-                    acc.mx[q] = max(acc.mx[q], e);
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += gridDim.x * blockDim.x) {
+        const int i = base + lane;
+        unsigned long long out_key = 0ull;
+        if (i < a.n) {
+            double s[6];
+            ld6(in, i, s);
+            if (!alive_in[i]) {
+                st6(out, i, s);
+                alive_out[i] = 0;
+                out_key = dead_key(g);
+            } else {
+                acc.props += 1;
+                unsigned long long key = 0ull;
+                double vb = 0.0;
+                if (a.screening) {
+                    key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
+                    vb = xsqrt(xdot3(s[3], s[4], s[5]));
                 }
+                rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
+                st6(out, i, s);
+                const bool alive = !(fma(s[0], s[0], fma(s[1], s[1], s[2] * s[2])) < re2);
+                alive_out[i] = alive ? 1 : 0;
+                if (alive) {
+                    acc.alive += 1;
+                    if (a.screening) {
+                        acc.vtrue = fmax(acc.vtrue, vb);
+                        acc.vnext = fmax(acc.vnext, xsqrt(xdot3(s[3], s[4], s[5])));
+                        for (int q = 0; q < 3; ++q) {
+                            const unsigned long long e = enc_double(s[q]);
+                            acc.mn[q] = min(acc.mn[q], e);
+                            acc.mx[q] = max(acc.mx[q], e);
+                        }
+                    }
+                }
+                out_key = alive ? key : dead_key(g);
             }
+            if (a.screening) keys[i] = out_key;
         }
-        if (a.screening) keys[i] = alive ? key : dead_key(g);
+        if (with_hist) {
+            __syncwarp();
+            warp_hist_add(sh_hist, i < a.n, out_key, a.sort_passes, lane);
+        }
+    }
+    if (with_hist) {
+        __syncthreads();
+        hist_flush(sh_hist, a.hist, a.sort_passes);
     }
     flush_spec(acc, a.ctrl, a.ctrl_next, a.screening != 0);
 }
@@ -464,8 +524,14 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
     if (threadIdx.x == 0) {
         make_grid(__longlong_as_double(static_cast<long long>(vt)), a.ctrl->bb_min, a.ctrl->bb_max, a.dt,
                   a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
-        if (blockIdx.x == 0) a.ctrl->grid = g;
+        if (blockIdx.x == 0) {
+            a.ctrl->grid = g;
+            atomicOr(&a.ctrl->flags, FLAG_KEYS_REBUILT);
+        }
     }
+    // The propagation's digit histogram described the old keys: clear it for the recount.
+    if (blockIdx.x == 0 && a.hist)
+        for (int t = threadIdx.x; t < a.sort_passes * 256; t += blockDim.x) a.hist[t] = 0u;
     __syncthreads();
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
@@ -603,10 +669,14 @@ __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
 }
 
 // Digit histograms of every pass in one read of the keys.
+// only_if_rebuilt: the propagation already counted the digits; recount only
+// if k_fix_keys rebuilt the keys (it cleared the histogram then).
 __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long long* __restrict__ keys, int n,
                                                          const int* __restrict__ n_dev, int passes,
-                                                         unsigned int* __restrict__ hist, Ctrl* ctrl) {
+                                                         unsigned int* __restrict__ hist, const Ctrl* ctrl,
+                                                         int only_if_rebuilt) {
     __shared__ unsigned int h[8][256];
+    if (only_if_rebuilt && !(ctrl->flags & FLAG_KEYS_REBUILT)) return;
     if (n_dev) n = min(n, *n_dev);
     if (blockIdx.x * kSortTile >= n) return;
     for (int p = 0; p < 8; ++p) h[p][threadIdx.x] = 0;
@@ -628,12 +698,13 @@ __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long lon
         const unsigned int c = h[pass][threadIdx.x];
         if (c) atomicAdd(&hist[pass * 256 + threadIdx.x], c);
     }
-    if (ctrl && blockIdx.x == 0 && threadIdx.x == 0 && ctrl->grid.bits + 1 > 8 * passes)
-        atomicOr(&ctrl->flags, FLAG_SORT_BITS);
 }
 
-// Exclusive scan over the 256 digits of each pass.
-__global__ void __launch_bounds__(kBlock) k_sort_digit_scan(unsigned int* __restrict__ hist, int passes) {
+// Exclusive scan over the 256 digits of each pass; flags keys wider than the
+// passes cover (ctrl, if given).
+__global__ void __launch_bounds__(kBlock) k_sort_digit_scan(unsigned int* __restrict__ hist, int passes,
+                                                            Ctrl* ctrl) {
+    if (ctrl && threadIdx.x == 0 && ctrl->grid.bits + 1 > 8 * passes) atomicOr(&ctrl->flags, FLAG_SORT_BITS);
     for (int pass = 0; pass < passes; ++pass) {
         const unsigned int c = hist[pass * 256 + threadIdx.x];
         unsigned int tot;
@@ -1722,11 +1793,15 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     if (n <= 0) return;  // nothing alive: the cell build sees n_alive == 0
     const int ntiles = (n + kSortTile - 1) / kSortTile;
     const int passes = a.sort_passes;
-    cudaMemsetAsync(b.sort_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
+    // With a.hist the propagation counted the digits (launch_propagate's
+    // caller cleared the histogram before it); otherwise count them here.
+    const bool counted = a.hist != nullptr;
+    if (!counted) cudaMemsetAsync(b.sort_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
     cudaMemsetAsync(b.sort_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
-    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, nullptr, passes, b.sort_hist, a.ctrl);
-    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.sort_hist, passes);
+    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, nullptr, passes, b.sort_hist, a.ctrl,
+                                                  counted ? 1 : 0);
+    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.sort_hist, passes, a.ctrl);
     for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
@@ -1768,8 +1843,9 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
     cudaMemsetAsync(b.conj_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.conj_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * kPasses, stream);
     k_conj_keys<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_cap, chunk, t_start, span_s, b.conj_keys[0]);
-    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.conj_keys[0], cap, &chunk->sort_n, kPasses, b.conj_hist, nullptr);
-    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.conj_hist, kPasses);
+    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.conj_keys[0], cap, &chunk->sort_n, kPasses, b.conj_hist, nullptr,
+                                                  0);
+    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.conj_hist, kPasses, nullptr);
     for (int pass = 0; pass < kPasses; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
