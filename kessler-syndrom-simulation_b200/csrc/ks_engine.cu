@@ -66,6 +66,7 @@ struct ks_ctx {
     ks_timing timing{};
     ks::Tuning tune;
     bool ckpt_states = false;  // the checkpoint holds states (chunks of more than one step)
+    bool pack_keys = true;     // object index packed below the cell key in the sort keys
     int realisations = 1;
     int rbits = 0;
     std::vector<int64_t> offsets;  // realisation offsets (batches)
@@ -190,7 +191,7 @@ int ensure_items(ks_ctx* ctx, int64_t want) {
 void free_conj(ks_ctx* ctx) {
     ks::DeviceBuffers& b = ctx->b;
     dfree(b.conj);
-    for (int k = 0; k < 2; ++k) { dfree(b.conj_keys[k]); dfree(b.conj_idx[k]); }
+    for (int k = 0; k < 2; ++k) dfree(b.conj_keys[k]);
     dfree(b.conj_status); dfree(b.conj_hist); dfree(b.conj_ctr); dfree(b.conj_sorted);
     b.conj_cap = 0;
 }
@@ -204,10 +205,7 @@ int ensure_conj(ks_ctx* ctx, int64_t want) {
         const int64_t tiles = (want + 2047) / 2048;
         KS_CUDA(cudaMalloc(&b.conj, sizeof(ks_conjunction) * want));
         KS_CUDA(cudaMalloc(&b.conj_sorted, sizeof(ks_conjunction) * want));
-        for (int k = 0; k < 2; ++k) {
-            KS_CUDA(cudaMalloc(&b.conj_keys[k], sizeof(unsigned long long) * want));
-            KS_CUDA(cudaMalloc(&b.conj_idx[k], sizeof(int) * want));
-        }
+        for (int k = 0; k < 2; ++k) KS_CUDA(cudaMalloc(&b.conj_keys[k], sizeof(unsigned long long) * want));
         KS_CUDA(cudaMalloc(&b.conj_status, sizeof(unsigned int) * 256 * 4 * tiles));
         KS_CUDA(cudaMalloc(&b.conj_hist, sizeof(unsigned int) * 8 * 256));
         KS_CUDA(cudaMalloc(&b.conj_ctr, sizeof(unsigned int) * 8));
@@ -305,6 +303,13 @@ void fill_params(ks_ctx* ctx, int k_steps, double t_start, int64_t step0, double
     *t_end = t;
 }
 
+// Bits that hold every object index 0 .. n-1 (at least 1).
+int index_bits(int64_t n) {
+    int b = 1;
+    while ((int64_t(1) << b) < n) ++b;
+    return b;
+}
+
 StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     StepArgs a{};
     a.tune = ctx->tune;
@@ -324,6 +329,7 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     a.ctrl_next = (k == k_steps - 1) ? carry_slot(ctx) : ctx->b.ctrl + k + 1;
     a.src = src;
     a.hist = ctx->screening ? ctx->b.sort_hist : nullptr;  // the propagation counts the sort's digits
+    a.pack_bits = ctx->pack_keys ? index_bits(ctx->n) : 0;
     return a;
 }
 
@@ -493,8 +499,13 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         const bool items_over = max_items > ctx->b.items_cap;
         if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits");
         if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
-        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) break;
+        if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS | ks::FLAG_PACK_WIDTH)) && !surv_over && !items_over)
+            break;
         if (attempt >= kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after replays");
+        if (flags & ks::FLAG_PACK_WIDTH) {
+            ctx->pack_keys = false;  // keys too wide to carry the object index: sort it separately
+            drop_graphs(ctx);
+        }
         if (flags & ks::FLAG_SORT_BITS) {
             ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(max_bits));
             drop_graphs(ctx);
@@ -578,8 +589,10 @@ int seed_speculation(ks_ctx* ctx) {
     Ctrl c{};
     KS_CUDA(cudaMemcpyAsync(&c, carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA(cudaStreamSynchronize(ctx->stream));
-    ctx->sort_passes = passes_for_bits(
-        estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale));
+    const int bits = estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale);
+    ctx->sort_passes = passes_for_bits(bits);
+    // Keys, dead flag and object index in 64 bits, with 2 bits to spare for the estimate.
+    ctx->pack_keys = bits + 1 + index_bits(ctx->n) + 2 <= 64;
     drop_graphs(ctx);
     return KS_OK;
 }
@@ -1572,6 +1585,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         ks::launch_chunk_init(ctx->b, 1, ctx->stream);
         StepArgs a = step_args(ctx, 0, 1, 0);
         a.hist = nullptr;  // keys come from k_screen_keys: the sort counts their digits itself
+        a.pack_bits = 0;
         ks::launch_seed_ctrl(ctx->b, static_cast<int>(n), 0, a.ctrl, 0, ctx->stream);
         ks::launch_screen_keys(ctx->b, a, ctx->stream);
         ks::launch_sort(ctx->b, a, ctx->stream);

@@ -57,6 +57,7 @@ enum : int {
     FLAG_ITEMS_OVERFLOW = 16,  // pair work list longer than its buffer
     FLAG_TIMEOUT = 32,       // a bounded device-side wait gave up
     FLAG_KEYS_REBUILT = 64,  // k_fix_keys rebuilt the keys: their digit histogram is recounted
+    FLAG_PACK_WIDTH = 128,   // cell key + dead flag + object index do not fit 64 bits: sort unpacked
 };
 
 
@@ -124,10 +125,9 @@ struct DeviceBuffers {
     ks_conjunction* conj = nullptr;
     int64_t conj_cap = 0;
     // Ordering of a chunk's conjunction records on the device (radix sort on a
-    // 32-bit key monotone in t): keys / indices ping-pong, look-back status,
+    // 32-bit key monotone in t, record index in the low bits): keys ping-pong, look-back status,
     // digit histograms, tile tickets, and the records in order.
     unsigned long long* conj_keys[2] = {nullptr, nullptr};
-    int* conj_idx[2] = {nullptr, nullptr};
     unsigned int* conj_status = nullptr;
     unsigned int* conj_hist = nullptr;
     unsigned int* conj_ctr = nullptr;
@@ -169,6 +169,7 @@ struct StepArgs {
     Ctrl* ctrl_next;           // next step's control block (speculation outputs)
     int src;                   // state buffer holding the start of the step (0 or 1)
     unsigned int* hist;        // radix digit histogram the propagation fills with the keys it emits, or null
+    int pack_bits;             // > 0: sort keys carry the object index in their low pack_bits bits
 };
 
 // Kernel launchers (ks_kernels.cu). All enqueue on `stream` and never synchronise.

@@ -107,6 +107,16 @@ __device__ __forceinline__ unsigned long long cell_key(const GridParams& g, doub
 
 __device__ __forceinline__ unsigned long long dead_key(const GridParams& g) { return 1ull << min(g.bits, 63); }
 
+// Sort key of object i: the cell key above the object index when packing (the
+// sort then carries no index array), else the cell key alone.
+__device__ __forceinline__ unsigned long long sort_key(unsigned long long key, int i, int pack_bits) {
+    return pack_bits ? (key << pack_bits) | static_cast<unsigned long long>(i) : key;
+}
+// Flags grids whose keys, dead flag and object index overflow 64 bits.
+__device__ __forceinline__ void check_pack_width(const GridParams& g, int pack_bits, Ctrl* ctrl) {
+    if (pack_bits && g.bits + 1 + pack_bits > 64) atomicOr(&ctrl->flags, FLAG_PACK_WIDTH);
+}
+
 __device__ __forceinline__ unsigned long long hash_slot(unsigned long long k, unsigned long long mask) {
     // 64-bit finaliser (Stafford's mix 13); spreads neighbouring keys.
     k ^= k >> 30; k *= 0xbf58476d1ce4e5b9ull;
@@ -322,7 +332,10 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
             make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
                       a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
         for (int q = 0; q < 3; ++q) moon[q] = a.sp->m[q];
-        if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
+        if (blockIdx.x == 0 && a.screening) {
+            a.ctrl->grid = g;
+            check_pack_width(g, a.pack_bits, a.ctrl);
+        }
     }
     __shared__ unsigned int sh_hist[8 * 256];
     const bool with_hist = a.screening && a.hist != nullptr;
@@ -371,7 +384,7 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
                 }
                 out_key = alive ? key : dead_key(g);
             }
-            if (a.screening) keys[i] = out_key;
+            if (a.screening) keys[i] = sort_key(out_key, i, a.pack_bits);
         }
         if (with_hist) {
             __syncwarp();
@@ -416,7 +429,10 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
             make_grid(__longlong_as_double(static_cast<long long>(a.ctrl->spec_vmax)), a.ctrl->bb_min,
                       a.ctrl->bb_max, a.dt, a.threshold_km, a.tune.subcell_bits, a.rbits, a.tune.cell_scale, g);
         for (int q = 0; q < 3; ++q) moon[q] = to_f32(a.sp->m[q]);
-        if (blockIdx.x == 0 && a.screening) a.ctrl->grid = g;
+        if (blockIdx.x == 0 && a.screening) {
+            a.ctrl->grid = g;
+            check_pack_width(g, a.pack_bits, a.ctrl);
+        }
     }
     __shared__ unsigned int sh_hist[8 * 256];
     const bool with_hist = a.screening && a.hist != nullptr;
@@ -463,7 +479,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, c
                 }
                 out_key = alive ? key : dead_key(g);
             }
-            if (a.screening) keys[i] = out_key;
+            if (a.screening) keys[i] = sort_key(out_key, i, a.pack_bits);
         }
         if (with_hist) {
             __syncwarp();
@@ -490,17 +506,19 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
         if (blockIdx.x == 0) {
             a.ctrl->grid = g;
             a.ctrl->vmax_true = a.ctrl->spec_vmax;
+            check_pack_width(g, a.pack_bits, a.ctrl);
         }
     }
     __syncthreads();
     int bad = 0, alive = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         if (alive_after[i]) {
-            keys[i] = cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
-                               before[6 * static_cast<int64_t>(i) + 2], a.real_id ? a.real_id[i] : 0u, &bad);
+            keys[i] = sort_key(cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
+                                        before[6 * static_cast<int64_t>(i) + 2], a.real_id ? a.real_id[i] : 0u, &bad),
+                               i, a.pack_bits);
             ++alive;
         } else {
-            keys[i] = dead_key(g);
+            keys[i] = sort_key(dead_key(g), i, a.pack_bits);
         }
     }
     alive = warp_sum(alive);
@@ -527,6 +545,7 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
         if (blockIdx.x == 0) {
             a.ctrl->grid = g;
             atomicOr(&a.ctrl->flags, FLAG_KEYS_REBUILT);
+            check_pack_width(g, a.pack_bits, a.ctrl);
         }
     }
     // The propagation's digit histogram described the old keys: clear it for the recount.
@@ -535,9 +554,12 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
     __syncthreads();
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
-        keys[i] = alive_after[i] ? cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
-                                            before[6 * static_cast<int64_t>(i) + 2], a.real_id ? a.real_id[i] : 0u, &bad)
-                                 : dead_key(g);
+        keys[i] = sort_key(alive_after[i] ? cell_key(g, before[6 * static_cast<int64_t>(i)],
+                                                     before[6 * static_cast<int64_t>(i) + 1],
+                                                     before[6 * static_cast<int64_t>(i) + 2],
+                                                     a.real_id ? a.real_id[i] : 0u, &bad)
+                                          : dead_key(g),
+                           i, a.pack_bits);
     bad = warp_max(bad);
     if ((threadIdx.x & 31) == 0 && bad) atomicOr(&a.ctrl->flags, FLAG_KEY_RANGE);
 }
@@ -674,7 +696,7 @@ __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
 __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long long* __restrict__ keys, int n,
                                                          const int* __restrict__ n_dev, int passes,
                                                          unsigned int* __restrict__ hist, const Ctrl* ctrl,
-                                                         int only_if_rebuilt) {
+                                                         int only_if_rebuilt, int shift0) {
     __shared__ unsigned int h[8][256];
     if (only_if_rebuilt && !(ctrl->flags & FLAG_KEYS_REBUILT)) return;
     if (n_dev) n = min(n, *n_dev);
@@ -688,7 +710,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long lon
         const bool valid = p < n;
         const unsigned long long k = valid ? keys[p] : 0ull;
         for (int pass = 0; pass < passes; ++pass) {
-            const unsigned d = valid ? static_cast<unsigned>((k >> (8 * pass)) & 0xFF) : 256u + lane;
+            const unsigned d = valid ? static_cast<unsigned>((k >> (shift0 + 8 * pass)) & 0xFF) : 256u + lane;
             const unsigned peers = __match_any_sync(0xffffffffu, d);
             if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[pass][d], __popc(peers));
         }
@@ -721,7 +743,8 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
                                                           const int* __restrict__ n_dev, int shift,
                                                           const unsigned int* __restrict__ digit_base,
                                                           unsigned int* __restrict__ status,
-                                                          unsigned int* __restrict__ ticket, int* flags) {
+                                                          unsigned int* __restrict__ ticket, int* flags,
+                                                          int packed) {
     __shared__ unsigned int wcnt[kWarps][256];
     __shared__ int gbase[256];
     __shared__ unsigned long long skeys[kSortTile];
@@ -751,7 +774,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
         const bool valid = l < count;
         const int p = tile0 + l;
         k[r] = valid ? keys_in[p] : 0ull;
-        id[r] = valid ? (idx_in ? idx_in[p] : p) : 0;
+        id[r] = (valid && !packed) ? (idx_in ? idx_in[p] : p) : 0;
         d[r] = valid ? static_cast<unsigned>((k[r] >> shift) & 0xFF) : 256u + lane;
         const unsigned peers = __match_any_sync(0xffffffffu, d[r]);
         if (valid && lane == __ffs(peers) - 1) wcnt[warp][d[r]] += __popc(peers);
@@ -804,7 +827,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
         if (valid) {
             const unsigned pos = wcnt[warp][d[r]] + __popc(peers & lanemask_lt());
             skeys[pos] = k[r];
-            sidx[pos] = id[r];
+            if (!packed) sidx[pos] = id[r];
         }
         __syncwarp();
         if (valid && lane == __ffs(peers) - 1) wcnt[warp][d[r]] += __popc(peers);
@@ -816,7 +839,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
         const int dst = gbase[static_cast<unsigned>((kk >> shift) & 0xFF)] + l;
         if (dst >= 0 && dst < n) {
             keys_out[dst] = kk;
-            idx_out[dst] = sidx[l];
+            if (!packed) idx_out[dst] = sidx[l];
         }
     }
 }
@@ -826,9 +849,10 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(kBlock) k_cell_count(const unsigned long long* __restrict__ keys,
-                                                       const Ctrl* __restrict__ ctrl, unsigned int* __restrict__ counts) {
+                                                       const Ctrl* __restrict__ ctrl, unsigned int* __restrict__ counts,
+                                                       int pack_bits) {
     const int m = ctrl->n_alive;
-    const int shift = 3 * ctrl->grid.sub;
+    const int shift = 3 * ctrl->grid.sub + pack_bits;
     const int base = blockIdx.x * kCellTile;
     int c = 0;
     for (int j = threadIdx.x; j < kCellTile; j += kBlock) {
@@ -855,7 +879,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                                                        unsigned long long* __restrict__ hk, int* __restrict__ hv,
                                                        unsigned long long hmask, const double* __restrict__ before,
                                                        double* __restrict__ sorted,
-                                                       int* __restrict__ sorted_orig, float4* __restrict__ sorted32) {
+                                                       int* __restrict__ sorted_orig, float4* __restrict__ sorted32,
+                                                       int pack_bits) {
     constexpr int kPer = kCellTile / kBlock;  // consecutive entries per thread
     const int m = ctrl->n_alive;
     if (m == 0) {
@@ -864,7 +889,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
     }
     if (blockIdx.x * kCellTile >= m) return;
     const int p0 = blockIdx.x * kCellTile + threadIdx.x * kPer;
-    const int sh = 3 * ctrl->grid.sub;
+    const int sh = 3 * ctrl->grid.sub + pack_bits;
+    const unsigned long long idx_mask = pack_bits ? (1ull << pack_bits) - 1 : 0ull;
     int heads[kPer];
     unsigned int local = 0;
     for (int j = 0; j < kPer; ++j) {
@@ -906,7 +932,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
         const int p = base + j * kBlock;
-        o[j] = p < m ? idx[p] : -1;
+        o[j] = p < m ? (pack_bits ? static_cast<int>(keys[p] & idx_mask) : idx[p]) : -1;
     }
     double2 st[kPer][3];
 #pragma unroll
@@ -1800,37 +1826,40 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     cudaMemsetAsync(b.sort_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
     k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, nullptr, passes, b.sort_hist, a.ctrl,
-                                                  counted ? 1 : 0);
+                                                  counted ? 1 : 0, a.pack_bits);
     k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.sort_hist, passes, a.ctrl);
     for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
-            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, nullptr, 8 * pass,
-            b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass, b.sort_ctr + pass,
-            &a.ctrl->flags);
+            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, nullptr,
+            a.pack_bits + 8 * pass, b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass,
+            b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0);
     }
 }
 
 // Key of each of the chunk's records: floor(2^32 (t - t_start) / span),
-// clamped, a non-decreasing function of t.
+// clamped, a non-decreasing function of t, above the record's index.
 __global__ void __launch_bounds__(kBlock) k_conj_keys(const ks_conjunction* __restrict__ conj, int64_t cap,
                                                       ChunkCtrl* chunk, const double* __restrict__ t_start,
-                                                      double span_s, unsigned long long* __restrict__ keys) {
+                                                      double span_s, unsigned long long* __restrict__ keys,
+                                                      int pack_bits) {
     const int n = static_cast<int>(min(chunk->conj_count, static_cast<unsigned long long>(cap)));
     if (blockIdx.x == 0 && threadIdx.x == 0) chunk->sort_n = n;
     const double t0 = *t_start;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const double f = xmul(xdiv(xsub(conj[q].t, t0), span_s), 4294967296.0);
         const double c = fmin(fmax(floor(f), 0.0), 4294967295.0);
-        keys[q] = static_cast<unsigned long long>(c);
+        keys[q] = (static_cast<unsigned long long>(c) << pack_bits) | static_cast<unsigned long long>(q);
     }
 }
 
 __global__ void __launch_bounds__(kBlock) k_conj_gather(const ks_conjunction* __restrict__ conj,
-                                                        const int* __restrict__ order, const ChunkCtrl* chunk,
+                                                        const unsigned long long* __restrict__ order,
+                                                        unsigned long long mask, const ChunkCtrl* chunk,
                                                         ks_conjunction* __restrict__ out) {
     const int n = chunk->sort_n;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = conj[order[q]];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        out[q] = conj[static_cast<int>(order[q] & mask)];
 }
 
 void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s,
@@ -1839,35 +1868,39 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
     if (cap <= 0) return;
     constexpr int kPasses = 4;
     const int ntiles = (cap + kSortTile - 1) / kSortTile;
+    int pb = 1;  // record index bits below the 32-bit key
+    while ((1ll << pb) < cap) ++pb;
     cudaMemsetAsync(b.conj_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
     cudaMemsetAsync(b.conj_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.conj_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * kPasses, stream);
-    k_conj_keys<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_cap, chunk, t_start, span_s, b.conj_keys[0]);
+    k_conj_keys<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_cap, chunk, t_start, span_s, b.conj_keys[0],
+                                                       pb);
     k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.conj_keys[0], cap, &chunk->sort_n, kPasses, b.conj_hist, nullptr,
-                                                  0);
+                                                  0, pb);
     k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.conj_hist, kPasses, nullptr);
     for (int pass = 0; pass < kPasses; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
-            b.conj_keys[in], pass == 0 ? nullptr : b.conj_idx[in], b.conj_keys[outb], b.conj_idx[outb], cap,
-            &chunk->sort_n, 8 * pass, b.conj_hist + 256 * pass,
-            b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass, &chunk->flags);
+            b.conj_keys[in], nullptr, b.conj_keys[outb], nullptr, cap, &chunk->sort_n, pb + 8 * pass,
+            b.conj_hist + 256 * pass, b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass,
+            &chunk->flags, 1);
     }
-    k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_idx[kPasses & 1], chunk, b.conj_sorted);
+    k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_keys[kPasses & 1], (1ull << pb) - 1, chunk,
+                                                         b.conj_sorted);
 }
 
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     const int sb = sorted_buffer(a.sort_passes);
     const int ntiles = a.n > 0 ? (a.n + kCellTile - 1) / kCellTile : 1;
     unsigned int* bc = reinterpret_cast<unsigned int*>(b.block_counts);
-    k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, bc);
+    k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, bc, a.pack_bits);
     k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr);
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
     k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], bc, a.ctrl, b.cell_begin, b.cell_key,
                                                b.hash_keys, b.hash_vals,
                                                static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src],
                                                b.sorted, b.sorted_orig,
-                                               a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr);
+                                               a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
     k_items_count<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
