@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--ens-steps", type=int, default=360)
     ap.add_argument("--ens-lc", type=float, default=0.05)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--cascade-realisations", type=int, default=16)
+    ap.add_argument("--cascade-steps", type=int, default=60)
+    ap.add_argument("--no-cascade", action="store_true")
     return ap.parse_args()
 
 
@@ -435,6 +438,8 @@ def main():
         line["e2e"] = e2e_run(ks, a, st, sz, al, local, barrier, pg, head)
     if not a.no_ensemble:
         line["ensemble"] = ensemble_run(ks, a, local, barrier, pg, rank)
+    if not a.no_cascade:
+        line["cascade"] = cascade_run(ks, a, local, barrier, pg, rank, st, sz, al)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         base = cpu_baseline(a, st, sz, al, a.cpu_steps)
         line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -502,6 +507,59 @@ def ensemble_run(ks, a, device, barrier, pg, rank):
             "steps": a.ens_steps, "conjunctions": int(len(conj)), "breakups_in_loop": int(len(more)),
             "autotune": choice, "autotune_s": tune_s,
             "l2": "flushed before every step (256 MiB write)"}
+
+
+def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
+    """Batched cascade: R realisations of the 1M-object population with collision
+    radii x50, fragmentation (NASA SBM, L_c 10 cm, the reference's draws, one
+    stream per realisation) in the loop, split precision, 5 km, 10 m/s. The
+    population grows as collisions fragment objects; chunks end at collision
+    steps. Timed on the device (CUDA events) with the fragmentation host work in
+    the wall time beside it."""
+    R = a.cascade_realisations
+    n0 = len(sz)
+    eng = ks.Engine(device)
+    eng.set_precision(ks.PRECISION_SPLIT)
+    eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
+    eng.set_screening(True, a.conj_km, 50.0, 0.01)
+    eng.set_steps_per_graph(a.steps_per_graph)
+    eng.set_population_batch(np.arange(R + 1) * n0, np.tile(st, (R, 1)), np.tile(sz, R), np.tile(al, R))
+    eng.set_breakup(True, 0.10, 40.0, realisation_seed(a.seed, rank))
+    eng.run(a.warmup)
+    eng.take_conjunctions()
+    eng.take_step_stats()
+    warm_events = eng.take_breakups()
+    n_start = eng.population_size()
+    eng.set_profiling(True)
+    barrier()
+    w0 = time.perf_counter()
+    eng.run(a.cascade_steps)
+    barrier()
+    wall = time.perf_counter() - w0
+    tm = eng.timing()
+    ev = eng.take_breakups()
+    conj = eng.take_conjunctions()
+    stats = eng.take_step_stats()
+    n_end = eng.population_size()
+    props = eng.objects()
+    eng.close()
+    frag = props["event"] >= 0
+    size = props["size_m"][frag]
+    dev_ms = max_over_ranks(pg, tm["total_ms"])
+    obj = sum_over_ranks(pg, float(tm["object_steps"]))
+    per_real = np.bincount(ev["realisation"], minlength=R) if len(ev) else np.zeros(R, int)
+    return {"workload": f"{R} realisations x the {n0}-object population, collision radii x50, fragmentation "
+                        f"in the loop (SBM, L_c 0.1 m), split precision, dt {a.dt} s, {a.conj_km} km",
+            "value": obj / (dev_ms * 1e-3), "unit": "object-steps/s", "ms_per_step": dev_ms / max(1, tm["steps"]),
+            "wall_s": wall, "wall_object_steps_per_s": obj / wall, "steps": a.cascade_steps,
+            "objects_start": int(n_start), "objects_end": int(n_end), "events": int(len(ev)),
+            "events_in_warmup": int(len(warm_events)), "catastrophic": int(ev["catastrophic"].sum()) if len(ev) else 0,
+            "fragments_created": int(ev["fragments"].sum()) if len(ev) else 0,
+            "events_per_realisation": {"min": int(per_real.min()), "max": int(per_real.max())},
+            "collisions": int(conj["collision"].sum()), "conjunctions": int(len(conj)),
+            "fragment_sizes_m": {"n_gt_lc": int((size > 0.1).sum()), "ratio_n_gt_2lc": float((size > 0.2).sum() /
+                                 max(1, (size > 0.1).sum())), "sbm_ratio": 2 ** -1.71},
+            "alive_end": int(stats["alive"][-1]) if len(stats) else None}
 
 
 def measure_fp32(eng):

@@ -15,9 +15,11 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <atomic>
 #include <set>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kessler_b200.h"
@@ -66,6 +68,9 @@ struct ks_ctx {
     ks_timing timing{};
     ks::Tuning tune;
     bool ckpt_states = false;  // the checkpoint holds states (chunks of more than one step)
+    int chunk_hint = 0;        // steps of the last chunk that ended early at a collision (0: none)
+    void* frag_scratch = nullptr;  // device staging of fragmentation work (parent rows, spans)
+    size_t frag_scratch_bytes = 0;
     bool pack_keys = true;     // object index packed below the cell key in the sort keys
     int realisations = 1;
     int rbits = 0;
@@ -520,6 +525,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         continue;
     }
     int64_t nc = 0;
+    bool was_cut = false;
     for (int cut = 0;; ++cut) {
         nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
         if (nc > 0) {
@@ -536,6 +542,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         if (cut > 0) return fail(ctx, KS_ERR_STATE, "replay to the first collision step did not end there");
         // Replay the chunk up to the step of the first collision (same inputs, same results).
         k_steps = static_cast<int>(first_hit - ctx->steps_done) + 1;
+        was_cut = true;
         fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
         rc = restore_checkpoint(ctx);
         if (rc) return rc;
@@ -580,6 +587,10 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     ctx->steps_done += k_steps;
     ctx->t = t_end;
     if (k_steps & 1) ctx->cur ^= 1;
+    // Chunk length after collisions: as long as the one that ended early, then
+    // doubling back while chunks run through.
+    if (was_cut) ctx->chunk_hint = k_steps;
+    else if (ctx->chunk_hint > 0) ctx->chunk_hint = 2 * ctx->chunk_hint >= ctx->max_chunk ? 0 : 2 * ctx->chunk_hint;
     if (!hits.empty()) return apply_collisions(ctx, ctx->steps_done - 1, t_last, hits);
     return KS_OK;
 }
@@ -616,6 +627,7 @@ int upload_population(ks_ctx* ctx, int64_t n, const double* states, const double
 // ---------------------------------------------------------------------------
 
 void reset_breakup_run(ks_ctx* ctx) {
+    ctx->chunk_hint = 0;
     ks_ctx::Breakup& k = ctx->bk;
     k.rng.clear();
     k.next_event.clear();
@@ -707,48 +719,66 @@ struct NewFragments {
     std::vector<int64_t> killed;
 };
 
+int ensure_frag_scratch(ks_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->frag_scratch_bytes) return KS_OK;
+    if (ctx->frag_scratch) cudaFree(ctx->frag_scratch);
+    ctx->frag_scratch = nullptr;
+    ctx->frag_scratch_bytes = 0;
+    const size_t want = std::max(bytes, size_t(1) << 20);
+    KS_CUDA(cudaMalloc(&ctx->frag_scratch, want));
+    ctx->frag_scratch_bytes = want;
+    return KS_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
 // Appends the fragments after the population, carries those born inside a
-// step to its end (on the device), and removes the destroyed parents.
+// step to its end (one device launch for all events), and removes the
+// destroyed parents.
 int commit_fragments(ks_ctx* ctx, const NewFragments& nf) {
     ks::DeviceBuffers& b = ctx->b;
     const int64_t n0 = ctx->n;
     const int64_t m = static_cast<int64_t>(nf.rows.size());
     int rc = grow_objects(ctx, n0 + m);
     if (rc) return rc;
+    const size_t ns = nf.spans.size(), nk = nf.killed.size();
+    const size_t bytes = align256(sizeof(ks::FragSpan) * std::max<size_t>(ns, 1)) +
+                         align256(sizeof(int) * std::max<int64_t>(m, 1)) + align256(sizeof(int64_t) * std::max<size_t>(nk, 1));
+    rc = ensure_frag_scratch(ctx, bytes);
+    if (rc) return rc;
+    char* base = static_cast<char*>(ctx->frag_scratch);
+    ks::FragSpan* d_spans = reinterpret_cast<ks::FragSpan*>(base);
+    int* d_row_span = reinterpret_cast<int*>(base + align256(sizeof(ks::FragSpan) * std::max<size_t>(ns, 1)));
+    int64_t* d_killed = reinterpret_cast<int64_t*>(reinterpret_cast<char*>(d_row_span) +
+                                                   align256(sizeof(int) * std::max<int64_t>(m, 1)));
     if (m > 0) {
         std::vector<double> st(static_cast<size_t>(6 * m)), sz(static_cast<size_t>(m));
-        std::vector<uint8_t> al(static_cast<size_t>(m), 1);
         for (int64_t q = 0; q < m; ++q) {
             const ks::SbmFragment& f = nf.rows[static_cast<size_t>(q)];
             std::copy(f.s, f.s + 6, &st[static_cast<size_t>(6 * q)]);
             sz[static_cast<size_t>(q)] = f.size_m;
         }
-        for (const NewFragments::Span& sp : nf.spans) {
-            if (sp.remaining_s > 0) continue;
-            // Born at the end of the interval: alive unless below the surface
-            // (src/core/breakup.cpp:305-306).
-            for (int q = 0; q < sp.count; ++q) {
-                const double* r = &st[static_cast<size_t>(6 * (sp.first - n0 + q))];
-                al[static_cast<size_t>(sp.first - n0 + q)] =
-                    std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) >= ks::kREarth ? 1 : 0;
-            }
+        std::vector<ks::FragSpan> spans(ns);
+        std::vector<int> row_span(static_cast<size_t>(m), 0);
+        for (size_t k = 0; k < ns; ++k) {
+            const NewFragments::Span& sp = nf.spans[k];
+            spans[k].dt = sp.remaining_s > 0 ? sp.remaining_s : 0.0;
+            if (sp.remaining_s > 0 && sp.count > 0) ks::moon_stages_from(sp.jd0, sp.remaining_s, spans[k].m);
+            for (int q = 0; q < sp.count; ++q) row_span[static_cast<size_t>(sp.first - n0 + q)] = static_cast<int>(k);
         }
-        double* dst = b.state[ctx->cur] + 6 * n0;
-        KS_CUDA(cudaMemcpyAsync(dst, st.data(), sizeof(double) * 6 * m, cudaMemcpyHostToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(b.state[ctx->cur] + 6 * n0, st.data(), sizeof(double) * 6 * m, cudaMemcpyHostToDevice, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(b.size_m + n0, sz.data(), sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(b.alive[ctx->cur] + n0, al.data(), m, cudaMemcpyHostToDevice, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(b.real_id + n0, nf.rid.data(), sizeof(uint16_t) * m, cudaMemcpyHostToDevice, ctx->stream));
-        const ks::ForceConsts fc = force_consts();
-        for (const NewFragments::Span& sp : nf.spans) {
-            if (sp.remaining_s <= 0 || sp.count == 0) continue;
-            ks::MoonStage ms[3];
-            ks::moon_stages_from(sp.jd0, sp.remaining_s, ms);
-            ks::launch_advance_rows(fc, sp.remaining_s, ms, b.state[ctx->cur], b.alive[ctx->cur], sp.first, sp.count,
-                                    ctx->stream);
-        }
-        KS_CUDA(cudaGetLastError());
+        KS_CUDA(cudaMemcpyAsync(d_spans, spans.data(), sizeof(ks::FragSpan) * ns, cudaMemcpyHostToDevice, ctx->stream));
+        KS_CUDA(cudaMemcpyAsync(d_row_span, row_span.data(), sizeof(int) * m, cudaMemcpyHostToDevice, ctx->stream));
+        ks::launch_advance_spans(force_consts(), d_spans, d_row_span, n0, static_cast<int>(m), b.state[ctx->cur],
+                                 b.alive[ctx->cur], ctx->stream);
     }
-    for (int64_t idx : nf.killed) KS_CUDA(cudaMemsetAsync(b.alive[ctx->cur] + idx, 0, 1, ctx->stream));
+    if (nk > 0) {
+        KS_CUDA(cudaMemcpyAsync(d_killed, nf.killed.data(), sizeof(int64_t) * nk, cudaMemcpyHostToDevice, ctx->stream));
+        ks::launch_clear_alive(b.alive[ctx->cur], d_killed, static_cast<int>(nk), ctx->stream);
+    }
+    KS_CUDA(cudaGetLastError());
     KS_CUDA(cudaStreamSynchronize(ctx->stream));
     ks_ctx::Breakup& k = ctx->bk;
     for (int64_t q = 0; q < m; ++q) {
@@ -765,55 +795,111 @@ int commit_fragments(ks_ctx* ctx, const NewFragments& nf) {
 
 // Fragments the collisions of the step that started at t0 (src/core/breakup.cpp:316-338):
 // in (t, i, j) order, skipping pairs with a parent destroyed earlier in the
-// step; parents are interpolated to the collision instant.
+// step; parents are interpolated to the collision instant. Realisations draw
+// from their own streams and own their objects, so they are fragmented in
+// parallel; fragments are appended in the order of the collisions.
 int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_conjunction>& hits) {
     int rc = ensure_mirrors(ctx);
     if (rc) return rc;
     ensure_streams(ctx);
     ks_ctx::Breakup& k = ctx->bk;
     const double dt = ctx->dt;
-    const double* before = ctx->b.state[ctx->cur ^ 1];
-    const double* after = ctx->b.state[ctx->cur];
-    std::set<int64_t> dead;
-    NewFragments nf;
+    // Start- and end-of-step states of every parent, in one gather.
+    std::vector<int64_t> idx;
+    idx.reserve(2 * hits.size());
     for (const ks_conjunction& c : hits) {
-        if (dead.count(c.i) || dead.count(c.j)) continue;
-        double rows[4][6];
-        KS_CUDA(cudaMemcpyAsync(rows[0], before + 6 * static_cast<int64_t>(c.i), 48, cudaMemcpyDeviceToHost, ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(rows[1], after + 6 * static_cast<int64_t>(c.i), 48, cudaMemcpyDeviceToHost, ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(rows[2], before + 6 * static_cast<int64_t>(c.j), 48, cudaMemcpyDeviceToHost, ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(rows[3], after + 6 * static_cast<int64_t>(c.j), 48, cudaMemcpyDeviceToHost, ctx->stream));
-        KS_CUDA(cudaStreamSynchronize(ctx->stream));
-        const double s = (c.t - t0) / dt;
-        auto parent = [&](int64_t idx, const double* b0, const double* b1) {
-            ks::SbmParent p;
-            p.index = idx;
-            ks::interpolate_state(b0, b1, dt, s, p.s);
-            p.mass_kg = ks::sbm_mass_or_default(k.mass_kg[static_cast<size_t>(idx)]);
-            p.size_m = k.size_m[static_cast<size_t>(idx)];
-            return p;
-        };
-        const ks::SbmParent pa = parent(c.i, rows[0], rows[1]), pb = parent(c.j, rows[2], rows[3]);
-        const bool a_heavier = pa.mass_kg >= pb.mass_kg;
-        const ks::SbmParent& tgt = a_heavier ? pa : pb;
-        const ks::SbmParent& prj = a_heavier ? pb : pa;
-        const int r = k.rid[static_cast<size_t>(c.i)];
+        idx.push_back(c.i);
+        idx.push_back(c.j);
+    }
+    std::sort(idx.begin(), idx.end());
+    idx.erase(std::unique(idx.begin(), idx.end()), idx.end());
+    const size_t u = idx.size();
+    rc = ensure_frag_scratch(ctx, align256(sizeof(int64_t) * u) + sizeof(double) * 12 * u);
+    if (rc) return rc;
+    int64_t* d_idx = static_cast<int64_t*>(ctx->frag_scratch);
+    double* d_rows = reinterpret_cast<double*>(static_cast<char*>(ctx->frag_scratch) + align256(sizeof(int64_t) * u));
+    std::vector<double> rows(12 * u);
+    KS_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int64_t) * u, cudaMemcpyHostToDevice, ctx->stream));
+    ks::launch_gather_rows(ctx->b.state[ctx->cur ^ 1], ctx->b.state[ctx->cur], d_idx, static_cast<int>(u), d_rows,
+                           ctx->stream);
+    KS_CUDA(cudaMemcpyAsync(rows.data(), d_rows, sizeof(double) * 12 * u, cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    auto row_of = [&](int64_t o) {
+        return &rows[12 * static_cast<size_t>(std::lower_bound(idx.begin(), idx.end(), o) - idx.begin())];
+    };
+
+    struct Result {
+        bool done = false;
         ks_breakup_event ev{};
-        ev.step = step;
-        ev.id = k.next_event[static_cast<size_t>(r)]++;
-        ev.realisation = r;
-        ev.target = tgt.index;
-        ev.projectile = prj.index;
-        ev.first_fragment = ctx->n + static_cast<int64_t>(nf.rows.size());
+        std::vector<ks::SbmFragment> frags;
         ks::SbmOutcome oc;
-        ks::sbm_fragment(k.rng[static_cast<size_t>(r)], k.params, tgt, prj, c.t, ev, nf.rows, oc);
-        if (oc.kill_projectile) { dead.insert(prj.index); nf.killed.push_back(prj.index); }
-        if (oc.kill_target) { dead.insert(tgt.index); nf.killed.push_back(tgt.index); }
-        if (oc.reduce_target) k.mass_kg[static_cast<size_t>(tgt.index)] = oc.target_mass_after;
-        nf.spans.push_back({ev.first_fragment, ev.fragments, t0 + dt - c.t, ctx->epoch_jd + c.t / 86400.0});
-        nf.rid.resize(nf.rows.size(), static_cast<uint16_t>(r));
-        nf.event.resize(nf.rows.size(), ev.id);
-        k.out.push_back(ev);
+        double remaining = 0, jd0 = 0;
+    };
+    std::vector<Result> res(hits.size());
+    std::vector<std::vector<size_t>> by_real(static_cast<size_t>(ctx->realisations));
+    for (size_t h = 0; h < hits.size(); ++h) by_real[k.rid[static_cast<size_t>(hits[h].i)]].push_back(h);
+    auto fragment_realisation = [&](size_t r) {
+        std::set<int64_t> dead;
+        for (size_t h : by_real[r]) {
+            const ks_conjunction& c = hits[h];
+            if (dead.count(c.i) || dead.count(c.j)) continue;
+            const double s = (c.t - t0) / dt;
+            auto parent = [&](int64_t o) {
+                const double* rw = row_of(o);
+                ks::SbmParent p;
+                p.index = o;
+                ks::interpolate_state(rw, rw + 6, dt, s, p.s);
+                p.mass_kg = ks::sbm_mass_or_default(k.mass_kg[static_cast<size_t>(o)]);
+                p.size_m = k.size_m[static_cast<size_t>(o)];
+                return p;
+            };
+            const ks::SbmParent pa = parent(c.i), pb = parent(c.j);
+            const bool a_heavier = pa.mass_kg >= pb.mass_kg;
+            const ks::SbmParent& tgt = a_heavier ? pa : pb;
+            const ks::SbmParent& prj = a_heavier ? pb : pa;
+            Result& out = res[h];
+            out.ev.step = step;
+            out.ev.id = k.next_event[r]++;
+            out.ev.realisation = static_cast<int32_t>(r);
+            out.ev.target = tgt.index;
+            out.ev.projectile = prj.index;
+            ks::sbm_fragment(k.rng[r], k.params, tgt, prj, c.t, out.ev, out.frags, out.oc);
+            if (out.oc.kill_projectile) dead.insert(prj.index);
+            if (out.oc.kill_target) dead.insert(tgt.index);
+            if (out.oc.reduce_target) k.mass_kg[static_cast<size_t>(tgt.index)] = out.oc.target_mass_after;
+            out.remaining = t0 + dt - c.t;
+            out.jd0 = ctx->epoch_jd + c.t / 86400.0;
+            out.done = true;
+        }
+    };
+    std::vector<size_t> active;
+    for (size_t r = 0; r < by_real.size(); ++r)
+        if (!by_real[r].empty()) active.push_back(r);
+    const size_t workers = std::min<size_t>(active.size(), std::max(1u, std::thread::hardware_concurrency()));
+    if (workers <= 1) {
+        for (size_t r : active) fragment_realisation(r);
+    } else {
+        std::atomic<size_t> next{0};
+        std::vector<std::thread> pool;
+        for (size_t w = 0; w < workers; ++w)
+            pool.emplace_back([&]() {
+                for (size_t q = next++; q < active.size(); q = next++) fragment_realisation(active[q]);
+            });
+        for (std::thread& th : pool) th.join();
+    }
+
+    NewFragments nf;
+    for (size_t h = 0; h < hits.size(); ++h) {
+        Result& out = res[h];
+        if (!out.done) continue;
+        out.ev.first_fragment = ctx->n + static_cast<int64_t>(nf.rows.size());
+        if (out.oc.kill_projectile) nf.killed.push_back(out.ev.projectile);
+        if (out.oc.kill_target) nf.killed.push_back(out.ev.target);
+        nf.spans.push_back({out.ev.first_fragment, out.ev.fragments, out.remaining, out.jd0});
+        nf.rows.insert(nf.rows.end(), out.frags.begin(), out.frags.end());
+        nf.rid.resize(nf.rows.size(), static_cast<uint16_t>(out.ev.realisation));
+        nf.event.resize(nf.rows.size(), out.ev.id);
+        k.out.push_back(out.ev);
     }
     return commit_fragments(ctx, nf);
 }
@@ -893,6 +979,7 @@ void ks_destroy(ks_ctx* ctx) {
     if (ctx->l2_flush) cudaFree(ctx->l2_flush);
     dfree(ctx->b.survivors);
     dfree(ctx->b.items);
+    if (ctx->frag_scratch) cudaFree(ctx->frag_scratch);
     free_conj(ctx);
     dfree(ctx->b.ctrl);
     dfree(ctx->b.chunk);
@@ -1280,8 +1367,10 @@ int ks_run(ks_ctx* ctx, int64_t steps) {
     if (rc) return rc;
     const int64_t end = ctx->steps_done + steps;
     while (ctx->steps_done < end) {
-        // A chunk may end early, at a step that holds a collision to fragment.
-        const int k = static_cast<int>(std::min<int64_t>(end - ctx->steps_done, chunk));
+        // A chunk may end early, at a step that holds a collision to fragment;
+        // while collisions are frequent the chunks stay short (chunk_hint).
+        const int want = ctx->bk.on && ctx->chunk_hint > 0 ? std::min(chunk, ctx->chunk_hint) : chunk;
+        const int k = static_cast<int>(std::min<int64_t>(end - ctx->steps_done, want));
         rc = run_chunk(ctx, k);
         if (rc) return rc;
     }

@@ -149,6 +149,13 @@ struct Tuning {
     int item_col_blocks = 16;     // column blocks of 32 per pair work item (1..64)
 };
 
+// Time from a fragmentation event to the end of its step and the lunar stages
+// of that sub-step (dt = 0: the event closes the step).
+struct FragSpan {
+    double dt;
+    MoonStage m[3];
+};
+
 // Everything a step's kernels need, by value.
 struct StepArgs {
     Tuning tune;
@@ -178,9 +185,15 @@ void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int 
                       cudaStream_t stream);
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_screen_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
-// One RK4 step of dt over rows [first, first + count) (fragments born inside a step).
-void launch_advance_rows(const ForceConsts& fc, double dt, const MoonStage m[3], double* state, uint8_t* alive,
-                         int64_t first, int count, cudaStream_t stream);
+// Fragments born inside a step: rows [first, first + count) advanced over
+// their events' remaining time (spans[row_span[k]]), then their alive flags set.
+void launch_advance_spans(const ForceConsts& fc, const FragSpan* spans, const int* row_span, int64_t first,
+                          int count, double* state, uint8_t* alive, cudaStream_t stream);
+// rows[12 q ..] = the 6 start-of-step then 6 end-of-step doubles of object idx[q].
+void launch_gather_rows(const double* before, const double* after, const int64_t* idx, int count, double* rows,
+                        cudaStream_t stream);
+// alive[idx[q]] = 0.
+void launch_clear_alive(uint8_t* alive, const int64_t* idx, int count, cudaStream_t stream);
 void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);

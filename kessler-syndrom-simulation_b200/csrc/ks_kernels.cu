@@ -398,21 +398,42 @@ __global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, c
     flush_spec(acc, a.ctrl, a.ctrl_next, a.screening != 0);
 }
 
-// One RK4 step of dt over rows [first, first + count) with given lunar stages,
-// for fragments born inside a step: their state is carried from the event to
-// the end of the step (src/core/breakup.cpp:304-306), and a fragment that ends
-// below the surface is not alive.
-__global__ void __launch_bounds__(kPropBlock) k_advance_rows(ForceConsts fc, double dt, MoonStage m0, MoonStage m1,
-                                                              MoonStage m2, double* __restrict__ state,
-                                                              uint8_t* __restrict__ alive, int64_t first, int count) {
+// Fragments born inside a step, carried from their event to the end of the
+// step (src/core/breakup.cpp:304-306): one RK4 step of the event's remaining
+// time with its lunar stages (none when the event closes the step), then
+// alive unless below the surface. Row first + k belongs to span row_span[k].
+__global__ void __launch_bounds__(kPropBlock) k_advance_spans(ForceConsts fc, const FragSpan* __restrict__ spans,
+                                                               const int* __restrict__ row_span, int64_t first,
+                                                               int count, double* __restrict__ state,
+                                                               uint8_t* __restrict__ alive) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const int64_t i = first + k;
+    const FragSpan& sp = spans[row_span[k]];
     double s[6];
     ld6(state, i, s);
-    rk4_exact(fc, dt, m0, m1, m2, s);
-    st6(state, i, s);
+    if (sp.dt > 0) {
+        rk4_exact(fc, sp.dt, sp.m[0], sp.m[1], sp.m[2], s);
+        st6(state, i, s);
+    }
     alive[i] = xsqrt(xdot3(s[0], s[1], s[2])) >= fc.r_earth ? 1 : 0;
+}
+
+// rows[2q] / rows[2q+1] = start / end-of-step state of object idx[q].
+__global__ void __launch_bounds__(kBlock) k_gather_rows(const double* __restrict__ before,
+                                                        const double* __restrict__ after,
+                                                        const int64_t* __restrict__ idx, int count,
+                                                        double* __restrict__ rows) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 12 * count) return;
+    const int q = t / 12, c = t % 12;
+    rows[12 * static_cast<int64_t>(q) + c] = (c < 6 ? before : after)[6 * idx[q] + (c % 6)];
+}
+
+__global__ void __launch_bounds__(kBlock) k_clear_alive(uint8_t* __restrict__ alive, const int64_t* __restrict__ idx,
+                                                        int count) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) alive[idx[t]] = 0;
 }
 
 // Split-precision propagation (FP32 J2 and lunar terms, FP64 state and central
@@ -1799,11 +1820,22 @@ void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t st
                                                                 b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 
-void launch_advance_rows(const ForceConsts& fc, double dt, const MoonStage m[3], double* state, uint8_t* alive,
-                         int64_t first, int count, cudaStream_t stream) {
+void launch_advance_spans(const ForceConsts& fc, const FragSpan* spans, const int* row_span, int64_t first,
+                          int count, double* state, uint8_t* alive, cudaStream_t stream) {
     if (count <= 0) return;
-    k_advance_rows<<<(count + kPropBlock - 1) / kPropBlock, kPropBlock, 0, stream>>>(fc, dt, m[0], m[1], m[2], state,
-                                                                                     alive, first, count);
+    k_advance_spans<<<(count + kPropBlock - 1) / kPropBlock, kPropBlock, 0, stream>>>(fc, spans, row_span, first,
+                                                                                      count, state, alive);
+}
+
+void launch_gather_rows(const double* before, const double* after, const int64_t* idx, int count, double* rows,
+                        cudaStream_t stream) {
+    if (count <= 0) return;
+    k_gather_rows<<<(12 * count + kBlock - 1) / kBlock, kBlock, 0, stream>>>(before, after, idx, count, rows);
+}
+
+void launch_clear_alive(uint8_t* alive, const int64_t* idx, int count, cudaStream_t stream) {
+    if (count <= 0) return;
+    k_clear_alive<<<(count + kBlock - 1) / kBlock, kBlock, 0, stream>>>(alive, idx, count);
 }
 
 void launch_screen_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
