@@ -148,16 +148,18 @@ __device__ __forceinline__ double closest_approach_exact(const Hermite& h) {
     double a = 0.0, b = 1.0;
     double c = xsub(b, xmul(g, xsub(b, a))), d = xadd(a, xmul(g, xsub(b, a)));
     double fc = h.f(c), fd = h.f(d);
+    // Branch-free form of the reference's loop (the same operations on every
+    // lane, one evaluation of f per iteration): keep [a, d] with a new point
+    // b - g (b - a) when f(c) < f(d), else [c, b] with a new point a + g (b - a).
     for (int it = 0; it < 60; ++it) {
-        if (fc < fd) {
-            b = d; d = c; fd = fc;
-            c = xsub(b, xmul(g, xsub(b, a)));
-            fc = h.f(c);
-        } else {
-            a = c; c = d; fc = fd;
-            d = xadd(a, xmul(g, xsub(b, a)));
-            fd = h.f(d);
-        }
+        const bool left = fc < fd;
+        const double na = left ? a : c, nb = left ? d : b;
+        const double step = xmul(g, xsub(nb, na));
+        const double x = left ? xsub(nb, step) : xadd(na, step);
+        const double fx = h.f(x);
+        const double nc = left ? x : d, nd = left ? c : x;
+        const double nfc = left ? fx : fd, nfd = left ? fc : fx;
+        a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
     }
     return xmul(0.5, xadd(a, b));
 }

@@ -1024,7 +1024,14 @@ __device__ __forceinline__ unsigned int row_block_items(int a, int tc, int per) 
     return static_cast<unsigned int>((tc - a + per - 1) / per);
 }
 
-// Warp per cell: the length L of the cell's column list (own objects plus the
+// Items of a cell with ta row blocks over tc column blocks.
+__device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
+    unsigned int items = 0;
+    for (int a = 0; a < ta; ++a) items += row_block_items(a, tc, per);
+    return items;
+}
+
+// Lane per cell: the length L of the cell's column list (own objects plus the
 // forward neighbours'), the candidate-pair count k(k-1)/2 + k(L-k) (the pairs
 // the reference visits, src/core/collision.cpp:522-538) and the work items.
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
@@ -1032,66 +1039,85 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
                                                         unsigned int* __restrict__ item_count,
                                                         int* __restrict__ cell_len, int per) {
     const int nc = ctrl->n_cells;
-    const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long cand = 0;
     int biggest = 0;
-    for (int c = gw; c < nc; c += nw) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
         int other = 0;
-        if (lane < 13) {
-            const int f = nbr[13 * static_cast<int64_t>(c) + lane];
-            if (f >= 0) other = cell_begin[f + 1] - cell_begin[f];
+        const int* nb = nbr + 13 * static_cast<int64_t>(c);
+#pragma unroll
+        for (int o = 0; o < 13; ++o) {
+            const int f = nb[o];
+            if (f >= 0) other += cell_begin[f + 1] - cell_begin[f];
         }
-        other = warp_sum(other);
         const int L = k + other;
-        const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-        unsigned int items = 0;
-        for (int a = lane; a < ta; a += 32) items += row_block_items(a, tc, per);
-        items = warp_sum(items);
-        if (lane == 0) {
-            item_count[c] = items;
-            cell_len[c] = L;
-            cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
-            biggest = max(biggest, k);
-        }
+        item_count[c] = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
+        cell_len[c] = L;
+        cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
+        biggest = max(biggest, k);
     }
-    if (lane == 0) {
+    cand = warp_sum(cand);
+    biggest = warp_max(biggest);
+    if ((threadIdx.x & 31) == 0) {
         if (cand) atomicAdd(&ctrl->candidates, cand);
         if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
     }
 }
 
-// Warp per cell: writes the cell's work items at its scanned offset, row
-// blocks spread over the lanes.
+// Writes every cell's work items at its scanned offset: a lane writes the
+// items of a cell with at most 32 of them; the warp writes larger cells'
+// together, row blocks spread over the lanes.
 __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ item_off,
                                                         int4* __restrict__ items, int64_t items_cap, int per) {
     const int nc = ctrl->n_cells;
     const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     bool over = false;
-    for (int c = gw; c < nc; c += nw) {
-        const int k = cell_begin[c + 1] - cell_begin[c];
-        const int L = cell_len[c];
-        const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-        int64_t base = item_off[c];
-        for (int a0 = 0; a0 < ta; a0 += 32) {
-            const int a = a0 + lane;
-            const unsigned int mine = a < ta ? row_block_items(a, tc, per) : 0u;
-            unsigned int incl = mine;
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nc; base += stride) {
+        const int c = base + lane;
+        int k = 0, L = 0;
+        unsigned int n_items = 0;
+        if (c < nc) {
+            k = cell_begin[c + 1] - cell_begin[c];
+            L = cell_len[c];
+            n_items = (c + 1 < nc ? item_off[c + 1] : static_cast<unsigned int>(ctrl->n_items)) - item_off[c];
+        }
+        const bool small = c < nc && n_items <= 32;
+        if (small) {
+            const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
+            int64_t w = item_off[c];
+            for (int a = 0; a < ta; ++a)
+                for (int cb = a; cb < tc; cb += per, ++w) {
+                    if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
+                    else over = true;
+                }
+        }
+        unsigned big = __ballot_sync(0xffffffffu, c < nc && !small);
+        while (big) {
+            const int src = __ffs(big) - 1;
+            big &= big - 1;
+            const int cc = base + src;
+            const int kk = __shfl_sync(0xffffffffu, k, src), LL = __shfl_sync(0xffffffffu, L, src);
+            const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
+            int64_t wbase = item_off[cc];
+            for (int a0 = 0; a0 < ta; a0 += 32) {
+                const int a = a0 + lane;
+                const unsigned int mine = a < ta ? row_block_items(a, tc, per) : 0u;
+                unsigned int incl = mine;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                int64_t w = wbase + (incl - mine);
+                for (int cb = a; a < ta && cb < tc; cb += per, ++w) {
+                    if (w < items_cap) items[w] = make_int4(cc, a, cb, min(per, tc - cb));
+                    else over = true;
+                }
+                wbase += __shfl_sync(0xffffffffu, incl, 31);
             }
-            int64_t w = base + (incl - mine);
-            for (int cb = a; a < ta && cb < tc; cb += per, ++w) {
-                if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
-                else over = true;
-            }
-            base += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
     if (over) atomicOr(&ctrl->flags, FLAG_ITEMS_OVERFLOW);
@@ -1935,14 +1961,14 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
                                                a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
-    k_items_count<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
+    k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_begin, b.nbr, b.item_count, b.cell_len, a.tune.item_col_blocks);
     // Offsets of each cell's work items, and their total.
     const int st = static_cast<int>((b.cap + kScanTile - 1) / kScanTile);
     k_scan_partials<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
     k_scan_small<<<1, 1024, 0, stream>>>(b.scan_part, st, reinterpret_cast<unsigned int*>(&a.ctrl->n_items));
     k_scan_apply<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
-    k_items_write<<<grid_for(32 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
+    k_items_write<<<grid_for(a.n, 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_begin, b.cell_len, b.item_count, b.items, b.items_cap, a.tune.item_col_blocks);
 }
 
