@@ -528,6 +528,7 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
             a.ctrl->grid = g;
             a.ctrl->vmax_true = a.ctrl->spec_vmax;
             check_pack_width(g, a.pack_bits, a.ctrl);
+            if (g.bits + 1 > 8 * a.sort_passes) atomicOr(&a.ctrl->flags, FLAG_SORT_BITS);
         }
     }
     __syncthreads();
@@ -557,6 +558,8 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
 __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* __restrict__ before,
                                                      const uint8_t* __restrict__ alive_after,
                                                      unsigned long long* __restrict__ keys) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.ctrl->grid.bits + 1 > 8 * a.sort_passes)
+        atomicOr(&a.ctrl->flags, FLAG_SORT_BITS);  // more key bits than the sort's passes cover
     const unsigned long long vt = a.ctrl->vmax_true;
     if (vt == a.ctrl->spec_vmax) return;
     __shared__ GridParams g;
@@ -567,6 +570,7 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
             a.ctrl->grid = g;
             atomicOr(&a.ctrl->flags, FLAG_KEYS_REBUILT);
             check_pack_width(g, a.pack_bits, a.ctrl);
+            if (g.bits + 1 > 8 * a.sort_passes) atomicOr(&a.ctrl->flags, FLAG_SORT_BITS);
         }
     }
     // The propagation's digit histogram described the old keys: clear it for the recount.
@@ -743,26 +747,12 @@ __global__ void __launch_bounds__(kBlock) k_sort_upsweep(const unsigned long lon
     }
 }
 
-// Exclusive scan over the 256 digits of each pass; flags keys wider than the
-// passes cover (ctrl, if given).
-__global__ void __launch_bounds__(kBlock) k_sort_digit_scan(unsigned int* __restrict__ hist, int passes,
-                                                            Ctrl* ctrl) {
-    if (ctrl && threadIdx.x == 0 && ctrl->grid.bits + 1 > 8 * passes) atomicOr(&ctrl->flags, FLAG_SORT_BITS);
-    for (int pass = 0; pass < passes; ++pass) {
-        const unsigned int c = hist[pass * 256 + threadIdx.x];
-        unsigned int tot;
-        const unsigned int e = block_exclusive_scan(c, &tot);
-        hist[pass * 256 + threadIdx.x] = e;
-        __syncthreads();
-    }
-}
-
 __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long long* __restrict__ keys_in,
                                                           const int* __restrict__ idx_in,
                                                           unsigned long long* __restrict__ keys_out,
                                                           int* __restrict__ idx_out, int n,
                                                           const int* __restrict__ n_dev, int shift,
-                                                          const unsigned int* __restrict__ digit_base,
+                                                          const unsigned int* __restrict__ digit_hist,
                                                           unsigned int* __restrict__ status,
                                                           unsigned int* __restrict__ ticket, int* flags,
                                                           int packed) {
@@ -784,18 +774,27 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
     const int tile0 = tile * kSortTile;
     if (tile0 >= n) return;  // tickets are in order: no later tile waits on this one
     const int count = min(kSortTile, n - tile0);
+    // Where each digit's keys start in the output: exclusive scan of the pass's histogram.
+    unsigned int hist_total;
+    const unsigned int digit_start = block_exclusive_scan(digit_hist[threadIdx.x], &hist_total);
 
     constexpr int kPerWarp = kSortTile / kWarps;
     constexpr int kRounds = kPerWarp / 32;
     unsigned long long k[kRounds];
     int id[kRounds];
     unsigned d[kRounds];
+    // Every load of the thread in flight first, then the ranking.
+#pragma unroll
     for (int r = 0; r < kRounds; ++r) {
         const int l = warp * kPerWarp + r * 32 + lane;
         const bool valid = l < count;
         const int p = tile0 + l;
         k[r] = valid ? keys_in[p] : 0ull;
         id[r] = (valid && !packed) ? (idx_in ? idx_in[p] : p) : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+        const bool valid = (warp * kPerWarp + r * 32 + lane) < count;
         d[r] = valid ? static_cast<unsigned>((k[r] >> shift) & 0xFF) : 256u + lane;
         const unsigned peers = __match_any_sync(0xffffffffu, d[r]);
         if (valid && lane == __ffs(peers) - 1) wcnt[warp][d[r]] += __popc(peers);
@@ -830,7 +829,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
     }
     unsigned int unused;
     const unsigned int start = block_exclusive_scan(tot, &unused);
-    gbase[t] = static_cast<int>(digit_base[t] + excl) - static_cast<int>(start);
+    gbase[t] = static_cast<int>(digit_start + excl) - static_cast<int>(start);
     unsigned int run = start;
     for (int w = 0; w < kWarps; ++w) {
         const unsigned int c = wcnt[w][t];
@@ -1885,7 +1884,6 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
     k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, nullptr, passes, b.sort_hist, a.ctrl,
                                                   counted ? 1 : 0, a.pack_bits);
-    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.sort_hist, passes, a.ctrl);
     for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
@@ -1935,7 +1933,6 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
                                                        pb);
     k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.conj_keys[0], cap, &chunk->sort_n, kPasses, b.conj_hist, nullptr,
                                                   0, pb);
-    k_sort_digit_scan<<<1, kBlock, 0, stream>>>(b.conj_hist, kPasses, nullptr);
     for (int pass = 0; pass < kPasses; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
