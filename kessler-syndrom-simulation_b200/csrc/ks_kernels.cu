@@ -1023,6 +1023,11 @@ __device__ __forceinline__ unsigned int row_block_items(int a, int tc, int per) 
     return static_cast<unsigned int>((tc - a + per - 1) / per);
 }
 
+// Cells whose items are expensive (more than one row block, or a long column
+// list): their items are handed out first, so that the pair kernel ends on
+// cheap items (largest first).
+__device__ __forceinline__ bool heavy_cell(int k, int L) { return k > 32 || L > 128; }
+
 // Items of a cell with ta row blocks over tc column blocks.
 __device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
     unsigned int items = 0;
@@ -1051,7 +1056,9 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
             if (f >= 0) other += cell_begin[f + 1] - cell_begin[f];
         }
         const int L = k + other;
-        item_count[c] = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
+        // Items of heavy cells get the first tickets of the pair kernel
+        // (scanned here); light cells' items are placed after them by k_items_write.
+        item_count[c] = heavy_cell(k, L) ? cell_items((k + 31) >> 5, (L + 31) >> 5, per) : 0u;
         cell_len[c] = L;
         cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
         biggest = max(biggest, k);
@@ -1064,41 +1071,52 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
     }
 }
 
-// Writes every cell's work items at its scanned offset: a lane writes the
-// items of a cell with at most 32 of them; the warp writes larger cells'
-// together, row blocks spread over the lanes.
+// Writes every cell's work items. Heavy cells' items go to their scanned
+// offsets (ctrl->n_items holds their total on entry); light cells' items
+// follow, one atomic per block for their place. A lane writes the items of a
+// cell with at most 32 of them; the warp writes larger cells' together, row
+// blocks spread over the lanes. On exit ctrl->n_items is the total.
 __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ item_off,
                                                         int4* __restrict__ items, int64_t items_cap, int per) {
+    __shared__ unsigned int light_base;
     const int nc = ctrl->n_cells;
     const int lane = threadIdx.x & 31;
     bool over = false;
     const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nc; base += stride) {
-        const int c = base + lane;
+    // Block-uniform loop: light cells take their places with one block-wide scan.
+    for (int blk = blockIdx.x * blockDim.x; blk < nc; blk += stride) {
+        const int c = blk + threadIdx.x;
         int k = 0, L = 0;
         unsigned int n_items = 0;
+        bool heavy = false;
         if (c < nc) {
             k = cell_begin[c + 1] - cell_begin[c];
             L = cell_len[c];
-            n_items = (c + 1 < nc ? item_off[c + 1] : static_cast<unsigned int>(ctrl->n_items)) - item_off[c];
+            heavy = heavy_cell(k, L);
+            n_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
         }
+        unsigned int light_total;
+        const unsigned int light_off = block_exclusive_scan(c < nc && !heavy ? n_items : 0u, &light_total);
+        if (threadIdx.x == 0) light_base = light_total ? atomicAdd(&ctrl->n_items, static_cast<int>(light_total)) : 0u;
+        __syncthreads();
         const bool small = c < nc && n_items <= 32;
         if (small) {
             const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-            int64_t w = item_off[c];
+            int64_t w = heavy ? static_cast<int64_t>(item_off[c]) : static_cast<int64_t>(light_base) + light_off;
             for (int a = 0; a < ta; ++a)
                 for (int cb = a; cb < tc; cb += per, ++w) {
                     if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
                     else over = true;
                 }
         }
+        // Cells with more than 32 items are heavy (more than one row block).
         unsigned big = __ballot_sync(0xffffffffu, c < nc && !small);
         while (big) {
             const int src = __ffs(big) - 1;
             big &= big - 1;
-            const int cc = base + src;
+            const int cc = blk + (threadIdx.x & ~31) + src;
             const int kk = __shfl_sync(0xffffffffu, k, src), LL = __shfl_sync(0xffffffffu, L, src);
             const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
             int64_t wbase = item_off[cc];
@@ -1118,6 +1136,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
                 wbase += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
+        __syncthreads();  // light_base is rewritten by the next round
     }
     if (over) atomicOr(&ctrl->flags, FLAG_ITEMS_OVERFLOW);
 }
