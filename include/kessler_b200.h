@@ -106,7 +106,9 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * apart, for tiles of at least this many rows; 0 = off), "cell_scale_permille"
  * (1000..4000: grid cell edge = the reference's edge x value/1000),
  * "prop_block" (32..128, threads per block of the propagation kernels),
- * "item_col_blocks" (1..64, column blocks of 32 per pair-kernel work item).
+ * "item_col_blocks" (1..64, column blocks of 32 per pair-kernel work item),
+ * "pack_keys" (1: the radix sort carries the object index in the low bits of
+ * its keys where they leave room, the default; 0: a separate index array).
  * Conjunctions, refined and co-orbiting counts and states never change;
  * candidate_pairs and cell_km change with the cell edge. */
 int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value);

@@ -72,6 +72,7 @@ struct ks_ctx {
     void* frag_scratch = nullptr;  // device staging of fragmentation work (parent rows, spans)
     size_t frag_scratch_bytes = 0;
     bool pack_keys = true;     // object index packed below the cell key in the sort keys
+    bool allow_pack = true;    // tuning: packing allowed where the keys leave room
     int realisations = 1;
     int rbits = 0;
     std::vector<int64_t> offsets;  // realisation offsets (batches)
@@ -603,7 +604,7 @@ int seed_speculation(ks_ctx* ctx) {
     const int bits = estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale);
     ctx->sort_passes = passes_for_bits(bits);
     // Keys, dead flag and object index in 64 bits, with 2 bits to spare for the estimate.
-    ctx->pack_keys = bits + 1 + index_bits(ctx->n) + 2 <= 64;
+    ctx->pack_keys = ctx->allow_pack && bits + 1 + index_bits(ctx->n) + 2 <= 64;
     drop_graphs(ctx);
     return KS_OK;
 }
@@ -1154,6 +1155,13 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     } else if (k == "box_min_rows" && value >= 0 && value <= 33) ctx->tune.box_min_rows = static_cast<int>(value);
     else if (k == "prop_block" && value >= 32 && value <= 128 && value % 32 == 0) ctx->tune.prop_block = static_cast<int>(value);
     else if (k == "item_col_blocks" && value >= 1 && value <= 64) ctx->tune.item_col_blocks = static_cast<int>(value);
+    else if (k == "pack_keys" && (value == 0 || value == 1)) {
+        ctx->allow_pack = value != 0;
+        if (ctx->has_pop) {
+            drop_graphs(ctx);
+            return seed_speculation(ctx);
+        }
+    }
     else if (k == "cell_scale_permille" && value >= 1000 && value <= 4000) {
         ctx->tune.cell_scale = static_cast<double>(value) / 1000.0;
         if (ctx->has_pop) {

@@ -59,3 +59,35 @@ def test_autotune_keeps_results(engine, oracle, ks, precision):
             engine.set_tuning(key, val)
         engine.set_steps_per_graph(32)
         engine.set_precision(ks.PRECISION_FP64)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_unpacked_sort_keys_give_the_same_results(engine, oracle, ks, precision):
+    # Sort keys without the packed object index (the path taken when cell keys
+    # are too wide to leave room for it) against the default packed keys.
+    st, sz, al = ks.generate_population(502, 5000, 30000, 8, 3600.0)
+    prec = ks.PRECISION_SPLIT if precision == "split" else ks.PRECISION_FP64
+
+    def run(pack):
+        engine.set_tuning("pack_keys", pack)
+        engine.set_precision(prec)
+        engine.set_steps_per_graph(16)
+        engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
+        engine.set_screening(True, 5.0, 1.0, 0.01)
+        engine.set_population(st, sz, al)
+        engine.run(20)
+        return engine.get_population(), engine.take_conjunctions(), engine.take_step_stats()
+
+    try:
+        packed, unpacked = run(1), run(0)
+    finally:
+        engine.set_tuning("pack_keys", 1)
+        engine.set_precision(ks.PRECISION_FP64)
+    assert np.array_equal(packed[0][0], unpacked[0][0]) and np.array_equal(packed[0][1], unpacked[0][1])
+    assert_same_conj(packed[1], unpacked[1])
+    for f in ("candidate_pairs", "refined_pairs", "co_orbiting", "conjunctions", "cell_km", "max_cell_objects"):
+        assert np.array_equal(packed[2][f], unpacked[2][f]), f
+    if precision == "fp64":
+        want = oracle.run(st, sz, al, steps=20)
+        assert np.array_equal(unpacked[0][0], want[0])
+        assert_same_conj(unpacked[1], want[2])
