@@ -126,8 +126,8 @@ void free_objects(ks_ctx* ctx) {
     ks::DeviceBuffers& b = ctx->b;
     for (int k = 0; k < 2; ++k) { dfree(b.state[k]); dfree(b.alive[k]); dfree(b.keys[k]); dfree(b.idx[k]); }
     dfree(b.size_m); dfree(b.real_id); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
-    dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr); dfree(b.scan_part); dfree(b.item_count);
-    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.cell_len); dfree(b.nbr); dfree(b.hash_keys); dfree(b.hash_vals);
+    dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr);
+    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted32); dfree(b.sorted_orig);
     b.cap = 0;
     b.hash_cap = 0;
@@ -155,13 +155,12 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.sort_hist, sizeof(unsigned int) * 8 * 256));
     KS_CUDA(cudaMalloc(&b.sort_status, sizeof(unsigned int) * b.sort_status_len));
     KS_CUDA(cudaMalloc(&b.sort_ctr, sizeof(unsigned int) * 8));
-    KS_CUDA(cudaMalloc(&b.scan_part, sizeof(unsigned int) * ((cap + 4095) / 4096 + 1)));
-    KS_CUDA(cudaMalloc(&b.item_count, sizeof(unsigned int) * (cap + 1)));
     KS_CUDA(cudaMalloc(&b.block_counts, sizeof(int) * ((cap + 1023) / 1024 + 1)));
     KS_CUDA(cudaMalloc(&b.cell_begin, sizeof(int) * (cap + 1)));
     KS_CUDA(cudaMalloc(&b.cell_key, sizeof(unsigned long long) * cap));
-    KS_CUDA(cudaMalloc(&b.cell_len, sizeof(int) * cap));
     KS_CUDA(cudaMalloc(&b.nbr, sizeof(int) * 13 * cap));
+    KS_CUDA(cudaMalloc(&b.cell_len, sizeof(int) * cap));
+    KS_CUDA(cudaMalloc(&b.item_part, sizeof(unsigned int) * ((cap + 255) / 256 + 1)));
     int64_t h = 16;
     while (h < 2 * cap) h <<= 1;
     b.hash_cap = h;
@@ -494,12 +493,13 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
         int flags = ctx->h_chunk->flags;
         unsigned long long max_refined = 0;
-        int max_bits = 0, max_items = 0;
+        int max_bits = 0;
+        int64_t max_items = 0;
         for (int k = 0; k < k_steps; ++k) {
             flags |= ctx->h_ctrl[k].flags;
             max_refined = std::max(max_refined, ctx->h_ctrl[k].refined);
             max_bits = std::max(max_bits, ctx->h_ctrl[k].grid.bits);
-            max_items = std::max(max_items, ctx->h_ctrl[k].n_items);
+            max_items = std::max(max_items, ks::items_total(ctx->h_ctrl[k]));
         }
         const bool surv_over = max_refined > static_cast<unsigned long long>(ctx->b.surv_cap);
         const bool items_over = max_items > ctx->b.items_cap;
@@ -517,7 +517,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
             drop_graphs(ctx);
         }
         if (surv_over && (rc = ensure_survivors(ctx, static_cast<int64_t>(max_refined) * 2))) return rc;
-        if (items_over && (rc = ensure_items(ctx, static_cast<int64_t>(max_items) * 3 / 2 + 1024))) return rc;
+        if (items_over && (rc = ensure_items(ctx, max_items * 3 / 2 + 1024))) return rc;
         if ((flags & ks::FLAG_CONJ_OVERFLOW) &&
             (rc = ensure_conj(ctx, static_cast<int64_t>(ctx->h_chunk->conj_count) * 2)))
             return rc;
@@ -1696,7 +1696,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         const Ctrl& c = ctx->h_ctrl[0];
         const int flags = c.flags | ctx->h_chunk->flags;
         const bool surv_over = c.refined > static_cast<unsigned long long>(ctx->b.surv_cap);
-        const bool items_over = c.n_items > ctx->b.items_cap;
+        const bool items_over = ks::items_total(c) > ctx->b.items_cap;
         if (flags & ks::FLAG_KEY_RANGE) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits"); }
         if (flags & ks::FLAG_TIMEOUT) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up"); }
         if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) {
@@ -1713,7 +1713,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         if (attempt >= kMaxReplays) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_OVERFLOW, "ks_screen: buffers overflow"); }
         if (flags & ks::FLAG_SORT_BITS) ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(c.grid.bits));
         if (surv_over && (rc = ensure_survivors(ctx, static_cast<int64_t>(c.refined) * 2))) { ctx->dt = saved_dt; return rc; }
-        if (items_over && (rc = ensure_items(ctx, static_cast<int64_t>(c.n_items) * 3 / 2 + 1024))) { ctx->dt = saved_dt; return rc; }
+        if (items_over && (rc = ensure_items(ctx, ks::items_total(c) * 3 / 2 + 1024))) { ctx->dt = saved_dt; return rc; }
         if ((flags & ks::FLAG_CONJ_OVERFLOW) && (rc = ensure_conj(ctx, static_cast<int64_t>(ctx->h_chunk->conj_count) * 2))) {
             ctx->dt = saved_dt;
             return rc;

@@ -78,12 +78,16 @@ struct Ctrl {
     unsigned long long exact_evals;    // candidates that needed the full filter
     int n_alive;                       // alive after the step
     int n_cells;
-    int n_items;                       // pair work items
+    unsigned int n_heavy;              // pair work items of heavy cells (front of the item array)
+    unsigned int n_light;              // pair work items of light cells (back of the item array)
     unsigned int item_ticket;          // next pair work item to hand out
     int max_cell;
     int flags;
     GridParams grid;
 };
+
+// Pair work items of a step.
+inline int64_t items_total(const Ctrl& c) { return static_cast<int64_t>(c.n_heavy) + c.n_light; }
 
 struct ChunkCtrl {
     unsigned long long conj_count;     // records appended in this chunk
@@ -105,13 +109,12 @@ struct DeviceBuffers {
     unsigned int* sort_status = nullptr;   // look-back words: passes x tiles x 256
     int64_t sort_status_len = 0;
     unsigned int* sort_ctr = nullptr;      // tile tickets, one per pass
-    unsigned int* scan_part = nullptr;     // partial sums of the device-wide scans
     int* block_counts = nullptr;           // cell heads per tile
     int* cell_begin = nullptr;             // cap + 1
     unsigned long long* cell_key = nullptr;
-    int* cell_len = nullptr;               // per cell: length of its column list
     int* nbr = nullptr;                    // 13 per cell
-    unsigned int* item_count = nullptr;    // work items per cell, then their offsets
+    int* cell_len = nullptr;               // per cell: length of its column list
+    unsigned int* item_part = nullptr;     // heavy cells' work items per chunk of 256 cells, then offsets
     int4* items = nullptr;
     int64_t items_cap = 0;
     unsigned long long* hash_keys = nullptr;

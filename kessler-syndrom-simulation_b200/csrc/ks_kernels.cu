@@ -246,7 +246,7 @@ __device__ void ctrl_reset(Ctrl& c) {
     c.vmax_true = 0ull;
     c.candidates = c.co_orbiting = c.refined = c.conj = c.object_steps = c.exact_evals = 0ull;
     c.n_alive = c.n_cells = c.max_cell = c.flags = 0;
-    c.n_items = 0;
+    c.n_heavy = c.n_light = 0u;
     c.item_ticket = 0u;
     c.grid = GridParams{};
 }
@@ -590,10 +590,8 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
 }
 
 // ---------------------------------------------------------------------------
-// Device-wide exclusive scan of u32 counters (length read from device memory)
+// Block and single-block exclusive scans of u32 counters
 // ---------------------------------------------------------------------------
-
-constexpr int kScanTile = 4096;  // 256 threads x 16
 
 __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int v, unsigned int* total) {
     __shared__ unsigned int wsum[kWarps];
@@ -615,32 +613,12 @@ __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int v, uns
     return off + incl - v;
 }
 
-// Per-tile sums of v[0..len).
-__global__ void __launch_bounds__(kBlock) k_scan_partials(const unsigned int* __restrict__ v, const int* len_ptr,
-                                                          int len_fixed, unsigned int* __restrict__ part) {
-    const int len = len_ptr ? *len_ptr : len_fixed;
-    const int base = blockIdx.x * kScanTile;
-    unsigned int s = 0;
-    if (base < len)
-        for (int j = threadIdx.x; j < kScanTile; j += kBlock) {
-            const int p = base + j;
-            if (p < len) s += v[p];
-        }
-    s = warp_sum(s);
-    __shared__ unsigned int sh[kWarps];
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int t = 0;
-        for (int w = 0; w < kWarps; ++w) t += sh[w];
-        part[blockIdx.x] = t;
-    }
-}
-
 // Exclusive scan in place, one block, coalesced rounds of 1024 entries.
 // Optionally stores the grand total.
+// With n_cells, the length is one entry per chunk of kBlock cells.
 __global__ void __launch_bounds__(1024) k_scan_small(unsigned int* __restrict__ v, int len,
-                                                     unsigned int* __restrict__ total) {
+                                                     unsigned int* __restrict__ total, const int* n_cells) {
+    if (n_cells) len = min(len, (*n_cells + kBlock - 1) / kBlock);
     __shared__ unsigned int wsum[32];
     __shared__ unsigned int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -672,28 +650,6 @@ __global__ void __launch_bounds__(1024) k_scan_small(unsigned int* __restrict__ 
         __syncthreads();
     }
     if (total && threadIdx.x == 0) *total = carry;
-}
-
-// out[p] = exclusive prefix of v at p (in place allowed), tile offsets from part.
-__global__ void __launch_bounds__(kBlock) k_scan_apply(unsigned int* __restrict__ v, const int* len_ptr, int len_fixed,
-                                                       const unsigned int* __restrict__ part) {
-    const int len = len_ptr ? *len_ptr : len_fixed;
-    const int base = blockIdx.x * kScanTile;
-    if (base >= len) return;
-    constexpr int kPer = kScanTile / kBlock;
-    const int p0 = base + threadIdx.x * kPer;
-    unsigned int x[kPer];
-    unsigned int s = 0;
-    for (int j = 0; j < kPer; ++j) {
-        x[j] = (p0 + j < len) ? v[p0 + j] : 0u;
-        s += x[j];
-    }
-    unsigned int tot;
-    unsigned int run = part[blockIdx.x] + block_exclusive_scan(s, &tot);
-    for (int j = 0; j < kPer; ++j) {
-        if (p0 + j < len) v[p0 + j] = run;
-        run += x[j];
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1037,31 +993,37 @@ __device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
 
 // Lane per cell: the length L of the cell's column list (own objects plus the
 // forward neighbours'), the candidate-pair count k(k-1)/2 + k(L-k) (the pairs
-// the reference visits, src/core/collision.cpp:522-538) and the work items.
+// the reference visits, src/core/collision.cpp:522-538), and per chunk of
+// kBlock cells the number of heavy cells' work items (part[chunk]).
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
-                                                        const int* __restrict__ nbr,
-                                                        unsigned int* __restrict__ item_count,
-                                                        int* __restrict__ cell_len, int per) {
+                                                        const int* __restrict__ nbr, int* __restrict__ cell_len,
+                                                        unsigned int* __restrict__ part, int per) {
     const int nc = ctrl->n_cells;
     unsigned long long cand = 0;
     int biggest = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-        const int b0 = cell_begin[c];
-        const int k = cell_begin[c + 1] - b0;
-        int other = 0;
-        const int* nb = nbr + 13 * static_cast<int64_t>(c);
+    // Block-uniform loop over chunks of kBlock cells.
+    for (int blk = blockIdx.x * blockDim.x; blk < nc; blk += gridDim.x * blockDim.x) {
+        const int c = blk + threadIdx.x;
+        unsigned int heavy_items = 0;
+        if (c < nc) {
+            const int b0 = cell_begin[c];
+            const int k = cell_begin[c + 1] - b0;
+            int other = 0;
+            const int* nb = nbr + 13 * static_cast<int64_t>(c);
 #pragma unroll
-        for (int o = 0; o < 13; ++o) {
-            const int f = nb[o];
-            if (f >= 0) other += cell_begin[f + 1] - cell_begin[f];
+            for (int o = 0; o < 13; ++o) {
+                const int f = nb[o];
+                if (f >= 0) other += cell_begin[f + 1] - cell_begin[f];
+            }
+            const int L = k + other;
+            if (heavy_cell(k, L)) heavy_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
+            cell_len[c] = L;
+            cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
+            biggest = max(biggest, k);
         }
-        const int L = k + other;
-        // Items of heavy cells get the first tickets of the pair kernel
-        // (scanned here); light cells' items are placed after them by k_items_write.
-        item_count[c] = heavy_cell(k, L) ? cell_items((k + 31) >> 5, (L + 31) >> 5, per) : 0u;
-        cell_len[c] = L;
-        cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
-        biggest = max(biggest, k);
+        unsigned int total;
+        block_exclusive_scan(heavy_items, &total);
+        if (threadIdx.x == 0) part[blk / kBlock] = total;
     }
     cand = warp_sum(cand);
     biggest = warp_max(biggest);
@@ -1071,21 +1033,23 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
     }
 }
 
-// Writes every cell's work items. Heavy cells' items go to their scanned
-// offsets (ctrl->n_items holds their total on entry); light cells' items
-// follow, one atomic per block for their place. A lane writes the items of a
-// cell with at most 32 of them; the warp writes larger cells' together, row
-// blocks spread over the lanes. On exit ctrl->n_items is the total.
+// Writes every cell's work items. Heavy cells' items fill the item array from
+// the front in cell order (part: scanned per-chunk offsets, ctrl->n_heavy their
+// total), light cells' from the back (one atomic per block for their place);
+// the pair kernel hands out the front first, so the long items start first. A
+// lane writes the items of a cell with at most 32 of them; the warp writes
+// larger cells' together, row blocks spread over the lanes. When the two ends
+// meet (more items than the array holds) the pair kernel does no work and the
+// host grows the array and replays.
 __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ cell_len,
-                                                        const unsigned int* __restrict__ item_off,
+                                                        const unsigned int* __restrict__ part,
                                                         int4* __restrict__ items, int64_t items_cap, int per) {
     __shared__ unsigned int light_base;
     const int nc = ctrl->n_cells;
     const int lane = threadIdx.x & 31;
     bool over = false;
     const int stride = gridDim.x * blockDim.x;
-    // Block-uniform loop: light cells take their places with one block-wide scan.
     for (int blk = blockIdx.x * blockDim.x; blk < nc; blk += stride) {
         const int c = blk + threadIdx.x;
         int k = 0, L = 0;
@@ -1097,17 +1061,19 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
             heavy = heavy_cell(k, L);
             n_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
         }
-        unsigned int light_total;
+        unsigned int light_total, heavy_total;
         const unsigned int light_off = block_exclusive_scan(c < nc && !heavy ? n_items : 0u, &light_total);
-        if (threadIdx.x == 0) light_base = light_total ? atomicAdd(&ctrl->n_items, static_cast<int>(light_total)) : 0u;
+        const int64_t hoff = static_cast<int64_t>(part[blk / kBlock]) +
+                             block_exclusive_scan(heavy ? n_items : 0u, &heavy_total);
+        if (threadIdx.x == 0) light_base = light_total ? atomicAdd(&ctrl->n_light, light_total) : 0u;
         __syncthreads();
         const bool small = c < nc && n_items <= 32;
         if (small) {
             const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-            int64_t w = heavy ? static_cast<int64_t>(item_off[c]) : static_cast<int64_t>(light_base) + light_off;
+            int64_t w = heavy ? hoff : static_cast<int64_t>(light_base) + light_off;
             for (int a = 0; a < ta; ++a)
                 for (int cb = a; cb < tc; cb += per, ++w) {
-                    if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
+                    if (w < items_cap) items[heavy ? w : items_cap - 1 - w] = make_int4(c, a, cb, min(per, tc - cb));
                     else over = true;
                 }
         }
@@ -1119,7 +1085,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
             const int cc = blk + (threadIdx.x & ~31) + src;
             const int kk = __shfl_sync(0xffffffffu, k, src), LL = __shfl_sync(0xffffffffu, L, src);
             const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
-            int64_t wbase = item_off[cc];
+            int64_t wbase = __shfl_sync(0xffffffffu, hoff, src);
             for (int a0 = 0; a0 < ta; a0 += 32) {
                 const int a = a0 + lane;
                 const unsigned int mine = a < ta ? row_block_items(a, tc, per) : 0u;
@@ -1363,7 +1329,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     __shared__ unsigned qmask[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
-    const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
+    // Heavy cells' items at the front of the array, light cells' at the back;
+    // no work when the two ends met (the host grows the array and replays).
+    const int n_heavy = static_cast<int>(a.ctrl->n_heavy);
+    const int64_t n_all = static_cast<int64_t>(a.ctrl->n_heavy) + a.ctrl->n_light;
+    const int n_items = n_all <= items_cap ? static_cast<int>(n_all) : 0;
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
@@ -1372,7 +1342,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     PairCounters pc;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
-        const int4 item = items[it];
+        const int4 item = items[it < n_heavy ? static_cast<int64_t>(it) : items_cap - 1 - (it - n_heavy)];
         const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
@@ -1598,7 +1568,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     __shared__ unsigned qmask[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
-    const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
+    // Heavy cells' items at the front of the array, light cells' at the back;
+    // no work when the two ends met (the host grows the array and replays).
+    const int n_heavy = static_cast<int>(a.ctrl->n_heavy);
+    const int64_t n_all = static_cast<int64_t>(a.ctrl->n_heavy) + a.ctrl->n_light;
+    const int n_items = n_all <= items_cap ? static_cast<int>(n_all) : 0;
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
@@ -1613,7 +1587,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     PairCounters pc;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
-        const int4 item = items[it];
+        const int4 item = items[it < n_heavy ? static_cast<int64_t>(it) : items_cap - 1 - (it - n_heavy)];
         const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
@@ -1968,7 +1942,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
     const int ntiles = a.n > 0 ? (a.n + kCellTile - 1) / kCellTile : 1;
     unsigned int* bc = reinterpret_cast<unsigned int*>(b.block_counts);
     k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, bc, a.pack_bits);
-    k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr);
+    k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr, nullptr);
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
     k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], bc, a.ctrl, b.cell_begin, b.cell_key,
                                                b.hash_keys, b.hash_vals,
@@ -1977,15 +1951,13 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
                                                a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
-    k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(
-        a.ctrl, b.cell_begin, b.nbr, b.item_count, b.cell_len, a.tune.item_col_blocks);
-    // Offsets of each cell's work items, and their total.
-    const int st = static_cast<int>((b.cap + kScanTile - 1) / kScanTile);
-    k_scan_partials<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
-    k_scan_small<<<1, 1024, 0, stream>>>(b.scan_part, st, reinterpret_cast<unsigned int*>(&a.ctrl->n_items));
-    k_scan_apply<<<st, kBlock, 0, stream>>>(b.item_count, &a.ctrl->n_cells, 0, b.scan_part);
-    k_items_write<<<grid_for(a.n, 8), kBlock, 0, stream>>>(
-        a.ctrl, b.cell_begin, b.cell_len, b.item_count, b.items, b.items_cap, a.tune.item_col_blocks);
+    k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.item_part,
+                                                           a.tune.item_col_blocks);
+    // Offsets of the heavy cells' items per chunk of cells, and their total.
+    k_scan_small<<<1, 1024, 0, stream>>>(b.item_part, static_cast<int>((b.cap + kBlock - 1) / kBlock),
+                                         &a.ctrl->n_heavy, &a.ctrl->n_cells);
+    k_items_write<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.cell_len, b.item_part, b.items,
+                                                           b.items_cap, a.tune.item_col_blocks);
 }
 
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {

@@ -45,13 +45,12 @@ constexpr int64_t scratch_bytes() {
     b += align256(sizeof(unsigned int) * 8 * 256);       // sort_hist
     b += align256(sizeof(unsigned int) * 8 * 256 * ((n + 2047) / 2048));  // sort_status
     b += align256(sizeof(unsigned int) * 8);             // sort_ctr
-    b += align256(sizeof(unsigned int) * ((n + 4095) / 4096 + 1));        // scan_part
     b += align256(sizeof(int) * ((n + 1023) / 1024 + 1));                // block_counts
     b += align256(sizeof(int) * (n + 1));                // cell_begin
     b += align256(sizeof(unsigned long long) * n);       // cell_key
-    b += align256(sizeof(int) * n);                      // cell_len
     b += align256(sizeof(int) * 13 * n);                 // nbr
-    b += align256(sizeof(unsigned int) * (n + 1));       // item_count
+    b += align256(sizeof(int) * n);                      // cell_len
+    b += align256(sizeof(unsigned int) * ((n + 255) / 256 + 1));  // item_part
     b += align256(sizeof(int4) * kNoAllocItems);         // items
     b += align256(sizeof(unsigned long long) * kNoAllocHash);  // hash keys
     b += align256(sizeof(int) * kNoAllocHash);           // hash values
@@ -103,13 +102,12 @@ ks::DeviceBuffers carve(unsigned char* base) {
     b.sort_status_len = 8 * 256 * ((n + 2047) / 2048);
     b.sort_status = take<unsigned int>(p, sizeof(unsigned int) * b.sort_status_len);
     b.sort_ctr = take<unsigned int>(p, sizeof(unsigned int) * 8);
-    b.scan_part = take<unsigned int>(p, sizeof(unsigned int) * ((n + 4095) / 4096 + 1));
     b.block_counts = take<int>(p, sizeof(int) * ((n + 1023) / 1024 + 1));
     b.cell_begin = take<int>(p, sizeof(int) * (n + 1));
     b.cell_key = take<unsigned long long>(p, sizeof(unsigned long long) * n);
-    b.cell_len = take<int>(p, sizeof(int) * n);
     b.nbr = take<int>(p, sizeof(int) * 13 * n);
-    b.item_count = take<unsigned int>(p, sizeof(unsigned int) * (n + 1));
+    b.cell_len = take<int>(p, sizeof(int) * n);
+    b.item_part = take<unsigned int>(p, sizeof(unsigned int) * ((n + 255) / 256 + 1));
     b.items = take<int4>(p, sizeof(int4) * kNoAllocItems);
     b.items_cap = kNoAllocItems;
     b.hash_keys = take<unsigned long long>(p, sizeof(unsigned long long) * kNoAllocHash);
@@ -264,7 +262,7 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
         if (c.refined > static_cast<unsigned long long>(kNoAllocSurvivors))
             return fail(KS_ERR_OVERFLOW, "ks_screen_noalloc: " + std::to_string(c.refined) +
                                              " pairs to refine, fixed capacity " + std::to_string(kNoAllocSurvivors));
-        if (c.n_items > kNoAllocItems)
+        if (ks::items_total(c) > kNoAllocItems)
             return fail(KS_ERR_OVERFLOW, "ks_screen_noalloc: pair work list beyond its fixed capacity");
         if ((flags & ks::FLAG_CONJ_OVERFLOW) || ch.conj_count > static_cast<unsigned long long>(kNoAllocConj))
             return fail(KS_ERR_OVERFLOW, "ks_screen_noalloc: more conjunctions than the fixed capacity " +
