@@ -160,7 +160,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.cell_key, sizeof(unsigned long long) * cap));
     KS_CUDA(cudaMalloc(&b.nbr, sizeof(int) * 13 * cap));
     KS_CUDA(cudaMalloc(&b.cell_len, sizeof(int) * cap));
-    KS_CUDA(cudaMalloc(&b.item_part, sizeof(unsigned int) * ((cap + 255) / 256 + 1)));
+    KS_CUDA(cudaMalloc(&b.item_part, sizeof(unsigned int) * 2 * ((cap + 255) / 256 + 1)));
     int64_t h = 16;
     while (h < 2 * cap) h <<= 1;
     b.hash_cap = h;

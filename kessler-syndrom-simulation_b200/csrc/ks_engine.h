@@ -78,8 +78,7 @@ struct Ctrl {
     unsigned long long exact_evals;    // candidates that needed the full filter
     int n_alive;                       // alive after the step
     int n_cells;
-    unsigned int n_heavy;              // pair work items of heavy cells (front of the item array)
-    unsigned int n_light;              // pair work items of light cells (back of the item array)
+    unsigned int n_items;              // pair work items
     unsigned int item_ticket;          // next pair work item to hand out
     int max_cell;
     int flags;
@@ -87,7 +86,7 @@ struct Ctrl {
 };
 
 // Pair work items of a step.
-inline int64_t items_total(const Ctrl& c) { return static_cast<int64_t>(c.n_heavy) + c.n_light; }
+inline int64_t items_total(const Ctrl& c) { return static_cast<int64_t>(c.n_items); }
 
 struct ChunkCtrl {
     unsigned long long conj_count;     // records appended in this chunk
@@ -114,7 +113,7 @@ struct DeviceBuffers {
     unsigned long long* cell_key = nullptr;
     int* nbr = nullptr;                    // 13 per cell
     int* cell_len = nullptr;               // per cell: length of its column list
-    unsigned int* item_part = nullptr;     // heavy cells' work items per chunk of 256 cells, then offsets
+    unsigned int* item_part = nullptr;     // heavy, then light cells' work items per chunk of 256 cells, then offsets
     int4* items = nullptr;
     int64_t items_cap = 0;
     unsigned long long* hash_keys = nullptr;

@@ -246,7 +246,7 @@ __device__ void ctrl_reset(Ctrl& c) {
     c.vmax_true = 0ull;
     c.candidates = c.co_orbiting = c.refined = c.conj = c.object_steps = c.exact_evals = 0ull;
     c.n_alive = c.n_cells = c.max_cell = c.flags = 0;
-    c.n_heavy = c.n_light = 0u;
+    c.n_items = 0u;
     c.item_ticket = 0u;
     c.grid = GridParams{};
 }
@@ -615,10 +615,11 @@ __device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int v, uns
 
 // Exclusive scan in place, one block, coalesced rounds of 1024 entries.
 // Optionally stores the grand total.
-// With n_cells, the length is one entry per chunk of kBlock cells.
+// With n_cells, the length is per_chunk entries per chunk of kBlock cells.
 __global__ void __launch_bounds__(1024) k_scan_small(unsigned int* __restrict__ v, int len,
-                                                     unsigned int* __restrict__ total, const int* n_cells) {
-    if (n_cells) len = min(len, (*n_cells + kBlock - 1) / kBlock);
+                                                     unsigned int* __restrict__ total, const int* n_cells,
+                                                     int per_chunk) {
+    if (n_cells) len = min(len, per_chunk * ((*n_cells + kBlock - 1) / kBlock));
     __shared__ unsigned int wsum[32];
     __shared__ unsigned int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -994,17 +995,20 @@ __device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
 // Lane per cell: the length L of the cell's column list (own objects plus the
 // forward neighbours'), the candidate-pair count k(k-1)/2 + k(L-k) (the pairs
 // the reference visits, src/core/collision.cpp:522-538), and per chunk of
-// kBlock cells the number of heavy cells' work items (part[chunk]).
+// kBlock cells the number of heavy cells' work items (part[chunk]) and of
+// light cells' (part[chunks + chunk]), so that one scan of part places every
+// heavy item before every light item, each group in cell order.
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr, int* __restrict__ cell_len,
                                                         unsigned int* __restrict__ part, int per) {
     const int nc = ctrl->n_cells;
+    const int chunks = (nc + kBlock - 1) / kBlock;
     unsigned long long cand = 0;
     int biggest = 0;
     // Block-uniform loop over chunks of kBlock cells.
     for (int blk = blockIdx.x * blockDim.x; blk < nc; blk += gridDim.x * blockDim.x) {
         const int c = blk + threadIdx.x;
-        unsigned int heavy_items = 0;
+        unsigned int heavy_items = 0, light_items = 0;
         if (c < nc) {
             const int b0 = cell_begin[c];
             const int k = cell_begin[c + 1] - b0;
@@ -1016,14 +1020,20 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
                 if (f >= 0) other += cell_begin[f + 1] - cell_begin[f];
             }
             const int L = k + other;
-            if (heavy_cell(k, L)) heavy_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
+            const unsigned int n_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
+            if (heavy_cell(k, L)) heavy_items = n_items;
+            else light_items = n_items;
             cell_len[c] = L;
             cand += static_cast<unsigned long long>(k) * (k - 1) / 2 + static_cast<unsigned long long>(k) * other;
             biggest = max(biggest, k);
         }
-        unsigned int total;
-        block_exclusive_scan(heavy_items, &total);
-        if (threadIdx.x == 0) part[blk / kBlock] = total;
+        unsigned int heavy_total, light_total;
+        block_exclusive_scan(heavy_items, &heavy_total);
+        block_exclusive_scan(light_items, &light_total);
+        if (threadIdx.x == 0) {
+            part[blk / kBlock] = heavy_total;
+            part[chunks + blk / kBlock] = light_total;
+        }
     }
     cand = warp_sum(cand);
     biggest = warp_max(biggest);
@@ -1033,20 +1043,17 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
     }
 }
 
-// Writes every cell's work items. Heavy cells' items fill the item array from
-// the front in cell order (part: scanned per-chunk offsets, ctrl->n_heavy their
-// total), light cells' from the back (one atomic per block for their place);
-// the pair kernel hands out the front first, so the long items start first. A
-// lane writes the items of a cell with at most 32 of them; the warp writes
-// larger cells' together, row blocks spread over the lanes. When the two ends
-// meet (more items than the array holds) the pair kernel does no work and the
-// host grows the array and replays.
+// Writes every cell's work items at their scanned places: heavy cells' items
+// first, light cells' after them, each group in cell order (ctrl->n_items is
+// the total); the pair kernel hands them out in that order, so the long items
+// start first. A lane writes the items of a cell with at most 32 of them; the
+// warp writes larger cells' together, row blocks spread over the lanes.
 __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ part,
                                                         int4* __restrict__ items, int64_t items_cap, int per) {
-    __shared__ unsigned int light_base;
     const int nc = ctrl->n_cells;
+    const int chunks = (nc + kBlock - 1) / kBlock;
     const int lane = threadIdx.x & 31;
     bool over = false;
     const int stride = gridDim.x * blockDim.x;
@@ -1062,18 +1069,17 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
             n_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
         }
         unsigned int light_total, heavy_total;
-        const unsigned int light_off = block_exclusive_scan(c < nc && !heavy ? n_items : 0u, &light_total);
+        const int64_t loff = static_cast<int64_t>(part[chunks + blk / kBlock]) +
+                             block_exclusive_scan(c < nc && !heavy ? n_items : 0u, &light_total);
         const int64_t hoff = static_cast<int64_t>(part[blk / kBlock]) +
                              block_exclusive_scan(heavy ? n_items : 0u, &heavy_total);
-        if (threadIdx.x == 0) light_base = light_total ? atomicAdd(&ctrl->n_light, light_total) : 0u;
-        __syncthreads();
         const bool small = c < nc && n_items <= 32;
         if (small) {
             const int ta = (k + 31) >> 5, tc = (L + 31) >> 5;
-            int64_t w = heavy ? hoff : static_cast<int64_t>(light_base) + light_off;
+            int64_t w = heavy ? hoff : loff;
             for (int a = 0; a < ta; ++a)
                 for (int cb = a; cb < tc; cb += per, ++w) {
-                    if (w < items_cap) items[heavy ? w : items_cap - 1 - w] = make_int4(c, a, cb, min(per, tc - cb));
+                    if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
                     else over = true;
                 }
         }
@@ -1102,7 +1108,6 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
                 wbase += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
-        __syncthreads();  // light_base is rewritten by the next round
     }
     if (over) atomicOr(&ctrl->flags, FLAG_ITEMS_OVERFLOW);
 }
@@ -1329,11 +1334,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     __shared__ unsigned qmask[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
-    // Heavy cells' items at the front of the array, light cells' at the back;
-    // no work when the two ends met (the host grows the array and replays).
-    const int n_heavy = static_cast<int>(a.ctrl->n_heavy);
-    const int64_t n_all = static_cast<int64_t>(a.ctrl->n_heavy) + a.ctrl->n_light;
-    const int n_items = n_all <= items_cap ? static_cast<int>(n_all) : 0;
+    const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
@@ -1342,7 +1343,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     PairCounters pc;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
-        const int4 item = items[it < n_heavy ? static_cast<int64_t>(it) : items_cap - 1 - (it - n_heavy)];
+        const int4 item = items[it];
         const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
@@ -1568,11 +1569,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     __shared__ unsigned qmask[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
-    // Heavy cells' items at the front of the array, light cells' at the back;
-    // no work when the two ends met (the host grows the array and replays).
-    const int n_heavy = static_cast<int>(a.ctrl->n_heavy);
-    const int64_t n_all = static_cast<int64_t>(a.ctrl->n_heavy) + a.ctrl->n_light;
-    const int n_items = n_all <= items_cap ? static_cast<int>(n_all) : 0;
+    const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
@@ -1587,7 +1584,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     PairCounters pc;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
-        const int4 item = items[it < n_heavy ? static_cast<int64_t>(it) : items_cap - 1 - (it - n_heavy)];
+        const int4 item = items[it];
         const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
@@ -1942,7 +1939,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
     const int ntiles = a.n > 0 ? (a.n + kCellTile - 1) / kCellTile : 1;
     unsigned int* bc = reinterpret_cast<unsigned int*>(b.block_counts);
     k_cell_count<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], a.ctrl, bc, a.pack_bits);
-    k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr, nullptr);
+    k_scan_small<<<1, 1024, 0, stream>>>(bc, ntiles, nullptr, nullptr, 1);
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
     k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], bc, a.ctrl, b.cell_begin, b.cell_key,
                                                b.hash_keys, b.hash_vals,
@@ -1953,9 +1950,9 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
     k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.item_part,
                                                            a.tune.item_col_blocks);
-    // Offsets of the heavy cells' items per chunk of cells, and their total.
-    k_scan_small<<<1, 1024, 0, stream>>>(b.item_part, static_cast<int>((b.cap + kBlock - 1) / kBlock),
-                                         &a.ctrl->n_heavy, &a.ctrl->n_cells);
+    // Offsets of the heavy, then the light cells' items per chunk of cells, and their total.
+    k_scan_small<<<1, 1024, 0, stream>>>(b.item_part, static_cast<int>(2 * ((b.cap + kBlock - 1) / kBlock)),
+                                         &a.ctrl->n_items, &a.ctrl->n_cells, 2);
     k_items_write<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.cell_len, b.item_part, b.items,
                                                            b.items_cap, a.tune.item_col_blocks);
 }
