@@ -1512,43 +1512,68 @@ __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, 
     return fast && separating && convex;
 }
 
+// Exact FP64 filter (src/core/collision_filter.hpp) of up to 32 queued pairs
+// (column's sorted position, row of the tile), one pair per lane.
+__device__ __forceinline__ void exact_flush(const int2* fq, int count, const double* __restrict__ sorted,
+                                            const int* __restrict__ orig, const double2 (*rows)[3], const int* rorig,
+                                            const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
+                                            PairCounters& pc) {
+    const int lane = threadIdx.x & 31;
+    int res = FILTER_REJECT;
+    int row_orig = 0, col_orig = 0;
+    if (lane < count) {
+        const int2 e = fq[lane];
+        const SortedState col = load_sorted(sorted, e.x);
+        col_orig = orig[e.x];
+        const double2 ra = rows[e.y][0], rb = rows[e.y][1], rc = rows[e.y][2];
+        row_orig = rorig[e.y];
+        ++pc.full;
+        res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
+                                xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
+        if (res == FILTER_CO_ORBITING) ++pc.co;
+    }
+    append_pairs(res == FILTER_REFINE, row_orig, col_orig, a.ctrl, surv, surv_cap);
+}
+
+// Rows flagged by the FP32 gate for the lane's column q: the FP32 convexity
+// test drops the pairs it proves rejected, the rest join the warp's queue fq
+// (fcount entries, at most 63), which runs the exact filter 32 pairs at a time.
 __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ sorted,
                                                const int* __restrict__ orig, const float4 (*rows32)[2],
                                                const double2 (*rows)[3], const int* rorig, float vmin2e,
                                                const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
-                                               PairCounters& pc) {
+                                               PairCounters& pc, int2* fq, int& fcount) {
+    const int lane = threadIdx.x & 31;
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
     // FP32 convexity pass: drop rows no lane still needs.
     unsigned still = 0u;
-    {
-        unsigned t = todo;
-        while (t) {
-            const int r = __ffs(t) - 1;
-            t &= t - 1;
-            if ((need >> r) & 1u) {
-                const float4 rp = rows32[r][0], rv = rows32[r][1];
-                if (!certainly_convex_reject_f32(cp.x - rp.x, cp.y - rp.y, cp.z - rp.z, cv.x - rv.x, cv.y - rv.y,
-                                                 cv.z - rv.z, vmin2e))
-                    still |= 1u << r;
-            }
-        }
-    }
-    todo = __reduce_or_sync(0xffffffffu, still);
-    if (!todo) return;
-    const SortedState col = load_sorted(sorted, q);
-    const int col_orig = orig[q];
     while (todo) {
         const int r = __ffs(todo) - 1;
         todo &= todo - 1;
-        int res = FILTER_REJECT;
-        if ((still >> r) & 1u) {
-            const double2 ra = rows[r][0], rb = rows[r][1], rc = rows[r][2];
-            ++pc.full;
-            res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
-                                    xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
-            if (res == FILTER_CO_ORBITING) ++pc.co;
+        if ((need >> r) & 1u) {
+            const float4 rp = rows32[r][0], rv = rows32[r][1];
+            if (!certainly_convex_reject_f32(cp.x - rp.x, cp.y - rp.y, cp.z - rp.z, cv.x - rv.x, cv.y - rv.y,
+                                             cv.z - rv.z, vmin2e))
+                still |= 1u << r;
         }
-        append_pairs(res == FILTER_REFINE, rorig[r], col_orig, a.ctrl, surv, surv_cap);
+    }
+    // One flagged row per lane and round into the queue.
+    while (__any_sync(0xffffffffu, still != 0u)) {
+        const bool have = still != 0u;
+        const unsigned bal = __ballot_sync(0xffffffffu, have);
+        if (have) {
+            fq[fcount + __popc(bal & lanemask_lt())] = make_int2(q, __ffs(still) - 1);
+            still &= still - 1;
+        }
+        fcount += __popc(bal);
+        if (fcount >= 32) {
+            __syncwarp();
+            exact_flush(fq, 32, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
+            __syncwarp();
+            if (lane < fcount - 32) fq[lane] = fq[32 + lane];
+            __syncwarp();
+            fcount -= 32;
+        }
     }
 }
 
@@ -1567,6 +1592,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     __shared__ float4 qcol[kWarps][64][2];
     __shared__ int qidx[kWarps][64];
     __shared__ unsigned qmask[kWarps][64];
+    // Per-warp queue of pairs for the exact filter (column's sorted position, row).
+    __shared__ int2 fq[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
@@ -1582,6 +1609,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     const float vmin2e = static_cast<float>(vme * vme * (1.0 + 1e-6));
     const int box_rows = a.tune.box_min_rows;
     PairCounters pc;
+    int fcount = 0;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
         const int4 item = items[it];
@@ -1622,7 +1650,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
             need &= valid;
             if (__any_sync(0xffffffffu, need != 0u))
                 exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, a, surv,
-                               surv_cap, pc);
+                               surv_cap, pc, fq[warp], fcount);
         };
         auto drain = [&](int count) {
             __syncwarp();
@@ -1673,6 +1701,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
             }
         }
         if (queued > 0) drain(queued);
+        __syncwarp();
+        // The rows change with the next item: run the queued pairs now.
+        if (fcount > 0) exact_flush(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
+        fcount = 0;
         __syncwarp();
     }
     pc.co = warp_sum(pc.co);
