@@ -1194,31 +1194,77 @@ __device__ __forceinline__ void append_pairs(bool keep, int row_orig, int col_or
     }
 }
 
-// Exact filter for the rows flagged in `need` against this lane's column.
-__device__ __forceinline__ void exact_rows(unsigned need, const SortedState& col, int col_orig,
+// Exact FP64 filter (src/core/collision_filter.hpp) of up to 32 queued pairs
+// (column's sorted position, row of the tile), one pair per lane.
+__device__ __forceinline__ void exact_flush(const int2* fq, int count, const double* __restrict__ sorted,
+                                            const int* __restrict__ orig, const double2 (*rows)[3], const int* rorig,
+                                            const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
+                                            PairCounters& pc) {
+    const int lane = threadIdx.x & 31;
+    int res = FILTER_REJECT;
+    int row_orig = 0, col_orig = 0;
+    if (lane < count) {
+        const int2 e = fq[lane];
+        const SortedState col = load_sorted(sorted, e.x);
+        col_orig = orig[e.x];
+        const double2 ra = rows[e.y][0], rb = rows[e.y][1], rc = rows[e.y][2];
+        row_orig = rorig[e.y];
+        ++pc.full;
+        res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
+                                xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
+        if (res == FILTER_CO_ORBITING) ++pc.co;
+    }
+    append_pairs(res == FILTER_REFINE, row_orig, col_orig, a.ctrl, surv, surv_cap);
+}
+
+// Adds the pairs (q, r) for the rows r in `still` to the warp's queue fq
+// (fcount entries, at most 63), one row per lane and round; every 32 queued
+// pairs run the exact filter.
+__device__ __forceinline__ void queue_exact(unsigned still, int q, int2* fq, int& fcount,
+                                            const double* __restrict__ sorted, const int* __restrict__ orig,
+                                            const double2 (*rows)[3], const int* rorig, const StepArgs& a,
+                                            int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc) {
+    const int lane = threadIdx.x & 31;
+    while (__any_sync(0xffffffffu, still != 0u)) {
+        const bool have = still != 0u;
+        const unsigned bal = __ballot_sync(0xffffffffu, have);
+        if (have) {
+            fq[fcount + __popc(bal & lanemask_lt())] = make_int2(q, __ffs(still) - 1);
+            still &= still - 1;
+        }
+        fcount += __popc(bal);
+        if (fcount >= 32) {
+            __syncwarp();
+            exact_flush(fq, 32, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
+            __syncwarp();
+            if (lane < fcount - 32) fq[lane] = fq[32 + lane];
+            __syncwarp();
+            fcount -= 32;
+        }
+    }
+}
+
+// Rows flagged by the gate for the lane's column q (state col): the
+// convexity test drops the pairs it proves rejected, the rest join the warp's
+// queue for the exact filter.
+__device__ __forceinline__ void exact_rows(unsigned need, const SortedState& col, int q,
+                                           const double* __restrict__ sorted, const int* __restrict__ orig,
                                            const double2 (*rows)[3], const int* rorig, const StepArgs& a,
-                                           int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc) {
+                                           int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc, int2* fq,
+                                           int& fcount) {
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
+    unsigned still = 0u;
     while (todo) {
         const int r = __ffs(todo) - 1;
         todo &= todo - 1;
-        bool mine = (need >> r) & 1u;
-        double rx = 0, ry = 0, rz = 0, vx = 0, vy = 0, vz = 0;
-        if (mine) {
+        if ((need >> r) & 1u) {
             const double2 ra = rows[r][0], rb = rows[r][1], rc = rows[r][2];
-            rx = xsub(col.rx, ra.x); ry = xsub(col.ry, ra.y); rz = xsub(col.rz, rb.x);
-            vx = xsub(col.vx, rb.y); vy = xsub(col.vy, rc.x); vz = xsub(col.vz, rc.y);
-            mine = !certainly_convex_reject(rx, ry, rz, vx, vy, vz, a.vmin2);
+            if (!certainly_convex_reject(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x),
+                                         xsub(col.vx, rb.y), xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.vmin2))
+                still |= 1u << r;
         }
-        if (!__any_sync(0xffffffffu, mine)) continue;
-        int res = FILTER_REJECT;
-        if (mine) {
-            ++pc.full;
-            res = filter_pair_exact(rx, ry, rz, vx, vy, vz, a.dt, a.threshold_km, a.vmin2);
-            if (res == FILTER_CO_ORBITING) ++pc.co;
-        }
-        append_pairs(res == FILTER_REFINE, rorig[r], col_orig, a.ctrl, surv, surv_cap);
     }
+    queue_exact(still, q, fq, fcount, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
 }
 
 // Per-warp table of the item's non-empty column segments (the cell itself and
@@ -1332,6 +1378,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     // Per-warp queue of columns that survived the row-box test (sorted index, valid rows).
     __shared__ int qidx[kWarps][64];
     __shared__ unsigned qmask[kWarps][64];
+    // Per-warp queue of pairs for the exact filter (column's sorted position, row).
+    __shared__ int2 fq[kWarps][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
@@ -1341,6 +1389,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     const double gate_hi2 = gate_hi * gate_hi;
     const int box_rows = kCols == 1 ? a.tune.box_min_rows : 0;
     PairCounters pc;
+    int fcount = 0;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
         const int4 item = items[it];
@@ -1377,7 +1426,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
                     need |= gate_open(col, rows[warp][r][0], rows[warp][r][1], rows[warp][r][2], gate_hi2) << r;
                 need &= valid;
                 if (__any_sync(0xffffffffu, need != 0u))
-                    exact_rows(need, col, orig[q], rows[warp], rorig[warp], a, surv, surv_cap, pc);
+                    exact_rows(need, col, q, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc, fq[warp],
+                               fcount);
             };
             int queued = 0;
             for (int cb = cb0; cb < cb0 + ncb; ++cb) {
@@ -1405,11 +1455,15 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
             }
             if (queued > 0) drain(queued);
             __syncwarp();
+            // The rows change with the next item: run the queued pairs now.
+            if (fcount > 0) exact_flush(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
+            fcount = 0;
+            __syncwarp();
             continue;
         }
         for (int cb = cb0; cb < cb0 + ncb; cb += kCols) {
             SortedState col[kCols];
-            int corig[kCols];
+            int qs[kCols];
             unsigned valid[kCols];
             for (int h = 0; h < kCols; ++h) {
                 const int p = 32 * (cb + h) + lane;
@@ -1417,7 +1471,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
                 int sid;
                 const int q = ok ? locate(segs[warp], nseg, p, &sid) : b0;
                 col[h] = load_sorted(sorted, q);
-                corig[h] = orig[q];
+                qs[h] = q;
                 // The block that starts at the row block's own columns keeps only column > row.
                 valid[h] = ok ? (cb + h == ra ? ((1u << lane) - 1u) : 0xffffffffu) & nrmask : 0u;
             }
@@ -1431,9 +1485,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
             for (int h = 0; h < kCols; ++h) {
                 need[h] &= valid[h];
                 if (__any_sync(0xffffffffu, need[h] != 0u))
-                    exact_rows(need[h], col[h], corig[h], rows[warp], rorig[warp], a, surv, surv_cap, pc);
+                    exact_rows(need[h], col[h], qs[h], sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap,
+                               pc, fq[warp], fcount);
             }
         }
+        __syncwarp();
+        if (fcount > 0) exact_flush(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
+        fcount = 0;
+        __syncwarp();
     }
     pc.co = warp_sum(pc.co);
     pc.full = warp_sum(pc.full);
@@ -1512,38 +1571,14 @@ __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, 
     return fast && separating && convex;
 }
 
-// Exact FP64 filter (src/core/collision_filter.hpp) of up to 32 queued pairs
-// (column's sorted position, row of the tile), one pair per lane.
-__device__ __forceinline__ void exact_flush(const int2* fq, int count, const double* __restrict__ sorted,
-                                            const int* __restrict__ orig, const double2 (*rows)[3], const int* rorig,
-                                            const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
-                                            PairCounters& pc) {
-    const int lane = threadIdx.x & 31;
-    int res = FILTER_REJECT;
-    int row_orig = 0, col_orig = 0;
-    if (lane < count) {
-        const int2 e = fq[lane];
-        const SortedState col = load_sorted(sorted, e.x);
-        col_orig = orig[e.x];
-        const double2 ra = rows[e.y][0], rb = rows[e.y][1], rc = rows[e.y][2];
-        row_orig = rorig[e.y];
-        ++pc.full;
-        res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
-                                xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
-        if (res == FILTER_CO_ORBITING) ++pc.co;
-    }
-    append_pairs(res == FILTER_REFINE, row_orig, col_orig, a.ctrl, surv, surv_cap);
-}
-
 // Rows flagged by the FP32 gate for the lane's column q: the FP32 convexity
-// test drops the pairs it proves rejected, the rest join the warp's queue fq
-// (fcount entries, at most 63), which runs the exact filter 32 pairs at a time.
+// test drops the pairs it proves rejected, the rest join the warp's queue for
+// the exact filter.
 __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ sorted,
                                                const int* __restrict__ orig, const float4 (*rows32)[2],
                                                const double2 (*rows)[3], const int* rorig, float vmin2e,
                                                const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
                                                PairCounters& pc, int2* fq, int& fcount) {
-    const int lane = threadIdx.x & 31;
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
     // FP32 convexity pass: drop rows no lane still needs.
     unsigned still = 0u;
@@ -1557,24 +1592,7 @@ __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 
                 still |= 1u << r;
         }
     }
-    // One flagged row per lane and round into the queue.
-    while (__any_sync(0xffffffffu, still != 0u)) {
-        const bool have = still != 0u;
-        const unsigned bal = __ballot_sync(0xffffffffu, have);
-        if (have) {
-            fq[fcount + __popc(bal & lanemask_lt())] = make_int2(q, __ffs(still) - 1);
-            still &= still - 1;
-        }
-        fcount += __popc(bal);
-        if (fcount >= 32) {
-            __syncwarp();
-            exact_flush(fq, 32, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
-            __syncwarp();
-            if (lane < fcount - 32) fq[lane] = fq[32 + lane];
-            __syncwarp();
-            fcount -= 32;
-        }
-    }
+    queue_exact(still, q, fq, fcount, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
 }
 
 template <int kMinBlocks>
