@@ -101,7 +101,7 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
 
 /* Launch-shape knobs (no counterpart in the reference): "pair_variant" (0: two
  * columns per lane, 1: one), "pair_blocks_per_sm" (0 = default),
- * "subcell_bits" (0..3: Morton order of objects inside a cell), "box_min_rows"
+ * "subcell_bits" (0..3: Morton order of objects inside a cell; default 1), "box_min_rows"
  * (split pair kernel: skip tiles whose row and column blocks are provably
  * apart, for tiles of at least this many rows; 0 = off), "cell_scale_permille"
  * (1000..4000: grid cell edge = the reference's edge x value/1000),

@@ -144,7 +144,7 @@ struct DeviceBuffers {
 struct Tuning {
     int pair_variant = 1;         // 0: two columns per lane, 1: one column per lane
     int pair_blocks_per_sm = 0;   // resident blocks of the pair kernel
-    int subcell_bits = 2;         // Morton order inside cells, bits per axis (0..3)
+    int subcell_bits = 1;         // Morton order inside cells, bits per axis (0..3)
     int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
     double cell_scale = 1.0;      // cell edge = reference edge x this (>= 1; changes only candidate counts)
     int prop_block = 128;         // threads per block of the propagation kernels (32..128, multiple of 32)

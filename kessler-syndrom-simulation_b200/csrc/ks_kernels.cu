@@ -2010,8 +2010,9 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     // Default: the resident block count of each kernel.
     if (a.precision == KS_PRECISION_SPLIT) {
-        // Register budget for 3 resident blocks per SM (80 registers), or for 4 (64).
-        const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 3;
+        // Register budget for 3 resident blocks per SM (80 registers), or for 4
+        // (64; the default: the higher occupancy outweighs a few spilled registers).
+        const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 4;
         if (bps >= 4)
             k_pairs_split<4><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
                                                                      b.cell_begin, b.nbr, b.items, b.items_cap,
