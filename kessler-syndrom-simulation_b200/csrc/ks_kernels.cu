@@ -1553,11 +1553,10 @@ __device__ __forceinline__ bool boxes_apart(const Box& a, const Box& b, float dt
 }
 
 // FP32 version of certainly_convex_reject for FP32 records whose dr, dv carry
-// absolute errors up to e_r, e_v (kF32PosErrKm, kF32VelErrKmS); vmin2e is
-// (vmin + e_v)^2. Margins as derived in the comments below.
+// absolute errors up to er, ev (f32_pos_err, f32_vel_err); vmin2e is
+// (vmin + ev)^2. Margins as derived in the comments below.
 __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, float rz, float vx, float vy,
-                                                            float vz, float vmin2e) {
-    constexpr float er = kF32PosErrKm, ev = kF32VelErrKmS;
+                                                            float vz, float vmin2e, float er, float ev) {
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
     const float dv2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
     const float rv = fmaf(rx, vx, fmaf(ry, vy, rz * vz));
@@ -1566,8 +1565,12 @@ __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, 
     // rv >= rv' - (|dr'| ev + |dv'| er + er ev + 2e-7 |dr'||dv'|); squared bound.
     const bool separating =
         rv > 0.f && rv * rv > 4.01f * (r2 * (ev * ev) + dv2 * (er * er) + (er * ev) * (er * ev) + 4e-14f * r2 * dv2);
-    // dv2 >= dv2'(1 - ev - 1e-6) - ev - ev^2 and r2 <= r2'(1 + er + 1e-6) + er + er^2 (|x| <= (x^2 + 1) / 2).
-    const bool convex = dv2 * 0.99999f - 6.1e-6f > static_cast<float>(kGravityGradient) * 1.0011f * r2 + 1.1e-9f;
+    // With 2|x| <= x^2 + 1 and 1e-6 for the FP32 rounding of the sums:
+    // dv2' >= dv2 (1 - ev - 1e-6) - ev - ev^2 and r2' <= r2 (1 + er + 1e-6) + er + er^2;
+    // the factors below take about twice those margins.
+    const bool convex = dv2 * (1.0f - 2.0f * ev - 4e-6f) - 1.25f * (ev + ev * ev) >
+                        static_cast<float>(kGravityGradient * 1.0002) *
+                            fmaf(r2, 1.0f + 2.0f * er + 2e-6f, 1.25f * (er + er * er));
     return fast && separating && convex;
 }
 
@@ -1577,8 +1580,8 @@ __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, 
 __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ sorted,
                                                const int* __restrict__ orig, const float4 (*rows32)[2],
                                                const double2 (*rows)[3], const int* rorig, float vmin2e,
-                                               const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
-                                               PairCounters& pc, int2* fq, int& fcount) {
+                                               float er, float ev, const StepArgs& a, int2* __restrict__ surv,
+                                               int64_t surv_cap, PairCounters& pc, int2* fq, int& fcount) {
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
     // FP32 convexity pass: drop rows no lane still needs.
     unsigned still = 0u;
@@ -1588,7 +1591,7 @@ __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 
         if ((need >> r) & 1u) {
             const float4 rp = rows32[r][0], rv = rows32[r][1];
             if (!certainly_convex_reject_f32(cp.x - rp.x, cp.y - rp.y, cp.z - rp.z, cv.x - rv.x, cv.y - rv.y,
-                                             cv.z - rv.z, vmin2e))
+                                             cv.z - rv.z, vmin2e, er, ev))
                 still |= 1u << r;
         }
     }
@@ -1618,12 +1621,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     const double vmax = __longlong_as_double(static_cast<long long>(a.ctrl->vmax_true));
     const double dt3 = a.dt * a.dt * a.dt;
     const double gate_hi = (a.threshold_km + kGravityGradient * (2.0 * vmax) * dt3 + 1e-3) * (1.0 + 1e-9);
-    const double gate_e = (gate_hi + kF32PosErrKm + kF32VelErrKmS * a.dt) * (1.0 + 1e-6);
+    // Error bounds of the FP32 records for this grid and these speeds.
+    const double er_d = f32_pos_err(a.ctrl->grid.cell), ev_d = f32_vel_err(vmax);
+    const float er = static_cast<float>(er_d), ev = static_cast<float>(ev_d);
+    const double gate_e = (gate_hi + er_d + ev_d * a.dt) * (1.0 + 1e-6);
     const float gate_f = static_cast<float>(gate_e);
     const float gate2 = gate_f * gate_f;
     const float dt_f = static_cast<float>(a.dt);
     const float cell_f = static_cast<float>(a.ctrl->grid.cell);
-    const double vme = sqrt(a.vmin2) + kF32VelErrKmS;
+    const double vme = sqrt(a.vmin2) + ev_d;
     const float vmin2e = static_cast<float>(vme * vme * (1.0 + 1e-6));
     const int box_rows = a.tune.box_min_rows;
     PairCounters pc;
@@ -1667,8 +1673,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
                 need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
             need &= valid;
             if (__any_sync(0xffffffffu, need != 0u))
-                exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, a, surv,
-                               surv_cap, pc, fq[warp], fcount);
+                exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, er, ev,
+                               a, surv, surv_cap, pc, fq[warp], fcount);
         };
         auto drain = [&](int count) {
             __syncwarp();

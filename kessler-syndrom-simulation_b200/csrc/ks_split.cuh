@@ -80,13 +80,25 @@ __device__ __forceinline__ void rk4_split(const SplitConsts& sc, double dt, cons
 
 // Conservative FP32 distance gate on recentred coordinates: 1 if the pair may
 // pass filter_pair's distance gate. Inputs carry absolute errors of at most
-// kF32PosErrKm (positions: cell-relative values below two cell edges, rounded
-// to FP32) and kF32VelErrKmS (velocities rounded to FP32, then subtracted):
-// the true relative motion stays within e = kF32PosErrKm + kF32VelErrKmS * dt
-// of the computed one over the step, so the gate widens by e, and the 1e-5 P
-// term covers the FP32 rounding of P - m^2 (P = |dr|^2 |dv|^2).
-constexpr float kF32PosErrKm = 5e-4f;
-constexpr float kF32VelErrKmS = 5e-6f;
+// e_r (positions) and e_v (velocities), f32_pos_err and f32_vel_err: the true
+// relative motion stays within e = e_r + e_v dt of the computed one over the
+// step, so the gate widens by e, and the 1e-5 P term covers the FP32 rounding
+// of P - m^2 (P = |dr|^2 |dv|^2).
+constexpr float kF32PosErrKm = 5e-4f;   // floor of e_r
+constexpr float kF32VelErrKmS = 5e-6f;  // floor of e_v
+
+// e_r for records of a grid with cell edge `cell` km. A row record is its
+// position relative to its cell's corner, in [0, cell], rounded to FP32
+// (<= 2^-24 cell per component); a column record from a neighbour cell is also
+// moved by an FP32 copy of the edge (<= 2^-24 cell) and rounded again within
+// 2 cell (<= 2^-23 cell). Per component of dr: <= 2^-24 (1 + 1 + 2 + 1) cell
+// < 3e-7 cell; over the three components < 5.2e-7 cell.
+__host__ __device__ inline double f32_pos_err(double cell) { return fmax(static_cast<double>(kF32PosErrKm), 6e-7 * cell); }
+
+// e_v when no record is faster than vmax km/s: velocities rounded to FP32
+// (<= 2^-24 |v| per component each), so dv errs by < 1.2e-7 vmax per
+// component, < 2.1e-7 vmax over the three.
+__host__ __device__ inline double f32_vel_err(double vmax) { return fmax(static_cast<double>(kF32VelErrKmS), 2.2e-7 * vmax); }
 
 __device__ __forceinline__ unsigned gate_open_f32(float4 cp, float4 cv, float4 rp, float4 rv, float gate2) {
     const float rx = cp.x - rp.x, ry = cp.y - rp.y, rz = cp.z - rp.z;

@@ -41,6 +41,28 @@ def test_split_screening_decides_like_fp64(engine, ks, age, thr):
         assert s32[f] == s64[f], f
 
 
+@pytest.mark.parametrize("dt,fast", [(120.0, False), (120.0, True), (600.0, False)])
+def test_split_screening_decides_like_fp64_on_large_cells(engine, ks, dt, fast):
+    # Long steps (cell edges of 2 500 to 13 000 km) and objects at 33 km/s: the
+    # FP32 record error bounds grow with the cell edge and the largest speed.
+    st, sz, al = ks.generate_population(52, 4000, 24000, 10, 3600.0)
+    if fast:
+        st = st.copy()
+        st[:40, 3:] *= 4.3
+    after, alive_after = engine.propagate(st, al, ks.DEFAULT_EPOCH_JD, 0.0, dt, 1)
+    out = {}
+    for prec in (ks.PRECISION_FP64, ks.PRECISION_SPLIT):
+        engine.set_precision(prec)
+        engine.set_screening(True, 5.0, 1.0, 0.01)
+        out[prec] = engine.screen(st, after, alive_after, sz, 0.0, dt)
+    engine.set_precision(ks.PRECISION_FP64)
+    (c64, s64), (c32, s32) = out[ks.PRECISION_FP64], out[ks.PRECISION_SPLIT]
+    assert s64["cell_km"] > 2000.0 and len(c64) > 0
+    same_conj(c32, c64)
+    for f in STAT_FIELDS:
+        assert s32[f] == s64[f], f
+
+
 def test_split_run_screening_matches_fp64_screening_of_its_own_states(engine, ks):
     """Over a multi-step split run, each step's conjunctions equal a one-shot
     FP64 screen of that step's split-precision before/after states."""
