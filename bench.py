@@ -261,8 +261,9 @@ def roofline_of(tm, a, fp64_rate, fp32_rate, split):
     pair_ops = FLOPS_PAIR_CHEAP * tm["candidate_pairs"] / steps
     kernels = {
         "propagate": {"ms": phases["propagate_ms"], "ops": prop_ops, "pipe": "fp64", "peak": fp64_rate},
-        "pairs": {"ms": phases["pairs_ms"], "ops": pair_ops, "pipe": "fp32" if split else "fp64",
-                  "peak": fp32_rate if split else fp64_rate},
+        # Both precisions gate pairs in FP32 (FP64 precision: pair variant 2,
+        # the default) and decide with the exact FP64 filter.
+        "pairs": {"ms": phases["pairs_ms"], "ops": pair_ops, "pipe": "fp32", "peak": fp32_rate},
     }
     for k in kernels.values():
         k["tflops"] = k["ops"] / (k["ms"] * 1e-3) / 1e12 if k["ms"] > 0 else None
@@ -281,7 +282,7 @@ def roofline_of(tm, a, fp64_rate, fp32_rate, split):
 def traffic_of(kernel, split):
     """DRAM bytes per launch of the kernel from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
-    key = f"{kernel}_{'split' if split else 'fp64'}"
+    key = "pairs_split" if kernel == "pairs" else f"{kernel}_{'split' if split else 'exact'}"
     try:
         for line in open(path):
             f = line.split()
@@ -293,9 +294,14 @@ def traffic_of(kernel, split):
 
 
 def launches_per_step(sort_passes):
-    # propagate, fix_keys, sort (upsweep, digit scan, one kernel per pass),
-    # cells (count, scan, write, neighbours, 3 scan kernels, items), pairs, refine
-    return 1 + 1 + (2 + sort_passes) + 8 + 1 + 1
+    # propagate, fix_keys, sort (upsweep, one kernel per pass), cells (count,
+    # scan, write, neighbours, item count, scan, item write), pairs, refine
+    return 1 + 1 + (1 + sort_passes) + 7 + 1 + 1
+
+
+# Per graph chunk: chunk_init, ctrl_reset, and the ordering of the chunk's
+# conjunction records (keys, upsweep, 4 passes, gather).
+LAUNCHES_PER_CHUNK = 9
 
 
 BORDER_TOL_KM = 1e-5  # 1 cm: the agreement the plain form is held to after 24 h
@@ -422,7 +428,7 @@ def main():
             "data": "synthetic (seeded generator; no dataset)", "config": config_of(a),
             "pairs_per_s": main_s["pairs_per_s"], "conjunctions_per_step": main_s["conjunctions_per_step"],
             "gpu_launches": a.steps * launches_per_step(tm_head["sort_passes"]) +
-                            -(-a.steps // max(1, a.steps_per_graph)),
+                            LAUNCHES_PER_CHUNK * -(-a.steps // max(1, a.steps_per_graph)),
             "roofline": main_s["roofline"], "clocks": clk,
             "fp64" if head == ks.PRECISION_SPLIT else "split": other_s,
             "conjunction_sets": dict(

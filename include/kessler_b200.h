@@ -99,8 +99,11 @@ int ks_set_buffer_limits(ks_ctx* ctx, int64_t survivor_pairs, int64_t conjunctio
  * starts with a cold L2; for measurements. */
 int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
 
-/* Launch-shape knobs (no counterpart in the reference): "pair_variant" (0: two
- * columns per lane, 1: one), "pair_blocks_per_sm" (0 = default),
+/* Launch-shape knobs (no counterpart in the reference): "pair_variant" (FP64
+ * precision's pair kernel: 0 FP64 gate, two columns per lane; 1 FP64 gate, one
+ * column per lane; 2, the default, the split kernel's FP32 gate on
+ * cell-relative records; every variant decides with the exact FP64 filter),
+ * "pair_blocks_per_sm" (0 = default),
  * "subcell_bits" (0..3: Morton order of objects inside a cell; default 1), "box_min_rows"
  * (split pair kernel: skip tiles whose row and column blocks are provably
  * apart, for tiles of at least this many rows; 0 = off), "cell_scale_permille"

@@ -1144,7 +1144,7 @@ int ks_set_buffer_limits(ks_ctx* ctx, int64_t survivor_pairs, int64_t conjunctio
 int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     if (!ctx || !key) return KS_ERR_ARG;
     const std::string k(key);
-    if (k == "pair_variant" && (value == 0 || value == 1)) ctx->tune.pair_variant = static_cast<int>(value);
+    if (k == "pair_variant" && value >= 0 && value <= 2) ctx->tune.pair_variant = static_cast<int>(value);
     else if (k == "pair_blocks_per_sm" && value >= 0 && value <= 32) ctx->tune.pair_blocks_per_sm = static_cast<int>(value);
     else if (k == "subcell_bits" && value >= 0 && value <= 3) {
         ctx->tune.subcell_bits = static_cast<int>(value);
@@ -1303,7 +1303,7 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
     };
     if (!rc) for (int v : kSpg) if (!rc && v != best.spg) { Knobs c = best; c.spg = v; rc = consider(c); }
     if (ctx->screening) {
-        const int pv_bps[][2] = {{1, 0}, {1, 2}, {1, 4}, {0, 0}, {0, 3}};
+        const int pv_bps[][2] = {{1, 0}, {1, 2}, {1, 4}, {0, 0}, {0, 3}, {2, 0}, {2, 3}};
         for (const auto& pb : pv_bps)
             if (!rc && !(pb[0] == best.pair_variant && pb[1] == best.pair_bps)) {
                 Knobs c = best;

@@ -120,7 +120,7 @@ struct DeviceBuffers {
     int* hash_vals = nullptr;
     int64_t hash_cap = 0;                  // power of two
     double* sorted = nullptr;              // 6 per sorted entry
-    float4* sorted32 = nullptr;            // split precision: cell-relative position, velocity
+    float4* sorted32 = nullptr;            // FP32 records: cell-relative position, velocity
     int* sorted_orig = nullptr;
     int2* survivors = nullptr;
     int64_t surv_cap = 0;
@@ -142,7 +142,7 @@ struct DeviceBuffers {
 
 // Launch-shape knobs (set through ks_set_tuning; 0 = default).
 struct Tuning {
-    int pair_variant = 1;         // 0: two columns per lane, 1: one column per lane
+    int pair_variant = 2;         // FP64 gate: 0 two columns per lane, 1 one; 2: FP32 gate on cell-relative records
     int pair_blocks_per_sm = 0;   // resident blocks of the pair kernel
     int subcell_bits = 1;         // Morton order inside cells, bits per axis (0..3)
     int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
@@ -198,6 +198,7 @@ void launch_gather_rows(const double* before, const double* after, const int64_t
 void launch_clear_alive(uint8_t* alive, const int64_t* idx, int count, cudaStream_t stream);
 void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+bool f32_records(const StepArgs& a);
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 // Orders the chunk's conjunction records by TCA into conj_sorted (records

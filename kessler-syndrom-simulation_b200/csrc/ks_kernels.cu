@@ -1990,6 +1990,11 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
                                                          b.conj_sorted);
 }
 
+// The pair kernel gates on FP32 cell-relative records (and decides with the
+// exact FP64 filter): always in split precision, and in FP64 precision with
+// pair variant 2.
+bool f32_records(const StepArgs& a) { return a.precision == KS_PRECISION_SPLIT || a.tune.pair_variant == 2; }
+
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     const int sb = sorted_buffer(a.sort_passes);
     const int ntiles = a.n > 0 ? (a.n + kCellTile - 1) / kCellTile : 1;
@@ -2001,7 +2006,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
                                                b.hash_keys, b.hash_vals,
                                                static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src],
                                                b.sorted, b.sorted_orig,
-                                               a.precision == KS_PRECISION_SPLIT ? b.sorted32 : nullptr, a.pack_bits);
+                                               f32_records(a) ? b.sorted32 : nullptr, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
     k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.item_part,
@@ -2015,7 +2020,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     // Default: the resident block count of each kernel.
-    if (a.precision == KS_PRECISION_SPLIT) {
+    if (f32_records(a)) {
         // Register budget for 3 resident blocks per SM (80 registers), or for 4
         // (64; the default: the higher occupancy outweighs a few spilled registers).
         const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 4;

@@ -55,6 +55,7 @@ constexpr int64_t scratch_bytes() {
     b += align256(sizeof(unsigned long long) * kNoAllocHash);  // hash keys
     b += align256(sizeof(int) * kNoAllocHash);           // hash values
     b += align256(sizeof(double) * 6 * n);               // sorted
+    b += align256(sizeof(float4) * 2 * n);               // sorted32
     b += align256(sizeof(int) * n);                      // sorted_orig
     b += align256(sizeof(int2) * kNoAllocSurvivors);     // survivors
     b += align256(sizeof(ks_conjunction) * kNoAllocConj);  // conjunctions
@@ -114,6 +115,7 @@ ks::DeviceBuffers carve(unsigned char* base) {
     b.hash_vals = take<int>(p, sizeof(int) * kNoAllocHash);
     b.hash_cap = kNoAllocHash;
     b.sorted = take<double>(p, sizeof(double) * 6 * n);
+    b.sorted32 = take<float4>(p, sizeof(float4) * 2 * n);
     b.sorted_orig = take<int>(p, sizeof(int) * n);
     b.survivors = take<int2>(p, sizeof(int2) * kNoAllocSurvivors);
     b.surv_cap = kNoAllocSurvivors;

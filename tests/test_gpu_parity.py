@@ -68,7 +68,7 @@ def test_chunking_and_graph_parity_do_not_change_results(engine):
         assert_same_stats(got[3], base[3])
 
 
-@pytest.mark.parametrize("variant,bps", [(0, 0), (0, 1), (1, 5)])
+@pytest.mark.parametrize("variant,bps", [(0, 0), (0, 1), (1, 5), (1, 0), (2, 3), (2, 1)])
 def test_tuning_knobs_do_not_change_results(engine, variant, bps):
     fx = load("run_dense.npz")
     engine.set_tuning("pair_variant", variant)
@@ -76,7 +76,7 @@ def test_tuning_knobs_do_not_change_results(engine, variant, bps):
     try:
         fs, fa, conj, stats = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], int(fx["steps"]))
     finally:
-        engine.set_tuning("pair_variant", 1)
+        engine.set_tuning("pair_variant", 2)
         engine.set_tuning("pair_blocks_per_sm", 0)
     assert np.array_equal(fs, fx["final_states"])
     assert_same_conj(conj, fx["conj"])

@@ -8,7 +8,7 @@ larger cell).
 import numpy as np
 import pytest
 
-from test_gpu_parity import assert_same_conj
+from test_gpu_parity import assert_same_conj, run_engine
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +41,7 @@ def test_autotune_keeps_results(engine, oracle, ks, precision):
                 assert np.array_equal(stats[f], want[3][f]), f
         else:
             # the same split run with the default configuration
-            for key, val in (("pair_variant", 1), ("pair_blocks_per_sm", 0), ("subcell_bits", 1),
+            for key, val in (("pair_variant", 2), ("pair_blocks_per_sm", 0), ("subcell_bits", 1),
                              ("box_min_rows", 8), ("cell_scale_permille", 1000), ("prop_block", 128)):
                 engine.set_tuning(key, val)
             engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
@@ -54,7 +54,7 @@ def test_autotune_keeps_results(engine, oracle, ks, precision):
             assert_same_conj(conj, engine.take_conjunctions())
             engine.take_step_stats()
     finally:
-        for key, val in (("pair_variant", 1), ("pair_blocks_per_sm", 0), ("subcell_bits", 1), ("box_min_rows", 8),
+        for key, val in (("pair_variant", 2), ("pair_blocks_per_sm", 0), ("subcell_bits", 1), ("box_min_rows", 8),
                          ("cell_scale_permille", 1000), ("prop_block", 128)):
             engine.set_tuning(key, val)
         engine.set_steps_per_graph(32)
@@ -91,3 +91,22 @@ def test_unpacked_sort_keys_give_the_same_results(engine, oracle, ks, precision)
         want = oracle.run(st, sz, al, steps=20)
         assert np.array_equal(unpacked[0][0], want[0])
         assert_same_conj(unpacked[1], want[2])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_fp64_pair_variants_equal_the_oracle(engine, oracle, ks, variant):
+    # FP64 precision with each pair kernel: FP64 gate (two columns or one per
+    # lane) or the FP32 gate on cell-relative records; the exact FP64 filter
+    # decides in every case, so states, conjunctions and counters are the
+    # reference's bit for bit.
+    st, sz, al = ks.generate_population(503, 5000, 30000, 8, 3600.0)
+    engine.set_tuning("pair_variant", variant)
+    try:
+        got = run_engine(engine, st, sz, al, 12)
+    finally:
+        engine.set_tuning("pair_variant", 2)
+    want = oracle.run(st, sz, al, steps=12)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    assert_same_conj(got[2], want[2])
+    for f in ("candidate_pairs", "refined_pairs", "co_orbiting", "conjunctions", "alive"):
+        assert np.array_equal(got[3][f], want[3][f]), f
