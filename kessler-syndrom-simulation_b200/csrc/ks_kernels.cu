@@ -925,10 +925,12 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         const int p = base + j * kBlock;
         if (o[j] < 0) continue;
         sorted_orig[p] = o[j];
-        double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
-        dst[0] = st[j][0];
-        dst[1] = st[j][1];
-        dst[2] = st[j][2];
+        if (sorted) {
+            double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
+            dst[0] = st[j][0];
+            dst[1] = st[j][1];
+            dst[2] = st[j][2];
+        }
         if (sorted32) {
             // Position relative to the corner of the object's own cell, velocity, in FP32.
             const unsigned long long key = keys[p] >> sh;
@@ -1195,8 +1197,11 @@ __device__ __forceinline__ void append_pairs(bool keep, int row_orig, int col_or
 }
 
 // Exact FP64 filter (src/core/collision_filter.hpp) of up to 32 queued pairs
-// (column's sorted position, row of the tile), one pair per lane.
-__device__ __forceinline__ void exact_flush(const int2* fq, int count, const double* __restrict__ sorted,
+// (column's sorted position, row of the tile), one pair per lane. kByObject:
+// both states come from `states` by object index (the start-of-step states);
+// otherwise the column from `states` in sorted order and the row from `rows`.
+template <bool kByObject>
+__device__ __forceinline__ void exact_flush(const int2* fq, int count, const double* __restrict__ states,
                                             const int* __restrict__ orig, const double2 (*rows)[3], const int* rorig,
                                             const StepArgs& a, int2* __restrict__ surv, int64_t surv_cap,
                                             PairCounters& pc) {
@@ -1205,13 +1210,21 @@ __device__ __forceinline__ void exact_flush(const int2* fq, int count, const dou
     int row_orig = 0, col_orig = 0;
     if (lane < count) {
         const int2 e = fq[lane];
-        const SortedState col = load_sorted(sorted, e.x);
         col_orig = orig[e.x];
-        const double2 ra = rows[e.y][0], rb = rows[e.y][1], rc = rows[e.y][2];
         row_orig = rorig[e.y];
+        SortedState col, row;
+        if (kByObject) {
+            col = load_sorted(states, col_orig);
+            row = load_sorted(states, row_orig);
+        } else {
+            col = load_sorted(states, e.x);
+            const double2 ra = rows[e.y][0], rb = rows[e.y][1], rc = rows[e.y][2];
+            row = SortedState{ra.x, ra.y, rb.x, rb.y, rc.x, rc.y};
+        }
         ++pc.full;
-        res = filter_pair_exact(xsub(col.rx, ra.x), xsub(col.ry, ra.y), xsub(col.rz, rb.x), xsub(col.vx, rb.y),
-                                xsub(col.vy, rc.x), xsub(col.vz, rc.y), a.dt, a.threshold_km, a.vmin2);
+        res = filter_pair_exact(xsub(col.rx, row.rx), xsub(col.ry, row.ry), xsub(col.rz, row.rz),
+                                xsub(col.vx, row.vx), xsub(col.vy, row.vy), xsub(col.vz, row.vz), a.dt,
+                                a.threshold_km, a.vmin2);
         if (res == FILTER_CO_ORBITING) ++pc.co;
     }
     append_pairs(res == FILTER_REFINE, row_orig, col_orig, a.ctrl, surv, surv_cap);
@@ -1220,6 +1233,7 @@ __device__ __forceinline__ void exact_flush(const int2* fq, int count, const dou
 // Adds the pairs (q, r) for the rows r in `still` to the warp's queue fq
 // (fcount entries, at most 63), one row per lane and round; every 32 queued
 // pairs run the exact filter.
+template <bool kByObject>
 __device__ __forceinline__ void queue_exact(unsigned still, int q, int2* fq, int& fcount,
                                             const double* __restrict__ sorted, const int* __restrict__ orig,
                                             const double2 (*rows)[3], const int* rorig, const StepArgs& a,
@@ -1235,7 +1249,7 @@ __device__ __forceinline__ void queue_exact(unsigned still, int q, int2* fq, int
         fcount += __popc(bal);
         if (fcount >= 32) {
             __syncwarp();
-            exact_flush(fq, 32, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
+            exact_flush<kByObject>(fq, 32, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
             __syncwarp();
             if (lane < fcount - 32) fq[lane] = fq[32 + lane];
             __syncwarp();
@@ -1264,7 +1278,7 @@ __device__ __forceinline__ void exact_rows(unsigned need, const SortedState& col
                 still |= 1u << r;
         }
     }
-    queue_exact(still, q, fq, fcount, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
+    queue_exact<false>(still, q, fq, fcount, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
 }
 
 // Per-warp table of the item's non-empty column segments (the cell itself and
@@ -1456,7 +1470,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
             if (queued > 0) drain(queued);
             __syncwarp();
             // The rows change with the next item: run the queued pairs now.
-            if (fcount > 0) exact_flush(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
+            if (fcount > 0) exact_flush<false>(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
             fcount = 0;
             __syncwarp();
             continue;
@@ -1490,7 +1504,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
             }
         }
         __syncwarp();
-        if (fcount > 0) exact_flush(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
+        if (fcount > 0) exact_flush<false>(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
         fcount = 0;
         __syncwarp();
     }
@@ -1577,11 +1591,11 @@ __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, 
 // Rows flagged by the FP32 gate for the lane's column q: the FP32 convexity
 // test drops the pairs it proves rejected, the rest join the warp's queue for
 // the exact filter.
-__device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ sorted,
+__device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ before,
                                                const int* __restrict__ orig, const float4 (*rows32)[2],
-                                               const double2 (*rows)[3], const int* rorig, float vmin2e,
-                                               float er, float ev, const StepArgs& a, int2* __restrict__ surv,
-                                               int64_t surv_cap, PairCounters& pc, int2* fq, int& fcount) {
+                                               const int* rorig, float vmin2e, float er, float ev, const StepArgs& a,
+                                               int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc, int2* fq,
+                                               int& fcount) {
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
     // FP32 convexity pass: drop rows no lane still needs.
     unsigned still = 0u;
@@ -1595,18 +1609,17 @@ __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 
                 still |= 1u << r;
         }
     }
-    queue_exact(still, q, fq, fcount, sorted, orig, rows, rorig, a, surv, surv_cap, pc);
+    queue_exact<true>(still, q, fq, fcount, before, orig, nullptr, rorig, a, surv, surv_cap, pc);
 }
 
 template <int kMinBlocks>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, const double* __restrict__ sorted,
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, const double* __restrict__ before,
                                                         const float4* __restrict__ sorted32,
                                                         const int* __restrict__ orig,
                                                         const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr, const int4* __restrict__ items,
                                                         int64_t items_cap, int2* __restrict__ surv, int64_t surv_cap) {
     __shared__ float4 rows32[kWarps][32][2];
-    __shared__ double2 rows[kWarps][32][3];
     __shared__ int rorig[kWarps][32];
     __shared__ SegTable segs[kWarps];
     // Per-warp queue of columns that survived the row-box test, drained 32 at a time.
@@ -1652,10 +1665,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
         if (lane < nr) {
             rows32[warp][lane][0] = my_rp;
             rows32[warp][lane][1] = my_rv;
-            const double2* s = reinterpret_cast<const double2*>(sorted + 6 * static_cast<int64_t>(rl));
-            rows[warp][lane][0] = s[0];
-            rows[warp][lane][1] = s[1];
-            rows[warp][lane][2] = s[2];
             rorig[warp][lane] = orig[rl];
         }
         // Tiles of at least box_rows rows test each column against the rows'
@@ -1673,8 +1682,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
                 need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
             need &= valid;
             if (__any_sync(0xffffffffu, need != 0u))
-                exact_rows_f32(need, cp, cv, q, sorted, orig, rows32[warp], rows[warp], rorig[warp], vmin2e, er, ev,
-                               a, surv, surv_cap, pc, fq[warp], fcount);
+                exact_rows_f32(need, cp, cv, q, before, orig, rows32[warp], rorig[warp], vmin2e, er, ev, a, surv,
+                               surv_cap, pc, fq[warp], fcount);
         };
         auto drain = [&](int count) {
             __syncwarp();
@@ -1727,7 +1736,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
         if (queued > 0) drain(queued);
         __syncwarp();
         // The rows change with the next item: run the queued pairs now.
-        if (fcount > 0) exact_flush(fq[warp], fcount, sorted, orig, rows[warp], rorig[warp], a, surv, surv_cap, pc);
+        if (fcount > 0) exact_flush<true>(fq[warp], fcount, before, orig, nullptr, rorig[warp], a, surv, surv_cap, pc);
         fcount = 0;
         __syncwarp();
     }
@@ -2005,7 +2014,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
     k_cell_write<<<ntiles, kBlock, 0, stream>>>(b.keys[sb], b.idx[sb], bc, a.ctrl, b.cell_begin, b.cell_key,
                                                b.hash_keys, b.hash_vals,
                                                static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src],
-                                               b.sorted, b.sorted_orig,
+                                               f32_records(a) ? nullptr : b.sorted, b.sorted_orig,
                                                f32_records(a) ? b.sorted32 : nullptr, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
@@ -2025,11 +2034,11 @@ void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
         // (64; the default: the higher occupancy outweighs a few spilled registers).
         const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 4;
         if (bps >= 4)
-            k_pairs_split<4><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
+            k_pairs_split<4><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
                                                                      b.cell_begin, b.nbr, b.items, b.items_cap,
                                                                      b.survivors, b.surv_cap);
         else
-            k_pairs_split<3><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.sorted, b.sorted32, b.sorted_orig,
+            k_pairs_split<3><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
                                                                      b.cell_begin, b.nbr, b.items, b.items_cap,
                                                                      b.survivors, b.surv_cap);
         return;
