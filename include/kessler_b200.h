@@ -246,6 +246,8 @@ typedef struct ks_timing {
     int64_t candidate_pairs;     /* summed over steps */
     int64_t exact_filter_pairs;  /* candidates that needed the full FP64 filter_pair */
     int64_t refined_pairs;       /* pairs refined (Hermite TCA) */
+    double chunk_ms;       /* device work of the chunks outside their steps: set-up, checkpoint,
+                              ordering of the chunk's conjunction records, replays (L2 flushes excluded) */
 } ks_timing;
 int ks_get_timing(const ks_ctx* ctx, ks_timing* out);
 

@@ -31,7 +31,8 @@ class Timing(C.Structure):
     _fields_ = [("propagate_ms", C.c_double), ("sort_ms", C.c_double), ("cells_ms", C.c_double),
                 ("pairs_ms", C.c_double), ("refine_ms", C.c_double), ("total_ms", C.c_double),
                 ("steps", C.c_int64), ("object_steps", C.c_int64), ("sort_passes", C.c_int64),
-                ("candidate_pairs", C.c_int64), ("exact_filter_pairs", C.c_int64), ("refined_pairs", C.c_int64)]
+                ("candidate_pairs", C.c_int64), ("exact_filter_pairs", C.c_int64), ("refined_pairs", C.c_int64),
+                ("chunk_ms", C.c_double)]
 
 
 class TuningChoice(C.Structure):

@@ -33,7 +33,7 @@ using ks::StepParams;
 
 namespace {
 
-constexpr int kPhases = 6;  // event slots per step
+constexpr int kPhases = 7;  // event slots per step: 0..5 the phases, 6 before the step's L2 flush
 constexpr int kMaxReplays = 6;
 
 }  // namespace
@@ -65,6 +65,7 @@ struct ks_ctx {
     std::vector<ks_step_stats> stats_out;
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> ev;
+    cudaEvent_t ev_chunk[2] = {nullptr, nullptr};  // around a chunk's device work (profiling)
     ks_timing timing{};
     ks::Tuning tune;
     bool ckpt_states = false;  // the checkpoint holds states (chunks of more than one step)
@@ -72,6 +73,7 @@ struct ks_ctx {
     void* frag_scratch = nullptr;  // device staging of fragmentation work (parent rows, spans)
     size_t frag_scratch_bytes = 0;
     bool pack_keys = true;     // object index packed below the cell key in the sort keys
+    int64_t max_step_conj = 0; // most conjunction records of one step so far (record buffer sizing)
     bool allow_pack = true;    // tuning: packing allowed where the keys leave room
     int realisations = 1;
     int rbits = 0;
@@ -251,6 +253,8 @@ int ensure_chunk(ks_ctx* ctx, int k) {
     for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
     ctx->ev.assign(static_cast<size_t>(k) * kPhases, nullptr);
     for (auto& e : ctx->ev) KS_CUDA(cudaEventCreate(&e));
+    for (cudaEvent_t& e : ctx->ev_chunk)
+        if (!e) KS_CUDA(cudaEventCreate(&e));
     ctx->max_chunk = k;
     return KS_OK;
 }
@@ -351,6 +355,7 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
     int src = src0;
     for (int k = 0; k < k_steps; ++k) {
         const StepArgs a = step_args(ctx, k, k_steps, src);
+        record(ctx, k, 6, capturing);
         if (ctx->l2_flush_bytes > 0) cudaMemsetAsync(ctx->l2_flush, k & 0xFF, ctx->l2_flush_bytes, s);
         record(ctx, k, 0, capturing);
         if (a.hist) cudaMemsetAsync(a.hist, 0, sizeof(unsigned int) * 8 * 256, s);
@@ -373,13 +378,10 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
         ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, s);
 }
 
-int launch_chunk(ks_ctx* ctx, int k_steps) {
+// Captures and instantiates the chunk's graph if it does not exist yet.
+int ensure_graph(ks_ctx* ctx, int k_steps) {
     const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
-    if (!use_graph) {
-        enqueue_chunk(ctx, k_steps, ctx->cur, false);
-        KS_CUDA(cudaGetLastError());
-        return KS_OK;
-    }
+    if (!use_graph) return KS_OK;
     cudaGraphExec_t& exec = ctx->graph_exec[ctx->cur];
     if (!exec) {
         cudaGraph_t g = nullptr;
@@ -395,8 +397,22 @@ int launch_chunk(ks_ctx* ctx, int k_steps) {
             exec = nullptr;
             return fail(ctx, KS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
         }
+        // Uploaded now rather than by its first launch.
+        KS_CUDA(cudaGraphUpload(exec, ctx->stream));
     }
-    KS_CUDA(cudaGraphLaunch(exec, ctx->stream));
+    return KS_OK;
+}
+
+int launch_chunk(ks_ctx* ctx, int k_steps) {
+    const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
+    if (!use_graph) {
+        enqueue_chunk(ctx, k_steps, ctx->cur, false);
+        KS_CUDA(cudaGetLastError());
+        return KS_OK;
+    }
+    const int rc = ensure_graph(ctx, k_steps);
+    if (rc) return rc;
+    KS_CUDA(cudaGraphLaunch(ctx->graph_exec[ctx->cur], ctx->stream));
     return KS_OK;
 }
 
@@ -454,18 +470,25 @@ void accumulate_timing(ks_ctx* ctx, int k_steps) {
         cudaEventElapsedTime(&ms, ctx->ev[static_cast<size_t>(k) * kPhases + p0], ctx->ev[static_cast<size_t>(k) * kPhases + p1]);
         return static_cast<double>(ms);
     };
+    double steps_ms = 0.0, flush_ms = 0.0;
     for (int k = 0; k < k_steps; ++k) {
         ctx->timing.propagate_ms += el(k, 0, 1);
+        const double step_ms = ctx->screening ? el(k, 0, 5) : el(k, 0, 1);
         if (ctx->screening) {
             ctx->timing.sort_ms += el(k, 1, 2);
             ctx->timing.cells_ms += el(k, 2, 3);
             ctx->timing.pairs_ms += el(k, 3, 4);
             ctx->timing.refine_ms += el(k, 4, 5);
-            ctx->timing.total_ms += el(k, 0, 5);
-        } else {
-            ctx->timing.total_ms += el(k, 0, 1);
         }
+        ctx->timing.total_ms += step_ms;
+        steps_ms += step_ms;
+        flush_ms += el(k, 6, 0);
     }
+    // The chunk's work outside its steps: set-up, checkpoint, ordering of its
+    // records (and any replay); the L2 flushes are left out.
+    float chunk = 0.f;
+    cudaEventElapsedTime(&chunk, ctx->ev_chunk[0], ctx->ev_chunk[1]);
+    ctx->timing.chunk_ms += std::max(0.0, static_cast<double>(chunk) - steps_ms - flush_ms);
 }
 
 int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_conjunction>& hits);
@@ -481,6 +504,16 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     double t_end = 0.0;
     fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
     KS_CUDA(cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, ctx->stream));
+    // Room for the chunk's records at the largest per-step count seen so far,
+    // so that a longer chunk does not overflow and replay.
+    if (ctx->screening && ctx->max_step_conj > 0) {
+        const int64_t want = std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, int64_t(1) << 30);
+        if (want > ctx->b.conj_cap && (rc = ensure_conj(ctx, want))) return rc;
+    }
+    // A new graph is built before the chunk's start is recorded, so that the
+    // chunk's device time holds no wait for the host.
+    if ((rc = ensure_graph(ctx, k_steps))) return rc;
+    if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[0], ctx->stream));
     if (ctx->screening) {
         rc = save_checkpoint(ctx, k_steps);
         if (rc) return rc;
@@ -488,6 +521,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     for (int attempt = 0;; ++attempt) {
         rc = launch_chunk(ctx, k_steps);
         if (rc) return rc;
+        if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[1], ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -549,6 +583,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         if (rc) return rc;
         rc = launch_chunk(ctx, k_steps);
         if (rc) return rc;
+        if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[1], ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -577,6 +612,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         st.max_cell_objects = c.max_cell;
         st.alive = c.n_alive;
         ctx->stats_out.push_back(st);
+        ctx->max_step_conj = std::max(ctx->max_step_conj, static_cast<int64_t>(c.conj));
         ctx->timing.object_steps += static_cast<int64_t>(c.object_steps);
         ctx->timing.candidate_pairs += static_cast<int64_t>(c.candidates);
         ctx->timing.exact_filter_pairs += static_cast<int64_t>(c.exact_evals);
@@ -990,6 +1026,7 @@ void ks_destroy(ks_ctx* ctx) {
     if (ctx->h_chunk) cudaFreeHost(ctx->h_chunk);
     if (ctx->h_conj) cudaFreeHost(ctx->h_conj);
     for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->ev_chunk) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
