@@ -74,6 +74,7 @@ struct ks_ctx {
     size_t frag_scratch_bytes = 0;
     bool pack_keys = true;     // object index packed below the cell key in the sort keys
     int64_t max_step_conj = 0; // most conjunction records of one step so far (record buffer sizing)
+    bool conj_small = false;   // chunks order their records in one block (few expected)
     bool allow_pack = true;    // tuning: packing allowed where the keys leave room
     int realisations = 1;
     int rbits = 0;
@@ -375,7 +376,7 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
         src ^= 1;
     }
     if (ctx->screening)
-        ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, s);
+        ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, ctx->conj_small, s);
 }
 
 // Captures and instantiates the chunk's graph if it does not exist yet.
@@ -510,6 +511,13 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         const int64_t want = std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, int64_t(1) << 30);
         if (want > ctx->b.conj_cap && (rc = ensure_conj(ctx, want))) return rc;
     }
+    // One-block ordering of the records where the chunk should hold few.
+    const bool small = ctx->screening && ctx->max_step_conj > 0 &&
+                       ctx->max_step_conj * k_steps * 5 / 4 + 256 <= ks::kConjSmall;
+    if (small != ctx->conj_small) {
+        ctx->conj_small = small;
+        drop_graphs(ctx);
+    }
     // A new graph is built before the chunk's start is recorded, so that the
     // chunk's device time holds no wait for the host.
     if ((rc = ensure_graph(ctx, k_steps))) return rc;
@@ -518,13 +526,22 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         rc = save_checkpoint(ctx, k_steps);
         if (rc) return rc;
     }
+    // Records copied with the control blocks, up to the expected count, so
+    // that a chunk with no more than that needs one host round trip.
+    const int64_t spec = ctx->screening ? std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, ctx->b.conj_cap) : 0;
+    const bool speculate = ctx->max_step_conj > 0 && spec <= (int64_t(1) << 16);
+    int64_t have = 0;  // leading records of this chunk's run already in h_conj
     for (int attempt = 0;; ++attempt) {
         rc = launch_chunk(ctx, k_steps);
         if (rc) return rc;
         if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[1], ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        if (speculate)
+            KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj_sorted, sizeof(ks_conjunction) * spec,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        have = speculate ? spec : 0;
         int flags = ctx->h_chunk->flags;
         unsigned long long max_refined = 0;
         int max_bits = 0;
@@ -563,9 +580,18 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     bool was_cut = false;
     for (int cut = 0;; ++cut) {
         nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
-        if (nc > 0) {
+        if (ctx->h_chunk->flags & ks::FLAG_CONJ_LARGE) {
+            // More records than the one-block ordering takes: the multi-block sort.
+            ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, false, ctx->stream);
+            KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+            KS_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (ctx->h_chunk->flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+            have = 0;
+        }
+        if (nc > have) {
             // Records already ordered by TCA on the device (conj_sorted).
-            KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj_sorted, sizeof(ks_conjunction) * nc,
+            KS_CUDA(cudaMemcpyAsync(ctx->h_conj + have, ctx->b.conj_sorted + have, sizeof(ks_conjunction) * (nc - have),
                                     cudaMemcpyDeviceToHost, ctx->stream));
             KS_CUDA(cudaStreamSynchronize(ctx->stream));
         }
@@ -587,6 +613,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        have = 0;
         if (ctx->h_chunk->flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_TIMEOUT | ks::FLAG_KEY_RANGE))
             return fail(ctx, KS_ERR_STATE, "replay to the first collision step overflowed");
     }

@@ -58,6 +58,7 @@ enum : int {
     FLAG_TIMEOUT = 32,       // a bounded device-side wait gave up
     FLAG_KEYS_REBUILT = 64,  // k_fix_keys rebuilt the keys: their digit histogram is recounted
     FLAG_PACK_WIDTH = 128,   // cell key + dead flag + object index do not fit 64 bits: sort unpacked
+    FLAG_CONJ_LARGE = 256,   // more records than the one-block ordering takes: ordered by the multi-block sort
 };
 
 
@@ -205,7 +206,9 @@ void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 // whose TCAs share a 32-bit key keep their append order; the host finishes
 // the (t, i, j) order). t_start: device address of the chunk's first step
 // start time; span_s: the chunk's duration.
-void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s,
+// Records ordered by one block in shared memory (chunks expected to hold few).
+constexpr int kConjSmall = 16384;
+void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s, bool small,
                       cudaStream_t stream);
 void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,
                    ChunkCtrl* chunk, cudaStream_t stream);

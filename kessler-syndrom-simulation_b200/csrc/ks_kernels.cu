@@ -1973,10 +1973,63 @@ __global__ void __launch_bounds__(kBlock) k_conj_gather(const ks_conjunction* __
         out[q] = conj[static_cast<int>(order[q] & mask)];
 }
 
-void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s,
+// Up to kConjSmall records of a chunk ordered by one block: the keys of
+// k_conj_keys (14 index bits here) sorted by a bitonic network in shared
+// memory, then the records gathered. With more records it sets
+// FLAG_CONJ_LARGE and leaves them to the multi-block sort.
+__global__ void __launch_bounds__(1024) k_conj_sort_small(const ks_conjunction* __restrict__ conj, int64_t cap,
+                                                          ChunkCtrl* chunk, const double* __restrict__ t_start,
+                                                          double span_s, ks_conjunction* __restrict__ out) {
+    extern __shared__ unsigned long long sk[];
+    const int n = static_cast<int>(min(chunk->conj_count, static_cast<unsigned long long>(cap)));
+    if (n > kConjSmall) {
+        if (threadIdx.x == 0) {
+            chunk->sort_n = 0;
+            atomicOr(&chunk->flags, FLAG_CONJ_LARGE);
+        }
+        return;
+    }
+    if (threadIdx.x == 0) chunk->sort_n = n;
+    int m = 2;
+    while (m < n) m <<= 1;
+    const double t0 = *t_start;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        unsigned long long key = ~0ull;  // padding sorts last
+        if (q < n) {
+            const double f = xmul(xdiv(xsub(conj[q].t, t0), span_s), 4294967296.0);
+            const double c = fmin(fmax(floor(f), 0.0), 4294967295.0);
+            key = (static_cast<unsigned long long>(c) << 14) | static_cast<unsigned long long>(q);
+        }
+        sk[q] = key;
+    }
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int p = i ^ j;
+                if (p > i) {
+                    const unsigned long long a = sk[i], b = sk[p];
+                    if ((a > b) == ((i & k) == 0)) {
+                        sk[i] = b;
+                        sk[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int q = threadIdx.x; q < n; q += blockDim.x) out[q] = conj[static_cast<int>(sk[q] & 0x3FFFull)];
+}
+
+void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s, bool small,
                       cudaStream_t stream) {
     const int cap = static_cast<int>(b.conj_cap);
     if (cap <= 0) return;
+    if (small) {
+        constexpr int kBytes = kConjSmall * sizeof(unsigned long long);
+        cudaFuncSetAttribute(k_conj_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, kBytes);
+        k_conj_sort_small<<<1, 1024, kBytes, stream>>>(b.conj, b.conj_cap, chunk, t_start, span_s, b.conj_sorted);
+        return;
+    }
     constexpr int kPasses = 4;
     const int ntiles = (cap + kSortTile - 1) / kSortTile;
     int pb = 1;  // record index bits below the 32-bit key

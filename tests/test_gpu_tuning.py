@@ -110,3 +110,30 @@ def test_fp64_pair_variants_equal_the_oracle(engine, oracle, ks, variant):
     assert_same_conj(got[2], want[2])
     for f in ("candidate_pairs", "refined_pairs", "co_orbiting", "conjunctions", "alive"):
         assert np.array_equal(got[3][f], want[3][f]), f
+
+
+def test_record_ordering_falls_back_when_a_chunk_holds_many(engine, oracle, ks):
+    # One-step chunks after a step with few records order them in one block;
+    # a step with more records than that takes (16 384) falls back to the
+    # multi-block sort. Its records equal the oracle's for that step.
+    st, sz, al = ks.generate_population(504, 28340, 150000, 30, 86400.0)
+    engine.set_steps_per_graph(1)
+    engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
+    engine.set_screening(True, 1.0, 1.0, 0.01)
+    engine.set_population(st, sz, al)
+    try:
+        engine.run(1)
+        few = engine.take_conjunctions()
+        s1, a1 = engine.get_population()
+        engine.set_screening(True, 90.0, 1.0, 0.01)
+        engine.run(1)
+        many = engine.take_conjunctions()
+        engine.take_step_stats()
+    finally:
+        engine.set_screening(True, 5.0, 1.0, 0.01)
+        engine.set_steps_per_graph(32)
+    want = oracle.run(s1, sz, a1, t_start=10.0, steps=1, threshold_km=90.0)[2]
+    assert 0 < len(few) < 1000 and len(many) > 16384
+    many = many.copy()
+    many["step"] -= 1
+    assert_same_conj(many, want)
