@@ -31,7 +31,7 @@ constexpr int kSortTile = 2048;            // keys per radix tile (256 threads x
 constexpr int kSortItems = kSortTile / kBlock;
 constexpr int kWarps = kBlock / 32;
 constexpr int kCellTile = 1024;            // sorted entries per cell-build tile
-constexpr int kPropBlock = 128;            // propagation: 168 registers, 3 blocks per SM
+constexpr int kPropBlock = 128;            // propagation: 4 blocks per SM (at most 128 registers)
 
 // Forward neighbour offsets (src/core/collision_filter.hpp:137-140): with the
 // pairs inside a cell they visit every pair of neighbouring cells once.
@@ -320,7 +320,7 @@ __device__ __forceinline__ void hist_flush(const unsigned int* sh, unsigned int*
     }
 }
 
-__global__ void __launch_bounds__(kPropBlock, 3) k_propagate_exact(StepArgs a, const double* __restrict__ in,
+__global__ void __launch_bounds__(kPropBlock, 4) k_propagate_exact(StepArgs a, const double* __restrict__ in,
                                                             double* __restrict__ out,
                                                             const uint8_t* __restrict__ alive_in,
                                                             uint8_t* __restrict__ alive_out,
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(kBlock) k_clear_alive(uint8_t* __restrict__ al
 
 // Split-precision propagation (FP32 J2 and lunar terms, FP64 state and central
 // term); keys and speculation exactly as in k_propagate_exact.
-__global__ void __launch_bounds__(kPropBlock, 4) k_propagate_split(StepArgs a, const double* __restrict__ in,
+__global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, const double* __restrict__ in,
                                                                    double* __restrict__ out,
                                                                    const uint8_t* __restrict__ alive_in,
                                                                    uint8_t* __restrict__ alive_out,
@@ -1892,11 +1892,11 @@ void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int 
 
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     if (a.precision == KS_PRECISION_SPLIT) {
-        k_propagate_split<<<grid_for_block(a.n, 4 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(
+        k_propagate_split<<<grid_for_block(a.n, 5 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(
             a, b.state[a.src], b.state[1 - a.src], b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
         return;
     }
-    k_propagate_exact<<<grid_for_block(a.n, 3 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
+    k_propagate_exact<<<grid_for_block(a.n, 4 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
                                                                 b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 
