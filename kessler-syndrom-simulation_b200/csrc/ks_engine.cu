@@ -131,7 +131,7 @@ void free_objects(ks_ctx* ctx) {
     dfree(b.size_m); dfree(b.real_id); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr);
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
-    dfree(b.sorted); dfree(b.sorted32); dfree(b.sorted_orig);
+    dfree(b.sorted); dfree(b.sorted32); dfree(b.rec32); dfree(b.sorted_orig);
     b.cap = 0;
     b.hash_cap = 0;
     b.sort_status_len = 0;
@@ -171,6 +171,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.hash_vals, sizeof(int) * h));
     KS_CUDA(cudaMalloc(&b.sorted, sizeof(double) * 6 * cap));
     KS_CUDA(cudaMalloc(&b.sorted32, sizeof(float4) * 2 * cap));
+    KS_CUDA(cudaMalloc(&b.rec32, sizeof(float4) * 2 * cap));
     KS_CUDA(cudaMalloc(&b.sorted_orig, sizeof(int) * cap));
     b.cap = cap;
     return KS_OK;
@@ -339,6 +340,7 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     a.ctrl_next = (k == k_steps - 1) ? carry_slot(ctx) : ctx->b.ctrl + k + 1;
     a.src = src;
     a.hist = ctx->screening ? ctx->b.sort_hist : nullptr;  // the propagation counts the sort's digits
+    a.rec32 = ctx->b.rec32;
     a.pack_bits = ctx->pack_keys ? index_bits(ctx->n) : 0;
     return a;
 }

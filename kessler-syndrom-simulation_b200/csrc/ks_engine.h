@@ -121,7 +121,8 @@ struct DeviceBuffers {
     int* hash_vals = nullptr;
     int64_t hash_cap = 0;                  // power of two
     double* sorted = nullptr;              // 6 per sorted entry
-    float4* sorted32 = nullptr;            // FP32 records: cell-relative position, velocity
+    float4* sorted32 = nullptr;            // FP32 records: cell-relative position, velocity, in cell order
+    float4* rec32 = nullptr;               // the same records in object order, written with the keys
     int* sorted_orig = nullptr;
     int2* survivors = nullptr;
     int64_t surv_cap = 0;
@@ -179,6 +180,7 @@ struct StepArgs {
     Ctrl* ctrl_next;           // next step's control block (speculation outputs)
     int src;                   // state buffer holding the start of the step (0 or 1)
     unsigned int* hist;        // radix digit histogram the propagation fills with the keys it emits, or null
+    float4* rec32;             // FP32 record of each object, written with its key (object order)
     int pack_bits;             // > 0: sort keys carry the object index in their low pack_bits bits
 };
 

@@ -107,6 +107,21 @@ __device__ __forceinline__ unsigned long long cell_key(const GridParams& g, doub
 
 __device__ __forceinline__ unsigned long long dead_key(const GridParams& g) { return 1ull << min(g.bits, 63); }
 
+// FP32 record of an object whose cell key (sub-cell bits included) is `key`
+// and whose start-of-step state is s: position relative to its cell's corner
+// and velocity, rounded to FP32 (separately rounded FP64 steps before that).
+__device__ __forceinline__ void f32_record(const GridParams& g, unsigned long long key, double x, double y, double z,
+                                           double vx, double vy, double vz, float4* __restrict__ out) {
+    const unsigned long long cell = key >> (3 * g.sub);
+    const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1, mx = (1ull << g.w[0]) - 1;
+    const double cx = xmul(static_cast<double>(static_cast<long long>((cell >> (g.w[1] + g.w[2])) & mx) + g.lo[0]), g.cell);
+    const double cy = xmul(static_cast<double>(static_cast<long long>((cell >> g.w[2]) & my) + g.lo[1]), g.cell);
+    const double cz = xmul(static_cast<double>(static_cast<long long>(cell & mz) + g.lo[2]), g.cell);
+    out[0] = make_float4(static_cast<float>(xsub(x, cx)), static_cast<float>(xsub(y, cy)),
+                         static_cast<float>(xsub(z, cz)), 0.0f);
+    out[1] = make_float4(static_cast<float>(vx), static_cast<float>(vy), static_cast<float>(vz), 0.0f);
+}
+
 // Sort key of object i: the cell key above the object index when packing (the
 // sort then carries no index array), else the cell key alone.
 __device__ __forceinline__ unsigned long long sort_key(unsigned long long key, int i, int pack_bits) {
@@ -364,6 +379,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_exact(StepArgs a, c
                 if (a.screening) {
                     key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
                     vb = xsqrt(xdot3(s[3], s[4], s[5]));
+                    if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
                 }
                 rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
                 st6(out, i, s);
@@ -481,6 +497,7 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
                 if (a.screening) {
                     key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
                     vb = xsqrt(xdot3(s[3], s[4], s[5]));
+                    if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
                 }
                 rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
                 st6(out, i, s);
@@ -535,9 +552,10 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
     int bad = 0, alive = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         if (alive_after[i]) {
-            keys[i] = sort_key(cell_key(g, before[6 * static_cast<int64_t>(i)], before[6 * static_cast<int64_t>(i) + 1],
-                                        before[6 * static_cast<int64_t>(i) + 2], a.real_id ? a.real_id[i] : 0u, &bad),
-                               i, a.pack_bits);
+            const double* s = before + 6 * static_cast<int64_t>(i);
+            const unsigned long long key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &bad);
+            if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
+            keys[i] = sort_key(key, i, a.pack_bits);
             ++alive;
         } else {
             keys[i] = sort_key(dead_key(g), i, a.pack_bits);
@@ -578,13 +596,15 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
         for (int t = threadIdx.x; t < a.sort_passes * 256; t += blockDim.x) a.hist[t] = 0u;
     __syncthreads();
     int bad = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
-        keys[i] = sort_key(alive_after[i] ? cell_key(g, before[6 * static_cast<int64_t>(i)],
-                                                     before[6 * static_cast<int64_t>(i) + 1],
-                                                     before[6 * static_cast<int64_t>(i) + 2],
-                                                     a.real_id ? a.real_id[i] : 0u, &bad)
-                                          : dead_key(g),
-                           i, a.pack_bits);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        unsigned long long key = dead_key(g);
+        if (alive_after[i]) {
+            const double* s = before + 6 * static_cast<int64_t>(i);
+            key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &bad);
+            if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
+        }
+        keys[i] = sort_key(key, i, a.pack_bits);
+    }
     bad = warp_max(bad);
     if ((threadIdx.x & 31) == 0 && bad) atomicOr(&a.ctrl->flags, FLAG_KEY_RANGE);
 }
@@ -857,7 +877,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                                                        unsigned long long hmask, const double* __restrict__ before,
                                                        double* __restrict__ sorted,
                                                        int* __restrict__ sorted_orig, float4* __restrict__ sorted32,
-                                                       int pack_bits) {
+                                                       const float4* __restrict__ rec32, int pack_bits) {
     constexpr int kPer = kCellTile / kBlock;  // consecutive entries per thread
     const int m = ctrl->n_alive;
     if (m == 0) {
@@ -898,9 +918,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
             cell_begin[cid + 1] = m;
         }
     }
-    // Gather of the start-of-step states in sorted order: entries strided
-    // across the block so that stores coalesce, every load of a thread's
-    // entries issued before the first store (random rows of `before`).
+    // Gather in sorted order: entries strided across the block so that stores
+    // coalesce, every load of a thread's entries issued before the first store.
     __shared__ GridParams g;
     if (threadIdx.x == 0) g = ctrl->grid;
     __syncthreads();
@@ -911,6 +930,26 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         const int p = base + j * kBlock;
         o[j] = p < m ? (pack_bits ? static_cast<int>(keys[p] & idx_mask) : idx[p]) : -1;
     }
+    if (!sorted) {
+        // FP32 records only: the ones written with the keys (one 32-byte row each).
+        float4 r[kPer][2];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            if (o[j] < 0) continue;
+            r[j][0] = rec32[2 * static_cast<int64_t>(o[j])];
+            r[j][1] = rec32[2 * static_cast<int64_t>(o[j]) + 1];
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int p = base + j * kBlock;
+            if (o[j] < 0) continue;
+            sorted_orig[p] = o[j];
+            sorted32[2 * static_cast<int64_t>(p)] = r[j][0];
+            sorted32[2 * static_cast<int64_t>(p) + 1] = r[j][1];
+        }
+        return;
+    }
+    // FP64 states (random rows of `before`), and FP32 records from them when asked.
     double2 st[kPer][3];
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
@@ -925,26 +964,13 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
         const int p = base + j * kBlock;
         if (o[j] < 0) continue;
         sorted_orig[p] = o[j];
-        if (sorted) {
-            double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
-            dst[0] = st[j][0];
-            dst[1] = st[j][1];
-            dst[2] = st[j][2];
-        }
-        if (sorted32) {
-            // Position relative to the corner of the object's own cell, velocity, in FP32.
-            const unsigned long long key = keys[p] >> sh;
-            const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
-            const unsigned long long mx = (1ull << g.w[0]) - 1;
-            const double cx = static_cast<double>(static_cast<long long>((key >> (g.w[1] + g.w[2])) & mx) + g.lo[0]) * g.cell;
-            const double cy = static_cast<double>(static_cast<long long>((key >> g.w[2]) & my) + g.lo[1]) * g.cell;
-            const double cz = static_cast<double>(static_cast<long long>(key & mz) + g.lo[2]) * g.cell;
-            sorted32[2 * static_cast<int64_t>(p)] = make_float4(static_cast<float>(st[j][0].x - cx),
-                                                                static_cast<float>(st[j][0].y - cy),
-                                                                static_cast<float>(st[j][1].x - cz), 0.0f);
-            sorted32[2 * static_cast<int64_t>(p) + 1] = make_float4(
-                static_cast<float>(st[j][1].y), static_cast<float>(st[j][2].x), static_cast<float>(st[j][2].y), 0.0f);
-        }
+        double2* dst = reinterpret_cast<double2*>(sorted + 6 * static_cast<int64_t>(p));
+        dst[0] = st[j][0];
+        dst[1] = st[j][1];
+        dst[2] = st[j][2];
+        if (sorted32)
+            f32_record(g, keys[p] >> pack_bits, st[j][0].x, st[j][0].y, st[j][1].x, st[j][1].y, st[j][2].x,
+                       st[j][2].y, sorted32 + 2 * static_cast<int64_t>(p));
     }
 }
 
@@ -2068,7 +2094,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
                                                b.hash_keys, b.hash_vals,
                                                static_cast<unsigned long long>(b.hash_cap - 1), b.state[a.src],
                                                f32_records(a) ? nullptr : b.sorted, b.sorted_orig,
-                                               f32_records(a) ? b.sorted32 : nullptr, a.pack_bits);
+                                               f32_records(a) ? b.sorted32 : nullptr, b.rec32, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
     k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.item_part,

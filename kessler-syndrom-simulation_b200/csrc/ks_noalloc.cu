@@ -56,6 +56,7 @@ constexpr int64_t scratch_bytes() {
     b += align256(sizeof(int) * kNoAllocHash);           // hash values
     b += align256(sizeof(double) * 6 * n);               // sorted
     b += align256(sizeof(float4) * 2 * n);               // sorted32
+    b += align256(sizeof(float4) * 2 * n);               // rec32
     b += align256(sizeof(int) * n);                      // sorted_orig
     b += align256(sizeof(int2) * kNoAllocSurvivors);     // survivors
     b += align256(sizeof(ks_conjunction) * kNoAllocConj);  // conjunctions
@@ -116,6 +117,7 @@ ks::DeviceBuffers carve(unsigned char* base) {
     b.hash_cap = kNoAllocHash;
     b.sorted = take<double>(p, sizeof(double) * 6 * n);
     b.sorted32 = take<float4>(p, sizeof(float4) * 2 * n);
+    b.rec32 = take<float4>(p, sizeof(float4) * 2 * n);
     b.sorted_orig = take<int>(p, sizeof(int) * n);
     b.survivors = take<int2>(p, sizeof(int2) * kNoAllocSurvivors);
     b.surv_cap = kNoAllocSurvivors;
@@ -205,6 +207,7 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
     a.ctrl = b.ctrl;
     a.ctrl_next = b.ctrl + 1;
     a.src = 0;
+    a.rec32 = b.rec32;
 
     // The array keeps the previous call's contents: the control blocks are
     // reset here, the sort and hash buffers by the launches that use them.
