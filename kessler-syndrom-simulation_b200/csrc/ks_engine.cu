@@ -75,6 +75,8 @@ struct ks_ctx {
     bool pack_keys = true;     // object index packed below the cell key in the sort keys
     int64_t max_step_conj = 0; // most conjunction records of one step so far (record buffer sizing)
     bool conj_small = false;   // chunks order their records in one block (few expected)
+    int64_t chunk_spec = 0;    // records a chunk copies back with its control blocks
+    int64_t graph_spec[2] = {0, 0};  // the same, as captured in graph_exec[]
     bool allow_pack = true;    // tuning: packing allowed where the keys leave room
     int realisations = 1;
     int rbits = 0;
@@ -221,6 +223,7 @@ int ensure_conj(ks_ctx* ctx, int64_t want) {
         b.conj_cap = want;
     }
     if (want > ctx->h_conj_cap) {
+        drop_graphs(ctx);  // graphs copy records into h_conj
         if (ctx->h_conj) cudaFreeHost(ctx->h_conj);
         ctx->h_conj = nullptr;
         ctx->h_conj_cap = 0;
@@ -352,9 +355,21 @@ void record(ks_ctx* ctx, int k, int phase, bool capturing) {
     else cudaEventRecord(e, ctx->stream);
 }
 
+// End of a chunk's device work, before its results are copied back.
+void record_chunk_end(ks_ctx* ctx, bool capturing) {
+    if (!ctx->profiling) return;
+    if (capturing) cudaEventRecordWithFlags(ctx->ev_chunk[1], ctx->stream, cudaEventRecordExternal);
+    else cudaEventRecord(ctx->ev_chunk[1], ctx->stream);
+}
+
+// A chunk in stream order: its step parameters up (from h_params), set-up
+// (with the checkpoint of the carried speculation), the steps, the ordering
+// of its records, and its control blocks and first chunk_spec records back to
+// the host, so that running it takes one launch and one synchronisation.
 void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
     cudaStream_t s = ctx->stream;
-    ks::launch_chunk_init(ctx->b, k_steps, s);
+    cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, s);
+    ks::launch_chunk_init(ctx->b, k_steps, s, true);
     int src = src0;
     for (int k = 0; k < k_steps; ++k) {
         const StepArgs a = step_args(ctx, k, k_steps, src);
@@ -379,6 +394,12 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
     }
     if (ctx->screening)
         ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, ctx->conj_small, s);
+    record_chunk_end(ctx, capturing);
+    cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, s);
+    if (ctx->chunk_spec > 0)
+        cudaMemcpyAsync(ctx->h_conj, ctx->b.conj_sorted, sizeof(ks_conjunction) * ctx->chunk_spec,
+                        cudaMemcpyDeviceToHost, s);
 }
 
 // Captures and instantiates the chunk's graph if it does not exist yet.
@@ -402,6 +423,7 @@ int ensure_graph(ks_ctx* ctx, int k_steps) {
         }
         // Uploaded now rather than by its first launch.
         KS_CUDA(cudaGraphUpload(exec, ctx->stream));
+        ctx->graph_spec[ctx->cur] = ctx->chunk_spec;
     }
     return KS_OK;
 }
@@ -420,8 +442,8 @@ int launch_chunk(ks_ctx* ctx, int k_steps) {
 }
 
 // Start-of-chunk checkpoint for replays. A one-step chunk never overwrites
-// its input states (steps ping-pong between two buffers), so only the
-// carried control block is saved then.
+// its input states (steps ping-pong between two buffers), so its states need
+// none; the carried control block is saved by the chunk's own set-up kernel.
 int save_checkpoint(ks_ctx* ctx, int k_steps) {
     ks::DeviceBuffers& b = ctx->b;
     ctx->ckpt_states = k_steps > 1;
@@ -429,7 +451,6 @@ int save_checkpoint(ks_ctx* ctx, int k_steps) {
         KS_CUDA(cudaMemcpyAsync(b.ckpt_state, b.state[ctx->cur], sizeof(double) * 6 * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
         KS_CUDA(cudaMemcpyAsync(b.ckpt_alive, b.alive[ctx->cur], ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
     }
-    KS_CUDA(cudaMemcpyAsync(carry_ckpt_slot(ctx), carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToDevice, ctx->stream));
     return KS_OK;
 }
 
@@ -505,8 +526,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     int rc = ensure_chunk(ctx, k_steps);
     if (rc) return rc;
     double t_end = 0.0;
-    fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
-    KS_CUDA(cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, ctx->stream));
+    fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);  // uploaded by the chunk itself
     // Room for the chunk's records at the largest per-step count seen so far,
     // so that a longer chunk does not overflow and replay.
     if (ctx->screening && ctx->max_step_conj > 0) {
@@ -520,6 +540,12 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         ctx->conj_small = small;
         drop_graphs(ctx);
     }
+    // Records copied back with the control blocks, up to the expected count,
+    // so that a chunk with no more than that needs one host round trip.
+    const int64_t spec = ctx->screening ? std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, ctx->b.conj_cap) : 0;
+    ctx->chunk_spec = ctx->max_step_conj > 0 && spec <= (int64_t(1) << 16) ? spec : 0;
+    const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
+    if (use_graph && ctx->graph_exec[ctx->cur] && ctx->graph_spec[ctx->cur] < ctx->chunk_spec) drop_graphs(ctx);
     // A new graph is built before the chunk's start is recorded, so that the
     // chunk's device time holds no wait for the host.
     if ((rc = ensure_graph(ctx, k_steps))) return rc;
@@ -528,22 +554,12 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         rc = save_checkpoint(ctx, k_steps);
         if (rc) return rc;
     }
-    // Records copied with the control blocks, up to the expected count, so
-    // that a chunk with no more than that needs one host round trip.
-    const int64_t spec = ctx->screening ? std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, ctx->b.conj_cap) : 0;
-    const bool speculate = ctx->max_step_conj > 0 && spec <= (int64_t(1) << 16);
     int64_t have = 0;  // leading records of this chunk's run already in h_conj
     for (int attempt = 0;; ++attempt) {
         rc = launch_chunk(ctx, k_steps);
         if (rc) return rc;
-        if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[1], ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
-        if (speculate)
-            KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj_sorted, sizeof(ks_conjunction) * spec,
-                                    cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
-        have = speculate ? spec : 0;
+        have = use_graph ? ctx->graph_spec[ctx->cur] : ctx->chunk_spec;
         int flags = ctx->h_chunk->flags;
         unsigned long long max_refined = 0;
         int max_bits = 0;
@@ -611,11 +627,8 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         if (rc) return rc;
         rc = launch_chunk(ctx, k_steps);
         if (rc) return rc;
-        if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[1], ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(ctx->h_ctrl, ctx->b.ctrl, sizeof(Ctrl) * k_steps, cudaMemcpyDeviceToHost, ctx->stream));
-        KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
-        have = 0;
+        have = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph ? ctx->graph_spec[ctx->cur] : ctx->chunk_spec;
         if (ctx->h_chunk->flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_TIMEOUT | ks::FLAG_KEY_RANGE))
             return fail(ctx, KS_ERR_STATE, "replay to the first collision step overflowed");
     }

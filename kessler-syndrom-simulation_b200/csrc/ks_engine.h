@@ -185,7 +185,8 @@ struct StepArgs {
 };
 
 // Kernel launchers (ks_kernels.cu). All enqueue on `stream` and never synchronise.
-void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream);
+// checkpoint: also save the carried speculation into its checkpoint slot (replays restore it).
+void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream, bool checkpoint = false);
 void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int use_alive_src,
                       cudaStream_t stream);
 void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);

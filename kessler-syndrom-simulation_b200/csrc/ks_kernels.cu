@@ -267,9 +267,12 @@ __device__ void ctrl_reset(Ctrl& c) {
 }
 
 // ctrl[0..k) reset; ctrl[0] takes the carried speculation, the carry slot is reset.
-__global__ void k_chunk_init(Ctrl* ctrl, int k_steps, Ctrl* carry, ChunkCtrl* chunk) {
+__global__ void k_chunk_init(Ctrl* ctrl, int k_steps, Ctrl* carry, ChunkCtrl* chunk, Ctrl* carry_ckpt) {
     __shared__ Ctrl saved;
-    if (threadIdx.x == 0) saved = *carry;
+    if (threadIdx.x == 0) {
+        saved = *carry;
+        if (carry_ckpt) *carry_ckpt = saved;  // the chunk's checkpoint of the carried speculation
+    }
     __syncthreads();
     for (int s = threadIdx.x; s < k_steps; s += blockDim.x) ctrl_reset(ctrl[s]);
     __syncthreads();
@@ -1906,8 +1909,9 @@ int sm_count() {
     return g_sm_count;
 }
 
-void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream) {
-    k_chunk_init<<<1, kBlock, 0, stream>>>(b.ctrl, k_steps, b.ctrl + b.ctrl_len - 2, b.chunk);
+void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream, bool checkpoint) {
+    k_chunk_init<<<1, kBlock, 0, stream>>>(b.ctrl, k_steps, b.ctrl + b.ctrl_len - 2, b.chunk,
+                                           checkpoint ? b.ctrl + b.ctrl_len - 1 : nullptr);
 }
 
 void launch_seed_ctrl(const DeviceBuffers& b, int n, int src, Ctrl* target, int use_alive_src, cudaStream_t stream) {
