@@ -273,13 +273,35 @@ def roofline_of(tm, a, fp64_rate, fp32_rate, split):
         k["frac"] = (k["tflops"] * 1e12 / k["peak"]) if k["tflops"] else None
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     d = kernels[dom]
+    # The memory-side phases against HBM: algorithmic bytes per step over the
+    # phase's device time (the sort moves u64 keys that carry the object index).
+    peaks, peak_src = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    n_obj = tm["object_steps"] / steps
+    passes = tm["sort_passes"]
+    hbm_phases = {
+        "sort": (16.0 * passes * n_obj, phases["sort_ms"],
+                 f"{passes} radix passes x (8 B key read + 8 B key written) per object"),
+        "cells": (76.0 * n_obj, phases["cells_ms"],
+                  "per object: 8 B key read, 32 B FP32 record gathered, 32 B record + 4 B index written"),
+        "pairs": (32.0 * n_obj, phases["pairs_ms"], "per object: its 32 B FP32 record read once"),
+    }
+    hbm_kernels = {}
+    for k, (nbytes, ms, what) in hbm_phases.items():
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+        hbm_kernels[k] = {"ms": ms, "algorithmic_bytes": nbytes, "gbs": gbs, "frac": gbs / hbm if gbs else None,
+                          "what": what}
     return {"bound": d["pipe"], "kernel": dom, "achieved": d["tflops"], "peak": d["peak"] / 1e12,
             "unit": "TFLOP/s", "frac": d["frac"], "traffic": traffic_of(dom, split),
             "peak_source": "measured on this GPU by the project microbenchmark (dependent add/mul chains, no FMA); "
                            "MEASURED_PEAKS.json has no FP64/FP32 SIMT figure",
             "algorithmic_ops_per_launch": d["ops"], "phase_ms_per_step": phases,
             "kernels": {k: {"ms": v["ms"], "pipe": v["pipe"], "tflops": v["tflops"], "frac": v["frac"]}
-                        for k, v in kernels.items()}}
+                        for k, v in kernels.items()},
+            "hbm": {"peak_gbs": hbm,
+                    "peak_source": ("copy bandwidth measured on this pool (MEASURED_PEAKS.json hbm_gbs)"
+                                    if peak_src == "measured" else "the profiling recipe's fallback (6.65 TB/s)"),
+                    "phases": hbm_kernels}}
 
 
 def traffic_of(kernel, split):
