@@ -154,7 +154,7 @@ class Engine:
     def take_conjunctions(self):
         cnt = C.c_int64()
         self._check(self._lib.ks_take_conjunctions(self._h, None, 0, C.byref(cnt)))
-        out = np.zeros(cnt.value, dtype=CONJ_DTYPE)
+        out = np.empty(cnt.value, dtype=CONJ_DTYPE)  # every record is written below
         if cnt.value:
             self._check(self._lib.ks_take_conjunctions(self._h, ptr(out), cnt.value, C.byref(cnt)))
         return out[: cnt.value]
@@ -162,7 +162,7 @@ class Engine:
     def take_step_stats(self):
         cnt = C.c_int64()
         self._check(self._lib.ks_take_step_stats(self._h, None, 0, C.byref(cnt)))
-        out = np.zeros(cnt.value, dtype=STATS_DTYPE)
+        out = np.empty(cnt.value, dtype=STATS_DTYPE)  # every row is written below
         if cnt.value:
             self._check(self._lib.ks_take_step_stats(self._h, ptr(out), cnt.value, C.byref(cnt)))
         return out[: cnt.value]

@@ -62,6 +62,10 @@ struct ks_ctx {
     ks_conjunction* h_conj = nullptr;
     int64_t h_conj_cap = 0;
     std::vector<ks_conjunction> conj_out;
+    // The last chunk's ordered records, still in h_conj[pend_begin, pend_end):
+    // newer than conj_out, moved into it before anything reuses h_conj, so
+    // that a caller taking records after every step copies them only once.
+    int64_t pend_begin = 0, pend_end = 0;
     std::vector<ks_step_stats> stats_out;
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     std::vector<cudaEvent_t> ev;
@@ -207,6 +211,19 @@ void free_conj(ks_ctx* ctx) {
     b.conj_cap = 0;
 }
 
+// Moves the pending records of the last chunk behind conj_out.
+void stash_pending(ks_ctx* ctx) {
+    if (ctx->pend_end > ctx->pend_begin)
+        ctx->conj_out.insert(ctx->conj_out.end(), ctx->h_conj + ctx->pend_begin, ctx->h_conj + ctx->pend_end);
+    ctx->pend_begin = ctx->pend_end = 0;
+}
+
+// Forgets every record not yet taken.
+void clear_records(ks_ctx* ctx) {
+    ctx->conj_out.clear();
+    ctx->pend_begin = ctx->pend_end = 0;
+}
+
 int ensure_conj(ks_ctx* ctx, int64_t want) {
     if (want > ctx->b.conj_cap) {
         if (want > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "more than 2^30 conjunctions in one chunk");
@@ -223,6 +240,7 @@ int ensure_conj(ks_ctx* ctx, int64_t want) {
         b.conj_cap = want;
     }
     if (want > ctx->h_conj_cap) {
+        stash_pending(ctx);
         drop_graphs(ctx);  // graphs copy records into h_conj
         if (ctx->h_conj) cudaFreeHost(ctx->h_conj);
         ctx->h_conj = nullptr;
@@ -523,6 +541,7 @@ int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_
 // fragmented before the next step, as the reference's loop does after each
 // step (src/main.cpp:401-407).
 int run_chunk(ks_ctx* ctx, int k_steps) {
+    stash_pending(ctx);  // this chunk's records land in h_conj
     int rc = ensure_chunk(ctx, k_steps);
     if (rc) return rc;
     double t_end = 0.0;
@@ -635,12 +654,12 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     std::vector<ks_conjunction> hits;
     const double t_last = ctx->h_params[k_steps - 1].t0;
     if (nc > 0) {
-        const size_t base = ctx->conj_out.size();
-        ctx->conj_out.insert(ctx->conj_out.end(), ctx->h_conj, ctx->h_conj + nc);
-        finish_order(ctx->conj_out.begin() + base, ctx->conj_out.end());
+        finish_order(ctx->h_conj, ctx->h_conj + nc);
+        ctx->pend_begin = 0;
+        ctx->pend_end = nc;
         if (ctx->bk.on)
-            for (size_t q = base; q < ctx->conj_out.size(); ++q)
-                if (ctx->conj_out[q].collision) hits.push_back(ctx->conj_out[q]);
+            for (int64_t q = 0; q < nc; ++q)
+                if (ctx->h_conj[q].collision) hits.push_back(ctx->h_conj[q]);
     }
     for (int k = 0; k < k_steps; ++k) {
         const Ctrl& c = ctx->h_ctrl[k];
@@ -1094,7 +1113,7 @@ int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double
     if (rc) return rc;
     ctx->has_pop = true;
     ctx->steps_done = 0;
-    ctx->conj_out.clear();
+    clear_records(ctx);
     ctx->stats_out.clear();
     return KS_OK;
 }
@@ -1129,7 +1148,7 @@ int ks_set_population_batch(ks_ctx* ctx, int32_t realisations, const int64_t* of
     if (rc) return rc;
     ctx->has_pop = true;
     ctx->steps_done = 0;
-    ctx->conj_out.clear();
+    clear_records(ctx);
     ctx->stats_out.clear();
     return KS_OK;
 }
@@ -1294,6 +1313,7 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
     const int cur0 = ctx->cur;
     const int64_t steps0 = ctx->steps_done;
     const double t0 = ctx->t;
+    stash_pending(ctx);
     const size_t conj0 = ctx->conj_out.size(), stats0 = ctx->stats_out.size();
     const ks_timing timing0 = ctx->timing;
     const bool breakup0 = ctx->bk.on;
@@ -1331,6 +1351,7 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
         KS_CUDA(cudaMemcpyAsync(carry_slot(ctx), &carry, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->conj_out.resize(conj0);
+        ctx->pend_begin = ctx->pend_end = 0;
         ctx->stats_out.resize(stats0);
         return KS_OK;
     };
@@ -1466,14 +1487,22 @@ int ks_run(ks_ctx* ctx, int64_t steps) {
 
 int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t* count) {
     if (!ctx || !count || cap < 0) return KS_ERR_ARG;
-    const int64_t avail = static_cast<int64_t>(ctx->conj_out.size());
+    const int64_t older = static_cast<int64_t>(ctx->conj_out.size());
+    const int64_t avail = older + (ctx->pend_end - ctx->pend_begin);
     if (!out) {
         *count = avail;
         return KS_OK;
     }
     const int64_t m = std::min(avail, cap);
-    std::memcpy(out, ctx->conj_out.data(), sizeof(ks_conjunction) * m);
-    ctx->conj_out.erase(ctx->conj_out.begin(), ctx->conj_out.begin() + m);
+    const int64_t m1 = std::min(older, m);  // the older records first
+    if (m1 > 0) {
+        std::memcpy(out, ctx->conj_out.data(), sizeof(ks_conjunction) * m1);
+        ctx->conj_out.erase(ctx->conj_out.begin(), ctx->conj_out.begin() + m1);
+    }
+    if (m > m1) {
+        std::memcpy(out + m1, ctx->h_conj + ctx->pend_begin, sizeof(ks_conjunction) * (m - m1));
+        ctx->pend_begin += m - m1;
+    }
     *count = m;
     return KS_OK;
 }
@@ -1692,7 +1721,7 @@ int ks_load_population(ks_ctx* ctx, const char* path) {
     rc = seed_speculation(ctx);
     if (rc) return rc;
     ctx->has_pop = true;
-    ctx->conj_out.clear();
+    clear_records(ctx);
     ctx->stats_out.clear();
     return KS_OK;
 }
@@ -1800,6 +1829,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
     }
     ctx->dt = saved_dt;
     const int64_t nc = static_cast<int64_t>(ctx->h_chunk->conj_count);
+    stash_pending(ctx);
     if (nc > 0) {
         KS_CUDA(cudaMemcpyAsync(ctx->h_conj, ctx->b.conj, sizeof(ks_conjunction) * nc, cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
