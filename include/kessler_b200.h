@@ -212,7 +212,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
  *     a time-critical loop that cannot afford cudaMalloc / cudaFree, which
  *     synchronise the device. Same inputs, outputs and results as ks_screen
  *     (thresholds passed explicitly, no context), on device buffers carved from
- *     one fixed array in the library's device image (about 11 MB, held by every
+ *     one fixed array in the library's device image (about 9.3 MB, held by every
  *     GPU that loads the library until exit). Limits: n <= 16384 objects,
  *     <= 131072 pairs sent to refinement, <= 32768 conjunctions; beyond them it
  *     returns KS_ERR_RANGE / KS_ERR_OVERFLOW and writes no records. cap must

@@ -66,7 +66,7 @@ constexpr int64_t scratch_bytes() {
     return b;
 }
 
-constexpr int64_t kScratchBytes = scratch_bytes();  // about 11 MB
+constexpr int64_t kScratchBytes = scratch_bytes();  // about 9.3 MB
 
 // The scratch array. In host code this name is only a stand-in for the
 // device symbol: its device address comes from cudaGetSymbolAddress.
