@@ -160,3 +160,38 @@ def test_edge_populations(engine, oracle):
     dead = np.zeros(4, np.uint8)
     got = run_engine(engine, np.tile(one, (4, 1)), np.ones(4), dead, 3)
     assert got[3]["alive"].max() == 0 and got[3]["candidate_pairs"].sum() == 0
+
+
+def test_partial_takes_return_records_in_order(engine, ks):
+    # Records taken a few at a time, between chunks and across them, come out
+    # in the same (t, i, j) order as one take after the whole run.
+    import ctypes as C
+    from importlib import import_module
+    ptr = import_module(ks.__name__ + "._abi").ptr
+    st, sz, al = ks.generate_population(505, 5000, 30000, 8, 3600.0)
+    want = run_engine(engine, st, sz, al, 24, spg=8)[2]
+    assert len(want) > 40
+
+    def take(cap):
+        out = np.empty(cap, dtype=ks.CONJ_DTYPE)
+        cnt = C.c_int64()
+        assert engine._lib.ks_take_conjunctions(engine._h, ptr(out), cap, C.byref(cnt)) == 0
+        return out[: cnt.value]
+
+    engine.set_steps_per_graph(8)
+    engine.set_clock(2461253.916666667, 0.0, 10.0)
+    engine.set_screening(True, 5.0, 1.0, 0.01)
+    engine.set_population(st, sz, al)
+    parts = []
+    engine.run(8)
+    parts.append(take(3))          # from the last chunk's records
+    engine.run(8)                  # the rest of the first chunk moves behind
+    parts.append(take(5))
+    parts.append(take(1))
+    engine.run(8)
+    parts.append(take(len(want)))  # everything left, older records first
+    parts.append(take(10))         # nothing left
+    engine.take_step_stats()
+    got = np.concatenate(parts)
+    assert len(parts[-1]) == 0
+    assert_same_conj(got, want)
