@@ -988,12 +988,18 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
     const int64_t total = 13 * static_cast<int64_t>(nc);
     for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
          t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(t / 13), o = static_cast<int>(t % 13);
+        const int c = static_cast<int>(t / 13), o = static_cast<int>(t - 13 * static_cast<int64_t>(c));
+        // Offset o of c_forward, computed rather than read from constant memory
+        // at a lane-varying index (which serialises): o < 9 is (1, o/3 - 1, o%3 - 1),
+        // 9..11 is (0, 1, o - 10), 12 is (0, 0, 1).
+        const int dx = o < 9 ? 1 : 0;
+        const int dy = o < 9 ? o / 3 - 1 : (o < 12 ? 1 : 0);
+        const int dz = o < 9 ? o % 3 - 1 : (o < 12 ? o - 10 : 1);
         const unsigned long long key = cell_key_in[c];
         const unsigned long long rid = key >> (g.w[0] + g.w[1] + g.w[2]);
-        const long long x = static_cast<long long>((key >> (g.w[1] + g.w[2])) & ((1ull << g.w[0]) - 1)) + c_forward[o][0];
-        const long long y = static_cast<long long>((key >> g.w[2]) & my) + c_forward[o][1];
-        const long long z = static_cast<long long>(key & mz) + c_forward[o][2];
+        const long long x = static_cast<long long>((key >> (g.w[1] + g.w[2])) & ((1ull << g.w[0]) - 1)) + dx;
+        const long long y = static_cast<long long>((key >> g.w[2]) & my) + dy;
+        const long long z = static_cast<long long>(key & mz) + dz;
         int found = -1;
         if (x >= 0 && x <= g.span[0] && y >= 0 && y <= g.span[1] && z >= 0 && z <= g.span[2]) {
             const unsigned long long nk = (rid << (g.w[0] + g.w[1] + g.w[2])) |
