@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--dt", type=float, default=10.0)
     ap.add_argument("--conj-km", type=float, default=5.0)
     ap.add_argument("--steps-per-graph", type=int, default=32)
-    ap.add_argument("--cpu-steps", type=int, default=8, help="steps of the CPU baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=24, help="steps of the CPU baseline sample (~13 s on 16 cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-error-study", action="store_true")
