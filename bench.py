@@ -324,9 +324,10 @@ def launches_per_step(sort_passes):
     return 1 + 1 + (1 + sort_passes) + 7 + 1 + 1
 
 
-# Per graph chunk: chunk_init, ctrl_reset, and the ordering of the chunk's
-# conjunction records (keys, upsweep, 4 passes, gather).
-LAUNCHES_PER_CHUNK = 9
+# Per graph chunk of the timed run: chunk_init and the ordering of the chunk's
+# conjunction records (keys, upsweep, 4 passes, gather; chunks this long take
+# the multi-block sort).
+LAUNCHES_PER_CHUNK = 8
 
 
 BORDER_TOL_KM = 1e-5  # 1 cm: the agreement the plain form is held to after 24 h
