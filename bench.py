@@ -158,50 +158,105 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
-def cpu_baseline(a, st, sz, al, steps):
-    """The reference CPU path (oracle/_ref, else the oracle port) on this host."""
+def _checkers():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import checkers
-    threads = os.cpu_count() or 1
+    return checkers
+
+
+def cpu_checker():
+    """The reference CPU path (oracle/_ref, built from the reference's sources)
+    on all host threads, else the oracle port on one."""
+    checkers = _checkers()
     if checkers.reference_available():
-        chk, kind = checkers.Reference(), "reference"
-    else:
-        chk, kind, threads = checkers.Oracle(), "port", 1
+        return checkers.Reference(), "reference", os.cpu_count() or 1
+    return checkers.Oracle(), "port", 1
+
+
+def cpu_baseline(a, st, sz, al, steps):
+    """The reference CPU path on this host: the first `steps` steps of the population."""
+    chk, kind, threads = cpu_checker()
     t0 = time.perf_counter()
-    _, fa, conj, stats = chk.run(st, sz, al, epoch_jd=2461253.916666667, dt=a.dt, steps=steps, screen=True,
-                                 threshold_km=a.conj_km, threads=threads)
+    fs, fa, conj, stats = chk.run(st, sz, al, epoch_jd=2461253.916666667, dt=a.dt, steps=steps, screen=True,
+                                  threshold_km=a.conj_km, threads=threads)
     wall = time.perf_counter() - t0
-    obj_steps = int(np.sum(stats["alive"])) if steps else 0
     # objects propagated = alive at the start of each step
     alive_start = int(al.sum()) + int(np.sum(stats["alive"][:-1]))
     return {"value": alive_start / wall, "unit": "object-steps/s", "cores": threads, "kind": kind,
             "sample": f"first {steps} steps of the same {len(st)}-object population, screening included",
             "pairs_per_s": float(stats["candidate_pairs"].sum()) / wall, "wall_s": wall,
-            "conjunctions": int(len(conj)), "_obj_steps_after": obj_steps}
+            "conjunctions": int(len(conj)), "_run": (fs, fa, conj, stats)}
 
 
 def run_reference_arm(a):
+    """The reference's own CPU implementation of the path (oracle/_ref) on the
+    host's cores, on this arm's workload: W untimed steps, then K timed steps
+    continuing from them. Its inputs come from oracle/libks_workload.so, so
+    this arm loads nothing of the engine."""
     world, rank, local = dist_env()
     if rank != 0:
         return 0
-    ks = importlib.import_module("kessler-syndrom-simulation_b200")
-    st, sz, al = ks.generate_population(a.seed, a.base, a.objects, a.parents, a.frag_age_s)
-    steps = max(1, min(a.steps, 24))
-    warm = max(0, min(a.warmup, 1))
-    base = cpu_baseline(a, st, sz, al, warm + steps)
-    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "object-steps/s",
-            "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * base["wall_s"] / (warm + steps),
+    checkers = _checkers()
+    st, sz, al = checkers.generate_population(a.seed, a.base, a.objects, a.parents, a.frag_age_s)
+    chk, kind, threads = cpu_checker()
+    steps, warm = a.steps, a.warmup
+    kw = dict(epoch_jd=2461253.916666667, dt=a.dt, screen=True, threshold_km=a.conj_km, threads=threads)
+    if warm > 0:
+        st, al, _, _ = chk.run(st, sz, al, t_start=0.0, steps=warm, **kw)
+    t0 = time.perf_counter()
+    _, _, conj, stats = chk.run(st, sz, al, t_start=warm * a.dt, steps=steps, **kw)
+    wall = time.perf_counter() - t0
+    alive_start = int(al.sum()) + int(np.sum(stats["alive"][:-1]))
+    value = alive_start / wall
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "object-steps/s",
+            "n_gpus": a.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * wall / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded generator)", "config": config_of(a),
-            "pairs_per_s": base["pairs_per_s"],
-            "cpu_baseline": {"value": base["value"], "unit": "object-steps/s", "cores": base["cores"],
-                             "kind": base["kind"],
-                             "sample": f"{warm + steps} steps of the {a.objects}-object workload "
-                                       f"(of the K={a.steps} requested), all host threads"},
-            "e2e": {"value": base["value"], "unit": "object-steps/s", "h2d_bytes_per_step": 0,
+            "data": "synthetic (seeded generator; no dataset)", "config": config_of(a),
+            "pairs_per_s": float(stats["candidate_pairs"].sum()) / wall,
+            "conjunctions_per_step": len(conj) / steps,
+            "cpu_baseline": {"value": value, "unit": "object-steps/s", "cores": threads, "kind": kind,
+                             "sample": f"all {steps} timed steps (after {warm} untimed) of the {a.objects}-object "
+                                       f"workload, every host thread"},
+            "e2e": {"value": value, "unit": "object-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def parity_vs_reference(ks, eng, a, st, sz, al, ref_run, steps):
+    """The GPU FP64 path against the reference CPU path's own run of the first
+    `steps` steps of the same population (the cpu_baseline sample): conjunction
+    records and per-step counters compared bit for bit, final states too; and
+    the split path's position error against the same reference states."""
+    fs_ref, fa_ref, conj_ref, stats_ref = ref_run
+    out = {"n_objects": int(len(st)), "steps": int(steps), "reference_conjunctions": int(len(conj_ref))}
+    for name, prec in (("fp64", ks.PRECISION_FP64), ("split", ks.PRECISION_SPLIT)):
+        eng.set_precision(prec)
+        eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
+        eng.set_screening(True, a.conj_km, 1.0, 0.01)
+        eng.set_l2_flush(0)
+        eng.set_profiling(False)
+        eng.set_population(st, sz, al)
+        eng.run(steps)
+        fs, fa = eng.get_population()
+        conj = eng.take_conjunctions()
+        stats = eng.take_step_stats()
+        recs = len(conj) == len(conj_ref) and all(np.array_equal(conj[f], conj_ref[f]) for f in
+                                                  ("i", "j", "step", "t", "miss_km", "v_rel_km_s", "collision"))
+        ctrs = all(np.array_equal(stats[f], stats_ref[f]) for f in
+                   ("candidate_pairs", "refined_pairs", "co_orbiting", "conjunctions", "cell_km",
+                    "max_cell_objects", "alive"))
+        live = (fa == 1) & (fa_ref == 1)
+        dr = np.linalg.norm(fs[live, :3] - fs_ref[live, :3], axis=1) * 1e3
+        dv = np.linalg.norm(fs[live, 3:] - fs_ref[live, 3:], axis=1) * 1e6
+        kg = set(zip(conj["i"].tolist(), conj["j"].tolist(), conj["step"].tolist()))
+        kr = set(zip(conj_ref["i"].tolist(), conj_ref["j"].tolist(), conj_ref["step"].tolist()))
+        out[name] = {"records_equal": bool(recs), "counters_equal": bool(ctrs),
+                     "states_equal": bool(np.array_equal(fs, fs_ref) and np.array_equal(fa, fa_ref)),
+                     "conjunctions": int(len(conj)), "pairs_only_here": len(kg - kr), "pairs_only_reference": len(kr - kg),
+                     "max_pos_err_m": float(dr.max()) if dr.size else 0.0,
+                     "max_vel_err_mm_s": float(dv.max()) if dv.size else 0.0}
+    return out
 
 
 def timed_run(ks, eng, a, st, sz, al, precision, barrier):
@@ -478,6 +533,8 @@ def main():
         base = cpu_baseline(a, st, sz, al, a.cpu_steps)
         line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
         line["cpu_baseline"]["pairs_per_s"] = base["pairs_per_s"]
+        line["parity_vs_reference"] = dict(parity_vs_reference(ks, eng, a, st, sz, al, base["_run"], a.cpu_steps),
+                                           reference_kind=base["kind"])
     eng.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

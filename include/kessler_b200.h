@@ -49,7 +49,7 @@ enum {
 };
 
 /* --- lifecycle: replaces gpu::create / gpu::destroy (src/core/collision_gpu.hpp:47-48)
- *     and the device side of Screener::set_gpu (src/core/collision.hpp:235). */
+ *     and the device side of Screener::set_gpu (src/core/collision.hpp:93). */
 int ks_create(int device, ks_ctx** out);
 void ks_destroy(ks_ctx* ctx);
 const char* ks_last_error(const ks_ctx* ctx);
@@ -81,7 +81,7 @@ int64_t ks_population_size(const ks_ctx* ctx);
 int ks_set_clock(ks_ctx* ctx, double epoch_jd, double t, double dt);
 int ks_get_clock(const ks_ctx* ctx, double* t, int64_t* steps_done);
 
-/* --- screening configuration: ScreeningConfig (src/core/collision.hpp:168-179);
+/* --- screening configuration: ScreeningConfig (src/core/collision.hpp:26-37);
  *     enabled=0 runs propagation only (the CLI without --screen, src/main.cpp:352). */
 int ks_set_screening(ks_ctx* ctx, int enabled, double threshold_km, double radius_scale,
                      double min_encounter_speed_km_s);
@@ -111,7 +111,11 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * "prop_block" (32..128, threads per block of the propagation kernels),
  * "item_col_blocks" (1..64, column blocks of 32 per pair-kernel work item),
  * "pack_keys" (1: the radix sort carries the object index in the low bits of
- * its keys where they leave room, the default; 0: a separate index array).
+ * its keys where they leave room, the default; 0: a separate index array),
+ * "lookback_polls" (0..2^30, default 2^22: polls a radix-sort tile makes of a
+ * predecessor's unpublished digit counts before it gives up; a wait that runs
+ * out fails the run with KS_ERR_TIMEOUT and leaves the simulation where the
+ * failed chunk of steps began, with no records from it).
  * Conjunctions, refined and co-orbiting counts and states never change;
  * candidate_pairs and cell_km change with the cell edge. */
 int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value);
@@ -199,7 +203,7 @@ int ks_get_objects(ks_ctx* ctx, int64_t n, double* size_m, double* mass_kg, doub
                    int32_t* realisation);
 
 /* --- one-shot screening on host states: replaces Screener::screen and screen_step
- *     (src/core/collision.hpp:242-244, 266-270). before/after: n x 6 doubles,
+ *     (src/core/collision.hpp:100-102, 124-128). before/after: n x 6 doubles,
  *     alive_after: n bytes, size_m: n doubles. Results sorted by (t, i, j), step = 0.
  *     Uses the context's device buffers: a resident population is discarded. */
 int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
@@ -210,14 +214,19 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
  *     exists for callers that must not allocate GPU memory at call time, such as
  *     an application whose device memory is already handed to its own pool, or
  *     a time-critical loop that cannot afford cudaMalloc / cudaFree, which
- *     synchronise the device. Same inputs, outputs and results as ks_screen
- *     (thresholds passed explicitly, no context), on device buffers carved from
- *     one fixed array in the library's device image (about 9.3 MB, held by every
- *     GPU that loads the library until exit). Limits: n <= 16384 objects,
- *     <= 131072 pairs sent to refinement, <= 32768 conjunctions; beyond them it
- *     returns KS_ERR_RANGE / KS_ERR_OVERFLOW and writes no records. cap must
- *     hold every conjunction found (*count is set either way). stream is a
- *     cudaStream_t or NULL. error (optional, error_len bytes) receives a message.
+ *     synchronise the device. Same inputs and outputs as ks_screen (thresholds
+ *     passed explicitly, no context). It always screens in FP64 precision with
+ *     the default launch shapes, so its records and counters equal those of
+ *     ks_screen on a context left in FP64 precision with default tuning. Its
+ *     device buffers are carved from one fixed array in the library's device
+ *     image (about 9.3 MB, held by every GPU that loads the library until
+ *     exit). Limits: n <= 16384 objects, <= 131072 pairs sent to refinement,
+ *     <= 32768 conjunctions; beyond them it returns KS_ERR_RANGE /
+ *     KS_ERR_OVERFLOW and writes no records. *count receives the number of
+ *     conjunctions found, also when cap or the fixed conjunction capacity is
+ *     too small for them, and 0 on every other error. stream is a
+ *     cudaStream_t or NULL; the call waits for its own work on it before
+ *     returning. error (optional, error_len bytes) receives a message.
  *     The first call on each device looks up the array's device address, so
  *     make that first call before any stream capture. Calls share the array:
  *     calls that overlap on the GPU (other threads, other streams) race. */

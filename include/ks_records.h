@@ -15,7 +15,7 @@ extern "C" {
 #endif
 
 /* One close approach found inside a step.
- * Mirrors kessler::Conjunction (src/core/collision.hpp:181-187) and adds the
+ * Mirrors kessler::Conjunction (src/core/collision.hpp:39-45) and adds the
  * step index so that a multi-step run can be returned as one flat list. */
 typedef struct ks_conjunction {
     int32_t i;            /* index into the population, i < j (whole batch for a batched population) */
@@ -30,7 +30,7 @@ typedef struct ks_conjunction {
 
 /* Per-step screening counters.
  * Mirrors the counting fields of kessler::ScreeningStats
- * (src/core/collision.hpp:189-204); timings are reported separately. */
+ * (src/core/collision.hpp:47-62); timings are reported separately. */
 typedef struct ks_step_stats {
     int64_t step;              /* global step index */
     int64_t candidate_pairs;   /* pairs produced by the grid (own cell + 13 forward cells) */

@@ -592,7 +592,12 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
         const bool surv_over = max_refined > static_cast<unsigned long long>(ctx->b.surv_cap);
         const bool items_over = max_items > ctx->b.items_cap;
         if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits");
-        if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+        if (flags & ks::FLAG_TIMEOUT) {
+            // The chunk's results are void: put the simulation back at the
+            // chunk's start, so that the caller may simply run it again.
+            if (ctx->screening) restore_checkpoint(ctx);
+            return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+        }
         if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS | ks::FLAG_PACK_WIDTH)) && !surv_over && !items_over)
             break;
         if (attempt >= kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after replays");
@@ -1253,6 +1258,10 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     } else if (k == "box_min_rows" && value >= 0 && value <= 33) ctx->tune.box_min_rows = static_cast<int>(value);
     else if (k == "prop_block" && value >= 32 && value <= 128 && value % 32 == 0) ctx->tune.prop_block = static_cast<int>(value);
     else if (k == "item_col_blocks" && value >= 1 && value <= 64) ctx->tune.item_col_blocks = static_cast<int>(value);
+    else if (k == "lookback_polls" && value >= 0 && value <= (int64_t(1) << 30)) {
+        ctx->tune.lookback_polls = static_cast<int>(value);
+        drop_graphs(ctx);  // graphs hold the limit in their kernel arguments
+    }
     else if (k == "pack_keys" && (value == 0 || value == 1)) {
         ctx->allow_pack = value != 0;
         if (ctx->has_pop) {

@@ -151,6 +151,7 @@ struct Tuning {
     double cell_scale = 1.0;      // cell edge = reference edge x this (>= 1; changes only candidate counts)
     int prop_block = 128;         // threads per block of the propagation kernels (32..128, multiple of 32)
     int item_col_blocks = 16;     // column blocks of 32 per pair work item (1..64)
+    int lookback_polls = 1 << 22; // polls of a radix-sort look-back before it gives up (FLAG_TIMEOUT)
 };
 
 // Time from a fragmentation event to the end of its step and the lunar stages

@@ -15,6 +15,7 @@
 //               compaction of the pairs sent to refinement
 //   refine      one thread per surviving pair: Hermite + golden-section TCA
 //               (src/core/collision.cpp:77-132)
+#include <atomic>
 #include <cstdio>
 
 #include "kessler_b200.h"
@@ -684,7 +685,7 @@ __global__ void __launch_bounds__(1024) k_scan_small(unsigned int* __restrict__ 
 constexpr unsigned int kStatAgg = 1u << 30;   // tile's own count is published
 constexpr unsigned int kStatInc = 2u << 30;   // count includes all previous tiles
 constexpr unsigned int kStatMask = (1u << 30) - 1;
-constexpr int kLookbackLimit = 1 << 22;       // polls before a wait gives up
+constexpr int kLookbackLimit = 1 << 22;       // polls before a wait gives up (default)
 
 __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int* p) {
     unsigned int v;
@@ -694,6 +695,12 @@ __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int* p) {
 __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+
+// A radix pass whose look-back gave up (FLAG_TIMEOUT) leaves the step's keys
+// unordered and partly stale, and packed keys carry object indices: every
+// kernel of the step that consumes them returns at once, so that no index read
+// from such a key is ever used. The host discards the step.
+__device__ __forceinline__ bool sort_gave_up(const Ctrl* c) { return (c->flags & FLAG_TIMEOUT) != 0; }
 
 // Digit histograms of every pass in one read of the keys.
 // only_if_rebuilt: the propagation already counted the digits; recount only
@@ -735,7 +742,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
                                                           const unsigned int* __restrict__ digit_hist,
                                                           unsigned int* __restrict__ status,
                                                           unsigned int* __restrict__ ticket, int* flags,
-                                                          int packed) {
+                                                          int packed, int poll_limit) {
     __shared__ unsigned int wcnt[kWarps][256];
     __shared__ int gbase[256];
     __shared__ unsigned long long skeys[kSortTile];
@@ -795,7 +802,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
             const unsigned int v = ld_relaxed(status + static_cast<int64_t>(j) * 256 + t);
             const unsigned int flag = v & ~kStatMask;
             if (flag == 0) {
-                if (++polls > kLookbackLimit) {
+                if (++polls > poll_limit) {
                     timed_out = 1;
                     break;
                 }
@@ -851,6 +858,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
 __global__ void __launch_bounds__(kBlock) k_cell_count(const unsigned long long* __restrict__ keys,
                                                        const Ctrl* __restrict__ ctrl, unsigned int* __restrict__ counts,
                                                        int pack_bits) {
+    if (sort_gave_up(ctrl)) return;
     const int m = ctrl->n_alive;
     const int shift = 3 * ctrl->grid.sub + pack_bits;
     const int base = blockIdx.x * kCellTile;
@@ -881,6 +889,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                                                        double* __restrict__ sorted,
                                                        int* __restrict__ sorted_orig, float4* __restrict__ sorted32,
                                                        const float4* __restrict__ rec32, int pack_bits) {
+    if (sort_gave_up(ctrl)) return;
     constexpr int kPer = kCellTile / kBlock;  // consecutive entries per thread
     const int m = ctrl->n_alive;
     if (m == 0) {
@@ -982,6 +991,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
                                                        const unsigned long long* __restrict__ hk,
                                                        const int* __restrict__ hv, unsigned long long hmask,
                                                        int* __restrict__ nbr) {
+    if (sort_gave_up(ctrl)) return;
     const int nc = ctrl->n_cells;
     const GridParams g = ctrl->grid;
     const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
@@ -1038,6 +1048,7 @@ __device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr, int* __restrict__ cell_len,
                                                         unsigned int* __restrict__ part, int per) {
+    if (sort_gave_up(ctrl)) return;
     const int nc = ctrl->n_cells;
     const int chunks = (nc + kBlock - 1) / kBlock;
     unsigned long long cand = 0;
@@ -1089,6 +1100,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
                                                         const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ part,
                                                         int4* __restrict__ items, int64_t items_cap, int per) {
+    if (sort_gave_up(ctrl)) return;
     const int nc = ctrl->n_cells;
     const int chunks = (nc + kBlock - 1) / kBlock;
     const int lane = threadIdx.x & 31;
@@ -1429,6 +1441,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     __shared__ unsigned qmask[kWarps][64];
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
     __shared__ int2 fq[kWarps][64];
+    if (sort_gave_up(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
@@ -1663,6 +1676,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     __shared__ unsigned qmask[kWarps][64];
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
     __shared__ int2 fq[kWarps][64];
+    if (sort_gave_up(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
@@ -1793,6 +1807,7 @@ __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const doubl
                                                          const int2* __restrict__ surv, int64_t surv_cap,
                                                          ks_conjunction* __restrict__ out, int64_t cap,
                                                          ChunkCtrl* chunk) {
+    if (sort_gave_up(a.ctrl)) return;
     const unsigned long long ns = min(a.ctrl->refined, static_cast<unsigned long long>(surv_cap));
     const double t0 = a.sp->t0;
     const double s_hi = xsub(1.0, 1e-9);
@@ -1887,7 +1902,11 @@ __global__ void __launch_bounds__(256) k_fp32_fma(float* out, int iters, float a
     if (s == 1.2345f) out[0] = s;
 }
 
-int g_sm_count = 0;
+// SM count per device index, looked up on first use from each device. The
+// entries are atomics so that threads driving different devices (or the
+// allocation-free entry point from any thread) neither race nor share a count.
+constexpr int kMaxSmDevices = 64;
+std::atomic<int> g_sm_count[kMaxSmDevices];
 
 int grid_for_block(int64_t n, int per_sm_blocks, int block) {
     const int sms = sm_count();
@@ -1906,13 +1925,20 @@ int grid_for(int64_t n, int per_sm_blocks) {
 }  // namespace
 
 int sm_count() {
-    if (g_sm_count == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-        if (g_sm_count <= 0) g_sm_count = 1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+    if (dev >= kMaxSmDevices) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        return sms > 0 ? sms : 1;
     }
-    return g_sm_count;
+    int sms = g_sm_count[dev].load(std::memory_order_relaxed);
+    if (sms == 0) {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+        g_sm_count[dev].store(sms, std::memory_order_relaxed);
+    }
+    return sms;
 }
 
 void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream, bool checkpoint) {
@@ -1980,7 +2006,7 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
             b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, nullptr,
             a.pack_bits + 8 * pass, b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass,
-            b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0);
+            b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0, a.tune.lookback_polls);
     }
 }
 
@@ -2082,7 +2108,7 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
             b.conj_keys[in], nullptr, b.conj_keys[outb], nullptr, cap, &chunk->sort_n, pb + 8 * pass,
             b.conj_hist + 256 * pass, b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass,
-            &chunk->flags, 1);
+            &chunk->flags, 1, kLookbackLimit);
     }
     k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_keys[kPasses & 1], (1ull << pb) - 1, chunk,
                                                          b.conj_sorted);

@@ -30,6 +30,7 @@ constexpr int64_t kNoAllocItems = 4 * kNoAllocMaxObjects;
 constexpr int64_t kNoAllocConj = 1 << 15;
 constexpr int64_t kNoAllocHash = 2 * kNoAllocMaxObjects;  // power of two >= 2 x objects
 constexpr int kMaxDevices = 64;
+constexpr int kMaxAttempts = 3;  // first run + replays with more radix passes
 
 constexpr int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
 
@@ -131,7 +132,10 @@ ks::DeviceBuffers carve(unsigned char* base) {
 }
 
 // Device address of the scratch array on the current device, resolved once
-// per device (the first call on each device does this set-up).
+// per device (the first call on each device does this set-up). The cached
+// address belongs to the device's primary context: a cudaDeviceReset between
+// calls would leave it stale, so the library does not support resetting a
+// device it has screened on.
 int scratch_for_current_device(unsigned char** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -172,6 +176,7 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
     if (n < 0 || !count || cap < 0 || (n > 0 && (!before || !after || !alive_after || !size_m)) || !(dt > 0.0) ||
         threshold_km < 0.0 || radius_scale < 0.0 || min_encounter_speed_km_s < 0.0)
         return fail(KS_ERR_ARG, "ks_screen_noalloc: bad arguments");
+    *count = 0;
     if (n > kNoAllocMaxObjects)
         return fail(KS_ERR_RANGE, "ks_screen_noalloc: " + std::to_string(n) + " objects, at most " +
                                       std::to_string(kNoAllocMaxObjects) + " per call");
@@ -242,7 +247,7 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
         }
         a.sort_passes = std::max(1, (bits + 3 * a.tune.subcell_bits + 1 + 7) / 8);
     }
-    for (int attempt = 0;; ++attempt) {
+    for (int attempt = 0; attempt < kMaxAttempts; ++attempt) {
         if (attempt > 0) {
             ks::launch_chunk_init(b, 1, s);
             ks::launch_seed_ctrl(b, a.n, 0, a.ctrl, 0, s);
@@ -260,7 +265,9 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
         const int flags = c.flags | ch.flags;
         if (flags & ks::FLAG_KEY_RANGE) return fail(KS_ERR_RANGE, "ks_screen_noalloc: cell key outside its grid");
         if (flags & ks::FLAG_TIMEOUT) return fail(KS_ERR_TIMEOUT, "ks_screen_noalloc: radix sort wait gave up");
-        if ((flags & ks::FLAG_SORT_BITS) && attempt == 0) {
+        if (flags & ks::FLAG_SORT_BITS) {
+            // The keys needed more radix passes than launched: replay with
+            // enough of them. Records of such a run are never returned.
             a.sort_passes = std::max(a.sort_passes, (c.grid.bits + 1 + 7) / 8);
             continue;
         }
@@ -269,9 +276,11 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
                                              " pairs to refine, fixed capacity " + std::to_string(kNoAllocSurvivors));
         if (ks::items_total(c) > kNoAllocItems)
             return fail(KS_ERR_OVERFLOW, "ks_screen_noalloc: pair work list beyond its fixed capacity");
-        if ((flags & ks::FLAG_CONJ_OVERFLOW) || ch.conj_count > static_cast<unsigned long long>(kNoAllocConj))
+        if ((flags & ks::FLAG_CONJ_OVERFLOW) || ch.conj_count > static_cast<unsigned long long>(kNoAllocConj)) {
+            *count = static_cast<int64_t>(ch.conj_count);
             return fail(KS_ERR_OVERFLOW, "ks_screen_noalloc: more conjunctions than the fixed capacity " +
                                              std::to_string(kNoAllocConj));
+        }
         const int64_t nc = static_cast<int64_t>(ch.conj_count);
         *count = nc;
         if (stats) {
@@ -294,6 +303,8 @@ int screen_noalloc(int64_t n, const double* before, const double* after, const u
         }
         return KS_OK;
     }
+    return fail(KS_ERR_RANGE, "ks_screen_noalloc: cell keys still wider than the radix passes after " +
+                                  std::to_string(kMaxAttempts) + " attempts");
 }
 
 }  // namespace

@@ -38,7 +38,7 @@ inline void check(ks_ctx* ctx, int rc, const char* where) {
     if (rc != KS_OK) throw Error(rc, std::string(where) + ": " + ks_last_error(ctx));
 }
 
-// ScreeningConfig (src/core/collision.hpp:168-179).
+// ScreeningConfig (src/core/collision.hpp:26-37).
 struct ScreeningConfig {
     double threshold_km = 5.0;
     double radius_scale = 1.0;
@@ -90,7 +90,7 @@ ConjT to_conjunction(const ks_conjunction& c) {
 
 }  // namespace detail
 
-// Screener (src/core/collision.hpp:217-262): one-shot screening of a step
+// Screener (src/core/collision.hpp:75-120): one-shot screening of a step
 // from host states, on the GPU. No CPU fallback: set_gpu(true) fails when no
 // device is usable, and screen() throws.
 class Screener {

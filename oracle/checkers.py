@@ -17,7 +17,15 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libks_oracle.so")
+WORKLOAD_SO = os.path.join(HERE, "libks_workload.so")
 REF_SO = os.path.join(HERE, "_ref", "libksref.so")
+# Source tree of the reference, read only to build oracle/_ref and the golden
+# fixtures. One environment variable names it everywhere.
+REFERENCE_TREE = os.environ.get("KESSLER_REFERENCE", "/root/reference")
+
+
+def reference_tree_present():
+    return os.path.isdir(os.path.join(REFERENCE_TREE, "src"))
 
 CONJ_DTYPE = np.dtype(
     [("i", "<i4"), ("j", "<i4"), ("step", "<i8"), ("t", "<f8"), ("miss_km", "<f8"),
@@ -45,9 +53,30 @@ def _p(a):
 def build(ref=True):
     """Builds the checkers (ref=True also builds the reference when its tree exists)."""
     targets = ["oracle"]
-    if ref and os.path.isdir("/root/reference/src"):
+    if ref and reference_tree_present():
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "REF=" + REFERENCE_TREE] + targets, check=True)
+
+
+def generate_population(seed, n_base, n_total=None, n_parents=200, frag_age_max_s=0.0):
+    """The seeded synthetic population, from oracle/libks_workload.so: the
+    engine's own generator source built as a separate library, so that the
+    CPU-baseline harness builds its inputs without loading the engine. Same
+    arrays as the engine's ks_generate_population, bit for bit."""
+    if not os.path.exists(WORKLOAD_SO):
+        build(ref=False)
+    lib = C.CDLL(WORKLOAD_SO)
+    f = lib.ks_generate_population
+    f.restype = C.c_int
+    n_total = n_base if n_total is None else n_total
+    st = np.zeros((n_total, 6))
+    sz = np.zeros(n_total)
+    al = np.zeros(n_total, dtype=np.uint8)
+    rc = f(C.c_uint64(seed), C.c_int64(n_base), C.c_int64(n_total), C.c_int(int(n_parents)),
+           _D(float(frag_age_max_s)), _p(st), _p(sz), _p(al))
+    if rc != 0:
+        raise ValueError("ks_generate_population: bad arguments")
+    return st, sz, al
 
 
 class _Checker:

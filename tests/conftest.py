@@ -8,7 +8,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-REFERENCE_TREE = "/root/reference"
+from checkers import REFERENCE_TREE  # noqa: E402  (KESSLER_REFERENCE, else the default tree)
 
 
 def pytest_configure(config):

@@ -49,7 +49,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import checkers  # noqa: E402
 
 EPOCH = 2461253.916666667
-CATALOG = "/root/reference/data/satellites_20260801_1000Z.txt"
+CATALOG = os.path.join(checkers.REFERENCE_TREE, "data", "satellites_20260801_1000Z.txt")
 
 
 def population(seed, n_base, n_total, n_parents, age):
@@ -220,6 +220,59 @@ def catalogue_kat():
     print("catalogue 1h", out["conjunctions"], out["closest"])
 
 
+CONJ_FIELDS = ("i", "j", "step", "t", "miss_km", "v_rel_km_s", "collision")
+STAT_FIELDS = ("candidate_pairs", "refined_pairs", "co_orbiting", "conjunctions", "cell_km", "max_cell_objects",
+               "alive")
+
+
+def digest(arrays):
+    """SHA-256 over the raw bytes of each array in turn (C order)."""
+    import hashlib
+    h = hashlib.sha256()
+    for x in arrays:
+        h.update(np.ascontiguousarray(x).tobytes())
+    return h.hexdigest()
+
+
+def catalogue_24h_kat():
+    """24 h of the shipped catalogue (8 640 steps of 10 s, --conj-km 5): the
+    README's own run. The reference's inputs (states, sizes and NORAD ids as
+    its loader reads them) are kept as catalog_28340.npz so the check runs
+    without the reference tree; its outputs are kept as SHA-256 digests of the
+    final states, of every conjunction record field and of every per-step
+    counter, plus the summary the README quotes."""
+    ref = checkers.Reference()
+    st, sz, ids, epoch = ref.load_catalog(CATALOG)
+    np.savez_compressed(os.path.join(HERE, "catalog_28340.npz"), states=st, size_m=sz, ids=ids.astype(np.int32),
+                        epoch_jd=epoch)
+    steps = 8640
+    fs, fa, conj, stats = ref.run(st, sz, None, epoch_jd=epoch, t_start=0.0, dt=10.0, steps=steps, screen=True,
+                                  threshold_km=5.0, radius_scale=1.0, min_vrel_km_s=0.01, threads=os.cpu_count())
+    ps, pa, _, _ = ref.run(st, sz, None, epoch_jd=epoch, t_start=0.0, dt=10.0, steps=steps, screen=False,
+                           threads=os.cpu_count())
+    assert np.array_equal(ps, fs) and np.array_equal(pa, fa), "screening changed the states"
+    k = int(np.argmin(conj["miss_km"]))
+    out = {
+        "source": "reference CLI step loop (oracle/_ref) on data/satellites_20260801_1000Z.txt, 24 h",
+        "objects": int(len(st)), "epoch_jd": epoch, "dt": 10.0, "steps": steps, "threshold_km": 5.0,
+        "radius_scale": 1.0, "min_vrel_km_s": 0.01,
+        "conjunctions": int(len(conj)),
+        "below_km": {str(b): int((conj["miss_km"] < b).sum()) for b in (0.1, 1.0, 5.0)},
+        "collisions": int(conj["collision"].sum()),
+        "closest": {"miss_m": float(conj["miss_km"][k] * 1000.0), "t_h": float(conj["t"][k] / 3600.0),
+                    "id1": int(ids[conj["i"][k]]), "id2": int(ids[conj["j"][k]])},
+        "alive_end": int(fa.sum()),
+        "sha256_final_states": digest([fs, fa]),
+        "sha256_conjunctions": digest([conj[f] for f in CONJ_FIELDS]),
+        "sha256_step_counters": digest([stats[f] for f in STAT_FIELDS]),
+        "readme": {"conjunctions": 38367, "below_1km": 1493, "below_100m": 14, "collisions": 0,
+                   "closest_m": 7.2, "where": "README.md:179-186"},
+    }
+    with open(os.path.join(HERE, "ref_catalog_24h.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("catalogue 24h", out["conjunctions"], out["below_km"], out["closest"])
+
+
 CLI_ARGS = ["0.25", "10", "--conj-km", "5"]
 
 
@@ -300,6 +353,10 @@ def cli_snapshot_golden():
 
 def main():
     checkers.build(ref=True)
+    if len(sys.argv) > 1:  # regenerate only the named fixtures, e.g. catalogue_24h_kat
+        for name in sys.argv[1:]:
+            globals()[name]()
+        return
     st, sz, al = population(20260801, 1500, 3000, 3, 7200.0)
     plant_reentries(st, al)
     plant_encounters(st, 2, 12, 40, 10.0, 11)
@@ -314,6 +371,7 @@ def main():
     breakup_run()
     if os.path.exists(CATALOG):
         catalogue_kat()
+        catalogue_24h_kat()
 
 
 if __name__ == "__main__":

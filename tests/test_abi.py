@@ -124,3 +124,15 @@ def test_generator_fragment_clouds(ks):
     assert abs(np.median(r) - med) < 0.003
     aged = ks.generate_population(5, 2000, 12000, 10, 86400.0)[0][2000:]
     assert len({tuple(np.round(x[:3], 6)) for x in aged}) > 9000
+
+
+def test_checker_generator_equals_engine_generator(ks):
+    """The CPU-baseline harness's copy of the generator (oracle/libks_workload.so)
+    gives the engine's populations bit for bit."""
+    import checkers
+
+    for args in ((7, 500, 500, 1, 0.0), (20260801, 2000, 9000, 12, 86400.0), (3, 300, 4000, 3, 0.0)):
+        got = checkers.generate_population(*args)
+        want = ks.generate_population(*args)
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w)
