@@ -73,7 +73,9 @@ def parse():
     ap.add_argument("--ens-lc", type=float, default=0.05)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--cascade-realisations", type=int, default=16)
-    ap.add_argument("--cascade-steps", type=int, default=60)
+    ap.add_argument("--cascade-steps", type=int, default=360)
+    ap.add_argument("--cascade-budget", type=float, default=1.25,
+                    help="population budget of the cascade, as a multiple of its starting size")
     ap.add_argument("--no-cascade", action="store_true")
     return ap.parse_args()
 
@@ -602,14 +604,16 @@ def ensemble_run(ks, a, device, barrier, pg, rank):
 
 def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     """Batched cascade: R realisations of the 1M-object population with collision
-    radii x50, fragmentation (NASA SBM, L_c 10 cm, the reference's draws, one
-    stream per realisation) in the loop, split precision, 5 km, 10 m/s. The
-    population grows as collisions fragment objects; chunks end at collision
-    steps. Timed on the device (CUDA events) with the fragmentation host work in
-    the wall time beside it."""
+    radii x50 and fragmentation in the loop on the device (NASA SBM, L_c 10 cm,
+    counter-based draws, one stream per realisation), split precision, 5 km,
+    10 m/s, within a fixed population budget. Every collision fragments inside
+    the step that found it, so chunks of steps run through collisions. Timed on
+    the device (CUDA events) with the wall time beside it."""
     R = a.cascade_realisations
     n0 = len(sz)
+    budget = int(R * n0 * a.cascade_budget)
     eng = ks.Engine(device)
+    eng.set_breakup_mode(ks.BREAKUP_DEVICE, budget)
     eng.set_precision(ks.PRECISION_SPLIT)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
     eng.set_screening(True, a.conj_km, 50.0, 0.01)
@@ -640,12 +644,15 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     obj = sum_over_ranks(pg, float(tm["object_steps"]))
     per_real = np.bincount(ev["realisation"], minlength=R) if len(ev) else np.zeros(R, int)
     return {"workload": f"{R} realisations x the {n0}-object population, collision radii x50, fragmentation "
-                        f"in the loop (SBM, L_c 0.1 m), split precision, dt {a.dt} s, {a.conj_km} km",
+                        f"in the loop on the device (SBM, L_c 0.1 m, counter-based draws), split precision, "
+                        f"dt {a.dt} s, {a.conj_km} km, population budget {budget} objects",
             "value": obj / (dev_ms * 1e-3), "unit": "object-steps/s", "ms_per_step": dev_ms / max(1, tm["steps"]),
             "wall_s": wall, "wall_object_steps_per_s": obj / wall, "steps": a.cascade_steps,
+            "simulated_hours": a.cascade_steps * a.dt / 3600.0,
             "objects_start": int(n_start), "objects_end": int(n_end), "events": int(len(ev)),
             "events_in_warmup": int(len(warm_events)), "catastrophic": int(ev["catastrophic"].sum()) if len(ev) else 0,
             "fragments_created": int(ev["fragments"].sum()) if len(ev) else 0,
+            "escaped": int(ev["escaped"].sum()) if len(ev) else 0,
             "events_per_realisation": {"min": int(per_real.min()), "max": int(per_real.max())},
             "collisions": int(conj["collision"].sum()), "conjunctions": int(len(conj)),
             "fragment_sizes_m": {"n_gt_lc": int((size > 0.1).sum()), "ratio_n_gt_2lc": float((size > 0.2).sum() /
@@ -661,12 +668,16 @@ def measure_fp32(eng):
 
 
 def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
-    """Through the C ABI with host buffers: upload the population from pinned
-    memory, then per step upload that step's lunar rows, run the step and read
-    its conjunction records and counters back (one chunk per step), finally
-    read the population back. Timed end to end on the host, max over ranks."""
+    """Through the C ABI with host buffers, the way a caller drives a run:
+    upload the population from pinned host memory, then ks_run over chunks of
+    steps (each chunk one graph launch that uploads every step's lunar rows
+    and brings back every step's ordered conjunction records and counters),
+    taking each chunk's records and counters as it ends, and finally read the
+    population back into pinned host memory. Timed end to end on the host,
+    max over ranks."""
     import torch
     steps = a.e2e_steps or a.steps
+    chunk = max(1, a.steps_per_graph)
     pin_st = torch.from_numpy(st).pin_memory().numpy()
     pin_sz = torch.from_numpy(sz).pin_memory().numpy()
     pin_al = torch.from_numpy(al).pin_memory().numpy()
@@ -676,21 +687,22 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     eng.set_precision(precision)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
     eng.set_screening(True, a.conj_km, 1.0, 0.01)
-    eng.set_steps_per_graph(1)
+    eng.set_steps_per_graph(chunk)
     # Untimed warm-up on the same population: device buffers reach their
-    # working sizes here, as they would after the first steps of a run.
+    # working sizes and the chunk graphs are built, as after a run's first chunk.
     eng.set_population(pin_st, pin_sz, pin_al)
-    eng.run(max(3, a.warmup))
+    eng.run(min(steps, chunk))
     eng.take_conjunctions()
     eng.take_step_stats()
+    eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
     barrier()
     t0 = time.perf_counter()
     eng.set_population(pin_st, pin_sz, pin_al)
-    nconj = 0
-    for _ in range(steps):
-        eng.run(1)
+    nconj = nstats = 0
+    for done in range(0, steps, chunk):
+        eng.run(min(chunk, steps - done))
         nconj += len(eng.take_conjunctions())
-        eng.take_step_stats()
+        nstats += len(eng.take_step_stats())
     fs, fa = eng.get_population(out_st, out_al)
     barrier()
     wall = time.perf_counter() - t0
@@ -698,13 +710,18 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     world = pg.get_world_size() if pg else 1
     obj = float(al.sum()) * steps * world
     eng.close()
-    h2d = (st.nbytes + sz.nbytes + al.nbytes) / steps + 3 * 56 + 16
-    d2h = (fs.nbytes + fa.nbytes) / steps + nconj * 48 / steps + 200
+    assert nstats == steps
+    # Per step up: the step's start time, index and 3 lunar stages (position and
+    # indirect term), 160 B; down: its 48 B conjunction records and its 216 B
+    # control block (the counters).
+    h2d = (st.nbytes + sz.nbytes + al.nbytes) / steps + 160
+    d2h = (fs.nbytes + fa.nbytes) / steps + nconj * 48 / steps + 216
     return {"value": obj / wall, "unit": "object-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "steps": steps,
-            "what": "ks_set_population from pinned host memory, then per step ks_run(1) (host->device lunar "
-                    "rows, device->host conjunctions in (t, i, j) order and counters, host sync), then "
-                    "ks_get_population into pinned host memory; wall clock, max over ranks"}
+            "steps": steps, "steps_per_call": chunk,
+            "what": f"ks_set_population from pinned host memory, then ks_run of {chunk}-step chunks (per step: "
+                    "host->device lunar rows, device->host conjunction records in (t, i, j) order and counters, "
+                    "taken after each call), then ks_get_population into pinned host memory; wall clock, max over "
+                    "ranks"}
 
 
 if __name__ == "__main__":

@@ -166,6 +166,22 @@ int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* co
  * catastrophic_j_per_g: specific-energy threshold; realisation r of a batch
  * draws from its own stream seeded seed + r. BreakupConfig (breakup.hpp:75-79). */
 int ks_set_breakup(ks_ctx* ctx, int on, double lc_m, double catastrophic_j_per_g, uint64_t seed);
+/* Where fragmentation runs when ks_set_breakup is on (no counterpart in the
+ * reference, which fragments on the host after each step, src/main.cpp:401-407).
+ * KS_BREAKUP_HOST (the default): the reference's own draws on the host,
+ * fragments identical to the reference's; a chunk of steps ends at each step
+ * that holds a collision. KS_BREAKUP_DEVICE: the NASA SBM on the device inside
+ * every step, its random numbers drawn from Philox counters named by (seed +
+ * realisation, event, fragment, draw); the laws are the reference's, the draws
+ * are not, so fragments agree with the reference's in distribution, not one by
+ * one. Chunks then run through collisions. The population may grow to
+ * max_objects objects, the memory budget allocated when the population is
+ * set; fragments that would pass it fail the run with KS_ERR_OVERFLOW, as does
+ * a step with more than 1024 collisions. Call before ks_set_population(_batch).
+ * ks_autotune, ks_save/load_population, ks_screen and ks_propagate are not
+ * available in this mode (KS_ERR_STATE). */
+enum { KS_BREAKUP_HOST = 0, KS_BREAKUP_DEVICE = 1 };
+int ks_set_breakup_mode(ks_ctx* ctx, int mode, int64_t max_objects);
 /* Masses (kg) of the population's objects, 0 = unknown (fragmentation then
  * uses 100 kg): the output of assign_masses (src/core/breakup.cpp:104-111). */
 int ks_set_masses(ks_ctx* ctx, int64_t n, const double* mass_kg);

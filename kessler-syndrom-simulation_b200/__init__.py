@@ -23,6 +23,7 @@ __all__ = ["Engine", "KsError", "BREAKUP_DTYPE", "CONJ_DTYPE", "STATS_DTYPE", "P
 
 # src/core/orbital.hpp:30
 DEFAULT_EPOCH_JD = 2461253.916666667
+BREAKUP_HOST, BREAKUP_DEVICE = 0, 1
 
 
 class KsError(RuntimeError):
@@ -179,6 +180,12 @@ class Engine:
     def set_breakup(self, on=True, lc_m=0.10, catastrophic_j_per_g=40.0, seed=1):
         self._check(self._lib.ks_set_breakup(self._h, 1 if on else 0, float(lc_m), float(catastrophic_j_per_g),
                                              int(seed)))
+
+    def set_breakup_mode(self, mode, max_objects=0):
+        """BREAKUP_HOST (the reference's draws, on the host) or BREAKUP_DEVICE
+        (the SBM inside every step on the device, population budget max_objects).
+        Call before set_population / set_population_batch."""
+        self._check(self._lib.ks_set_breakup_mode(self._h, int(mode), int(max_objects)))
 
     def set_masses(self, mass_kg):
         m = np.ascontiguousarray(mass_kg, dtype=np.float64)

@@ -79,6 +79,7 @@ SIGNATURES = {
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_set_breakup": (C.c_int, [_P, C.c_int, _D, _D, C.c_uint64]),
     "ks_set_masses": (C.c_int, [_P, _I64, _P]),
+    "ks_set_breakup_mode": (C.c_int, [_P, C.c_int, _I64]),
     "ks_impact": (C.c_int, [_P, _I64, _D, _D]),
     "ks_take_breakups": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_save_population": (C.c_int, [_P, C.c_char_p]),

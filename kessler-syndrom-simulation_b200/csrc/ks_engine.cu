@@ -35,6 +35,7 @@ namespace {
 
 constexpr int kPhases = 7;  // event slots per step: 0..5 the phases, 6 before the step's L2 flush
 constexpr int kMaxReplays = 6;
+constexpr int64_t kSbmChunkEvents = 65536;  // breakup records one chunk holds (device fragmentation)
 
 }  // namespace
 
@@ -88,6 +89,14 @@ struct ks_ctx {
     void* l2_flush = nullptr;
     int64_t l2_flush_bytes = 0;
 
+    // Fragmentation on the device (ks_set_breakup_mode KS_BREAKUP_DEVICE):
+    // the population grows inside chunks up to dev_cap objects; no replays,
+    // a chunk whose step was left void restarts at that step.
+    bool dev_sbm = false;
+    int64_t dev_cap = 0;
+    ks_breakup_event* h_sbm_events = nullptr;  // pinned copy of a chunk's breakup records
+    int dev_stalls = 0;                        // chunks in a row that ended void at their first step
+
     // Fragmentation (NASA SBM) on the host, between steps. Per-object
     // properties the device does not need are mirrored here, built on first
     // use; one random stream and event counter per realisation.
@@ -138,18 +147,27 @@ void free_objects(ks_ctx* ctx) {
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr);
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted32); dfree(b.rec32); dfree(b.sorted_orig);
+    dfree(b.n_live); dfree(b.mass_kg); dfree(b.a2m); dfree(b.event_of); dfree(b.coll); dfree(b.sbm_work);
+    dfree(b.sbm_events); dfree(b.sbm_next_event);
+    if (ctx->h_sbm_events) cudaFreeHost(ctx->h_sbm_events);
+    ctx->h_sbm_events = nullptr;
+    b.coll_cap = 0;
+    b.sbm_events_cap = 0;
     b.cap = 0;
     b.hash_cap = 0;
     b.sort_status_len = 0;
 }
 
 int ensure_objects(ks_ctx* ctx, int64_t n) {
-    if (n <= ctx->b.cap) return KS_OK;
-    if (n > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "population larger than 2^30 objects");
+    // With fragmentation on the device the arrays are sized once for the
+    // population's budget: fragments are appended inside the chunks' graphs.
+    const int64_t want = ctx->dev_sbm ? std::max(n, ctx->dev_cap) : n;
+    if (want <= ctx->b.cap && (!ctx->dev_sbm || ctx->b.n_live)) return KS_OK;
+    if (want > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "population larger than 2^30 objects");
     drop_graphs(ctx);
     free_objects(ctx);
     ks::DeviceBuffers& b = ctx->b;
-    const int64_t cap = std::max<int64_t>(n, 1024);
+    const int64_t cap = std::max<int64_t>(want, 1024);
     for (int k = 0; k < 2; ++k) {
         KS_CUDA(cudaMalloc(&b.state[k], sizeof(double) * 6 * cap));
         KS_CUDA(cudaMalloc(&b.alive[k], cap));
@@ -179,6 +197,19 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.sorted32, sizeof(float4) * 2 * cap));
     KS_CUDA(cudaMalloc(&b.rec32, sizeof(float4) * 2 * cap));
     KS_CUDA(cudaMalloc(&b.sorted_orig, sizeof(int) * cap));
+    if (ctx->dev_sbm) {
+        KS_CUDA(cudaMalloc(&b.n_live, sizeof(int)));
+        KS_CUDA(cudaMalloc(&b.mass_kg, sizeof(double) * cap));
+        KS_CUDA(cudaMalloc(&b.a2m, sizeof(double) * cap));
+        KS_CUDA(cudaMalloc(&b.event_of, sizeof(int32_t) * cap));
+        b.coll_cap = ks::kSbmStepEvents;
+        KS_CUDA(cudaMalloc(&b.coll, sizeof(ks::CollisionRec) * b.coll_cap));
+        KS_CUDA(cudaMalloc(&b.sbm_work, sizeof(ks::SbmEventWork) * b.coll_cap));
+        b.sbm_events_cap = kSbmChunkEvents;
+        KS_CUDA(cudaMalloc(&b.sbm_events, sizeof(ks_breakup_event) * b.sbm_events_cap));
+        KS_CUDA(cudaHostAlloc(&ctx->h_sbm_events, sizeof(ks_breakup_event) * b.sbm_events_cap, cudaHostAllocDefault));
+        KS_CUDA(cudaMalloc(&b.sbm_next_event, sizeof(int) * 65536));
+    }
     b.cap = cap;
     return KS_OK;
 }
@@ -363,7 +394,28 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     a.hist = ctx->screening ? ctx->b.sort_hist : nullptr;  // the propagation counts the sort's digits
     a.rec32 = ctx->b.rec32;
     a.pack_bits = ctx->pack_keys ? index_bits(ctx->n) : 0;
+    if (ctx->dev_sbm) {
+        // Grids sized for the capacity, loops bounded by the live count; the
+        // packed object index must hold every index the population can reach.
+        a.n = static_cast<int>(ctx->b.cap);
+        a.n_live = ctx->b.n_live;
+        a.chunk = ctx->b.chunk;
+        a.step_in_chunk = k;
+        a.steps_in_chunk = k_steps;
+        a.coll = ctx->bk.on ? ctx->b.coll : nullptr;
+        a.coll_cap = ctx->b.coll_cap;
+        a.pack_bits = ctx->pack_keys ? index_bits(ctx->b.cap) : 0;
+    }
     return a;
+}
+
+ks::SbmArgs sbm_args(const ks_ctx* ctx) {
+    ks::SbmArgs s{};
+    s.lc_m = ctx->bk.params.lc_m;
+    s.catastrophic_j_per_g = ctx->bk.params.catastrophic_j_per_g;
+    s.seed = ctx->bk.seed;
+    s.cap = static_cast<int>(ctx->b.cap);
+    return s;
 }
 
 void record(ks_ctx* ctx, int k, int phase, bool capturing) {
@@ -406,10 +458,16 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
             ks::launch_pairs(ctx->b, a, s);
             record(ctx, k, 4, capturing);
             ks::launch_refine(ctx->b, a, ctx->b.conj, ctx->b.conj_cap, ctx->b.chunk, s);
+            if (ctx->dev_sbm) {
+                ks::launch_step_gate(ctx->b, a, s);
+                if (ctx->bk.on) ks::launch_sbm_step(ctx->b, a, sbm_args(ctx), s);
+            }
             record(ctx, k, 5, capturing);
         }
         src ^= 1;
     }
+    if (ctx->dev_sbm)
+        cudaMemcpyAsync(&ctx->b.chunk->n_live, ctx->b.n_live, sizeof(int), cudaMemcpyDeviceToDevice, s);
     if (ctx->screening)
         ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, ctx->conj_small, s);
     record_chunk_end(ctx, capturing);
@@ -540,7 +598,150 @@ int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_
 // collision (the chunk is replayed up to that step), and the collisions are
 // fragmented before the next step, as the reference's loop does after each
 // step (src/main.cpp:401-407).
+// Sizes the chunk's record buffer and its ordering, and which records come
+// back with the control blocks (shared by both chunk loops).
+int plan_records(ks_ctx* ctx, int k_steps) {
+    int rc = KS_OK;
+    // Room for the chunk's records at the largest per-step count seen so far,
+    // so that a longer chunk does not overflow and replay.
+    if (ctx->screening && ctx->max_step_conj > 0) {
+        const int64_t want = std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, int64_t(1) << 30);
+        if (want > ctx->b.conj_cap && (rc = ensure_conj(ctx, want))) return rc;
+    }
+    // One-block ordering of the records where the chunk should hold few.
+    const bool small = ctx->screening && ctx->max_step_conj > 0 &&
+                       ctx->max_step_conj * k_steps * 5 / 4 + 256 <= ks::kConjSmall;
+    if (small != ctx->conj_small) {
+        ctx->conj_small = small;
+        drop_graphs(ctx);
+    }
+    // Records copied back with the control blocks, up to the expected count,
+    // so that a chunk with no more than that needs one host round trip.
+    const int64_t spec = ctx->screening ? std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, ctx->b.conj_cap) : 0;
+    ctx->chunk_spec = ctx->max_step_conj > 0 && spec <= (int64_t(1) << 16) ? spec : 0;
+    const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
+    if (use_graph && ctx->graph_exec[ctx->cur] && ctx->graph_spec[ctx->cur] < ctx->chunk_spec) drop_graphs(ctx);
+    return KS_OK;
+}
+
+// One chunk with fragmentation on the device. The population grows inside the
+// chunk's graph; nothing is replayed: a step whose buffers overflowed (or whose
+// sort gave up) is left void together with the rest of the chunk, its
+// predecessors' results are kept, the buffers grow, and the next chunk starts
+// at the void step from the states the chunk left (a void step never writes
+// its start-of-step buffer).
+int run_chunk_dev(ks_ctx* ctx, int k_steps) {
+    stash_pending(ctx);
+    int rc = ensure_chunk(ctx, k_steps);
+    if (rc) return rc;
+    double t_end = 0.0;
+    fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);
+    if ((rc = plan_records(ctx, k_steps))) return rc;
+    if ((rc = ensure_graph(ctx, k_steps))) return rc;
+    if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[0], ctx->stream));
+    rc = launch_chunk(ctx, k_steps);
+    if (rc) return rc;
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    const ks::ChunkCtrl ch = *ctx->h_chunk;
+    if (ch.flags & ks::FLAG_POP_BUDGET)
+        return fail(ctx, KS_ERR_OVERFLOW, "fragments would pass the population budget of " +
+                                              std::to_string(ctx->b.cap) + " objects (ks_set_breakup_mode)");
+    const int h = ch.halt_step;
+    const int done = h < 0 ? k_steps : h;
+    const int64_t last_step = ctx->steps_done + done;  // records of steps before this one are complete
+    // Conjunction records, ordered on the device; those of the void step are dropped.
+    int64_t have = (ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph) ? ctx->graph_spec[ctx->cur]
+                                                                                : ctx->chunk_spec;
+    int64_t nc = std::min<int64_t>(static_cast<int64_t>(ch.conj_count), ctx->b.conj_cap);
+    if (ch.flags & ks::FLAG_CONJ_LARGE) {
+        ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, false, ctx->stream);
+        KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_chunk->flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+        have = 0;
+    }
+    if (nc > have) {
+        KS_CUDA(cudaMemcpyAsync(ctx->h_conj + have, ctx->b.conj_sorted + have, sizeof(ks_conjunction) * (nc - have),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    int64_t kept = 0;
+    for (int64_t q = 0; q < nc; ++q)
+        if (ctx->h_conj[q].step < last_step) ctx->h_conj[kept++] = ctx->h_conj[q];
+    if (kept > 0) {
+        finish_order(ctx->h_conj, ctx->h_conj + kept);
+        ctx->pend_begin = 0;
+        ctx->pend_end = kept;
+    }
+    // Breakup records of the kept steps (the void step fragmented nothing).
+    if (ch.events > 0) {
+        const int64_t ne = std::min<int64_t>(ch.events, ctx->b.sbm_events_cap);
+        KS_CUDA(cudaMemcpyAsync(ctx->h_sbm_events, ctx->b.sbm_events, sizeof(ks_breakup_event) * ne,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->bk.out.insert(ctx->bk.out.end(), ctx->h_sbm_events, ctx->h_sbm_events + ne);
+    }
+    for (int k = 0; k < done; ++k) {
+        const Ctrl& c = ctx->h_ctrl[k];
+        ks_step_stats st{};
+        st.step = ctx->steps_done + k;
+        st.candidate_pairs = static_cast<int64_t>(c.candidates);
+        st.refined_pairs = static_cast<int64_t>(c.refined);
+        st.co_orbiting = static_cast<int64_t>(c.co_orbiting);
+        st.conjunctions = static_cast<int64_t>(c.conj);
+        st.cell_km = ctx->screening ? c.grid.cell : 0.0;
+        st.max_cell_objects = c.max_cell;
+        st.alive = c.n_alive;
+        ctx->stats_out.push_back(st);
+        ctx->max_step_conj = std::max(ctx->max_step_conj, static_cast<int64_t>(c.conj));
+        ctx->timing.object_steps += static_cast<int64_t>(c.object_steps);
+        ctx->timing.candidate_pairs += static_cast<int64_t>(c.candidates);
+        ctx->timing.exact_filter_pairs += static_cast<int64_t>(c.exact_evals);
+        ctx->timing.refined_pairs += static_cast<int64_t>(c.refined);
+    }
+    accumulate_timing(ctx, done);
+    ctx->timing.steps += done;
+    ctx->timing.sort_passes = ctx->sort_passes;
+    ctx->steps_done += done;
+    ctx->t = done == k_steps ? t_end : ctx->h_params[done].t0;
+    if (done & 1) ctx->cur ^= 1;
+    ctx->n = ch.n_live;
+    if (h < 0) {
+        ctx->dev_stalls = 0;
+        return KS_OK;
+    }
+    // The void step restarts the next chunk: its speculation becomes the carry.
+    KS_CUDA(cudaMemcpyAsync(carry_slot(ctx), ctx->b.ctrl + h, sizeof(Ctrl), cudaMemcpyDeviceToDevice, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->dev_stalls = done == 0 ? ctx->dev_stalls + 1 : 0;
+    if (ctx->dev_stalls > kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after regrowth");
+    const Ctrl& c = ctx->h_ctrl[h];
+    const int flags = c.flags | (ch.flags & ks::FLAG_CONJ_OVERFLOW);
+    if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+    if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits");
+    if (flags & ks::FLAG_COLL_OVERFLOW)
+        return fail(ctx, KS_ERR_OVERFLOW, "more than " + std::to_string(ks::kSbmStepEvents) +
+                                              " collisions in one step, or more breakup records in one chunk than " +
+                                              std::to_string(ctx->b.sbm_events_cap));
+    if (flags & ks::FLAG_PACK_WIDTH) {
+        ctx->pack_keys = false;
+        drop_graphs(ctx);
+    }
+    if (flags & ks::FLAG_SORT_BITS) {
+        ctx->sort_passes = std::max(ctx->sort_passes, passes_for_bits(c.grid.bits));
+        drop_graphs(ctx);
+    }
+    if (c.refined > static_cast<unsigned long long>(ctx->b.surv_cap) &&
+        (rc = ensure_survivors(ctx, static_cast<int64_t>(c.refined) * 2)))
+        return rc;
+    if (ks::items_total(c) > ctx->b.items_cap && (rc = ensure_items(ctx, ks::items_total(c) * 3 / 2 + 1024))) return rc;
+    if ((ch.flags & ks::FLAG_CONJ_OVERFLOW) && (rc = ensure_conj(ctx, static_cast<int64_t>(ch.conj_count) * 2 + 1024)))
+        return rc;
+    return KS_OK;
+}
+
 int run_chunk(ks_ctx* ctx, int k_steps) {
+    if (ctx->dev_sbm) return run_chunk_dev(ctx, k_steps);
     stash_pending(ctx);  // this chunk's records land in h_conj
     int rc = ensure_chunk(ctx, k_steps);
     if (rc) return rc;
@@ -706,8 +907,26 @@ int seed_speculation(ks_ctx* ctx) {
     const int bits = estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale);
     ctx->sort_passes = passes_for_bits(bits);
     // Keys, dead flag and object index in 64 bits, with 2 bits to spare for the estimate.
-    ctx->pack_keys = ctx->allow_pack && bits + 1 + index_bits(ctx->n) + 2 <= 64;
+    const int64_t indices = ctx->dev_sbm ? ctx->b.cap : ctx->n;  // fragments take indices up to the capacity
+    ctx->pack_keys = ctx->allow_pack && bits + 1 + index_bits(indices) + 2 <= 64;
     drop_graphs(ctx);
+    return KS_OK;
+}
+
+// Device fragmentation: live count, masses (unknown), area-to-mass ratios,
+// provenance and event counters of a freshly uploaded population.
+int init_device_fragmentation(ks_ctx* ctx, bool single_population) {
+    if (!ctx->dev_sbm) return KS_OK;
+    ks::DeviceBuffers& b = ctx->b;
+    const int n = static_cast<int>(ctx->n);
+    KS_CUDA(cudaMemcpyAsync(b.n_live, &n, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    KS_CUDA(cudaMemsetAsync(b.mass_kg, 0, sizeof(double) * b.cap, ctx->stream));
+    KS_CUDA(cudaMemsetAsync(b.a2m, 0, sizeof(double) * b.cap, ctx->stream));
+    KS_CUDA(cudaMemsetAsync(b.event_of, 0xFF, sizeof(int32_t) * b.cap, ctx->stream));
+    KS_CUDA(cudaMemsetAsync(b.sbm_next_event, 0, sizeof(int) * 65536, ctx->stream));
+    if (single_population) KS_CUDA(cudaMemsetAsync(b.real_id, 0, sizeof(uint16_t) * b.cap, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->dev_stalls = 0;
     return KS_OK;
 }
 
@@ -1114,6 +1333,7 @@ int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double
     ctx->cur = 0;
     rc = upload_population(ctx, n, states, size_m, alive, 0);
     if (rc) return rc;
+    if ((rc = init_device_fragmentation(ctx, true))) return rc;
     rc = seed_speculation(ctx);
     if (rc) return rc;
     ctx->has_pop = true;
@@ -1149,6 +1369,7 @@ int ks_set_population_batch(ks_ctx* ctx, int32_t realisations, const int64_t* of
     drop_graphs(ctx);
     rc = upload_population(ctx, n, states, size_m, alive, 0);
     if (rc) return rc;
+    if ((rc = init_device_fragmentation(ctx, false))) return rc;
     rc = seed_speculation(ctx);
     if (rc) return rc;
     ctx->has_pop = true;
@@ -1312,6 +1533,7 @@ void put_knobs(ks_ctx* ctx, const Knobs& k, const Ctrl& carry) {
 int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out) {
     if (!ctx || trial_steps < 1 || trial_steps > 4096) return fail(ctx, KS_ERR_ARG, "ks_autotune: bad arguments");
     if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_autotune: no population");
+    if (ctx && ctx->dev_sbm) return fail(ctx, KS_ERR_STATE, "ks_autotune: not available with fragmentation on the device");
     cudaSetDevice(ctx->device);
     static const int kSpg[] = {8, 16, 32, 64};
     int rc = ensure_chunk(ctx, 64);
@@ -1541,13 +1763,106 @@ int ks_set_breakup(ks_ctx* ctx, int on, double lc_m, double catastrophic_j_per_g
     return KS_OK;
 }
 
+int ks_set_breakup_mode(ks_ctx* ctx, int mode, int64_t max_objects) {
+    if (!ctx || (mode != KS_BREAKUP_HOST && mode != KS_BREAKUP_DEVICE) ||
+        (mode == KS_BREAKUP_DEVICE && max_objects <= 0))
+        return fail(ctx, KS_ERR_ARG, "ks_set_breakup_mode: bad arguments");
+    if (max_objects > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "ks_set_breakup_mode: budget above 2^30 objects");
+    if (ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_set_breakup_mode: set the mode before the population");
+    cudaSetDevice(ctx->device);
+    if (mode == KS_BREAKUP_DEVICE) KS_CUDA(ks::sbm_init_attributes());
+    ctx->dev_sbm = mode == KS_BREAKUP_DEVICE;
+    ctx->dev_cap = ctx->dev_sbm ? max_objects : 0;
+    drop_graphs(ctx);
+    return KS_OK;
+}
+
 int ks_set_masses(ks_ctx* ctx, int64_t n, const double* mass_kg) {
     if (!ctx || !ctx->has_pop || n != ctx->n || (n > 0 && !mass_kg))
         return fail(ctx, KS_ERR_ARG, "ks_set_masses: needs one mass per object of the population");
     cudaSetDevice(ctx->device);
+    if (ctx->dev_sbm) {
+        if (n > 0) KS_CUDA(cudaMemcpy(ctx->b.mass_kg, mass_kg, sizeof(double) * n, cudaMemcpyHostToDevice));
+        return KS_OK;
+    }
     const int rc = ensure_mirrors(ctx);
     if (rc) return rc;
     std::copy(mass_kg, mass_kg + n, ctx->bk.mass_kg.begin());
+    return KS_OK;
+}
+
+// Forced impact with fragmentation on the device: the parents as the host SBM
+// builds them (one uniform draw for the side of the crossing, from a stream
+// of its own), then the device SBM for this one event at the current time.
+static int impact_device(ks_ctx* ctx, int64_t target, double projectile_mass_kg, double v_rel_km_s) {
+    ks::DeviceBuffers& b = ctx->b;
+    double s[6], mass = 0.0, size = 0.0;
+    uint16_t rid = 0;
+    int next = 0;
+    KS_CUDA(cudaMemcpyAsync(s, b.state[ctx->cur] + 6 * target, 48, cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(&mass, b.mass_kg + target, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(&size, b.size_m + target, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(&rid, b.real_id + target, 2, cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int r = ctx->rbits > 0 ? rid : 0;
+    KS_CUDA(cudaMemcpy(&next, b.sbm_next_event + r, sizeof(int), cudaMemcpyDeviceToHost));
+    const int id = next++;
+    KS_CUDA(cudaMemcpy(b.sbm_next_event + r, &next, sizeof(int), cudaMemcpyHostToDevice));
+    ks::SbmRng side(ctx->bk.seed ^ (0x9E3779B97F4A7C15ull * (static_cast<uint64_t>(r) * 65536u + static_cast<uint64_t>(id) + 1)));
+    ks::SbmParent tgt, prj;
+    ks::sbm_impact_parents(side, target, s, ks::sbm_mass_or_default(mass), size, projectile_mass_kg, v_rel_km_s, tgt,
+                           prj);
+    ks::SbmEventWork w{};
+    for (int q = 0; q < 6; ++q) {
+        w.s[0][q] = tgt.s[q];
+        w.s[1][q] = prj.s[q];
+    }
+    w.size_m[0] = tgt.size_m;
+    w.size_m[1] = prj.size_m;
+    w.mass[0] = tgt.mass_kg;
+    w.mass[1] = prj.mass_kg;
+    double dv2 = 0.0;
+    for (int q = 3; q < 6; ++q) dv2 += (w.s[0][q] - w.s[1][q]) * (w.s[0][q] - w.s[1][q]);
+    w.vrel = std::sqrt(dv2);
+    const double energy = 500.0 * w.mass[1] * w.vrel * w.vrel / w.mass[0];
+    w.catastrophic = energy >= ctx->bk.params.catastrophic_j_per_g ? 1 : 0;
+    w.budget[0] = w.catastrophic ? w.mass[0] : std::max(0.0, w.mass[1] * w.vrel * w.vrel - w.mass[1]);
+    w.budget[1] = w.mass[1];
+    w.t = ctx->t;
+    w.rem = 0.0;
+    w.target = static_cast<int>(tgt.index);
+    w.projectile = static_cast<int>(prj.index);
+    w.realisation = r;
+    w.id = id;
+    w.record = 0;
+    KS_CUDA(cudaMemcpy(b.sbm_work, &w, sizeof(w), cudaMemcpyHostToDevice));
+    KS_CUDA(cudaMemsetAsync(&b.chunk->flags, 0, sizeof(int), ctx->stream));
+    ks::launch_sbm_prepared(b, sbm_args(ctx), force_consts(), 1, ctx->steps_done, b.state[ctx->cur], b.alive[ctx->cur],
+                            carry_slot(ctx), b.chunk, ctx->stream);
+    KS_CUDA(cudaGetLastError());
+    ks_breakup_event ev{};
+    int n_live = 0, flags = 0;
+    KS_CUDA(cudaMemcpyAsync(&ev, b.sbm_events, sizeof(ev), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(&n_live, b.n_live, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaMemcpyAsync(&flags, &b.chunk->flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (flags & ks::FLAG_POP_BUDGET)
+        return fail(ctx, KS_ERR_OVERFLOW, "fragments would pass the population budget of " + std::to_string(b.cap) +
+                                              " objects (ks_set_breakup_mode)");
+    // The real object's fate: destroyed as the SBM projectile or above the
+    // catastrophic threshold, else eroded by the ejected mass.
+    const uint8_t dead = 0;
+    if (prj.index >= 0) KS_CUDA(cudaMemcpy(b.alive[ctx->cur] + prj.index, &dead, 1, cudaMemcpyHostToDevice));
+    if (tgt.index >= 0) {
+        if (w.catastrophic) KS_CUDA(cudaMemcpy(b.alive[ctx->cur] + tgt.index, &dead, 1, cudaMemcpyHostToDevice));
+        else {
+            const double left = std::max(w.mass[0] - w.budget[0], 0.0);
+            KS_CUDA(cudaMemcpy(b.mass_kg + tgt.index, &left, sizeof(left), cudaMemcpyHostToDevice));
+        }
+    }
+    ctx->n = n_live;
+    ctx->bk.out.push_back(ev);
+    drop_graphs(ctx);
     return KS_OK;
 }
 
@@ -1555,6 +1870,7 @@ int ks_impact(ks_ctx* ctx, int64_t target, double projectile_mass_kg, double v_r
     if (!ctx || !ctx->has_pop || target < 0 || target >= ctx->n || !(projectile_mass_kg > 0.0) || !(v_rel_km_s >= 0.0))
         return fail(ctx, KS_ERR_ARG, "ks_impact: bad arguments");
     cudaSetDevice(ctx->device);
+    if (ctx->dev_sbm) return impact_device(ctx, target, projectile_mass_kg, v_rel_km_s);
     int rc = ensure_mirrors(ctx);
     if (rc) return rc;
     ensure_streams(ctx);
@@ -1624,6 +1940,7 @@ int64_t ks_sbm_impact(uint64_t seed, double lc_m, double catastrophic_j_per_g, c
 int ks_save_population(ks_ctx* ctx, const char* path) {
     if (!ctx || !path) return fail(ctx, KS_ERR_ARG, "ks_save_population: bad arguments");
     if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_save_population: no population");
+    if (ctx && ctx->dev_sbm) return fail(ctx, KS_ERR_STATE, "ks_save_population: not available with fragmentation on the device");
     cudaSetDevice(ctx->device);
     int rc = ensure_mirrors(ctx);
     if (rc) return rc;
@@ -1664,6 +1981,7 @@ int ks_save_population(ks_ctx* ctx, const char* path) {
 }
 
 int ks_load_population(ks_ctx* ctx, const char* path) {
+    if (ctx && ctx->dev_sbm) return fail(ctx, KS_ERR_STATE, "ks_load_population: not available with fragmentation on the device");
     if (!ctx || !path) return fail(ctx, KS_ERR_ARG, "ks_load_population: bad arguments");
     std::ifstream f(path, std::ios::binary);
     PopHeader h{};
@@ -1753,6 +2071,23 @@ int ks_get_objects(ks_ctx* ctx, int64_t n, double* size_m, double* mass_kg, doub
                    int32_t* realisation) {
     if (!ctx || !ctx->has_pop || n != ctx->n) return fail(ctx, KS_ERR_ARG, "ks_get_objects: n must be the population size");
     cudaSetDevice(ctx->device);
+    if (ctx->dev_sbm) {
+        const ks::DeviceBuffers& b = ctx->b;
+        std::vector<uint16_t> rid(static_cast<size_t>(n));
+        if (n > 0) {
+            if (size_m) KS_CUDA(cudaMemcpyAsync(size_m, b.size_m, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+            if (mass_kg) KS_CUDA(cudaMemcpyAsync(mass_kg, b.mass_kg, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+            if (area_to_mass)
+                KS_CUDA(cudaMemcpyAsync(area_to_mass, b.a2m, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+            if (event) KS_CUDA(cudaMemcpyAsync(event, b.event_of, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+            if (realisation)
+                KS_CUDA(cudaMemcpyAsync(rid.data(), b.real_id, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (realisation)
+            for (int64_t i = 0; i < n; ++i) realisation[i] = rid[static_cast<size_t>(i)];
+        return KS_OK;
+    }
     const int rc = ensure_mirrors(ctx);
     if (rc) return rc;
     const ks_ctx::Breakup& k = ctx->bk;
@@ -1772,6 +2107,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
               ks_step_stats* stats) {
     if (!ctx || n < 0 || !count || (n > 0 && (!before || !after || !alive_after || !size_m)) || !(dt > 0.0))
         return fail(ctx, KS_ERR_ARG, "ks_screen: bad arguments");
+    if (ctx && ctx->dev_sbm) return fail(ctx, KS_ERR_STATE, "ks_screen: not available with fragmentation on the device");
     cudaSetDevice(ctx->device);
     int rc = ensure_objects(ctx, n);
     if (rc) return rc;
@@ -1886,6 +2222,7 @@ int ks_get_timing(const ks_ctx* ctx, ks_timing* out) {
 
 int ks_measure_fp64(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s) {
     if (!ctx || !addmul_per_s || !fma_per_s) return KS_ERR_ARG;
+    if (ctx && ctx->dev_sbm) return fail(ctx, KS_ERR_STATE, "ks_propagate: not available with fragmentation on the device");
     cudaSetDevice(ctx->device);
     KS_CUDA(ks::measure_fp64(addmul_per_s, fma_per_s, ctx->stream));
     return KS_OK;

@@ -26,6 +26,12 @@
 
 namespace ks {
 
+// A collision the refinement found, listed for the device SBM.
+struct CollisionRec {
+    int i, j;
+    double t;
+};
+
 // Per-step inputs computed on the host.
 struct StepParams {
     double t0;         // start of the step, seconds since epoch (Simulation::t)
@@ -59,6 +65,9 @@ enum : int {
     FLAG_KEYS_REBUILT = 64,  // k_fix_keys rebuilt the keys: their digit histogram is recounted
     FLAG_PACK_WIDTH = 128,   // cell key + dead flag + object index do not fit 64 bits: sort unpacked
     FLAG_CONJ_LARGE = 256,   // more records than the one-block ordering takes: ordered by the multi-block sort
+    FLAG_COLL_OVERFLOW = 512,   // device SBM: more collisions in one step than its event buffer holds
+    FLAG_POP_BUDGET = 1024,     // device SBM: fragments would pass the population's capacity
+    FLAG_HALTED = 2048,         // device SBM: an earlier step of the chunk was left void; this step does nothing
 };
 
 
@@ -83,6 +92,7 @@ struct Ctrl {
     unsigned int item_ticket;          // next pair work item to hand out
     int max_cell;
     int flags;
+    unsigned int n_coll;               // collisions of this step listed for the device SBM
     GridParams grid;
 };
 
@@ -90,6 +100,9 @@ struct Ctrl {
 inline int64_t items_total(const Ctrl& c) { return static_cast<int64_t>(c.n_items); }
 
 struct ChunkCtrl {
+    int halt_step;                     // device SBM: first step of the chunk left void (-1: none); later steps did nothing
+    int n_live;                        // device SBM: population size at the chunk's end
+    unsigned int events;               // device SBM: breakup records of the chunk
     unsigned long long conj_count;     // records appended in this chunk
     int flags;
     int sort_n;                        // records ordered by the chunk's conjunction sort
@@ -140,6 +153,18 @@ struct DeviceBuffers {
     int ctrl_len = 0;
     ChunkCtrl* chunk = nullptr;
     StepParams* params = nullptr;          // max_chunk entries
+    // Fragmentation on the device (NASA SBM, counter-based draws): the
+    // population grows inside a chunk up to `cap` objects.
+    int* n_live = nullptr;                 // current population size
+    double* mass_kg = nullptr;             // per object (0 = unknown)
+    double* a2m = nullptr;                 // area-to-mass ratio (m^2/kg), fragments
+    int32_t* event_of = nullptr;           // originating event (-1: initial population)
+    struct CollisionRec* coll = nullptr;   // this step's collisions (refinement output)
+    int coll_cap = 0;
+    struct SbmEventWork* sbm_work = nullptr;  // coll_cap events of a step
+    ks_breakup_event* sbm_events = nullptr;   // the chunk's breakup records
+    int64_t sbm_events_cap = 0;
+    int* sbm_next_event = nullptr;         // next event number per realisation
 };
 
 // Launch-shape knobs (set through ks_set_tuning; 0 = default).
@@ -183,6 +208,62 @@ struct StepArgs {
     unsigned int* hist;        // radix digit histogram the propagation fills with the keys it emits, or null
     float4* rec32;             // FP32 record of each object, written with its key (object order)
     int pack_bits;             // > 0: sort keys carry the object index in their low pack_bits bits
+    // Fragmentation on the device (null / 0 otherwise): the live population
+    // size (kernels bound their loops by it; n above is then the capacity the
+    // grids are sized for), and the chunk control whose halt_step voids the
+    // rest of the chunk.
+    const int* n_live;
+    ChunkCtrl* chunk;
+    int step_in_chunk;
+    int steps_in_chunk;
+    CollisionRec* coll;        // device SBM: collisions of the step, for fragmentation (null: not listed)
+    int coll_cap;
+};
+
+// A step whose results are void does nothing past that point:
+//  - a radix pass whose look-back gave up (FLAG_TIMEOUT) leaves the step's
+//    keys unordered and partly stale, and packed keys carry object indices:
+//    every kernel of the step that consumes them returns at once, so that no
+//    index read from such a key is ever used;
+//  - with fragmentation on the device, a step after one left void (FLAG_HALTED,
+//    set by launch_step_gate) runs nothing at all, and the next chunk starts
+//    again at the void step.
+// The host discards the void steps.
+__device__ __forceinline__ bool step_void(const Ctrl* c) { return (c->flags & (FLAG_TIMEOUT | FLAG_HALTED)) != 0; }
+
+// Population size a kernel works on: the live count when the population can
+// grow inside a chunk, else the fixed n.
+__device__ __forceinline__ int live_n(const StepArgs& a) { return a.n_live ? *a.n_live : a.n; }
+
+
+// One event of the device SBM, passed between its kernels.
+struct SbmEventWork {
+    double s[2][6];        // target, projectile: states at the event time
+    double size_m[2];      // characteristic sizes (upper bounds of their fragments)
+    double budget[2];      // mass each gives to fragments (kg)
+    double mass[2];        // masses before the event (kg)
+    double vrel;           // km/s
+    double t;              // event time, seconds since epoch
+    double rem;            // rest of the step after the event (s)
+    double expected;       // N(> L_c) of the number law
+    long long n_cand;      // candidates drawn (Poisson count, capped)
+    int target, projectile;  // object indices (-1: a forced impact's projectile)
+    int realisation;
+    int id;                // event number within its realisation
+    int catastrophic;
+    int kept;              // fragments kept (within budget, bound to the Earth)
+    int escaped;
+    int offset;            // first of its fragments after the population's end
+    double kept_mass;
+    int record;            // index of its breakup record in the chunk
+};
+
+// Device SBM parameters.
+struct SbmArgs {
+    double lc_m;
+    double catastrophic_j_per_g;
+    unsigned long long seed;
+    int cap;               // population capacity (memory budget)
 };
 
 // Kernel launchers (ks_kernels.cu). All enqueue on `stream` and never synchronise.
@@ -216,6 +297,21 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
                       cudaStream_t stream);
 void launch_refine(const DeviceBuffers& b, const StepArgs& a, ks_conjunction* conj_out, int64_t conj_cap,
                    ChunkCtrl* chunk, cudaStream_t stream);
+
+// Device SBM (ks_sbm.cu). After a step's refinement: voids the rest of the
+// chunk if the step's buffers overflowed, then fragments the step's
+// collisions in (t, i, j) order and appends the fragments, carried to the
+// step's end, after the live population.
+void launch_step_gate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+void launch_sbm_step(const DeviceBuffers& b, const StepArgs& a, const SbmArgs& s, cudaStream_t stream);
+// Fragments `count` events already in b.sbm_work (forced impacts, no step):
+// number draws, budgets, fragments appended at the end of state/alive.
+void launch_sbm_prepared(const DeviceBuffers& b, const SbmArgs& s, const ForceConsts& fc, int count, int64_t step,
+                         double* state, uint8_t* alive, Ctrl* spec, ChunkCtrl* chunk, cudaStream_t stream);
+// Collisions one step can fragment on the device (a step with more fails the run).
+constexpr int kSbmStepEvents = 1024;
+// Sets the kernels' launch attributes (dynamic shared memory); once per device.
+cudaError_t sbm_init_attributes();
 // Index of the key/idx buffer holding the sorted result after `passes` passes.
 inline int sorted_buffer(int passes) { return passes & 1; }
 

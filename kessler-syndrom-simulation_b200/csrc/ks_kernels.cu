@@ -49,6 +49,8 @@ __device__ __forceinline__ double dec_double(unsigned long long u) {
     return __longlong_as_double(static_cast<long long>((u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u));
 }
 
+
+
 // Cell edge (src/core/collision.cpp:339-356) from the largest start speed, and
 // the compact key layout over the position bounds.
 __device__ void make_grid(double vmax, const unsigned long long* bb_min, const unsigned long long* bb_max,
@@ -264,6 +266,7 @@ __device__ void ctrl_reset(Ctrl& c) {
     c.n_alive = c.n_cells = c.max_cell = c.flags = 0;
     c.n_items = 0u;
     c.item_ticket = 0u;
+    c.n_coll = 0u;
     c.grid = GridParams{};
 }
 
@@ -283,6 +286,8 @@ __global__ void k_chunk_init(Ctrl* ctrl, int k_steps, Ctrl* carry, ChunkCtrl* ch
         ctrl_reset(*carry);
         chunk->conj_count = 0ull;
         chunk->flags = 0;
+        chunk->halt_step = -1;
+        chunk->events = 0u;
     }
 }
 
@@ -344,6 +349,8 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_exact(StepArgs a, c
                                                             const uint8_t* __restrict__ alive_in,
                                                             uint8_t* __restrict__ alive_out,
                                                             unsigned long long* __restrict__ keys) {
+    if (step_void(a.ctrl)) return;  // an earlier step of the chunk was left void
+    const int n = live_n(a);
     __shared__ GridParams g;
     __shared__ MoonStage moon[3];
     if (threadIdx.x == 0) {
@@ -366,10 +373,10 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_exact(StepArgs a, c
     const int lane = threadIdx.x & 31;
     // Warp-uniform loop (whole warps iterate together) so that the digit
     // histogram can aggregate over the warp.
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += gridDim.x * blockDim.x) {
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
         const int i = base + lane;
         unsigned long long out_key = 0ull;
-        if (i < a.n) {
+        if (i < n) {
             double s[6];
             ld6(in, i, s);
             if (!alive_in[i]) {
@@ -408,7 +415,7 @@ __global__ void __launch_bounds__(kPropBlock, 4) k_propagate_exact(StepArgs a, c
         }
         if (with_hist) {
             __syncwarp();
-            warp_hist_add(sh_hist, i < a.n, out_key, a.sort_passes, lane);
+            warp_hist_add(sh_hist, i < n, out_key, a.sort_passes, lane);
         }
     }
     if (with_hist) {
@@ -463,6 +470,8 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
                                                                    const uint8_t* __restrict__ alive_in,
                                                                    uint8_t* __restrict__ alive_out,
                                                                    unsigned long long* __restrict__ keys) {
+    if (step_void(a.ctrl)) return;  // an earlier step of the chunk was left void
+    const int n = live_n(a);
     __shared__ GridParams g;
     __shared__ MoonStageF moon[3];
     if (threadIdx.x == 0) {
@@ -484,10 +493,10 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
     SpecAccum acc;
     acc.init();
     const int lane = threadIdx.x & 31;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.n; base += gridDim.x * blockDim.x) {
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
         const int i = base + lane;
         unsigned long long out_key = 0ull;
-        if (i < a.n) {
+        if (i < n) {
             double s[6];
             ld6(in, i, s);
             if (!alive_in[i]) {
@@ -525,7 +534,7 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
         }
         if (with_hist) {
             __syncwarp();
-            warp_hist_add(sh_hist, i < a.n, out_key, a.sort_passes, lane);
+            warp_hist_add(sh_hist, i < n, out_key, a.sort_passes, lane);
         }
     }
     if (with_hist) {
@@ -553,8 +562,9 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
         }
     }
     __syncthreads();
+    const int n = live_n(a);
     int bad = 0, alive = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (alive_after[i]) {
             const double* s = before + 6 * static_cast<int64_t>(i);
             const unsigned long long key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &bad);
@@ -580,6 +590,8 @@ __global__ void __launch_bounds__(kBlock) k_screen_keys(StepArgs a, const double
 __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* __restrict__ before,
                                                      const uint8_t* __restrict__ alive_after,
                                                      unsigned long long* __restrict__ keys) {
+    if (step_void(a.ctrl)) return;
+    const int n = live_n(a);
     if (blockIdx.x == 0 && threadIdx.x == 0 && a.ctrl->grid.bits + 1 > 8 * a.sort_passes)
         atomicOr(&a.ctrl->flags, FLAG_SORT_BITS);  // more key bits than the sort's passes cover
     const unsigned long long vt = a.ctrl->vmax_true;
@@ -600,7 +612,7 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
         for (int t = threadIdx.x; t < a.sort_passes * 256; t += blockDim.x) a.hist[t] = 0u;
     __syncthreads();
     int bad = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         unsigned long long key = dead_key(g);
         if (alive_after[i]) {
             const double* s = before + 6 * static_cast<int64_t>(i);
@@ -696,11 +708,7 @@ __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// A radix pass whose look-back gave up (FLAG_TIMEOUT) leaves the step's keys
-// unordered and partly stale, and packed keys carry object indices: every
-// kernel of the step that consumes them returns at once, so that no index read
-// from such a key is ever used. The host discards the step.
-__device__ __forceinline__ bool sort_gave_up(const Ctrl* c) { return (c->flags & FLAG_TIMEOUT) != 0; }
+
 
 // Digit histograms of every pass in one read of the keys.
 // only_if_rebuilt: the propagation already counted the digits; recount only
@@ -858,7 +866,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
 __global__ void __launch_bounds__(kBlock) k_cell_count(const unsigned long long* __restrict__ keys,
                                                        const Ctrl* __restrict__ ctrl, unsigned int* __restrict__ counts,
                                                        int pack_bits) {
-    if (sort_gave_up(ctrl)) return;
+    if (step_void(ctrl)) return;
     const int m = ctrl->n_alive;
     const int shift = 3 * ctrl->grid.sub + pack_bits;
     const int base = blockIdx.x * kCellTile;
@@ -889,7 +897,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_write(const unsigned long long*
                                                        double* __restrict__ sorted,
                                                        int* __restrict__ sorted_orig, float4* __restrict__ sorted32,
                                                        const float4* __restrict__ rec32, int pack_bits) {
-    if (sort_gave_up(ctrl)) return;
+    if (step_void(ctrl)) return;
     constexpr int kPer = kCellTile / kBlock;  // consecutive entries per thread
     const int m = ctrl->n_alive;
     if (m == 0) {
@@ -991,7 +999,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
                                                        const unsigned long long* __restrict__ hk,
                                                        const int* __restrict__ hv, unsigned long long hmask,
                                                        int* __restrict__ nbr) {
-    if (sort_gave_up(ctrl)) return;
+    if (step_void(ctrl)) return;
     const int nc = ctrl->n_cells;
     const GridParams g = ctrl->grid;
     const unsigned long long mz = (1ull << g.w[2]) - 1, my = (1ull << g.w[1]) - 1;
@@ -1048,7 +1056,7 @@ __device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr, int* __restrict__ cell_len,
                                                         unsigned int* __restrict__ part, int per) {
-    if (sort_gave_up(ctrl)) return;
+    if (step_void(ctrl)) return;
     const int nc = ctrl->n_cells;
     const int chunks = (nc + kBlock - 1) / kBlock;
     unsigned long long cand = 0;
@@ -1100,7 +1108,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
                                                         const int* __restrict__ cell_len,
                                                         const unsigned int* __restrict__ part,
                                                         int4* __restrict__ items, int64_t items_cap, int per) {
-    if (sort_gave_up(ctrl)) return;
+    if (step_void(ctrl)) return;
     const int nc = ctrl->n_cells;
     const int chunks = (nc + kBlock - 1) / kBlock;
     const int lane = threadIdx.x & 31;
@@ -1441,7 +1449,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     __shared__ unsigned qmask[kWarps][64];
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
     __shared__ int2 fq[kWarps][64];
-    if (sort_gave_up(a.ctrl)) return;
+    if (step_void(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
@@ -1614,11 +1622,27 @@ __device__ __forceinline__ bool boxes_apart(const Box& a, const Box& b, float dt
     return sqrtf(d2) * (1.0f - 1e-5f) - dt * sqrtf(w2) * (1.0f + 1e-5f) > gate;
 }
 
-// FP32 version of certainly_convex_reject for FP32 records whose dr, dv carry
-// absolute errors up to er, ev (f32_pos_err, f32_vel_err); vmin2e is
-// (vmin + ev)^2. Margins as derived in the comments below.
-__device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, float rz, float vx, float vy,
-                                                            float vz, float vmin2e, float er, float ev) {
+// Second FP32 stage for the pairs the gate lets through, on FP32 records whose
+// dr, dv carry absolute errors up to er, ev (f32_pos_err, f32_vel_err): true
+// only if filter_pair_exact certainly returns FILTER_REJECT, for one of two
+// reasons. vmin2e is (vmin + ev)^2; gate2 is the squared FP32 gate (the
+// exact filter's gate widened by e = er + ev dt, as gate_open_f32 takes it).
+//  (1) Separating, fast and convex: the reference's convexity rejection
+//      (src/core/collision_filter.hpp:63), FP32 version of
+//      certainly_convex_reject; margins as derived in the comments below.
+//  (2) Closest approach after the step: when -dr.dv > |dv|^2 dt the exact
+//      filter clamps ts to dt (src/core/collision_filter.hpp:45-47) and
+//      gates |dr + dv dt|. The true relative motion stays within e of the
+//      records' over the step, which gate2 covers. For the records' values,
+//      the FP32 rounding of dr + dv dt is below 3.1e-7 |dr| (|dv| dt <= |dr|
+//      when -dr.dv > |dv|^2 dt), and a pair wrongly classed as "after" by the
+//      rounding of dr.dv and |dv|^2 dt (a few ulps of |dr||dv|) has its true
+//      minimum within 4.8e-7 |dr| of |dr + dv dt|. With b = 1e-6 |dr| >= both:
+//      (g + b)^2 <= g^2 (1 + 1e-4) + 1.01e-8 |dr|^2, and the factors below add
+//      room for the rounding of the squares. In the bench workload these are
+//      two thirds of the pairs the convexity test leaves.
+__device__ __forceinline__ bool certainly_reject_f32(float rx, float ry, float rz, float vx, float vy, float vz,
+                                                     float vmin2e, float er, float ev, float dt, float gate2) {
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
     const float dv2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
     const float rv = fmaf(rx, vx, fmaf(ry, vy, rz * vz));
@@ -1633,15 +1657,20 @@ __device__ __forceinline__ bool certainly_convex_reject_f32(float rx, float ry, 
     const bool convex = dv2 * (1.0f - 2.0f * ev - 4e-6f) - 1.25f * (ev + ev * ev) >
                         static_cast<float>(kGravityGradient * 1.0002) *
                             fmaf(r2, 1.0f + 2.0f * er + 2e-6f, 1.25f * (er + er * er));
-    return fast && separating && convex;
+    if (fast && separating && convex) return true;
+    if (!(rv < 0.f) || !(-rv > dv2 * dt)) return false;
+    const float px = fmaf(vx, dt, rx), py = fmaf(vy, dt, ry), pz = fmaf(vz, dt, rz);
+    const float pe2 = fmaf(px, px, fmaf(py, py, pz * pz));
+    return pe2 > fmaf(gate2, 1.00012f, 1.2e-8f * r2);
 }
 
-// Rows flagged by the FP32 gate for the lane's column q: the FP32 convexity
-// test drops the pairs it proves rejected, the rest join the warp's queue for
-// the exact filter.
+// Rows flagged by the FP32 gate for the lane's column q: the second FP32
+// stage (certainly_reject_f32) drops the pairs it proves rejected, the rest
+// join the warp's queue for the exact filter.
 __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 cv, int q, const double* __restrict__ before,
                                                const int* __restrict__ orig, const float4 (*rows32)[2],
-                                               const int* rorig, float vmin2e, float er, float ev, const StepArgs& a,
+                                               const int* rorig, float vmin2e, float er, float ev, float dt_f,
+                                               float gate2, const StepArgs& a,
                                                int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc, int2* fq,
                                                int& fcount) {
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
@@ -1652,8 +1681,8 @@ __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 
         todo &= todo - 1;
         if ((need >> r) & 1u) {
             const float4 rp = rows32[r][0], rv = rows32[r][1];
-            if (!certainly_convex_reject_f32(cp.x - rp.x, cp.y - rp.y, cp.z - rp.z, cv.x - rv.x, cv.y - rv.y,
-                                             cv.z - rv.z, vmin2e, er, ev))
+            if (!certainly_reject_f32(cp.x - rp.x, cp.y - rp.y, cp.z - rp.z, cv.x - rv.x, cv.y - rv.y,
+                                      cv.z - rv.z, vmin2e, er, ev, dt_f, gate2))
                 still |= 1u << r;
         }
     }
@@ -1676,7 +1705,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     __shared__ unsigned qmask[kWarps][64];
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
     __shared__ int2 fq[kWarps][64];
-    if (sort_gave_up(a.ctrl)) return;
+    if (step_void(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const int n_items = static_cast<int>(min(static_cast<int64_t>(a.ctrl->n_items), items_cap));
@@ -1731,8 +1760,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
                 need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
             need &= valid;
             if (__any_sync(0xffffffffu, need != 0u))
-                exact_rows_f32(need, cp, cv, q, before, orig, rows32[warp], rorig[warp], vmin2e, er, ev, a, surv,
-                               surv_cap, pc, fq[warp], fcount);
+                exact_rows_f32(need, cp, cv, q, before, orig, rows32[warp], rorig[warp], vmin2e, er, ev, dt_f, gate2,
+                               a, surv, surv_cap, pc, fq[warp], fcount);
         };
         auto drain = [&](int count) {
             __syncwarp();
@@ -1807,7 +1836,7 @@ __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const doubl
                                                          const int2* __restrict__ surv, int64_t surv_cap,
                                                          ks_conjunction* __restrict__ out, int64_t cap,
                                                          ChunkCtrl* chunk) {
-    if (sort_gave_up(a.ctrl)) return;
+    if (step_void(a.ctrl)) return;
     const unsigned long long ns = min(a.ctrl->refined, static_cast<unsigned long long>(surv_cap));
     const double t0 = a.sp->t0;
     const double s_hi = xsub(1.0, 1e-9);
@@ -1843,6 +1872,11 @@ __global__ void __launch_bounds__(kBlock) k_refine_exact(StepArgs a, const doubl
         const double rj = xmul(xmul(xmul(0.5, size_m[j]), 1e-3), a.radius_scale);
         c.collision = miss < xadd(ri, rj) ? 1 : 0;
         c.realisation = a.real_id ? a.real_id[i] : 0;
+        if (c.collision && a.coll) {
+            const unsigned int k = atomicAdd(&a.ctrl->n_coll, 1u);
+            if (k < static_cast<unsigned int>(a.coll_cap)) a.coll[k] = CollisionRec{i, j, c.t};
+            else atomicOr(&a.ctrl->flags, FLAG_COLL_OVERFLOW);
+        }
         atomicAdd(&a.ctrl->conj, 1ull);
         const unsigned long long slot = atomicAdd(&chunk->conj_count, 1ull);
         if (slot < static_cast<unsigned long long>(cap)) out[slot] = c;
@@ -1999,12 +2033,12 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     if (!counted) cudaMemsetAsync(b.sort_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
     cudaMemsetAsync(b.sort_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
-    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, nullptr, passes, b.sort_hist, a.ctrl,
+    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, a.n_live, passes, b.sort_hist, a.ctrl,
                                                   counted ? 1 : 0, a.pack_bits);
     for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
-            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, nullptr,
+            b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, a.n_live,
             a.pack_bits + 8 * pass, b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass,
             b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0, a.tune.lookback_polls);
     }
