@@ -112,6 +112,9 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * "item_col_blocks" (1..64, column blocks of 32 per pair-kernel work item),
  * "pack_keys" (1: the radix sort carries the object index in the low bits of
  * its keys where they leave room, the default; 0: a separate index array),
+ * "pair_gate_x2" (1, the default: the FP32 pair gate evaluates two rows per
+ * instruction with packed f32x2 arithmetic, decisions identical to the scalar
+ * gate's; 0: one row at a time),
  * "lookback_polls" (0..2^30, default 2^22: polls a radix-sort tile makes of a
  * predecessor's unpublished digit counts before it gives up; a wait that runs
  * out fails the run with KS_ERR_TIMEOUT and leaves the simulation where the

@@ -177,6 +177,7 @@ struct Tuning {
     int prop_block = 128;         // threads per block of the propagation kernels (32..128, multiple of 32)
     int item_col_blocks = 16;     // column blocks of 32 per pair work item (1..64)
     int lookback_polls = 1 << 22; // polls of a radix-sort look-back before it gives up (FLAG_TIMEOUT)
+    int pair_gate_x2 = 1;         // FP32 pair gate on two rows per instruction (packed f32x2)
 };
 
 // Time from a fragmentation event to the end of its step and the lunar stages

@@ -1697,6 +1697,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
                                                         const int* __restrict__ nbr, const int4* __restrict__ items,
                                                         int64_t items_cap, int2* __restrict__ surv, int64_t surv_cap) {
     __shared__ float4 rows32[kWarps][32][2];
+    // The same rows in pairs, components interleaved, for the packed gate.
+    __shared__ float2 rows2[kWarps][16][6];
     __shared__ int rorig[kWarps][32];
     __shared__ SegTable segs[kWarps];
     // Per-warp queue of columns that survived the row-box test, drained 32 at a time.
@@ -1718,6 +1720,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     const double gate_e = (gate_hi + er_d + ev_d * a.dt) * (1.0 + 1e-6);
     const float gate_f = static_cast<float>(gate_e);
     const float gate2 = gate_f * gate_f;
+    const float2 gate2x2 = make_float2(gate2, gate2);
+    const bool gate_x2 = a.tune.pair_gate_x2 != 0;
     const float dt_f = static_cast<float>(a.dt);
     const float cell_f = static_cast<float>(a.ctrl->grid.cell);
     const double vme = sqrt(a.vmin2) + ev_d;
@@ -1745,6 +1749,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
             rows32[warp][lane][1] = my_rv;
             rorig[warp][lane] = orig[rl];
         }
+        if (gate_x2) {
+            // Lane l writes its row into pair l / 2, half l % 2 (rows past nr
+            // repeat the first row; their bits are masked off).
+            float* pr = reinterpret_cast<float*>(rows2[warp][lane >> 1]) + (lane & 1);
+            pr[0] = my_rp.x; pr[2] = my_rp.y; pr[4] = my_rp.z;
+            pr[6] = my_rv.x; pr[8] = my_rv.y; pr[10] = my_rv.z;
+        }
         // Tiles of at least box_rows rows test each column against the rows'
         // position / velocity box first and keep only columns that could come
         // within the gate of some row, compacted into full warps.
@@ -1755,9 +1766,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
         // Columns held by the lanes (entry `lane` of a batch) against every row.
         auto gate_rows = [&](float4 cp, float4 cv, int q, unsigned valid) {
             unsigned need = 0u;
+            if (gate_x2) {
+#pragma unroll 2
+                for (int r = 0; r < nr; r += 2) need |= gate_open_f32x2(cp, cv, rows2[warp][r >> 1], gate2x2) << r;
+            } else {
 #pragma unroll 4
-            for (int r = 0; r < nr; ++r)
-                need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
+                for (int r = 0; r < nr; ++r)
+                    need |= gate_open_f32(cp, cv, rows32[warp][r][0], rows32[warp][r][1], gate2) << r;
+            }
             need &= valid;
             if (__any_sync(0xffffffffu, need != 0u))
                 exact_rows_f32(need, cp, cv, q, before, orig, rows32[warp], rorig[warp], vmin2e, er, ev, dt_f, gate2,

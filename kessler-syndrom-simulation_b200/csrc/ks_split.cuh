@@ -110,4 +110,31 @@ __device__ __forceinline__ unsigned gate_open_f32(float4 cp, float4 cv, float4 r
     return fmaf(-m, m, P) <= fmaf(dv2, gate2, 1e-5f * P) ? 1u : 0u;
 }
 
+// gate_open_f32 for two rows at once with Blackwell's packed FP32 arithmetic
+// (FFMA2 / FMUL2: two lanes of an f32x2 per instruction, each rounded exactly
+// as the scalar instruction): the same operations in the same order as
+// gate_open_f32, so each of the two decisions equals the scalar gate's bit
+// for bit, with about half the instructions. rows: the two rows' six
+// components interleaved, {px0, px1}, {py0, py1}, {pz0, pz1}, {vx0, vx1},
+// {vy0, vy1}, {vz0, vz1}. Bit 0: first row, bit 1: second.
+__device__ __forceinline__ unsigned gate_open_f32x2(const float4 cp, const float4 cv, const float2* rows,
+                                                    const float2 gate2) {
+    const float2 m1 = make_float2(-1.0f, -1.0f);
+    // c - r, rounded once: fma(r, -1, c).
+    const float2 rx = __ffma2_rn(rows[0], m1, make_float2(cp.x, cp.x));
+    const float2 ry = __ffma2_rn(rows[1], m1, make_float2(cp.y, cp.y));
+    const float2 rz = __ffma2_rn(rows[2], m1, make_float2(cp.z, cp.z));
+    const float2 vx = __ffma2_rn(rows[3], m1, make_float2(cv.x, cv.x));
+    const float2 vy = __ffma2_rn(rows[4], m1, make_float2(cv.y, cv.y));
+    const float2 vz = __ffma2_rn(rows[5], m1, make_float2(cv.z, cv.z));
+    const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+    const float2 dv2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __fmul2_rn(vz, vz)));
+    const float2 rv = __ffma2_rn(rx, vx, __ffma2_rn(ry, vy, __fmul2_rn(rz, vz)));
+    const float2 m = make_float2(fminf(rv.x, 0.0f), fminf(rv.y, 0.0f));
+    const float2 P = __fmul2_rn(r2, dv2);
+    const float2 lhs = __ffma2_rn(make_float2(-m.x, -m.y), m, P);
+    const float2 rhs = __ffma2_rn(dv2, gate2, __fmul2_rn(make_float2(1e-5f, 1e-5f), P));
+    return (lhs.x <= rhs.x ? 1u : 0u) | (lhs.y <= rhs.y ? 2u : 0u);
+}
+
 }  // namespace ks

@@ -48,3 +48,31 @@ def test_kernel_counts(bench):
     assert bench.launches_per_step(4) == 16
     assert bench.launches_per_step(5) == 17
     assert bench.LAUNCHES_PER_CHUNK == 8
+
+
+def test_reference_arm_loads_nothing_of_the_engine():
+    """bench.py --impl reference runs the reference's own CPU path on inputs
+    from oracle/libks_workload.so: the engine library never enters the
+    process, and the line reports exactly the requested steps and warm-up."""
+    import json
+    import subprocess
+
+    code = r'''
+import json, runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--objects", "3000", "--base", "2000", "--parents", "2",
+            "--steps", "3", "--warmup", "2"]
+try:
+    runpy.run_path("bench.py", run_name="__main__")
+except SystemExit:
+    pass
+maps = open("/proc/self/maps").read()
+print(json.dumps({"maps": sorted(set(l.split()[-1] for l in maps.splitlines() if l.endswith(".so")))}))
+'''
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    line, maps = json.loads(lines[0]), json.loads(lines[-1])["maps"]
+    assert line["impl"] == "reference" and line["steps"] == 3 and line["warmup"] == 2
+    ours = [m for m in maps if m.startswith(ROOT)]
+    assert ours and all(m.startswith(os.path.join(ROOT, "oracle")) for m in ours), ours
+    assert not any("libkessler_b200" in m for m in maps)
