@@ -311,10 +311,16 @@ def realisation_seed(seed, rank):
     return seed + rank
 
 
-def roofline_of(tm, a, fp64_rate, fp32_rate, split):
+def roofline_of(tm, a, fp64_rate, fp32_rates, split):
     """Dominant kernel of the step and its achieved rate against the measured
     issue rate of the pipe that bounds it (algorithmic operations per launch
-    divided by the launch's average CUDA-event duration)."""
+    divided by the launch's average CUDA-event duration). fp32_rates: the
+    measured FP32 operation rates of this GPU (add/mul, FMA, packed FFMA2);
+    the pair kernel is held to the highest of them (its gate runs on packed
+    FMAs) and its fraction against each is listed."""
+    if not isinstance(fp32_rates, dict):
+        fp32_rates = {"addmul": fp32_rates}
+    fp32_rate = max(fp32_rates.values())
     steps = max(1, tm["steps"])
     phases = {k: tm[k] / steps for k in ("propagate_ms", "sort_ms", "cells_ms", "pairs_ms", "refine_ms", "chunk_ms")}
     prop_ops = FLOPS_OBJECT_STEP * tm["object_steps"] / steps
@@ -348,10 +354,15 @@ def roofline_of(tm, a, fp64_rate, fp32_rate, split):
         gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
         hbm_kernels[k] = {"ms": ms, "algorithmic_bytes": nbytes, "gbs": gbs, "frac": gbs / hbm if gbs else None,
                           "what": what}
+    fp32_fracs = {k: (kernels["pairs"]["tflops"] * 1e12 / v if kernels["pairs"]["tflops"] and v else None)
+                  for k, v in fp32_rates.items()}
     return {"bound": d["pipe"], "kernel": dom, "achieved": d["tflops"], "peak": d["peak"] / 1e12,
             "unit": "TFLOP/s", "frac": d["frac"], "traffic": traffic_of(dom, split),
-            "peak_source": "measured on this GPU by the project microbenchmark (dependent add/mul chains, no FMA); "
+            "peak_source": "measured on this GPU by the project microbenchmarks (dependent chains of FP32 add/mul, "
+                           "FMA and packed FFMA2, FP64 add/mul; the highest FP32 rate is the peak); "
                            "MEASURED_PEAKS.json has no FP64/FP32 SIMT figure",
+            "pairs_fp32_rates_tops": {k: v / 1e12 for k, v in fp32_rates.items()},
+            "pairs_frac_by_fp32_rate": fp32_fracs,
             "algorithmic_ops_per_launch": d["ops"], "phase_ms_per_step": phases,
             "kernels": {k: {"ms": v["ms"], "pipe": v["pipe"], "tflops": v["tflops"], "frac": v["frac"]}
                         for k, v in kernels.items()},
@@ -664,7 +675,10 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
 
 
 def measure_fp32(eng):
-    return eng.measure_fp32()[0]
+    """Measured FP32 operation rates: add/mul instructions, FMA instructions,
+    and FMA lanes of packed FFMA2 instructions, per second."""
+    am, fma = eng.measure_fp32()
+    return {"addmul": am, "fma": fma, "fma_x2": eng.measure_fp32x2()}
 
 
 def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):

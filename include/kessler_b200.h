@@ -299,6 +299,9 @@ int ks_generate_population(uint64_t seed, int64_t n_base, int64_t n_total, int n
 int ks_measure_fp64(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s);
 /* The same for FP32 (add/mul without contraction, and FMA). */
 int ks_measure_fp32(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s);
+/* Packed FP32 (Blackwell FFMA2, two FMAs per lane and instruction): FMA
+ * operations per second, each lane of an f32x2 counted once. */
+int ks_measure_fp32x2(ks_ctx* ctx, double* fma_ops_per_s);
 
 #ifdef __cplusplus
 }

@@ -264,6 +264,12 @@ class Engine:
         self._check(self._lib.ks_measure_fp32(self._h, C.byref(a), C.byref(f)))
         return a.value, f.value
 
+    def measure_fp32x2(self):
+        """Packed FP32 FMA operations per second (FFMA2, two per lane and instruction)."""
+        f = C.c_double()
+        self._check(self._lib.ks_measure_fp32x2(self._h, C.byref(f)))
+        return f.value
+
 
 def moon_position(jd):
     lib = load_library()

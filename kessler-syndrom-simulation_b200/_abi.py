@@ -95,6 +95,7 @@ SIGNATURES = {
     "ks_generate_population": (C.c_int, [C.c_uint64, _I64, _I64, C.c_int, _D, _P, _P, _P]),
     "ks_measure_fp64": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D)]),
     "ks_measure_fp32": (C.c_int, [_P, C.POINTER(_D), C.POINTER(_D)]),
+    "ks_measure_fp32x2": (C.c_int, [_P, C.POINTER(_D)]),
 }
 
 _lib = None

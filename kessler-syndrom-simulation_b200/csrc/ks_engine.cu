@@ -2236,4 +2236,11 @@ int ks_measure_fp32(ks_ctx* ctx, double* addmul_per_s, double* fma_per_s) {
     return KS_OK;
 }
 
+int ks_measure_fp32x2(ks_ctx* ctx, double* fma_ops_per_s) {
+    if (!ctx || !fma_ops_per_s) return KS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    KS_CUDA(ks::measure_fp32x2(fma_ops_per_s, ctx->stream));
+    return KS_OK;
+}
+
 }  // extern "C"

@@ -319,5 +319,6 @@ inline int sorted_buffer(int passes) { return passes & 1; }
 int sm_count();
 cudaError_t measure_fp64(double* addmul_per_s, double* fma_per_s, cudaStream_t stream);
 cudaError_t measure_fp32(double* addmul_per_s, double* fma_per_s, cudaStream_t stream);
+cudaError_t measure_fp32x2(double* fma_ops_per_s, cudaStream_t stream);
 
 }  // namespace ks

@@ -1952,6 +1952,20 @@ __global__ void __launch_bounds__(256) k_fp32_fma(float* out, int iters, float a
     if (s == 1.2345f) out[0] = s;
 }
 
+// Packed FP32: 8 independent chains of FFMA2 (two FP32 FMAs per lane and instruction).
+__global__ void __launch_bounds__(256) k_fp32x2_fma(float* out, int iters, float a, float b) {
+    float2 x[8];
+    for (int q = 0; q < 8; ++q) x[q] = make_float2(threadIdx.x * 1e-3f + q, threadIdx.x * 2e-3f + q);
+    const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) x[q] = __ffma2_rn(x[q], a2, b2);
+    }
+    float s = 0;
+    for (int q = 0; q < 8; ++q) s += x[q].x + x[q].y;
+    if (s == 1.2345f) out[0] = s;
+}
+
 // SM count per device index, looked up on first use from each device. The
 // entries are atomics so that threads driving different devices (or the
 // allocation-free entry point from any thread) neither race nor share a count.
@@ -2285,6 +2299,33 @@ cudaError_t measure_fp32(double* addmul_per_s, double* fma_per_s, cudaStream_t s
     e = cudaGetLastError();
     *addmul_per_s = 2.0 * ops / (best_am * 1e-3);
     *fma_per_s = ops / (best_f * 1e-3);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    return e;
+}
+
+cudaError_t measure_fp32x2(double* fma_ops_per_s, cudaStream_t stream) {
+    float* out = nullptr;
+    cudaError_t e = cudaMalloc(&out, sizeof(float));
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sm_count() * 8, threads = 256, iters = 8192;
+    const double ops = 2.0 * static_cast<double>(blocks) * threads * iters * 8;  // two lanes per FFMA2
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        float ms = 0;
+        cudaEventRecord(e0, stream);
+        k_fp32x2_fma<<<blocks, threads, 0, stream>>>(out, iters, 0.999999f, 1e-7f);
+        cudaEventRecord(e1, stream);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    e = cudaGetLastError();
+    *fma_ops_per_s = ops / (best * 1e-3);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(out);
