@@ -1480,6 +1480,7 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     else if (k == "prop_block" && value >= 32 && value <= 128 && value % 32 == 0) ctx->tune.prop_block = static_cast<int>(value);
     else if (k == "item_col_blocks" && value >= 1 && value <= 64) ctx->tune.item_col_blocks = static_cast<int>(value);
     else if (k == "pair_gate_x2" && (value == 0 || value == 1)) ctx->tune.pair_gate_x2 = static_cast<int>(value);
+    else if (k == "pair_stage2" && value >= 0 && value <= 2) ctx->tune.pair_stage2 = static_cast<int>(value);
     else if (k == "lookback_polls" && value >= 0 && value <= (int64_t(1) << 30)) {
         ctx->tune.lookback_polls = static_cast<int>(value);
         drop_graphs(ctx);  // graphs hold the limit in their kernel arguments

@@ -1672,9 +1672,61 @@ __device__ __forceinline__ void exact_rows_f32(unsigned need, float4 cp, float4 
                                                const int* rorig, float vmin2e, float er, float ev, float dt_f,
                                                float gate2, const StepArgs& a,
                                                int2* __restrict__ surv, int64_t surv_cap, PairCounters& pc, int2* fq,
-                                               int& fcount) {
+                                               int& fcount, float4 (*ccol)[2], int* cidx, bool staged,
+                                               unsigned short* pq) {
+    const int lane = threadIdx.x & 31;
     unsigned todo = __reduce_or_sync(0xffffffffu, need);
-    // FP32 convexity pass: drop rows no lane still needs.
+    // When the flagged pairs are sparse (under half the lanes busy per row of
+    // the loop below), they are queued one pair per lane instead and tested 32
+    // at a time; the same test on the same pairs, so the same survivors.
+    const int mode = a.tune.pair_stage2;
+    if (mode == 2 || (mode == 1 && 2u * __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popc(need))) <
+                                       32u * static_cast<unsigned>(__popc(todo)))) {
+        if (!staged) {  // the lanes' columns into the (empty) column queue
+            ccol[lane][0] = cp;
+            ccol[lane][1] = cv;
+            cidx[lane] = q;
+        }
+        __syncwarp();
+        unsigned mine = need;
+        int pn = 0;
+        auto test = [&](int count) {
+            __syncwarp();
+            unsigned keep = 0u;
+            int qs = 0;
+            if (lane < count) {
+                const unsigned e = pq[lane];
+                const int src = static_cast<int>(e >> 8), r = static_cast<int>(e & 0xFFu);
+                const float4 c0 = ccol[src][0], c1 = ccol[src][1];
+                const float4 rp = rows32[r][0], rv = rows32[r][1];
+                qs = cidx[src];
+                if (!certainly_reject_f32(c0.x - rp.x, c0.y - rp.y, c0.z - rp.z, c1.x - rv.x, c1.y - rv.y,
+                                          c1.z - rv.z, vmin2e, er, ev, dt_f, gate2))
+                    keep = 1u << r;
+            }
+            __syncwarp();
+            queue_exact<true>(keep, qs, fq, fcount, before, orig, nullptr, rorig, a, surv, surv_cap, pc);
+        };
+        while (__any_sync(0xffffffffu, mine != 0u)) {
+            const bool have = mine != 0u;
+            const unsigned bal = __ballot_sync(0xffffffffu, have);
+            if (have) {
+                pq[pn + __popc(bal & lanemask_lt())] = static_cast<unsigned short>((lane << 8) | (__ffs(mine) - 1));
+                mine &= mine - 1;
+            }
+            pn += __popc(bal);
+            if (pn >= 32) {
+                test(32);
+                __syncwarp();
+                if (lane < pn - 32) pq[lane] = pq[32 + lane];
+                pn -= 32;
+            }
+        }
+        if (pn > 0) test(pn);
+        __syncwarp();
+        return;
+    }
+    // FP32 second stage, row by row: drop rows no lane still needs.
     unsigned still = 0u;
     while (todo) {
         const int r = __ffs(todo) - 1;
@@ -1706,6 +1758,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     __shared__ int qidx[kWarps][64];
     __shared__ unsigned qmask[kWarps][64];
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
+    // Per-warp queue of flagged (column lane, row) pairs for the compacted second stage.
+    __shared__ unsigned short pq[kWarps][64];
     __shared__ int2 fq[kWarps][64];
     if (step_void(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1764,7 +1818,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
         if (use_box) rbox = warp_box(my_rp, my_rv);
         __syncwarp();
         // Columns held by the lanes (entry `lane` of a batch) against every row.
-        auto gate_rows = [&](float4 cp, float4 cv, int q, unsigned valid) {
+        auto gate_rows = [&](float4 cp, float4 cv, int q, unsigned valid, bool staged) {
             unsigned need = 0u;
             if (gate_x2) {
 #pragma unroll 2
@@ -1777,12 +1831,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
             need &= valid;
             if (__any_sync(0xffffffffu, need != 0u))
                 exact_rows_f32(need, cp, cv, q, before, orig, rows32[warp], rorig[warp], vmin2e, er, ev, dt_f, gate2,
-                               a, surv, surv_cap, pc, fq[warp], fcount);
+                               a, surv, surv_cap, pc, fq[warp], fcount, qcol[warp], qidx[warp], staged, pq[warp]);
         };
         auto drain = [&](int count) {
             __syncwarp();
             const int e = lane < count ? lane : 0;
-            gate_rows(qcol[warp][e][0], qcol[warp][e][1], qidx[warp][e], lane < count ? qmask[warp][e] : 0u);
+            gate_rows(qcol[warp][e][0], qcol[warp][e][1], qidx[warp][e], lane < count ? qmask[warp][e] : 0u, true);
             __syncwarp();
         };
         int queued = 0;
@@ -1800,7 +1854,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
             }
             const unsigned valid = ok ? (cb == ra ? lanes_below : 0xffffffffu) & nrmask : 0u;
             if (!use_box) {
-                gate_rows(cp, cv, q, valid);
+                gate_rows(cp, cv, q, valid, false);
                 continue;
             }
             Box cbox;

@@ -68,19 +68,22 @@ def test_chunking_and_graph_parity_do_not_change_results(engine):
         assert_same_stats(got[3], base[3])
 
 
-@pytest.mark.parametrize("variant,bps,x2", [(0, 0, 1), (0, 1, 1), (1, 5, 1), (1, 0, 1), (2, 3, 1), (2, 1, 1),
-                                            (2, 0, 0), (2, 3, 0)])
-def test_tuning_knobs_do_not_change_results(engine, variant, bps, x2):
+@pytest.mark.parametrize("variant,bps,x2,s2", [(0, 0, 1, 1), (0, 1, 1, 1), (1, 5, 1, 1), (1, 0, 1, 1), (2, 3, 1, 1),
+                                               (2, 1, 1, 1), (2, 0, 0, 1), (2, 3, 0, 0), (2, 0, 1, 0), (2, 0, 1, 2),
+                                               (2, 3, 0, 2)])
+def test_tuning_knobs_do_not_change_results(engine, variant, bps, x2, s2):
     fx = load("run_dense.npz")
     engine.set_tuning("pair_variant", variant)
     engine.set_tuning("pair_blocks_per_sm", bps)
     engine.set_tuning("pair_gate_x2", x2)
+    engine.set_tuning("pair_stage2", s2)
     try:
         fs, fa, conj, stats = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], int(fx["steps"]))
     finally:
         engine.set_tuning("pair_variant", 2)
         engine.set_tuning("pair_blocks_per_sm", 0)
         engine.set_tuning("pair_gate_x2", 1)
+        engine.set_tuning("pair_stage2", 1)
     assert np.array_equal(fs, fx["final_states"])
     assert_same_conj(conj, fx["conj"])
     assert_same_stats(stats, fx["stats"])
