@@ -311,7 +311,7 @@ void launch_sbm_step(const DeviceBuffers& b, const StepArgs& a, const SbmArgs& s
 void launch_sbm_prepared(const DeviceBuffers& b, const SbmArgs& s, const ForceConsts& fc, int count, int64_t step,
                          double* state, uint8_t* alive, Ctrl* spec, ChunkCtrl* chunk, cudaStream_t stream);
 // Collisions one step can fragment on the device (a step with more fails the run).
-constexpr int kSbmStepEvents = 1024;
+constexpr int kSbmStepEvents = 4096;
 // Sets the kernels' launch attributes (dynamic shared memory); once per device.
 cudaError_t sbm_init_attributes();
 // Index of the key/idx buffer holding the sorted result after `passes` passes.

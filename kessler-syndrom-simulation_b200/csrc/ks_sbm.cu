@@ -36,9 +36,10 @@
 namespace ks {
 namespace {
 
-constexpr int kCollectThreads = 1024;  // k_sbm_collect: one block, one thread per collision
+constexpr int kCollectThreads = 1024;  // k_sbm_collect: one block
+constexpr int kCollectMax = kSbmStepEvents;  // collisions a step can hold (power of two)
 constexpr int kFragWarps = 4;          // k_sbm_fragments: events per block (one warp each)
-constexpr int kDeadSlots = 4096;       // k_sbm_collect: shared table of parents touched this step
+constexpr int kDeadSlots = 2 * kCollectMax;  // k_sbm_collect: shared table of parents touched this step
 constexpr int kDeadProbeLimit = kDeadSlots;
 
 __device__ __forceinline__ unsigned long long enc_pos(double x) {
@@ -100,34 +101,40 @@ __global__ void __launch_bounds__(kCollectThreads) k_sbm_collect(StepArgs a, Sbm
                                                                 int64_t records_cap) {
     extern __shared__ __align__(16) unsigned char collect_smem[];
     CollisionRec* sc = reinterpret_cast<CollisionRec*>(collect_smem);
-    Touched& touched = *reinterpret_cast<Touched*>(sc + kCollectThreads);
+    Touched& touched = *reinterpret_cast<Touched*>(sc + kCollectMax);
     int* ord = reinterpret_cast<int*>(&touched + 1);
     if (step_void(a.ctrl)) return;
     const int E = static_cast<int>(min(a.ctrl->n_coll, static_cast<unsigned int>(a.coll_cap)));
     if (E == 0) return;
     const int t = threadIdx.x;
-    if (t < E) sc[t] = a.coll[t];
-    ord[t] = t;
+    int N = 1;  // sorted length: a power of two >= E
+    while (N < E) N <<= 1;
+    for (int e = t; e < N; e += blockDim.x) {
+        if (e < E) sc[e] = a.coll[e];
+        ord[e] = e;
+    }
     for (int k = t; k < kDeadSlots; k += blockDim.x) touched.key[k] = -1;
     __syncthreads();
     // Bitonic sort of the event order by (t, i, j); padding sorts last.
-    for (int size = 2; size <= kCollectThreads; size <<= 1) {
+    for (int size = 2; size <= N; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const int partner = t ^ stride;
-            if (partner > t) {
-                const int x = ord[t], y = ord[partner];
-                bool x_after_y;
-                if (x >= E) x_after_y = y < E || x > y;
-                else if (y >= E) x_after_y = false;
-                else {
-                    const CollisionRec& cx = sc[x];
-                    const CollisionRec& cy = sc[y];
-                    x_after_y = cx.t != cy.t ? cx.t > cy.t : (cx.i != cy.i ? cx.i > cy.i : cx.j > cy.j);
-                }
-                const bool up = (t & size) == 0;
-                if (x_after_y == up) {
-                    ord[t] = y;
-                    ord[partner] = x;
+            for (int u = t; u < N; u += blockDim.x) {
+                const int partner = u ^ stride;
+                if (partner > u) {
+                    const int x = ord[u], y = ord[partner];
+                    bool x_after_y;
+                    if (x >= E) x_after_y = y < E || x > y;
+                    else if (y >= E) x_after_y = false;
+                    else {
+                        const CollisionRec& cx = sc[x];
+                        const CollisionRec& cy = sc[y];
+                        x_after_y = cx.t != cy.t ? cx.t > cy.t : (cx.i != cy.i ? cx.i > cy.i : cx.j > cy.j);
+                    }
+                    const bool up = (u & size) == 0;
+                    if (x_after_y == up) {
+                        ord[u] = y;
+                        ord[partner] = x;
+                    }
                 }
             }
             __syncthreads();
@@ -135,9 +142,9 @@ __global__ void __launch_bounds__(kCollectThreads) k_sbm_collect(StepArgs a, Sbm
     }
     // Parents at the collision time (src/core/breakup.cpp:324-330).
     const double t0 = a.sp->t0;
-    if (t < E) {
-        const CollisionRec c = sc[ord[t]];
-        SbmEventWork& w = work[t];
+    for (int e = t; e < E; e += blockDim.x) {
+        const CollisionRec c = sc[ord[e]];
+        SbmEventWork& w = work[e];
         const double s = (c.t - t0) / a.dt;
         const int idx[2] = {c.i, c.j};
         for (int p = 0; p < 2; ++p) {
@@ -213,7 +220,9 @@ __global__ void __launch_bounds__(kCollectThreads) k_sbm_collect(StepArgs a, Sbm
     }
 }
 
-constexpr size_t kCollectSmem = sizeof(CollisionRec) * kCollectThreads + sizeof(Touched) + sizeof(int) * kCollectThreads;
+constexpr size_t kCollectSmem = sizeof(CollisionRec) * kCollectMax + sizeof(Touched) + sizeof(int) * kCollectMax;
+static_assert(kCollectSmem <= 227 * 1024, "k_sbm_collect's shared memory");
+static_assert((kCollectMax & (kCollectMax - 1)) == 0, "the bitonic sort needs a power of two");
 
 // Number of candidate fragments of each event (src/core/breakup.cpp:237-244)
 // and the event's record, except its fragment counts.

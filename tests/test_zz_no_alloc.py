@@ -55,9 +55,9 @@ def crossing_groups(per_group):
     k = np.arange(per_group)
     x, z = 0.04 * (k % nx), 0.04 * (k // nx)
     a = np.zeros((per_group, 6))
-    a[:, 0], a[:, 1], a[:, 2], a[:, 4] = 7000.0 + x, -75.0, z, 7.5
+    a[:, 0], a[:, 1], a[:, 2], a[:, 4] = 7000.0 + x, -37.5, z, 7.5
     b = np.zeros((per_group, 6))
-    b[:, 0], b[:, 1], b[:, 2], b[:, 4] = 7000.02 + x, 75.0, 0.02 + z, -7.5
+    b[:, 0], b[:, 1], b[:, 2], b[:, 4] = 7000.02 + x, 37.5, 0.02 + z, -7.5
     before = np.vstack([a, b])
     after = before.copy()
     after[:, :3] += 10.0 * before[:, 3:]
