@@ -1481,6 +1481,10 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     else if (k == "item_col_blocks" && value >= 1 && value <= 64) ctx->tune.item_col_blocks = static_cast<int>(value);
     else if (k == "pair_gate_x2" && (value == 0 || value == 1)) ctx->tune.pair_gate_x2 = static_cast<int>(value);
     else if (k == "pair_stage2" && value >= 0 && value <= 2) ctx->tune.pair_stage2 = static_cast<int>(value);
+    else if (k == "sort_rank_ballot" && (value == 0 || value == 1)) {
+        ctx->tune.sort_rank_ballot = static_cast<int>(value);
+        drop_graphs(ctx);
+    }
     else if (k == "lookback_polls" && value >= 0 && value <= (int64_t(1) << 30)) {
         ctx->tune.lookback_polls = static_cast<int>(value);
         drop_graphs(ctx);  // graphs hold the limit in their kernel arguments

@@ -710,6 +710,22 @@ __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
 
 
 
+// Lanes of the warp holding the same 8-bit digit as this lane, among the lanes
+// with `valid` set: either the hardware match, or eight ballots (one per digit
+// bit) intersected. The ballot form issues more instructions but each has the
+// short latency of a vote.
+__device__ __forceinline__ unsigned digit_peers(unsigned d, bool valid, bool by_ballot) {
+    if (!by_ballot) return __match_any_sync(0xffffffffu, valid ? d : 256u + (threadIdx.x & 31));
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned bal = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bal : ~bal;
+    }
+    return peers;
+}
+
 // Digit histograms of every pass in one read of the keys.
 // only_if_rebuilt: the propagation already counted the digits; recount only
 // if k_fix_keys rebuilt the keys (it cleared the histogram then).
@@ -750,7 +766,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
                                                           const unsigned int* __restrict__ digit_hist,
                                                           unsigned int* __restrict__ status,
                                                           unsigned int* __restrict__ ticket, int* flags,
-                                                          int packed, int poll_limit) {
+                                                          int packed, int poll_limit, int rank_by_ballot) {
     __shared__ unsigned int wcnt[kWarps][256];
     __shared__ int gbase[256];
     __shared__ unsigned long long skeys[kSortTile];
@@ -791,7 +807,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
     for (int r = 0; r < kRounds; ++r) {
         const bool valid = (warp * kPerWarp + r * 32 + lane) < count;
         d[r] = valid ? static_cast<unsigned>((k[r] >> shift) & 0xFF) : 256u + lane;
-        const unsigned peers = __match_any_sync(0xffffffffu, d[r]);
+        const unsigned peers = digit_peers(d[r] & 0xFFu, valid, rank_by_ballot != 0);
         if (valid && lane == __ffs(peers) - 1) wcnt[warp][d[r]] += __popc(peers);
         __syncwarp();
     }
@@ -838,7 +854,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
     }
     for (int r = 0; r < kRounds; ++r) {
         const bool valid = (warp * kPerWarp + r * 32 + lane) < count;
-        const unsigned peers = __match_any_sync(0xffffffffu, d[r]);
+        const unsigned peers = digit_peers(d[r] & 0xFFu, valid, rank_by_ballot != 0);
         if (valid) {
             const unsigned pos = wcnt[warp][d[r]] + __popc(peers & lanemask_lt());
             skeys[pos] = k[r];
@@ -2124,7 +2140,7 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
             b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, a.n_live,
             a.pack_bits + 8 * pass, b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass,
-            b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0, a.tune.lookback_polls);
+            b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0, a.tune.lookback_polls, a.tune.sort_rank_ballot);
     }
 }
 
@@ -2226,7 +2242,7 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
             b.conj_keys[in], nullptr, b.conj_keys[outb], nullptr, cap, &chunk->sort_n, pb + 8 * pass,
             b.conj_hist + 256 * pass, b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass,
-            &chunk->flags, 1, kLookbackLimit);
+            &chunk->flags, 1, kLookbackLimit, 0);
     }
     k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_keys[kPasses & 1], (1ull << pb) - 1, chunk,
                                                          b.conj_sorted);

@@ -201,3 +201,17 @@ def test_partial_takes_return_records_in_order(engine, ks):
     got = np.concatenate(parts)
     assert len(parts[-1]) == 0
     assert_same_conj(got, want)
+
+
+def test_ballot_ranking_of_the_radix_sort_changes_nothing(engine):
+    """The radix sort's warp ranking by eight ballots orders the keys exactly
+    as the hardware match does: the same run, bit for bit."""
+    fx = load("run_mixed.npz")
+    engine.set_tuning("sort_rank_ballot", 1)
+    try:
+        fs, fa, conj, stats = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], 40, spg=7)
+    finally:
+        engine.set_tuning("sort_rank_ballot", 0)
+    assert np.array_equal(fs, fx["final_states"]) and np.array_equal(fa, fx["final_alive"])
+    assert_same_conj(conj, fx["conj"])
+    assert_same_stats(stats, fx["stats"])
