@@ -387,9 +387,10 @@ def traffic_of(kernel, split):
 
 
 def launches_per_step(sort_passes):
-    # propagate, fix_keys, sort (upsweep, one kernel per pass), cells (count,
-    # scan, write, neighbours, item count, scan, item write), pairs, refine
-    return 1 + 1 + (1 + sort_passes) + 7 + 1 + 1
+    # propagate, fix_keys, sort (one kernel per pass; the propagation and, if
+    # it rebuilds keys, k_fix_keys count the digits), cells (count, scan,
+    # write, neighbours, item count, scan, item write), pairs, refine
+    return 1 + 1 + sort_passes + 7 + 1 + 1
 
 
 # Per graph chunk of the timed run: chunk_init and the ordering of the chunk's

@@ -179,7 +179,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.ckpt_state, sizeof(double) * 6 * cap));
     KS_CUDA(cudaMalloc(&b.ckpt_alive, cap));
     b.sort_status_len = 8 * 256 * ((cap + 2047) / 2048);
-    KS_CUDA(cudaMalloc(&b.sort_hist, sizeof(unsigned int) * 8 * 256));
+    KS_CUDA(cudaMalloc(&b.sort_hist, sizeof(unsigned int) * 2 * 8 * 256));  // propagation's counts, then k_fix_keys's
     KS_CUDA(cudaMalloc(&b.sort_status, sizeof(unsigned int) * b.sort_status_len));
     KS_CUDA(cudaMalloc(&b.sort_ctr, sizeof(unsigned int) * 8));
     KS_CUDA(cudaMalloc(&b.block_counts, sizeof(int) * ((cap + 1023) / 1024 + 1)));
@@ -446,7 +446,7 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
         record(ctx, k, 6, capturing);
         if (ctx->l2_flush_bytes > 0) cudaMemsetAsync(ctx->l2_flush, k & 0xFF, ctx->l2_flush_bytes, s);
         record(ctx, k, 0, capturing);
-        if (a.hist) cudaMemsetAsync(a.hist, 0, sizeof(unsigned int) * 8 * 256, s);
+        if (a.hist) cudaMemsetAsync(a.hist, 0, sizeof(unsigned int) * 2 * 8 * 256, s);
         ks::launch_propagate(ctx->b, a, s);
         record(ctx, k, 1, capturing);
         if (ctx->screening) {

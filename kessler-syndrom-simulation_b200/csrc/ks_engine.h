@@ -118,7 +118,8 @@ struct DeviceBuffers {
     uint8_t* ckpt_alive = nullptr;
     unsigned long long* keys[2] = {nullptr, nullptr};
     int* idx[2] = {nullptr, nullptr};
-    unsigned int* sort_hist = nullptr;     // 8 passes x 256 digits (global offsets)
+    unsigned int* sort_hist = nullptr;     // 8 passes x 256 digits (global offsets); in a context, a second
+                                           // 8 x 256 for keys k_fix_keys rebuilt
     unsigned int* sort_status = nullptr;   // look-back words: passes x tiles x 256
     int64_t sort_status_len = 0;
     unsigned int* sort_ctr = nullptr;      // tile tickets, one per pass

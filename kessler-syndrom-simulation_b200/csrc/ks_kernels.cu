@@ -607,19 +607,36 @@ __global__ void __launch_bounds__(kBlock) k_fix_keys(StepArgs a, const double* _
             if (g.bits + 1 > 8 * a.sort_passes) atomicOr(&a.ctrl->flags, FLAG_SORT_BITS);
         }
     }
-    // The propagation's digit histogram described the old keys: clear it for the recount.
-    if (blockIdx.x == 0 && a.hist)
-        for (int t = threadIdx.x; t < a.sort_passes * 256; t += blockDim.x) a.hist[t] = 0u;
+    // The propagation's digit histogram describes the old keys: the rebuilt
+    // keys' digits are counted into the histogram's second half (cleared with
+    // the first before the step), which the sort then reads.
+    __shared__ unsigned int sh_hist[8 * 256];
+    unsigned int* hist_rebuilt = a.hist ? a.hist + 8 * 256 : nullptr;
+    if (hist_rebuilt) hist_zero(sh_hist, a.sort_passes);
     __syncthreads();
     int bad = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    // Warp-uniform loop: the digit counts aggregate over whole warps.
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+        const int i = base + lane;
         unsigned long long key = dead_key(g);
-        if (alive_after[i]) {
-            const double* s = before + 6 * static_cast<int64_t>(i);
-            key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &bad);
-            if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
+        if (i < n) {
+            if (alive_after[i]) {
+                const double* s = before + 6 * static_cast<int64_t>(i);
+                key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &bad);
+                if (a.rec32)
+                    f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
+            }
+            keys[i] = sort_key(key, i, a.pack_bits);
         }
-        keys[i] = sort_key(key, i, a.pack_bits);
+        if (hist_rebuilt) {
+            __syncwarp();
+            warp_hist_add(sh_hist, i < n, key, a.sort_passes, lane);
+        }
+    }
+    if (hist_rebuilt) {
+        __syncthreads();
+        hist_flush(sh_hist, hist_rebuilt, a.sort_passes);
     }
     bad = warp_max(bad);
     if ((threadIdx.x & 31) == 0 && bad) atomicOr(&a.ctrl->flags, FLAG_KEY_RANGE);
@@ -764,6 +781,7 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
                                                           int* __restrict__ idx_out, int n,
                                                           const int* __restrict__ n_dev, int shift,
                                                           const unsigned int* __restrict__ digit_hist,
+                                                          const unsigned int* __restrict__ digit_hist_rebuilt,
                                                           unsigned int* __restrict__ status,
                                                           unsigned int* __restrict__ ticket, int* flags,
                                                           int packed, int poll_limit, int rank_by_ballot) {
@@ -787,7 +805,10 @@ __global__ void __launch_bounds__(kBlock) k_sort_onesweep(const unsigned long lo
     const int count = min(kSortTile, n - tile0);
     // Where each digit's keys start in the output: exclusive scan of the pass's histogram.
     unsigned int hist_total;
-    const unsigned int digit_start = block_exclusive_scan(digit_hist[threadIdx.x], &hist_total);
+    // Keys rebuilt by k_fix_keys after the propagation counted them: their
+    // own digit counts.
+    const unsigned int* hist = (digit_hist_rebuilt && (*flags & FLAG_KEYS_REBUILT)) ? digit_hist_rebuilt : digit_hist;
+    const unsigned int digit_start = block_exclusive_scan(hist[threadIdx.x], &hist_total);
 
     constexpr int kPerWarp = kSortTile / kWarps;
     constexpr int kRounds = kPerWarp / 32;
@@ -2133,13 +2154,17 @@ void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream)
     if (!counted) cudaMemsetAsync(b.sort_hist, 0, sizeof(unsigned int) * 8 * 256, stream);
     cudaMemsetAsync(b.sort_ctr, 0, sizeof(unsigned int) * 8, stream);
     cudaMemsetAsync(b.sort_status, 0, sizeof(unsigned int) * 256 * static_cast<size_t>(ntiles) * passes, stream);
-    k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, a.n_live, passes, b.sort_hist, a.ctrl,
-                                                  counted ? 1 : 0, a.pack_bits);
+    // Counted by the propagation (and, if it rebuilt the keys, by k_fix_keys):
+    // no counting pass of its own.
+    if (!counted)
+        k_sort_upsweep<<<ntiles, kBlock, 0, stream>>>(b.keys[0], n, a.n_live, passes, b.sort_hist, a.ctrl, 0,
+                                                      a.pack_bits);
     for (int pass = 0; pass < passes; ++pass) {
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
             b.keys[in], pass == 0 ? nullptr : b.idx[in], b.keys[outb], b.idx[outb], n, a.n_live,
-            a.pack_bits + 8 * pass, b.sort_hist + 256 * pass, b.sort_status + 256 * static_cast<size_t>(ntiles) * pass,
+            a.pack_bits + 8 * pass, b.sort_hist + 256 * pass, counted ? b.sort_hist + 8 * 256 + 256 * pass : nullptr,
+            b.sort_status + 256 * static_cast<size_t>(ntiles) * pass,
             b.sort_ctr + pass, &a.ctrl->flags, a.pack_bits > 0 ? 1 : 0, a.tune.lookback_polls, a.tune.sort_rank_ballot);
     }
 }
@@ -2241,7 +2266,7 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
         const int in = pass & 1, outb = 1 - in;
         k_sort_onesweep<<<ntiles, kBlock, 0, stream>>>(
             b.conj_keys[in], nullptr, b.conj_keys[outb], nullptr, cap, &chunk->sort_n, pb + 8 * pass,
-            b.conj_hist + 256 * pass, b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass,
+            b.conj_hist + 256 * pass, nullptr, b.conj_status + 256 * static_cast<size_t>(ntiles) * pass, b.conj_ctr + pass,
             &chunk->flags, 1, kLookbackLimit, 0);
     }
     k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_keys[kPasses & 1], (1ull << pb) - 1, chunk,

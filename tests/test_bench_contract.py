@@ -45,8 +45,8 @@ def test_hbm_phases_use_algorithmic_bytes(bench):
 def test_kernel_counts(bench):
     # propagate, fix_keys, upsweep, P passes, cell count, scan, cell write,
     # neighbours, item count, scan, item write, pairs, refine
-    assert bench.launches_per_step(4) == 16
-    assert bench.launches_per_step(5) == 17
+    assert bench.launches_per_step(4) == 15
+    assert bench.launches_per_step(5) == 16
     assert bench.LAUNCHES_PER_CHUNK == 8
 
 
