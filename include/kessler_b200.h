@@ -118,6 +118,8 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * "pair_stage2" (second FP32 stage of the pair kernel, on the pairs the gate
  * flags: 0 row by row over the warp's flagged rows, 1 the default, one pair
  * per lane from a queue when the flags are sparse, 2 always queued),
+ * "prop_min_blocks" (4..6, default 4: resident 128-thread blocks per SM the
+ * FP64 propagation kernel is compiled for; more blocks, fewer registers each),
  * "sort_rank_ballot" (radix-sort ranking within a warp: 0, the default, by
  * the hardware match instruction; 1 by eight ballots, one per digit bit),
  * "lookback_polls" (0..2^30, default 2^22: polls a radix-sort tile makes of a

@@ -1481,6 +1481,7 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     else if (k == "item_col_blocks" && value >= 1 && value <= 64) ctx->tune.item_col_blocks = static_cast<int>(value);
     else if (k == "pair_gate_x2" && (value == 0 || value == 1)) ctx->tune.pair_gate_x2 = static_cast<int>(value);
     else if (k == "pair_stage2" && value >= 0 && value <= 2) ctx->tune.pair_stage2 = static_cast<int>(value);
+    else if (k == "prop_min_blocks" && value >= 4 && value <= 6) ctx->tune.prop_min_blocks = static_cast<int>(value);
     else if (k == "sort_rank_ballot" && (value == 0 || value == 1)) {
         ctx->tune.sort_rank_ballot = static_cast<int>(value);
         drop_graphs(ctx);

@@ -181,6 +181,7 @@ struct Tuning {
     int pair_gate_x2 = 1;         // FP32 pair gate on two rows per instruction (packed f32x2)
     int pair_stage2 = 1;          // second FP32 stage: 0 row by row, 1 compacted when sparse, 2 always compacted
     int sort_rank_ballot = 0;     // radix ranking by eight ballots instead of the hardware match
+    int prop_min_blocks = 4;      // FP64 propagation: resident 128-thread blocks per SM it is compiled for (4..6)
 };
 
 // Time from a fragmentation event to the end of its step and the lunar stages

@@ -344,7 +344,8 @@ __device__ __forceinline__ void hist_flush(const unsigned int* sh, unsigned int*
     }
 }
 
-__global__ void __launch_bounds__(kPropBlock, 4) k_propagate_exact(StepArgs a, const double* __restrict__ in,
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kPropBlock, kMinBlocks) k_propagate_exact(StepArgs a, const double* __restrict__ in,
                                                             double* __restrict__ out,
                                                             const uint8_t* __restrict__ alive_in,
                                                             uint8_t* __restrict__ alive_out,
@@ -2113,8 +2114,19 @@ void launch_propagate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t st
             a, b.state[a.src], b.state[1 - a.src], b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
         return;
     }
-    k_propagate_exact<<<grid_for_block(a.n, 4 * kPropBlock / a.tune.prop_block, a.tune.prop_block), a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
-                                                                b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
+    // Resident blocks per SM of 128 threads: 4 (registers for the whole RK4
+    // in flight) or, by the tuning knob, 5 or 6 (fewer registers, more warps).
+    const int mb = a.tune.prop_min_blocks;
+    const int grid = grid_for_block(a.n, mb * kPropBlock / a.tune.prop_block, a.tune.prop_block);
+    if (mb >= 6)
+        k_propagate_exact<6><<<grid, a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
+                                                                      b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
+    else if (mb == 5)
+        k_propagate_exact<5><<<grid, a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
+                                                                      b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
+    else
+        k_propagate_exact<4><<<grid, a.tune.prop_block, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src],
+                                                                      b.alive[a.src], b.alive[1 - a.src], b.keys[0]);
 }
 
 void launch_advance_spans(const ForceConsts& fc, const FragSpan* spans, const int* row_span, int64_t first,
