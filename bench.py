@@ -539,10 +539,11 @@ def main():
         line["split_error_vs_fp64"] = error_study(ks, eng, a, st, al)
     if not a.no_e2e:
         line["e2e"] = e2e_run(ks, a, st, sz, al, local, barrier, pg, head)
+    # Side workloads report a failure inside the line instead of losing it.
     if not a.no_ensemble:
-        line["ensemble"] = ensemble_run(ks, a, local, barrier, pg, rank)
+        line["ensemble"] = side_run(ensemble_run, ks, a, local, barrier, pg, rank)
     if not a.no_cascade:
-        line["cascade"] = cascade_run(ks, a, local, barrier, pg, rank, st, sz, al)
+        line["cascade"] = side_run(cascade_run, ks, a, local, barrier, pg, rank, st, sz, al)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         base = cpu_baseline(a, st, sz, al, a.cpu_steps)
         line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -555,6 +556,13 @@ def main():
     if pg:
         pg.destroy_process_group()
     return 0
+
+
+def side_run(fn, *args):
+    try:
+        return fn(*args)
+    except Exception as e:  # noqa: BLE001 - reported in the JSON line
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def ensemble_run(ks, a, device, barrier, pg, rank):
