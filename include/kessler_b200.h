@@ -187,7 +187,7 @@ int ks_set_breakup(ks_ctx* ctx, int on, double lc_m, double catastrophic_j_per_g
  * one. Chunks then run through collisions. The population may grow to
  * max_objects objects, the memory budget allocated when the population is
  * set; fragments that would pass it fail the run with KS_ERR_OVERFLOW, as does
- * a step with more than 4096 collisions. Call before ks_set_population(_batch).
+ * a step with more than 16384 collisions (or more than 2048 whose parents collide earlier in the same step). Call before ks_set_population(_batch).
  * ks_autotune, ks_save/load_population, ks_screen and ks_propagate are not
  * available in this mode (KS_ERR_STATE). */
 enum { KS_BREAKUP_HOST = 0, KS_BREAKUP_DEVICE = 1 };

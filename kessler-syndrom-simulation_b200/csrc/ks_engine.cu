@@ -148,7 +148,8 @@ void free_objects(ks_ctx* ctx) {
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted32); dfree(b.rec32); dfree(b.sorted_orig);
     dfree(b.n_live); dfree(b.mass_kg); dfree(b.a2m); dfree(b.event_of); dfree(b.coll); dfree(b.sbm_work);
-    dfree(b.sbm_events); dfree(b.sbm_next_event);
+    dfree(b.sbm_events); dfree(b.sbm_next_event); dfree(b.sbm_order); dfree(b.sbm_first); dfree(b.sbm_pending);
+    dfree(b.sbm_misc);
     if (ctx->h_sbm_events) cudaFreeHost(ctx->h_sbm_events);
     ctx->h_sbm_events = nullptr;
     b.coll_cap = 0;
@@ -209,6 +210,11 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
         KS_CUDA(cudaMalloc(&b.sbm_events, sizeof(ks_breakup_event) * b.sbm_events_cap));
         KS_CUDA(cudaHostAlloc(&ctx->h_sbm_events, sizeof(ks_breakup_event) * b.sbm_events_cap, cudaHostAllocDefault));
         KS_CUDA(cudaMalloc(&b.sbm_next_event, sizeof(int) * 65536));
+        KS_CUDA(cudaMalloc(&b.sbm_order, sizeof(int) * b.coll_cap));
+        KS_CUDA(cudaMalloc(&b.sbm_first, sizeof(int) * cap));
+        KS_CUDA(cudaMemset(b.sbm_first, 0x7F, sizeof(int) * cap));  // "no event yet"
+        KS_CUDA(cudaMalloc(&b.sbm_pending, sizeof(int) * 2048));
+        KS_CUDA(cudaMalloc(&b.sbm_misc, sizeof(int) * 4));
     }
     b.cap = cap;
     return KS_OK;
@@ -415,6 +421,7 @@ ks::SbmArgs sbm_args(const ks_ctx* ctx) {
     s.catastrophic_j_per_g = ctx->bk.params.catastrophic_j_per_g;
     s.seed = ctx->bk.seed;
     s.cap = static_cast<int>(ctx->b.cap);
+    s.realisations = ctx->realisations;
     return s;
 }
 
@@ -649,6 +656,13 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     const int h = ch.halt_step;
     const int done = h < 0 ? k_steps : h;
     const int64_t last_step = ctx->steps_done + done;  // records of steps before this one are complete
+    // Limits met inside a step's fragmentation (after its gate) leave that
+    // step's fragmentation incomplete: the run fails rather than go on.
+    for (int k = 0; k < done; ++k)
+        if (ctx->h_ctrl[k].flags & ks::FLAG_COLL_OVERFLOW)
+            return fail(ctx, KS_ERR_OVERFLOW, "more than 2048 collisions in one step with a parent that collided earlier "
+                                              "in the step, or more breakup records in one chunk than " +
+                                              std::to_string(ctx->b.sbm_events_cap));
     // Conjunction records, ordered on the device; those of the void step are dropped.
     int64_t have = (ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph) ? ctx->graph_spec[ctx->cur]
                                                                                 : ctx->chunk_spec;
@@ -721,8 +735,7 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits");
     if (flags & ks::FLAG_COLL_OVERFLOW)
         return fail(ctx, KS_ERR_OVERFLOW, "more than " + std::to_string(ks::kSbmStepEvents) +
-                                              " collisions in one step, or more breakup records in one chunk than " +
-                                              std::to_string(ctx->b.sbm_events_cap));
+                                              " collisions in one step");
     if (flags & ks::FLAG_PACK_WIDTH) {
         ctx->pack_keys = false;
         drop_graphs(ctx);

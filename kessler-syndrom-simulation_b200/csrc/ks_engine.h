@@ -166,6 +166,10 @@ struct DeviceBuffers {
     ks_breakup_event* sbm_events = nullptr;   // the chunk's breakup records
     int64_t sbm_events_cap = 0;
     int* sbm_next_event = nullptr;         // next event number per realisation
+    int* sbm_order = nullptr;              // a step's collisions in (t, i, j) order (coll_cap)
+    int* sbm_first = nullptr;              // per object: its first event of the step (cap)
+    int* sbm_pending = nullptr;            // a step's events whose parents met an earlier event
+    int* sbm_misc = nullptr;               // [0]: how many of those
 };
 
 // Launch-shape knobs (set through ks_set_tuning; 0 = default).
@@ -269,6 +273,7 @@ struct SbmArgs {
     double catastrophic_j_per_g;
     unsigned long long seed;
     int cap;               // population capacity (memory budget)
+    int realisations;      // realisations of the batch (event numbers are per realisation)
 };
 
 // Kernel launchers (ks_kernels.cu). All enqueue on `stream` and never synchronise.
@@ -314,7 +319,7 @@ void launch_sbm_step(const DeviceBuffers& b, const StepArgs& a, const SbmArgs& s
 void launch_sbm_prepared(const DeviceBuffers& b, const SbmArgs& s, const ForceConsts& fc, int count, int64_t step,
                          double* state, uint8_t* alive, Ctrl* spec, ChunkCtrl* chunk, cudaStream_t stream);
 // Collisions one step can fragment on the device (a step with more fails the run).
-constexpr int kSbmStepEvents = 4096;
+constexpr int kSbmStepEvents = 16384;
 // Sets the kernels' launch attributes (dynamic shared memory); once per device.
 cudaError_t sbm_init_attributes();
 // Index of the key/idx buffer holding the sorted result after `passes` passes.

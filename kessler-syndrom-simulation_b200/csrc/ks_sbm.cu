@@ -14,10 +14,15 @@
 //   launch_step_gate  a step whose buffers overflowed (or whose sort gave up)
 //                     is void: it and every later step of the chunk do nothing
 //                     (FLAG_HALTED), and the host starts the next chunk at it
-//   k_sbm_collect     one block: the step's collisions (listed by the
-//                     refinement) in (t, i, j) order, parents at the collision
-//                     time (Hermite), the sequential part (destroyed parents,
-//                     target roles, eroded masses), event numbers and records
+//   k_sbm_order       one block: the step's collisions (listed by the
+//                     refinement) in (t, i, j) order
+//   k_sbm_parents     parents at the collision time (Hermite); each object's
+//                     first event of the step
+//   k_sbm_simple      events whose parents meet no earlier event: decided in
+//                     parallel (roles, catastrophic test, budgets, fates)
+//   k_sbm_conflicts   one block: the other events, in order, on the parents'
+//                     state the earlier events left
+//   k_sbm_number      one block: event numbers per realisation and records
 //   k_sbm_prepare     one thread per event: the Poisson number of candidates
 //   k_sbm_fragments   one warp per event, run twice: first counting the
 //                     fragments each event keeps, then (after k_sbm_place)
@@ -36,11 +41,8 @@
 namespace ks {
 namespace {
 
-constexpr int kCollectThreads = 1024;  // k_sbm_collect: one block
-constexpr int kCollectMax = kSbmStepEvents;  // collisions a step can hold (power of two)
-constexpr int kFragWarps = 4;          // k_sbm_fragments: events per block (one warp each)
-constexpr int kDeadSlots = 2 * kCollectMax;  // k_sbm_collect: shared table of parents touched this step
-constexpr int kDeadProbeLimit = kDeadSlots;
+constexpr int kFragWarps = 4;             // k_sbm_fragments: warps per block, one event at a time each
+constexpr int kNumberRealisations = 16384;  // k_sbm_number: realisations counted in shared memory
 
 __device__ __forceinline__ unsigned long long enc_pos(double x) {
     const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
@@ -75,88 +77,120 @@ __device__ MoonStage moon_at(const MoonStage* m, double tau) {
     return o;
 }
 
-// Shared table of the parents touched by this step's events: dead, or eroded
-// to a new mass. Open addressing on the object index; one thread uses it.
-struct Touched {
-    int key[kDeadSlots];
-    double mass[kDeadSlots];  // < 0: destroyed
-    __device__ int find(int idx) const {
-        unsigned h = (static_cast<unsigned>(idx) * 2654435761u) & (kDeadSlots - 1);
-        for (int p = 0; p < kDeadProbeLimit; ++p) {
-            if (key[h] == idx || key[h] == -1) return h;
-            h = (h + 1) & (kDeadSlots - 1);
-        }
-        return -1;
+// The fate of an event's parents and its roles (src/core/breakup.cpp:198-230):
+// masses mi, mj of the objects c.i, c.j now (0 or less: unknown, 100 kg), the
+// heavier is the target (ties: the first object), relative speed, specific
+// energy, catastrophic test, mass budgets.
+__device__ void decide_event(SbmEventWork& w, double mi, double mj, const SbmArgs& sa) {
+    if (mi <= 0.0) mi = kSbmFallbackMassKg;
+    if (mj <= 0.0) mj = kSbmFallbackMassKg;
+    w.mass[0] = mi;
+    w.mass[1] = mj;
+    if (!(mi >= mj)) {
+        for (int q = 0; q < 6; ++q) { const double x = w.s[0][q]; w.s[0][q] = w.s[1][q]; w.s[1][q] = x; }
+        double x = w.size_m[0]; w.size_m[0] = w.size_m[1]; w.size_m[1] = x;
+        x = w.mass[0]; w.mass[0] = w.mass[1]; w.mass[1] = x;
+        const int k = w.target; w.target = w.projectile; w.projectile = k;
     }
-};
+    double dv2 = 0.0;
+    for (int q = 3; q < 6; ++q) dv2 += (w.s[0][q] - w.s[1][q]) * (w.s[0][q] - w.s[1][q]);
+    w.vrel = sqrt(dv2);
+    const double energy = 500.0 * w.mass[1] * w.vrel * w.vrel / w.mass[0];
+    w.catastrophic = energy >= sa.catastrophic_j_per_g ? 1 : 0;
+    w.budget[0] = w.catastrophic ? w.mass[0] : fmax(0.0, w.mass[1] * w.vrel * w.vrel - w.mass[1]);
+    w.budget[1] = w.mass[1];
+}
 
-// The step's collisions into events. Tail of the sequential part of the
-// reference's loop (src/core/breakup.cpp:320-336, 192-230).
-__global__ void __launch_bounds__(kCollectThreads) k_sbm_collect(StepArgs a, SbmArgs sa, const double* __restrict__ before,
-                                                                const double* __restrict__ after,
-                                                                uint8_t* __restrict__ alive_after,
-                                                                const double* __restrict__ size_m, double* mass_kg,
-                                                                const uint16_t* __restrict__ real_id, int* next_event,
-                                                                SbmEventWork* work, ks_breakup_event* records,
-                                                                int64_t records_cap) {
-    extern __shared__ __align__(16) unsigned char collect_smem[];
-    CollisionRec* sc = reinterpret_cast<CollisionRec*>(collect_smem);
-    Touched& touched = *reinterpret_cast<Touched*>(sc + kCollectMax);
-    int* ord = reinterpret_cast<int*>(&touched + 1);
+constexpr int kOrderThreads = 1024;
+constexpr int kConflictMax = 2048;     // events per step whose parent met an earlier event of the step
+constexpr int kConflictSlots = 8192;   // shared table of those events' parents (power of two)
+constexpr int kNoEvent = 0x7F7F7F7F;   // "no event yet" in the per-object first-event array
+constexpr int kValidEvent = -2;        // an event that fragments, before its number is given
+
+// Order of the step's collisions by (t, i, j) (src/core/breakup.cpp:320, the
+// order Screener::finish sorts them in): 64-bit keys, the collision time as a
+// fraction of the step in 50 bits above the collision's index, sorted in
+// shared memory; runs with equal 50-bit times are put in exact (t, i, j) order.
+__global__ void __launch_bounds__(kOrderThreads) k_sbm_order(StepArgs a, int* order, int* misc) {
+    extern __shared__ unsigned long long okeys[];
     if (step_void(a.ctrl)) return;
-    const int E = static_cast<int>(min(a.ctrl->n_coll, static_cast<unsigned int>(a.coll_cap)));
+    const unsigned int n_coll = a.ctrl->n_coll;
+    const int E = static_cast<int>(min(n_coll, static_cast<unsigned int>(a.coll_cap)));
+    if (threadIdx.x == 0) misc[0] = 0;  // conflicting events of this step
     if (E == 0) return;
-    const int t = threadIdx.x;
-    int N = 1;  // sorted length: a power of two >= E
+    const double t0 = a.sp->t0;
+    int N = 1;
     while (N < E) N <<= 1;
-    for (int e = t; e < N; e += blockDim.x) {
-        if (e < E) sc[e] = a.coll[e];
-        ord[e] = e;
+    for (int u = threadIdx.x; u < N; u += blockDim.x) {
+        unsigned long long k = ~0ull;
+        if (u < E) {
+            double f = (a.coll[u].t - t0) / a.dt;
+            f = fmin(fmax(f, 0.0), 1.0 - 1e-15);
+            k = (static_cast<unsigned long long>(f * 1125899906842624.0) << 14) | static_cast<unsigned long long>(u);
+        }
+        okeys[u] = k;
     }
-    for (int k = t; k < kDeadSlots; k += blockDim.x) touched.key[k] = -1;
     __syncthreads();
-    // Bitonic sort of the event order by (t, i, j); padding sorts last.
     for (int size = 2; size <= N; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int u = t; u < N; u += blockDim.x) {
+            for (int u = threadIdx.x; u < N; u += blockDim.x) {
                 const int partner = u ^ stride;
                 if (partner > u) {
-                    const int x = ord[u], y = ord[partner];
-                    bool x_after_y;
-                    if (x >= E) x_after_y = y < E || x > y;
-                    else if (y >= E) x_after_y = false;
-                    else {
-                        const CollisionRec& cx = sc[x];
-                        const CollisionRec& cy = sc[y];
-                        x_after_y = cx.t != cy.t ? cx.t > cy.t : (cx.i != cy.i ? cx.i > cy.i : cx.j > cy.j);
-                    }
+                    const unsigned long long x = okeys[u], y = okeys[partner];
                     const bool up = (u & size) == 0;
-                    if (x_after_y == up) {
-                        ord[u] = y;
-                        ord[partner] = x;
+                    if ((x > y) == up) {
+                        okeys[u] = y;
+                        okeys[partner] = x;
                     }
                 }
             }
             __syncthreads();
         }
     }
-    // Parents at the collision time (src/core/breakup.cpp:324-330).
+    if (threadIdx.x == 0) {
+        // Equal 50-bit times (ties or nearly): insertion by the exact (t, i, j).
+        for (int p = 1; p < E; ++p) {
+            if ((okeys[p] >> 14) != (okeys[p - 1] >> 14)) continue;
+            const unsigned long long v = okeys[p];
+            const CollisionRec cv = a.coll[v & 0x3FFFull];
+            int q = p;
+            while (q > 0 && (okeys[q - 1] >> 14) == (v >> 14)) {
+                const CollisionRec cq = a.coll[okeys[q - 1] & 0x3FFFull];
+                const bool after = cq.t != cv.t ? cq.t > cv.t : (cq.i != cv.i ? cq.i > cv.i : cq.j > cv.j);
+                if (!after) break;
+                okeys[q] = okeys[q - 1];
+                --q;
+            }
+            okeys[q] = v;
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < E; p += blockDim.x) order[p] = static_cast<int>(okeys[p] & 0x3FFFull);
+}
+
+// Parents at the collision time (src/core/breakup.cpp:324-330) and each
+// object's first event of the step.
+__global__ void k_sbm_parents(StepArgs a, const double* __restrict__ before, const double* __restrict__ after,
+                              const double* __restrict__ size_m, const double* __restrict__ mass_kg,
+                              const uint16_t* __restrict__ real_id, const int* __restrict__ order, SbmEventWork* work,
+                              int* first) {
+    if (step_void(a.ctrl)) return;
+    const int E = static_cast<int>(min(a.ctrl->n_coll, static_cast<unsigned int>(a.coll_cap)));
     const double t0 = a.sp->t0;
-    for (int e = t; e < E; e += blockDim.x) {
-        const CollisionRec c = sc[ord[e]];
-        SbmEventWork& w = work[e];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += gridDim.x * blockDim.x) {
+        const CollisionRec c = a.coll[order[p]];
+        SbmEventWork& w = work[p];
         const double s = (c.t - t0) / a.dt;
         const int idx[2] = {c.i, c.j};
-        for (int p = 0; p < 2; ++p) {
+        for (int q2 = 0; q2 < 2; ++q2) {
             double b6[6], a6[6];
             for (int q = 0; q < 6; ++q) {
-                b6[q] = before[6 * static_cast<int64_t>(idx[p]) + q];
-                a6[q] = after[6 * static_cast<int64_t>(idx[p]) + q];
+                b6[q] = before[6 * static_cast<int64_t>(idx[q2]) + q];
+                a6[q] = after[6 * static_cast<int64_t>(idx[q2]) + q];
             }
-            hermite_state(b6, a6, a.dt, s, w.s[p]);
-            w.size_m[p] = size_m[idx[p]];
-            const double m = mass_kg[idx[p]];
-            w.mass[p] = m > 0.0 ? m : kSbmFallbackMassKg;
+            hermite_state(b6, a6, a.dt, s, w.s[q2]);
+            w.size_m[q2] = size_m[idx[q2]];
+            w.mass[q2] = mass_kg[idx[q2]];
         }
         w.target = c.i;
         w.projectile = c.j;
@@ -164,76 +198,187 @@ __global__ void __launch_bounds__(kCollectThreads) k_sbm_collect(StepArgs a, Sbm
         w.rem = t0 + a.dt - c.t;
         w.realisation = real_id ? real_id[c.i] : 0;
         w.id = -1;
+        w.record = -1;
+        atomicMin(&first[c.i], p);
+        atomicMin(&first[c.j], p);
+    }
+}
+
+// Events whose parents meet no earlier event of the step are independent of
+// every other: decided and applied in parallel. The rest are listed for the
+// ordered pass.
+__global__ void k_sbm_simple(StepArgs a, SbmArgs sa, uint8_t* alive_after, double* mass_kg, SbmEventWork* work,
+                             const int* __restrict__ first, int* misc, int* pending) {
+    if (step_void(a.ctrl)) return;
+    const int E = static_cast<int>(min(a.ctrl->n_coll, static_cast<unsigned int>(a.coll_cap)));
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += gridDim.x * blockDim.x) {
+        SbmEventWork& w = work[p];
+        if (first[w.target] == p && first[w.projectile] == p) {
+            decide_event(w, w.mass[0], w.mass[1], sa);
+            alive_after[w.projectile] = 0;
+            if (w.catastrophic) alive_after[w.target] = 0;
+            else mass_kg[w.target] = fmax(w.mass[0] - w.budget[0], 0.0);
+            w.id = kValidEvent;
+        } else {
+            const int k = atomicAdd(&misc[0], 1);
+            if (k < kConflictMax) pending[k] = p;
+            else atomicOr(&a.ctrl->flags, FLAG_COLL_OVERFLOW);
+        }
+    }
+}
+
+// Shared table of the parents of conflicting events: alive flag and mass now.
+struct ConflictTable {
+    int key[kConflictSlots];
+    double mass[kConflictSlots];
+    uint8_t alive[kConflictSlots];
+    __device__ int find(int idx) const {
+        unsigned h = (static_cast<unsigned>(idx) * 2654435761u) & (kConflictSlots - 1);
+        for (int p = 0; p < kConflictSlots; ++p) {
+            if (key[h] == idx || key[h] == -1) return static_cast<int>(h);
+            h = (h + 1) & (kConflictSlots - 1);
+        }
+        return -1;
+    }
+};
+
+// The conflicting events in order, one thread, on the parents' state as the
+// parallel events left it: a parent destroyed earlier in the step cannot
+// collide again (src/core/breakup.cpp:322-323), an eroded one collides with
+// its remaining mass.
+__global__ void __launch_bounds__(kOrderThreads) k_sbm_conflicts(StepArgs a, SbmArgs sa, uint8_t* alive_after,
+                                                                 double* mass_kg, SbmEventWork* work,
+                                                                 const int* misc, const int* pending_in) {
+    extern __shared__ __align__(16) unsigned char conflict_smem[];
+    ConflictTable& tab = *reinterpret_cast<ConflictTable*>(conflict_smem);
+    int* plist = reinterpret_cast<int*>(conflict_smem + sizeof(ConflictTable));
+    if (step_void(a.ctrl)) return;
+    const int P = min(misc[0], kConflictMax);
+    if (P == 0) return;
+    int N = 1;
+    while (N < P) N <<= 1;
+    for (int u = threadIdx.x; u < N; u += blockDim.x) plist[u] = u < P ? pending_in[u] : 0x7FFFFFFF;
+    for (int k = threadIdx.x; k < kConflictSlots; k += blockDim.x) tab.key[k] = -1;
+    __syncthreads();
+    for (int size = 2; size <= N; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int u = threadIdx.x; u < N; u += blockDim.x) {
+                const int partner = u ^ stride;
+                if (partner > u) {
+                    const int x = plist[u], y = plist[partner];
+                    const bool up = (u & size) == 0;
+                    if ((x > y) == up) {
+                        plist[u] = y;
+                        plist[partner] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // The parents into the table (at most 2 P <= 4096 keys in 8192 slots).
+    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) {
+        const SbmEventWork& w = work[plist[k >> 1]];
+        const int idx = (k & 1) ? w.projectile : w.target;
+        unsigned h = (static_cast<unsigned>(idx) * 2654435761u) & (kConflictSlots - 1);
+        for (int probe = 0; probe < kConflictSlots; ++probe) {
+            const int prev = atomicCAS(&tab.key[h], -1, idx);
+            if (prev == -1 || prev == idx) break;
+            h = (h + 1) & (kConflictSlots - 1);
+        }
     }
     __syncthreads();
-    // The order-dependent part, one thread: destroyed parents, roles, masses.
-    if (t == 0) {
+    for (int k = threadIdx.x; k < kConflictSlots; k += blockDim.x) {
+        const int idx = tab.key[k];
+        if (idx < 0) continue;
+        tab.alive[k] = alive_after[idx];
+        tab.mass[k] = mass_kg[idx];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < P; ++k) {
+            SbmEventWork& w = work[plist[k]];
+            const int hi = tab.find(w.target), hj = tab.find(w.projectile);
+            if (hi < 0 || hj < 0 || !tab.alive[hi] || !tab.alive[hj]) continue;  // destroyed earlier
+            const int i0 = w.target;
+            decide_event(w, tab.mass[hi], tab.mass[hj], sa);
+            const int ht = w.target == i0 ? hi : hj, hp = w.target == i0 ? hj : hi;
+            tab.alive[hp] = 0;
+            if (w.catastrophic) tab.alive[ht] = 0;
+            else tab.mass[ht] = fmax(w.mass[0] - w.budget[0], 0.0);
+            w.id = kValidEvent;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kConflictSlots; k += blockDim.x) {
+        const int idx = tab.key[k];
+        if (idx < 0) continue;
+        alive_after[idx] = tab.alive[k];
+        mass_kg[idx] = tab.mass[k];
+    }
+}
+
+// Event numbers (per realisation, in event order) and record slots of the
+// step's events; the per-object first-event marks are cleared for the next
+// step.
+__global__ void __launch_bounds__(kOrderThreads) k_sbm_number(StepArgs a, SbmEventWork* work, int* next_event,
+                                                              int* first, int64_t records_cap, int n_real) {
+    extern __shared__ __align__(16) unsigned char number_smem[];
+    uint8_t* valid = number_smem;                                         // kSbmStepEvents
+    uint16_t* real = reinterpret_cast<uint16_t*>(number_smem + kSbmStepEvents);  // kSbmStepEvents
+    int* counter = reinterpret_cast<int*>(number_smem + 3 * kSbmStepEvents);     // kNumberRealisations
+    if (step_void(a.ctrl)) return;
+    const int E = static_cast<int>(min(a.ctrl->n_coll, static_cast<unsigned int>(a.coll_cap)));
+    if (E == 0) return;
+    const bool few = n_real <= kNumberRealisations;
+    for (int p = threadIdx.x; p < E; p += blockDim.x) {
+        const SbmEventWork& w = work[p];
+        valid[p] = w.id == kValidEvent ? 1 : 0;
+        real[p] = static_cast<uint16_t>(w.realisation);
+        first[w.target] = kNoEvent;
+        first[w.projectile] = kNoEvent;
+    }
+    if (few)
+        for (int r = threadIdx.x; r < n_real; r += blockDim.x) counter[r] = next_event[r];
+    __syncthreads();
+    if (threadIdx.x == 0) {
         int nv = 0;
         const int base = static_cast<int>(a.chunk->events);
-        for (int e = 0; e < E; ++e) {
-            SbmEventWork& w = work[e];
-            const int hi = touched.find(w.target), hj = touched.find(w.projectile);
-            if (hi < 0 || hj < 0) { atomicOr(&a.ctrl->flags, FLAG_COLL_OVERFLOW); break; }
-            const bool dead_i = touched.key[hi] == w.target && touched.mass[hi] < 0.0;
-            const bool dead_j = touched.key[hj] == w.projectile && touched.mass[hj] < 0.0;
-            if (dead_i || dead_j) continue;  // destroyed earlier in this step
-            double mi = touched.key[hi] == w.target ? touched.mass[hi] : w.mass[0];
-            double mj = touched.key[hj] == w.projectile ? touched.mass[hj] : w.mass[1];
-            if (mi <= 0.0) mi = kSbmFallbackMassKg;
-            if (mj <= 0.0) mj = kSbmFallbackMassKg;
-            w.mass[0] = mi;
-            w.mass[1] = mj;
-            if (!(mi >= mj)) {  // the heavier body is the target (ties: the first object)
-                for (int q = 0; q < 6; ++q) { const double x = w.s[0][q]; w.s[0][q] = w.s[1][q]; w.s[1][q] = x; }
-                double x = w.size_m[0]; w.size_m[0] = w.size_m[1]; w.size_m[1] = x;
-                x = w.mass[0]; w.mass[0] = w.mass[1]; w.mass[1] = x;
-                const int k = w.target; w.target = w.projectile; w.projectile = k;
+        for (int p = 0; p < E; ++p) {
+            if (!valid[p]) continue;
+            SbmEventWork& w = work[p];
+            if (base + nv >= records_cap) {
+                atomicOr(&a.ctrl->flags, FLAG_COLL_OVERFLOW);
+                w.id = -1;
+                continue;
             }
-            double dv2 = 0.0;
-            for (int q = 3; q < 6; ++q) dv2 += (w.s[0][q] - w.s[1][q]) * (w.s[0][q] - w.s[1][q]);
-            w.vrel = sqrt(dv2);
-            const double energy = 500.0 * w.mass[1] * w.vrel * w.vrel / w.mass[0];
-            w.catastrophic = energy >= sa.catastrophic_j_per_g ? 1 : 0;
-            w.budget[0] = w.catastrophic ? w.mass[0] : fmax(0.0, w.mass[1] * w.vrel * w.vrel - w.mass[1]);
-            w.budget[1] = w.mass[1];
-            // Parents' fate, seen by the later events of this step.
-            const int ht = touched.find(w.target), hp = touched.find(w.projectile);
-            if (ht < 0 || hp < 0) { atomicOr(&a.ctrl->flags, FLAG_COLL_OVERFLOW); break; }
-            touched.key[hp] = w.projectile;
-            touched.mass[hp] = -1.0;
-            touched.key[ht] = w.target;
-            touched.mass[ht] = w.catastrophic ? -1.0 : fmax(w.mass[0] - w.budget[0], 0.0);
-            w.id = next_event[w.realisation]++;
-            w.record = base + nv;
-            if (base + nv >= records_cap) { atomicOr(&a.ctrl->flags, FLAG_COLL_OVERFLOW); w.id = -1; break; }
-            ++nv;
+            w.id = few ? counter[real[p]]++ : next_event[real[p]]++;
+            w.record = base + nv++;
         }
         a.chunk->events = static_cast<unsigned int>(base + nv);
     }
     __syncthreads();
-    // Write the parents' fate for the next step.
-    for (int k = t; k < kDeadSlots; k += blockDim.x) {
-        const int idx = touched.key[k];
-        if (idx < 0) continue;
-        if (touched.mass[k] < 0.0) alive_after[idx] = 0;
-        else mass_kg[idx] = touched.mass[k];
-    }
+    if (few)
+        for (int r = threadIdx.x; r < n_real; r += blockDim.x) next_event[r] = counter[r];
 }
 
-constexpr size_t kCollectSmem = sizeof(CollisionRec) * kCollectMax + sizeof(Touched) + sizeof(int) * kCollectMax;
-static_assert(kCollectSmem <= 227 * 1024, "k_sbm_collect's shared memory");
-static_assert((kCollectMax & (kCollectMax - 1)) == 0, "the bitonic sort needs a power of two");
+constexpr size_t kOrderSmem = sizeof(unsigned long long) * kSbmStepEvents;
+constexpr size_t kConflictSmem = sizeof(ConflictTable) + sizeof(int) * kConflictMax;
+constexpr size_t kNumberSmem = 3 * kSbmStepEvents + sizeof(int) * kNumberRealisations;
+static_assert(kOrderSmem <= 227 * 1024 && kConflictSmem <= 227 * 1024 && kNumberSmem <= 227 * 1024,
+              "shared memory of the device SBM's ordering kernels");
+static_assert((kSbmStepEvents & (kSbmStepEvents - 1)) == 0 && kSbmStepEvents <= 16384,
+              "collision indices take 14 bits of the ordering keys");
 
 // Number of candidate fragments of each event (src/core/breakup.cpp:237-244)
 // and the event's record, except its fragment counts.
 __global__ void k_sbm_prepare(const Ctrl* ctrl, int count, SbmArgs sa, const StepParams* sp, int64_t step,
                               SbmEventWork* work, ks_breakup_event* records) {
     if (ctrl && step_void(ctrl)) return;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int E = ctrl ? static_cast<int>(min(ctrl->n_coll, static_cast<unsigned int>(count))) : count;
-    if (e >= E) return;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
     SbmEventWork& w = work[e];
-    if (w.id < 0) return;
+    if (w.id < 0) continue;
     const double M = w.budget[0] + w.budget[1];
     w.expected = M > 0.0 ? 0.1 * pow(M, 0.75) * pow(sa.lc_m, -kSbmExponent) : 0.0;
     EventStream g{sa.seed + static_cast<unsigned long long>(w.realisation), static_cast<uint32_t>(w.id)};
@@ -262,6 +407,7 @@ __global__ void k_sbm_prepare(const Ctrl* ctrl, int count, SbmArgs sa, const Ste
     r.expected_fragments = w.expected;
     r.fragments_mass_kg = 0.0;
     for (int q = 0; q < 3; ++q) r.position[q] = w.s[0][q];
+    }
 }
 
 // Where a pass of k_sbm_fragments sends a kept fragment.
@@ -289,11 +435,10 @@ __global__ void __launch_bounds__(32 * kFragWarps) k_sbm_fragments(const Ctrl* c
     if (ctrl && step_void(ctrl)) return;
     if (sink.state && chunk && (chunk->flags & FLAG_POP_BUDGET)) return;
     const int lane = threadIdx.x & 31;
-    const int e = blockIdx.x * kFragWarps + (threadIdx.x >> 5);
     const int E = ctrl ? static_cast<int>(min(ctrl->n_coll, static_cast<unsigned int>(count))) : count;
-    if (e >= E) return;
+    for (int e = blockIdx.x * kFragWarps + (threadIdx.x >> 5); e < E; e += gridDim.x * kFragWarps) {
     SbmEventWork& w = work[e];
-    if (w.id < 0) return;
+    if (w.id < 0) continue;
     const uint64_t seed = sa.seed + static_cast<unsigned long long>(w.realisation);
     const double p_target = (w.budget[0] + w.budget[1]) > 0.0 ? w.budget[0] / (w.budget[0] + w.budget[1]) : 0.0;
     double used[2] = {0.0, 0.0};
@@ -383,6 +528,7 @@ __global__ void __launch_bounds__(32 * kFragWarps) k_sbm_fragments(const Ctrl* c
         w.kept = kept;
         w.escaped = escaped;
         w.kept_mass = kept_mass;
+    }
     }
 }
 
@@ -479,8 +625,15 @@ FragmentSink make_sink(const DeviceBuffers& b, double* state, uint8_t* alive, Ct
 }  // namespace
 
 cudaError_t sbm_init_attributes() {
-    return cudaFuncSetAttribute(k_sbm_collect, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kCollectSmem));
+    cudaError_t e = cudaFuncSetAttribute(k_sbm_order, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kOrderSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sbm_conflicts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kConflictSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sbm_number, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kNumberSmem));
+    return e;
 }
 
 void launch_step_gate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
@@ -489,24 +642,30 @@ void launch_step_gate(const DeviceBuffers& b, const StepArgs& a, cudaStream_t st
 
 void launch_sbm_step(const DeviceBuffers& b, const StepArgs& a, const SbmArgs& s, cudaStream_t stream) {
     const int cap = b.coll_cap;
-    k_sbm_collect<<<1, kCollectThreads, kCollectSmem, stream>>>(a, s, b.state[a.src], b.state[1 - a.src], b.alive[1 - a.src],
-                                                     b.size_m, b.mass_kg, a.real_id, b.sbm_next_event, b.sbm_work,
-                                                     b.sbm_events, b.sbm_events_cap);
-    k_sbm_prepare<<<(cap + 127) / 128, 128, 0, stream>>>(a.ctrl, cap, s, a.sp, -1, b.sbm_work, b.sbm_events);
-    const int blocks = (cap + kFragWarps - 1) / kFragWarps;
+    const int blocks = sm_count() * 2;
+    k_sbm_order<<<1, kOrderThreads, kOrderSmem, stream>>>(a, b.sbm_order, b.sbm_misc);
+    k_sbm_parents<<<blocks, 128, 0, stream>>>(a, b.state[a.src], b.state[1 - a.src], b.size_m, b.mass_kg, a.real_id,
+                                              b.sbm_order, b.sbm_work, b.sbm_first);
+    k_sbm_simple<<<blocks, 128, 0, stream>>>(a, s, b.alive[1 - a.src], b.mass_kg, b.sbm_work, b.sbm_first,
+                                             b.sbm_misc, b.sbm_pending);
+    k_sbm_conflicts<<<1, kOrderThreads, kConflictSmem, stream>>>(a, s, b.alive[1 - a.src], b.mass_kg, b.sbm_work,
+                                                                 b.sbm_misc, b.sbm_pending);
+    k_sbm_number<<<1, kOrderThreads, kNumberSmem, stream>>>(a, b.sbm_work, b.sbm_next_event, b.sbm_first,
+                                                           b.sbm_events_cap, s.realisations);
+    k_sbm_prepare<<<blocks, 128, 0, stream>>>(a.ctrl, cap, s, a.sp, -1, b.sbm_work, b.sbm_events);
     FragmentSink count_only{};
     count_only.fc = a.fc;
-    k_sbm_fragments<<<blocks, 32 * kFragWarps, 0, stream>>>(a.ctrl, cap, s, b.sbm_work, count_only, a.chunk);
+    k_sbm_fragments<<<blocks * 2, 32 * kFragWarps, 0, stream>>>(a.ctrl, cap, s, b.sbm_work, count_only, a.chunk);
     k_sbm_place<<<1, 1024, 0, stream>>>(a.ctrl, cap, s, b.sbm_work, b.sbm_events, b.n_live, a.chunk);
     const FragmentSink sink = make_sink(b, b.state[1 - a.src], b.alive[1 - a.src], a.ctrl_next, a.sp, a.dt, a.fc);
-    k_sbm_fragments<<<blocks, 32 * kFragWarps, 0, stream>>>(a.ctrl, cap, s, b.sbm_work, sink, a.chunk);
+    k_sbm_fragments<<<blocks * 2, 32 * kFragWarps, 0, stream>>>(a.ctrl, cap, s, b.sbm_work, sink, a.chunk);
 }
 
 void launch_sbm_prepared(const DeviceBuffers& b, const SbmArgs& s, const ForceConsts& fc, int count, int64_t step,
                          double* state, uint8_t* alive, Ctrl* spec, ChunkCtrl* chunk, cudaStream_t stream) {
     if (count <= 0) return;
     k_sbm_prepare<<<(count + 127) / 128, 128, 0, stream>>>(nullptr, count, s, nullptr, step, b.sbm_work, b.sbm_events);
-    const int blocks = (count + kFragWarps - 1) / kFragWarps;
+    const int blocks = (count + kFragWarps - 1) / kFragWarps;  // one warp per event
     FragmentSink count_only{};
     count_only.fc = fc;
     k_sbm_fragments<<<blocks, 32 * kFragWarps, 0, stream>>>(nullptr, count, s, b.sbm_work, count_only, chunk);

@@ -214,3 +214,63 @@ def test_device_population_budget_is_enforced(ks):
         assert e.value.code == 5 and "budget" in str(e.value)
         with pytest.raises(ks.KsError):
             eng.save_population("/nonexistent/never-written.kspop")
+
+
+def swarm_population(ks, per_target=300, seed=3):
+    """4 LEO targets (10 m, 1 000 kg), each crossed inside one 10 s step by
+    per_target small objects (0.1 m) at 10 km/s from random directions, at
+    distinct times: thousands of collisions in one step, most of them with a
+    parent that collided earlier in the step. Targets 0-1: 1 kg projectiles
+    (catastrophic: the first hit destroys the target, later hits are void);
+    targets 2-3: 50 g projectiles (cratering: every hit erodes the target)."""
+    rng = np.random.default_rng(seed)
+    st, sz, al = ks.generate_population(seed, 400)
+    leo = np.flatnonzero(np.linalg.norm(st[:, :3], axis=1) < 6378.137 + 1500.0)[:4]
+    states, sizes, masses = [st[leo]], [np.full(4, 10.0)], [np.full(4, 1000.0)]
+    for k in range(4):
+        d = rng.normal(size=(per_target, 3))
+        d *= 10.0 / np.linalg.norm(d, axis=1)[:, None]
+        tk = np.sort(rng.uniform(0.5, 9.5, per_target))
+        s = np.zeros((per_target, 6))
+        s[:, :3] = st[leo[k], :3] - d * tk[:, None]
+        s[:, 3:] = st[leo[k], 3:] + d
+        states.append(s)
+        sizes.append(np.full(per_target, 0.1))
+        masses.append(np.full(per_target, 1.0 if k < 2 else 0.05))
+    return np.vstack(states), np.concatenate(sizes), np.concatenate(masses)
+
+
+def test_device_conflicting_collisions_follow_the_reference_order(ks):
+    st, sz, mass = swarm_population(ks)
+
+    def one_step(mode):
+        with ks.Engine(0) as eng:
+            if mode == ks.BREAKUP_DEVICE:
+                eng.set_breakup_mode(mode, len(st) + 2_000_000)
+            eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
+            eng.set_screening(True, 5.0, 10.0, 0.01)  # radii x10: the hits are certain
+            eng.set_population(st, sz)
+            eng.set_masses(mass)
+            eng.set_breakup(True, 0.10, 40.0, 5)
+            eng.run(1)
+            conj = eng.take_conjunctions()
+            return conj, eng.take_breakups(), eng.get_population()[1]
+
+    hc, he, ha = one_step(ks.BREAKUP_HOST)
+    dc, de, da = one_step(ks.BREAKUP_DEVICE)
+    assert int(hc["collision"].sum()) == int(dc["collision"].sum()) > 1024
+    # Catastrophic swarms: one event each; cratering swarms: every hit.
+    assert len(de) == len(he)
+    for k, want in ((0, 1), (1, 1), (2, 300), (3, 300)):
+        assert int((he["target"] == k).sum()) == want, k
+    for f in ("t", "target", "projectile", "catastrophic"):
+        assert np.array_equal(de[f], he[f]), f
+    for f in ("target_mass_kg", "projectile_mass_kg", "sbm_mass_kg", "v_rel_km_s", "energy_j_per_g"):
+        assert np.allclose(de[f], he[f], rtol=1e-9, atol=0), f
+    # The eroded targets' masses fall hit after hit.
+    for k in (2, 3):
+        m = de["target_mass_kg"][de["target"] == k]
+        assert len(m) == 300 and np.all(np.diff(m) < 0)
+    # The parents' fates: targets 0-1 and every projectile destroyed, 2-3 alive.
+    n0 = len(st)
+    assert np.array_equal(da[:n0], ha[:n0])
