@@ -712,35 +712,51 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     eng.set_screening(True, a.conj_km, 1.0, 0.01)
     eng.set_steps_per_graph(chunk)
     # Untimed warm-up on the same population: device buffers reach their
-    # working sizes and the chunk graphs are built, as after a run's first chunk.
+    # working sizes and the chunk graphs are built, as after a run's first
+    # chunk; it also sizes the caller's pinned record buffer, reused by every take.
     eng.set_population(pin_st, pin_sz, pin_al)
     eng.run(min(steps, chunk))
-    eng.take_conjunctions()
+    warm = len(eng.take_conjunctions())
     eng.take_step_stats()
+    rec = torch.empty(max(4096, 2 * warm) * ks.CONJ_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
+    rec = rec.view(ks.CONJ_DTYPE)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
     barrier()
     t0 = time.perf_counter()
     eng.set_population(pin_st, pin_sz, pin_al)
+    t_up = time.perf_counter()
     nconj = nstats = 0
+    run_s = take_s = 0.0
     for done in range(0, steps, chunk):
+        r0 = time.perf_counter()
         eng.run(min(chunk, steps - done))
-        nconj += len(eng.take_conjunctions())
+        r1 = time.perf_counter()
+        while True:
+            got = len(eng.take_conjunctions(rec))
+            nconj += got
+            if got < len(rec):
+                break
         nstats += len(eng.take_step_stats())
+        run_s += r1 - r0
+        take_s += time.perf_counter() - r1
+    t_dn = time.perf_counter()
     fs, fa = eng.get_population(out_st, out_al)
     barrier()
-    wall = time.perf_counter() - t0
-    wall = max_over_ranks(pg, wall)
+    t1 = time.perf_counter()
+    wall = max_over_ranks(pg, t1 - t0)
     world = pg.get_world_size() if pg else 1
     obj = float(al.sum()) * steps * world
     eng.close()
     assert nstats == steps
+    phases = {"upload_ms": 1e3 * (t_up - t0), "runs_ms": 1e3 * run_s, "takes_ms": 1e3 * take_s,
+              "download_ms": 1e3 * (t1 - t_dn)}
     # Per step up: the step's start time, index and 3 lunar stages (position and
     # indirect term), 160 B; down: its 48 B conjunction records and its 216 B
     # control block (the counters).
     h2d = (st.nbytes + sz.nbytes + al.nbytes) / steps + 160
     d2h = (fs.nbytes + fa.nbytes) / steps + nconj * 48 / steps + 216
     return {"value": obj / wall, "unit": "object-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "steps": steps, "steps_per_call": chunk,
+            "steps": steps, "steps_per_call": chunk, "phases_ms": phases,
             "what": f"ks_set_population from pinned host memory, then ks_run of {chunk}-step chunks (per step: "
                     "host->device lunar rows, device->host conjunction records in (t, i, j) order and counters, "
                     "taken after each call), then ks_get_population into pinned host memory; wall clock, max over "

@@ -152,13 +152,22 @@ class Engine:
     def run(self, steps):
         self._check(self._lib.ks_run(self._h, int(steps)))
 
-    def take_conjunctions(self):
+    def take_conjunctions(self, out=None):
+        """Records found since the last take, in (t, i, j) order. With `out` (a
+        contiguous CONJ_DTYPE array, e.g. in pinned memory, reused from call to
+        call) up to len(out) records are moved into it and out[:count] is
+        returned; the rest stay for the next take."""
         cnt = C.c_int64()
+        if out is not None:
+            if out.dtype != CONJ_DTYPE or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError("out must be a contiguous CONJ_DTYPE array")
+            self._check(self._lib.ks_take_conjunctions(self._h, ptr(out), len(out), C.byref(cnt)))
+            return out[: cnt.value]
         self._check(self._lib.ks_take_conjunctions(self._h, None, 0, C.byref(cnt)))
-        out = np.empty(cnt.value, dtype=CONJ_DTYPE)  # every record is written below
+        res = np.empty(cnt.value, dtype=CONJ_DTYPE)  # every record is written below
         if cnt.value:
-            self._check(self._lib.ks_take_conjunctions(self._h, ptr(out), cnt.value, C.byref(cnt)))
-        return out[: cnt.value]
+            self._check(self._lib.ks_take_conjunctions(self._h, ptr(res), cnt.value, C.byref(cnt)))
+        return res[: cnt.value]
 
     def take_step_stats(self):
         cnt = C.c_int64()

@@ -918,11 +918,14 @@ int seed_speculation(ks_ctx* ctx) {
     KS_CUDA(cudaMemcpyAsync(&c, carry_slot(ctx), sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA(cudaStreamSynchronize(ctx->stream));
     const int bits = estimate_bits(c, ctx->dt, ctx->thr, ctx->tune.subcell_bits, ctx->rbits, ctx->tune.cell_scale);
-    ctx->sort_passes = passes_for_bits(bits);
+    const int passes = passes_for_bits(bits);
     // Keys, dead flag and object index in 64 bits, with 2 bits to spare for the estimate.
     const int64_t indices = ctx->dev_sbm ? ctx->b.cap : ctx->n;  // fragments take indices up to the capacity
-    ctx->pack_keys = ctx->allow_pack && bits + 1 + index_bits(indices) + 2 <= 64;
-    drop_graphs(ctx);
+    const bool pack = ctx->allow_pack && bits + 1 + index_bits(indices) + 2 <= 64;
+    // The chunk graphs hold both in their kernels' arguments: rebuilt only if they change.
+    if (passes != ctx->sort_passes || pack != ctx->pack_keys) drop_graphs(ctx);
+    ctx->sort_passes = passes;
+    ctx->pack_keys = pack;
     return KS_OK;
 }
 
@@ -1336,12 +1339,14 @@ void* ks_stream(ks_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nu
 int ks_set_population(ks_ctx* ctx, int64_t n, const double* states, const double* size_m, const uint8_t* alive) {
     if (!ctx || n < 0 || (n > 0 && (!states || !size_m))) return fail(ctx, KS_ERR_ARG, "ks_set_population: bad arguments");
     cudaSetDevice(ctx->device);
+    const int old_rbits = ctx->rbits;
     ctx->realisations = 1;
     ctx->rbits = 0;
     ctx->offsets.assign({0, n});
     reset_breakup_run(ctx);
     int rc = ensure_objects(ctx, n);
     if (rc) return rc;
+    if (n != ctx->n || old_rbits != 0) drop_graphs(ctx);  // graphs hold the population size in their arguments
     ctx->n = n;
     ctx->cur = 0;
     rc = upload_population(ctx, n, states, size_m, alive, 0);
@@ -1774,6 +1779,7 @@ int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* co
 
 int ks_set_breakup(ks_ctx* ctx, int on, double lc_m, double catastrophic_j_per_g, uint64_t seed) {
     if (!ctx || !(lc_m > 0.0) || !(catastrophic_j_per_g > 0.0)) return fail(ctx, KS_ERR_ARG, "ks_set_breakup: bad arguments");
+    drop_graphs(ctx);  // device fragmentation: its kernels and parameters are part of the graphs
     ctx->bk.on = on != 0;
     ctx->bk.params.lc_m = lc_m;
     ctx->bk.params.catastrophic_j_per_g = catastrophic_j_per_g;
