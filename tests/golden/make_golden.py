@@ -273,6 +273,34 @@ def catalogue_24h_kat():
     print("catalogue 24h", out["conjunctions"], out["below_km"], out["closest"])
 
 
+def million_kat(steps=24):
+    """The bench workload (seed 20260801: 28 340 catalogue objects + 971 660
+    fragments in 200 clouds released within the last day), dt 10 s, 5 km, run
+    by the reference build for `steps` steps: SHA-256 digests of its final
+    states, conjunction records and per-step counters. The population is the
+    seeded generator's, so only the digests are kept."""
+    st, sz, al = checkers.generate_population(20260801, 28340, 1_000_000, 200, 86400.0)
+    ref = checkers.Reference()
+    fs, fa, conj, stats = ref.run(st, sz, al, epoch_jd=EPOCH, t_start=0.0, dt=10.0, steps=steps, screen=True,
+                                  threshold_km=5.0, radius_scale=1.0, min_vrel_km_s=0.01, threads=os.cpu_count())
+    out = {
+        "source": "reference CLI step loop (oracle/_ref) on the seeded 1M-object bench population",
+        "population": {"seed": 20260801, "n_base": 28340, "n_total": 1000000, "parents": 200,
+                       "frag_age_max_s": 86400.0},
+        "epoch_jd": EPOCH, "dt": 10.0, "steps": steps, "threshold_km": 5.0, "radius_scale": 1.0,
+        "min_vrel_km_s": 0.01,
+        "conjunctions": int(len(conj)), "collisions": int(conj["collision"].sum()),
+        "candidate_pairs_total": int(stats["candidate_pairs"].sum()),
+        "refined_pairs_total": int(stats["refined_pairs"].sum()),
+        "sha256_final_states": digest([fs, fa]),
+        "sha256_conjunctions": digest([conj[f] for f in CONJ_FIELDS]),
+        "sha256_step_counters": digest([stats[f] for f in STAT_FIELDS]),
+    }
+    with open(os.path.join(HERE, "ref_1M_24steps.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("1M kat", out["conjunctions"], out["candidate_pairs_total"])
+
+
 CLI_ARGS = ["0.25", "10", "--conj-km", "5"]
 
 
@@ -372,6 +400,7 @@ def main():
     if os.path.exists(CATALOG):
         catalogue_kat()
         catalogue_24h_kat()
+    million_kat()
 
 
 if __name__ == "__main__":
