@@ -261,6 +261,15 @@ def parity_vs_reference(ks, eng, a, st, sz, al, ref_run, steps):
     return out
 
 
+def timed_chunk(steps, spg):
+    """Steps per graph launch of a timed run of `steps` steps: the largest
+    divisor of `steps` not above spg (every chunk then runs as one captured
+    graph), or spg itself when that divisor would be under half of it."""
+    spg = max(1, spg)
+    d = max(k for k in range(1, min(steps, spg) + 1) if steps % k == 0) if steps > 0 else spg
+    return d if 2 * d >= min(steps, spg) else spg
+
+
 def timed_run(ks, eng, a, st, sz, al, precision, barrier):
     """W untimed warm-up steps, then K timed steps; per-step device time from
     CUDA events on the engine's stream, L2 flushed before each step outside
@@ -275,9 +284,11 @@ def timed_run(ks, eng, a, st, sz, al, precision, barrier):
     # carries a one-time set-up cost of tens of milliseconds.
     eng.set_steps_per_graph(a.warmup)
     eng.run(a.warmup)
-    eng.set_steps_per_graph(a.steps_per_graph)
+    eng.set_steps_per_graph(timed_chunk(a.steps, a.steps_per_graph))
     eng.take_conjunctions()
     eng.take_step_stats()
+    # The timed chunks' graphs are captured now, outside the timed region.
+    eng.prepare_run()
     barrier()
     w0 = time.perf_counter()
     eng.run(a.steps)
@@ -349,6 +360,14 @@ def roofline_of(tm, a, fp64_rate, fp32_rates, split):
                   "per object: 8 B key read, 32 B FP32 record gathered, 32 B record + 4 B index written"),
         "pairs": (32.0 * n_obj, phases["pairs_ms"], "per object: its 32 B FP32 record read once"),
     }
+    if tm.get("sort_cells_fused"):
+        # One launch sorts and builds the cells: its time is the sort phase's.
+        hbm_phases = {
+            "sort_cells": ((16.0 * passes + 76.0) * n_obj, phases["sort_ms"] + phases["cells_ms"],
+                           f"{passes} radix passes x (8 B key read + 8 B key written) per object, then per "
+                           "object 8 B key read, 32 B FP32 record gathered, 32 B record + 4 B index written"),
+            "pairs": hbm_phases["pairs"],
+        }
     hbm_kernels = {}
     for k, (nbytes, ms, what) in hbm_phases.items():
         gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
@@ -386,10 +405,13 @@ def traffic_of(kernel, split):
     return None
 
 
-def launches_per_step(sort_passes):
-    # propagate, fix_keys, sort (one kernel per pass; the propagation and, if
-    # it rebuilds keys, k_fix_keys count the digits), cells (count, scan,
-    # write, neighbours, item count, scan, item write), pairs, refine
+def launches_per_step(sort_passes, fused=False):
+    # Fused: propagate, fix_keys, sort + cells (one cooperative launch), pairs,
+    # refine. Otherwise: propagate, fix_keys, sort (one kernel per pass; the
+    # propagation and, if it rebuilds keys, k_fix_keys count the digits), cells
+    # (count, scan, write, neighbours, item count, scan, item write), pairs, refine.
+    if fused:
+        return 1 + 1 + 1 + 1 + 1
     return 1 + 1 + sort_passes + 7 + 1 + 1
 
 
@@ -510,7 +532,8 @@ def main():
                 "conjunctions_per_step": len(conj) / steps, "refined_pairs_per_step": tm["refined_pairs"] / steps,
                 "exact_filter_pairs_per_step": tm["exact_filter_pairs"] / steps,
                 "roofline": roofline_of(tm, a, fp64_rate, fp32_rate, prec == ks.PRECISION_SPLIT),
-                "wall_s_timed_region": wall, "sort_passes": tm["sort_passes"]}
+                "wall_s_timed_region": wall, "sort_passes": tm["sort_passes"],
+                "sort_cells_fused": bool(tm.get("sort_cells_fused", 0))}
 
     main_s, other_s = summary(head), summary(other)
     c_head, c_other = runs[head][1], runs[other][1]
@@ -524,7 +547,7 @@ def main():
             "dtype": "f64+f32 (split)" if head == ks.PRECISION_SPLIT else "f64",
             "data": "synthetic (seeded generator; no dataset)", "config": config_of(a),
             "pairs_per_s": main_s["pairs_per_s"], "conjunctions_per_step": main_s["conjunctions_per_step"],
-            "gpu_launches": a.steps * launches_per_step(tm_head["sort_passes"]) +
+            "gpu_launches": a.steps * launches_per_step(tm_head["sort_passes"], tm_head.get("sort_cells_fused", 0)) +
                             LAUNCHES_PER_CHUNK * -(-a.steps // max(1, a.steps_per_graph)),
             "roofline": main_s["roofline"], "clocks": clk,
             "fp64" if head == ks.PRECISION_SPLIT else "split": other_s,
@@ -624,7 +647,7 @@ def ensemble_run(ks, a, device, barrier, pg, rank):
 
 def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     """Batched cascade: R realisations of the 1M-object population with collision
-    radii x50 and fragmentation in the loop on the device (NASA SBM, L_c 10 cm,
+    radii x5 and fragmentation in the loop on the device (NASA SBM, L_c 10 cm,
     counter-based draws, one stream per realisation), split precision, 5 km,
     10 m/s, within a fixed population budget. Every collision fragments inside
     the step that found it, so chunks of steps run through collisions. Timed on
@@ -636,7 +659,10 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     eng.set_breakup_mode(ks.BREAKUP_DEVICE, budget)
     eng.set_precision(ks.PRECISION_SPLIT)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
-    eng.set_screening(True, a.conj_km, 50.0, 0.01)
+    # Radii x5: a sustained cascade. At x50 the fragments of an event late in a
+    # step (radii 2.5-12.5 m there) still overlap at the next step and collide
+    # with each other, pairs by the hundred per event, past any per-step limit.
+    eng.set_screening(True, a.conj_km, 5.0, 0.01)
     eng.set_steps_per_graph(a.steps_per_graph)
     eng.set_population_batch(np.arange(R + 1) * n0, np.tile(st, (R, 1)), np.tile(sz, R), np.tile(al, R))
     eng.set_breakup(True, 0.10, 40.0, realisation_seed(a.seed, rank))
@@ -663,7 +689,7 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     dev_ms = max_over_ranks(pg, tm["total_ms"] + tm["chunk_ms"])
     obj = sum_over_ranks(pg, float(tm["object_steps"]))
     per_real = np.bincount(ev["realisation"], minlength=R) if len(ev) else np.zeros(R, int)
-    return {"workload": f"{R} realisations x the {n0}-object population, collision radii x50, fragmentation "
+    return {"workload": f"{R} realisations x the {n0}-object population, collision radii x5, fragmentation "
                         f"in the loop on the device (SBM, L_c 0.1 m, counter-based draws), split precision, "
                         f"dt {a.dt} s, {a.conj_km} km, population budget {budget} objects",
             "value": obj / (dev_ms * 1e-3), "unit": "object-steps/s", "ms_per_step": dev_ms / max(1, tm["steps"]),
@@ -700,7 +726,7 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     max over ranks."""
     import torch
     steps = a.e2e_steps or a.steps
-    chunk = max(1, a.steps_per_graph)
+    chunk = timed_chunk(steps, a.steps_per_graph)
     pin_st = torch.from_numpy(st).pin_memory().numpy()
     pin_sz = torch.from_numpy(sz).pin_memory().numpy()
     pin_al = torch.from_numpy(al).pin_memory().numpy()
@@ -718,6 +744,7 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     eng.run(min(steps, chunk))
     warm = len(eng.take_conjunctions())
     eng.take_step_stats()
+    eng.prepare_run()
     rec = torch.empty(max(4096, 2 * warm) * ks.CONJ_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
     rec = rec.view(ks.CONJ_DTYPE)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
@@ -727,10 +754,16 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     t_up = time.perf_counter()
     nconj = nstats = 0
     run_s = take_s = 0.0
+    host = {"prep_ms": 0.0, "launch_ms": 0.0, "sync_ms": 0.0, "after_ms": 0.0}
     for done in range(0, steps, chunk):
         r0 = time.perf_counter()
         eng.run(min(chunk, steps - done))
         r1 = time.perf_counter()
+        tm = eng.timing()
+        host["prep_ms"] += tm["host_prep_ms"]
+        host["launch_ms"] += tm["host_launch_ms"]
+        host["sync_ms"] += tm["host_sync_ms"]
+        host["after_ms"] += tm["host_chunk_ms"] - tm["host_prep_ms"] - tm["host_launch_ms"] - tm["host_sync_ms"]
         while True:
             got = len(eng.take_conjunctions(rec))
             nconj += got
@@ -749,7 +782,7 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision):
     eng.close()
     assert nstats == steps
     phases = {"upload_ms": 1e3 * (t_up - t0), "runs_ms": 1e3 * run_s, "takes_ms": 1e3 * take_s,
-              "download_ms": 1e3 * (t1 - t_dn)}
+              "download_ms": 1e3 * (t1 - t_dn), "runs_host_split": host}
     # Per step up: the step's start time, index and 3 lunar stages (position and
     # indirect term), 160 B; down: its 48 B conjunction records and its 216 B
     # control block (the counters).

@@ -122,10 +122,16 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * FP64 propagation kernel is compiled for; more blocks, fewer registers each),
  * "sort_rank_ballot" (radix-sort ranking within a warp: 0, the default, by
  * the hardware match instruction; 1 by eight ballots, one per digit bit),
+ * "sort_fused" (1, the default: the object sort and the cell build run as one
+ * cooperative launch of one 1024-thread block per SM, grid barriers between
+ * their phases, wherever the keys fit its registers (up to 12 288 per SM) and
+ * the keys carry the object index; 0: the separate radix passes and cell
+ * kernels),
  * "lookback_polls" (0..2^30, default 2^22: polls a radix-sort tile makes of a
- * predecessor's unpublished digit counts before it gives up; a wait that runs
- * out fails the run with KS_ERR_TIMEOUT and leaves the simulation where the
- * failed chunk of steps began, with no records from it).
+ * predecessor's unpublished digit counts, or a block of the fused sort makes of
+ * a grid barrier, before it gives up; a wait that runs out fails the run with
+ * KS_ERR_TIMEOUT and leaves the simulation where the failed chunk of steps
+ * began, with no records from it).
  * Conjunctions, refined and co-orbiting counts and states never change;
  * candidate_pairs and cell_km change with the cell edge. */
 int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value);
@@ -157,6 +163,14 @@ int ks_autotune(ks_ctx* ctx, int32_t trial_steps, ks_tuning_choice* out);
  *     (src/main.cpp:352-373). Conjunctions and per-step counters accumulate in
  *     the context until taken. */
 int ks_run(ks_ctx* ctx, int64_t steps);
+
+/* Captures, instantiates and uploads the graphs that the next ks_run calls
+ * launch for chunks of steps_per_graph steps (both step parities), sized as
+ * those calls would size them, without running a step, so that a timed run
+ * does not pay for their capture. A later change of population size, tuning
+ * or buffer sizes captures again where it must. No-op without graphs or with
+ * fragmentation on the device. */
+int ks_prepare_run(ks_ctx* ctx);
 
 /* Conjunctions found since the last take, ordered by (t, i, j) as Screener::finish
  * orders them (src/core/collision.cpp:743-747). With out == NULL only *count is
@@ -283,6 +297,17 @@ typedef struct ks_timing {
     int64_t refined_pairs;       /* pairs refined (Hermite TCA) */
     double chunk_ms;       /* device work of the chunks outside their steps: set-up, checkpoint,
                               ordering of the chunk's conjunction records, replays (L2 flushes excluded) */
+    int64_t sort_cells_fused;  /* 1: the last steps sorted and built the cells in one cooperative launch
+                                  (sort_ms then holds both, cells_ms is 0) */
+    /* Host wall time of the run's chunks (fragmentation on the host), always
+     * measured: in all, before the first launch of each chunk (parameters,
+     * buffer sizing, graph capture), in the launch calls, waiting for the
+     * device; the rest is record copies beyond those a chunk brings back,
+     * ordering of ties, counters, replays and fragmentation. */
+    double host_chunk_ms;
+    double host_prep_ms;
+    double host_launch_ms;
+    double host_sync_ms;
 } ks_timing;
 int ks_get_timing(const ks_ctx* ctx, ks_timing* out);
 

@@ -152,6 +152,10 @@ class Engine:
     def run(self, steps):
         self._check(self._lib.ks_run(self._h, int(steps)))
 
+    def prepare_run(self):
+        """Capture the chunk graphs the next run() calls launch, without running."""
+        self._check(self._lib.ks_prepare_run(self._h))
+
     def take_conjunctions(self, out=None):
         """Records found since the last take, in (t, i, j) order. With `out` (a
         contiguous CONJ_DTYPE array, e.g. in pinned memory, reused from call to

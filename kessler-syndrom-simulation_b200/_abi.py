@@ -32,7 +32,9 @@ class Timing(C.Structure):
                 ("pairs_ms", C.c_double), ("refine_ms", C.c_double), ("total_ms", C.c_double),
                 ("steps", C.c_int64), ("object_steps", C.c_int64), ("sort_passes", C.c_int64),
                 ("candidate_pairs", C.c_int64), ("exact_filter_pairs", C.c_int64), ("refined_pairs", C.c_int64),
-                ("chunk_ms", C.c_double)]
+                ("chunk_ms", C.c_double), ("sort_cells_fused", C.c_int64),
+                ("host_chunk_ms", C.c_double), ("host_prep_ms", C.c_double), ("host_launch_ms", C.c_double),
+                ("host_sync_ms", C.c_double)]
 
 
 class TuningChoice(C.Structure):
@@ -74,6 +76,7 @@ SIGNATURES = {
     "ks_set_l2_flush": (C.c_int, [_P, _I64]),
     "ks_set_tuning": (C.c_int, [_P, C.c_char_p, _I64]),
     "ks_run": (C.c_int, [_P, _I64]),
+    "ks_prepare_run": (C.c_int, [_P]),
     "ks_autotune": (C.c_int, [_P, C.c_int32, C.POINTER(TuningChoice)]),
     "ks_take_conjunctions": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),

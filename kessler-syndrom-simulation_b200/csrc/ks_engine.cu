@@ -16,6 +16,7 @@
 #include <cstring>
 #include <fstream>
 #include <atomic>
+#include <chrono>
 #include <set>
 #include <sstream>
 #include <string>
@@ -82,6 +83,7 @@ struct ks_ctx {
     bool conj_small = false;   // chunks order their records in one block (few expected)
     int64_t chunk_spec = 0;    // records a chunk copies back with its control blocks
     int64_t graph_spec[2] = {0, 0};  // the same, as captured in graph_exec[]
+    int64_t graph_n[2] = {-1, -1};   // population size graph_exec[] was captured for
     bool allow_pack = true;    // tuning: packing allowed where the keys leave room
     int realisations = 1;
     int rbits = 0;
@@ -146,7 +148,8 @@ void free_objects(ks_ctx* ctx) {
     dfree(b.size_m); dfree(b.real_id); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr);
     dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
-    dfree(b.sorted); dfree(b.sorted32); dfree(b.rec32); dfree(b.sorted_orig);
+    dfree(b.sorted); dfree(b.sorted32); dfree(b.rec32); dfree(b.sorted_orig); dfree(b.fused);
+    b.fused_grid = 0;
     dfree(b.n_live); dfree(b.mass_kg); dfree(b.a2m); dfree(b.event_of); dfree(b.coll); dfree(b.sbm_work);
     dfree(b.sbm_events); dfree(b.sbm_next_event); dfree(b.sbm_order); dfree(b.sbm_first); dfree(b.sbm_pending);
     dfree(b.sbm_misc);
@@ -198,6 +201,12 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.sorted32, sizeof(float4) * 2 * cap));
     KS_CUDA(cudaMalloc(&b.rec32, sizeof(float4) * 2 * cap));
     KS_CUDA(cudaMalloc(&b.sorted_orig, sizeof(int) * cap));
+    // Scratch of the fused sort + cell build, sized for this device's grid
+    // (looked up here, outside any stream capture).
+    if (const int fg = ks::fused_grid()) {
+        KS_CUDA(cudaMalloc(&b.fused, sizeof(unsigned int) * ks::fused_scratch_words(fg)));
+        b.fused_grid = fg;
+    }
     if (ctx->dev_sbm) {
         KS_CUDA(cudaMalloc(&b.n_live, sizeof(int)));
         KS_CUDA(cudaMalloc(&b.mass_kg, sizeof(double) * cap));
@@ -412,6 +421,8 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
         a.coll_cap = ctx->b.coll_cap;
         a.pack_bits = ctx->pack_keys ? index_bits(ctx->b.cap) : 0;
     }
+    // The fused sort counts its own digits: the propagation need not.
+    if (a.hist && ks::sort_cells_fused(ctx->b, a)) a.hist = nullptr;
     return a;
 }
 
@@ -458,10 +469,16 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
         record(ctx, k, 1, capturing);
         if (ctx->screening) {
             ks::launch_fix_keys(ctx->b, a, s);
-            ks::launch_sort(ctx->b, a, s);
-            record(ctx, k, 2, capturing);
-            ks::launch_cells(ctx->b, a, s);
-            record(ctx, k, 3, capturing);
+            if (ks::sort_cells_fused(ctx->b, a)) {
+                ks::launch_sort_cells(ctx->b, a, s);  // sort and cells in one launch: timed as the sort
+                record(ctx, k, 2, capturing);
+                record(ctx, k, 3, capturing);
+            } else {
+                ks::launch_sort(ctx->b, a, s);
+                record(ctx, k, 2, capturing);
+                ks::launch_cells(ctx->b, a, s);
+                record(ctx, k, 3, capturing);
+            }
             ks::launch_pairs(ctx->b, a, s);
             record(ctx, k, 4, capturing);
             ks::launch_refine(ctx->b, a, ctx->b.conj, ctx->b.conj_cap, ctx->b.chunk, s);
@@ -490,6 +507,10 @@ int ensure_graph(ks_ctx* ctx, int k_steps) {
     const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
     if (!use_graph) return KS_OK;
     cudaGraphExec_t& exec = ctx->graph_exec[ctx->cur];
+    // The population size is in the kernels' arguments (with fragmentation on
+    // the host; on the device they hold the capacity): a graph captured for
+    // another size, as after fragments were appended, is captured again.
+    if (exec && !ctx->dev_sbm && ctx->graph_n[ctx->cur] != ctx->n) drop_graphs(ctx);
     if (!exec) {
         cudaGraph_t g = nullptr;
         KS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -507,6 +528,7 @@ int ensure_graph(ks_ctx* ctx, int k_steps) {
         // Uploaded now rather than by its first launch.
         KS_CUDA(cudaGraphUpload(exec, ctx->stream));
         ctx->graph_spec[ctx->cur] = ctx->chunk_spec;
+        ctx->graph_n[ctx->cur] = ctx->n;
     }
     return KS_OK;
 }
@@ -551,6 +573,11 @@ bool conj_less(const ks_conjunction& a, const ks_conjunction& b) {
     if (a.t != b.t) return a.t < b.t;
     if (a.i != b.i) return a.i < b.i;
     return a.j < b.j;
+}
+
+using HostClock = std::chrono::steady_clock;
+double host_ms(HostClock::time_point a, HostClock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
 // (t, i, j) order of records the device already ordered by a key monotone in
@@ -671,7 +698,7 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
         ks::launch_conj_sort(ctx->b, ctx->b.chunk, &ctx->b.params[0].t0, k_steps * ctx->dt, false, ctx->stream);
         KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (ctx->h_chunk->flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+        if (ctx->h_chunk->flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back or grid barrier wait gave up");
         have = 0;
     }
     if (nc > have) {
@@ -716,6 +743,7 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     accumulate_timing(ctx, done);
     ctx->timing.steps += done;
     ctx->timing.sort_passes = ctx->sort_passes;
+    ctx->timing.sort_cells_fused = ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, 1, 0)) ? 1 : 0;
     ctx->steps_done += done;
     ctx->t = done == k_steps ? t_end : ctx->h_params[done].t0;
     if (done & 1) ctx->cur ^= 1;
@@ -731,7 +759,7 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     if (ctx->dev_stalls > kMaxReplays) return fail(ctx, KS_ERR_OVERFLOW, "device buffers still overflowing after regrowth");
     const Ctrl& c = ctx->h_ctrl[h];
     const int flags = c.flags | (ch.flags & ks::FLAG_CONJ_OVERFLOW);
-    if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+    if (flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back or grid barrier wait gave up");
     if (flags & ks::FLAG_KEY_RANGE) return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits");
     if (flags & ks::FLAG_COLL_OVERFLOW)
         return fail(ctx, KS_ERR_OVERFLOW, "more than " + std::to_string(ks::kSbmStepEvents) +
@@ -753,32 +781,40 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     return KS_OK;
 }
 
-int run_chunk(ks_ctx* ctx, int k_steps) {
-    if (ctx->dev_sbm) return run_chunk_dev(ctx, k_steps);
-    stash_pending(ctx);  // this chunk's records land in h_conj
-    int rc = ensure_chunk(ctx, k_steps);
-    if (rc) return rc;
-    double t_end = 0.0;
-    fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);  // uploaded by the chunk itself
-    // Room for the chunk's records at the largest per-step count seen so far,
-    // so that a longer chunk does not overflow and replay.
+// Buffer sizes and graph shape of a chunk of k_steps steps (fragmentation on
+// the host): room for its records at the largest per-step count seen so far
+// (so that a longer chunk does not overflow and replay), one-block ordering of
+// the records where it should hold few, and how many records come back with
+// its control blocks (up to the expected count: one host round trip).
+int plan_chunk(ks_ctx* ctx, int k_steps) {
+    int rc = KS_OK;
     if (ctx->screening && ctx->max_step_conj > 0) {
         const int64_t want = std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, int64_t(1) << 30);
         if (want > ctx->b.conj_cap && (rc = ensure_conj(ctx, want))) return rc;
     }
-    // One-block ordering of the records where the chunk should hold few.
     const bool small = ctx->screening && ctx->max_step_conj > 0 &&
                        ctx->max_step_conj * k_steps * 5 / 4 + 256 <= ks::kConjSmall;
     if (small != ctx->conj_small) {
         ctx->conj_small = small;
         drop_graphs(ctx);
     }
-    // Records copied back with the control blocks, up to the expected count,
-    // so that a chunk with no more than that needs one host round trip.
     const int64_t spec = ctx->screening ? std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, ctx->b.conj_cap) : 0;
     ctx->chunk_spec = ctx->max_step_conj > 0 && spec <= (int64_t(1) << 16) ? spec : 0;
     const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
     if (use_graph && ctx->graph_exec[ctx->cur] && ctx->graph_spec[ctx->cur] < ctx->chunk_spec) drop_graphs(ctx);
+    return KS_OK;
+}
+
+int run_chunk(ks_ctx* ctx, int k_steps) {
+    if (ctx->dev_sbm) return run_chunk_dev(ctx, k_steps);
+    const HostClock::time_point h0 = HostClock::now();
+    stash_pending(ctx);  // this chunk's records land in h_conj
+    int rc = ensure_chunk(ctx, k_steps);
+    if (rc) return rc;
+    double t_end = 0.0;
+    fill_params(ctx, k_steps, ctx->t, ctx->steps_done, &t_end);  // uploaded by the chunk itself
+    if ((rc = plan_chunk(ctx, k_steps))) return rc;
+    const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
     // A new graph is built before the chunk's start is recorded, so that the
     // chunk's device time holds no wait for the host.
     if ((rc = ensure_graph(ctx, k_steps))) return rc;
@@ -789,9 +825,14 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     }
     int64_t have = 0;  // leading records of this chunk's run already in h_conj
     for (int attempt = 0;; ++attempt) {
+        const HostClock::time_point hl = HostClock::now();
+        if (attempt == 0) ctx->timing.host_prep_ms += host_ms(h0, hl);
         rc = launch_chunk(ctx, k_steps);
         if (rc) return rc;
+        const HostClock::time_point hs = HostClock::now();
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->timing.host_launch_ms += host_ms(hl, hs);
+        ctx->timing.host_sync_ms += host_ms(hs, HostClock::now());
         have = use_graph ? ctx->graph_spec[ctx->cur] : ctx->chunk_spec;
         int flags = ctx->h_chunk->flags;
         unsigned long long max_refined = 0;
@@ -810,7 +851,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
             // The chunk's results are void: put the simulation back at the
             // chunk's start, so that the caller may simply run it again.
             if (ctx->screening) restore_checkpoint(ctx);
-            return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+            return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back or grid barrier wait gave up");
         }
         if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS | ks::FLAG_PACK_WIDTH)) && !surv_over && !items_over)
             break;
@@ -842,7 +883,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
             KS_CUDA(cudaMemcpyAsync(ctx->h_chunk, ctx->b.chunk, sizeof(ks::ChunkCtrl), cudaMemcpyDeviceToHost,
                                     ctx->stream));
             KS_CUDA(cudaStreamSynchronize(ctx->stream));
-            if (ctx->h_chunk->flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up");
+            if (ctx->h_chunk->flags & ks::FLAG_TIMEOUT) return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back or grid barrier wait gave up");
             have = 0;
         }
         if (nc > have) {
@@ -901,6 +942,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     accumulate_timing(ctx, k_steps);
     ctx->timing.steps += k_steps;
     ctx->timing.sort_passes = ctx->sort_passes;
+    ctx->timing.sort_cells_fused = ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, 1, 0)) ? 1 : 0;
     ctx->steps_done += k_steps;
     ctx->t = t_end;
     if (k_steps & 1) ctx->cur ^= 1;
@@ -1500,6 +1542,10 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     else if (k == "pair_gate_x2" && (value == 0 || value == 1)) ctx->tune.pair_gate_x2 = static_cast<int>(value);
     else if (k == "pair_stage2" && value >= 0 && value <= 2) ctx->tune.pair_stage2 = static_cast<int>(value);
     else if (k == "prop_min_blocks" && value >= 4 && value <= 6) ctx->tune.prop_min_blocks = static_cast<int>(value);
+    else if (k == "sort_fused" && (value == 0 || value == 1)) {
+        ctx->tune.sort_fused = static_cast<int>(value);
+        drop_graphs(ctx);
+    }
     else if (k == "sort_rank_ballot" && (value == 0 || value == 1)) {
         ctx->tune.sort_rank_ballot = static_cast<int>(value);
         drop_graphs(ctx);
@@ -1735,10 +1781,30 @@ int ks_run(ks_ctx* ctx, int64_t steps) {
         // while collisions are frequent the chunks stay short (chunk_hint).
         const int want = ctx->bk.on && ctx->chunk_hint > 0 ? std::min(chunk, ctx->chunk_hint) : chunk;
         const int k = static_cast<int>(std::min<int64_t>(end - ctx->steps_done, want));
+        const HostClock::time_point h0 = HostClock::now();
         rc = run_chunk(ctx, k);
+        ctx->timing.host_chunk_ms += host_ms(h0, HostClock::now());
         if (rc) return rc;
     }
     return KS_OK;
+}
+
+int ks_prepare_run(ks_ctx* ctx) {
+    if (!ctx) return KS_ERR_ARG;
+    if (!ctx->has_pop) return fail(ctx, KS_ERR_STATE, "ks_prepare_run: no population");
+    cudaSetDevice(ctx->device);
+    if (ctx->steps_per_graph <= 0 || ctx->dev_sbm) return KS_OK;
+    const int k = ctx->steps_per_graph;
+    int rc = ensure_chunk(ctx, k);
+    if (!rc) rc = plan_chunk(ctx, k);
+    // Both parities: a chunk of an odd number of steps leaves the next one on the other.
+    const int cur = ctx->cur;
+    for (int p = 0; p < 2 && !rc; ++p) {
+        ctx->cur = p;
+        rc = ensure_graph(ctx, k);
+    }
+    ctx->cur = cur;
+    return rc;
 }
 
 int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t* count) {
@@ -2177,7 +2243,7 @@ int ks_screen(ks_ctx* ctx, int64_t n, const double* before, const double* after,
         const bool surv_over = c.refined > static_cast<unsigned long long>(ctx->b.surv_cap);
         const bool items_over = ks::items_total(c) > ctx->b.items_cap;
         if (flags & ks::FLAG_KEY_RANGE) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_RANGE, "cell key outside its grid bounds or wider than 63 bits"); }
-        if (flags & ks::FLAG_TIMEOUT) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back wait gave up"); }
+        if (flags & ks::FLAG_TIMEOUT) { ctx->dt = saved_dt; return fail(ctx, KS_ERR_TIMEOUT, "radix sort look-back or grid barrier wait gave up"); }
         if (!(flags & (ks::FLAG_CONJ_OVERFLOW | ks::FLAG_SORT_BITS)) && !surv_over && !items_over) {
             st.step = 0;
             st.candidate_pairs = static_cast<int64_t>(c.candidates);

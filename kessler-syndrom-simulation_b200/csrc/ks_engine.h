@@ -124,6 +124,8 @@ struct DeviceBuffers {
     int64_t sort_status_len = 0;
     unsigned int* sort_ctr = nullptr;      // tile tickets, one per pass
     int* block_counts = nullptr;           // cell heads per tile
+    unsigned int* fused = nullptr;         // k_sort_cells: barrier, digit totals, per-block counts and starts
+    int fused_grid = 0;                    // blocks the fused scratch is sized for
     int* cell_begin = nullptr;             // cap + 1
     unsigned long long* cell_key = nullptr;
     int* nbr = nullptr;                    // 13 per cell
@@ -186,6 +188,7 @@ struct Tuning {
     int pair_stage2 = 1;          // second FP32 stage: 0 row by row, 1 compacted when sparse, 2 always compacted
     int sort_rank_ballot = 0;     // radix ranking by eight ballots instead of the hardware match
     int prop_min_blocks = 4;      // FP64 propagation: resident 128-thread blocks per SM it is compiled for (4..6)
+    int sort_fused = 1;           // object sort and cell build in one cooperative launch (k_sort_cells) where it fits
 };
 
 // Time from a fragmentation event to the end of its step and the lunar stages
@@ -296,6 +299,12 @@ void launch_fix_keys(const DeviceBuffers& b, const StepArgs& a, cudaStream_t str
 void launch_sort(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 bool f32_records(const StepArgs& a);
 void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
+// Fused sort + cell build: blocks per launch on the current device (0: not
+// available), scratch words for that grid, whether a step takes the fused path.
+int fused_grid();
+int64_t fused_scratch_words(int grid);
+bool sort_cells_fused(const DeviceBuffers& b, const StepArgs& a);
+void launch_sort_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream);
 // Orders the chunk's conjunction records by TCA into conj_sorted (records
 // whose TCAs share a 32-bit key keep their append order; the host finishes

