@@ -271,8 +271,14 @@ void clear_records(ks_ctx* ctx) {
 }
 
 int ensure_conj(ks_ctx* ctx, int64_t want) {
-    if (want > ctx->b.conj_cap) {
+    if (want > ctx->b.conj_cap || want > ctx->h_conj_cap) {
         if (want > (int64_t(1) << 30)) return fail(ctx, KS_ERR_RANGE, "more than 2^30 conjunctions in one chunk");
+        // Room to grow: callers ask for a margin over the largest count so far,
+        // which rises a little at a time; regrowing (and capturing the graphs
+        // again) at each rise cost milliseconds per chunk.
+        want = std::min<int64_t>(want + want / 2, int64_t(1) << 30);
+    }
+    if (want > ctx->b.conj_cap) {
         drop_graphs(ctx);
         free_conj(ctx);
         ks::DeviceBuffers& b = ctx->b;
@@ -458,6 +464,10 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
     cudaStream_t s = ctx->stream;
     cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, s);
     ks::launch_chunk_init(ctx->b, k_steps, s, true);
+    // The fused sort + cell build leaves the cell-key hash empty for the next
+    // step; it is cleared once here for the chunk's first.
+    if (ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, k_steps, src0)))
+        cudaMemsetAsync(ctx->b.hash_keys, 0xFF, sizeof(unsigned long long) * ctx->b.hash_cap, s);
     int src = src0;
     for (int k = 0; k < k_steps; ++k) {
         const StepArgs a = step_args(ctx, k, k_steps, src);
@@ -1542,6 +1552,14 @@ int ks_set_tuning(ks_ctx* ctx, const char* key, int64_t value) {
     else if (k == "pair_gate_x2" && (value == 0 || value == 1)) ctx->tune.pair_gate_x2 = static_cast<int>(value);
     else if (k == "pair_stage2" && value >= 0 && value <= 2) ctx->tune.pair_stage2 = static_cast<int>(value);
     else if (k == "prop_min_blocks" && value >= 4 && value <= 6) ctx->tune.prop_min_blocks = static_cast<int>(value);
+    else if (k == "hash_slots_per_cell" && value >= 0 && value <= 64) {
+        ctx->tune.hash_slots_per_cell = static_cast<int>(value);
+        drop_graphs(ctx);
+    }
+    else if (k == "sort_digit_bits" && (value == 8 || value == 11)) {
+        ctx->tune.sort_digit_bits = static_cast<int>(value);
+        drop_graphs(ctx);
+    }
     else if (k == "sort_fused" && (value == 0 || value == 1)) {
         ctx->tune.sort_fused = static_cast<int>(value);
         drop_graphs(ctx);

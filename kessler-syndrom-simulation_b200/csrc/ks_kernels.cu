@@ -728,15 +728,16 @@ __device__ __forceinline__ void st_relaxed(unsigned int* p, unsigned int v) {
 
 
 
-// Lanes of the warp holding the same 8-bit digit as this lane, among the lanes
-// with `valid` set: either the hardware match, or eight ballots (one per digit
-// bit) intersected. The ballot form issues more instructions but each has the
+// Lanes of the warp holding the same DB-bit digit as this lane, among the
+// lanes with `valid` set: either the hardware match, or DB ballots (one per
+// digit bit) intersected. The ballot form issues more instructions but each has the
 // short latency of a vote.
+template <int DB = 8>
 __device__ __forceinline__ unsigned digit_peers(unsigned d, bool valid, bool by_ballot) {
-    if (!by_ballot) return __match_any_sync(0xffffffffu, valid ? d : 256u + (threadIdx.x & 31));
+    if (!by_ballot) return __match_any_sync(0xffffffffu, valid ? d : (1u << DB) + (threadIdx.x & 31));
     unsigned peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
+    for (int b = 0; b < DB; ++b) {
         const bool bit = (d >> b) & 1u;
         const unsigned bal = __ballot_sync(0xffffffffu, bit);
         peers &= bit ? bal : ~bal;
@@ -2099,7 +2100,8 @@ std::atomic<int> g_sm_count[kMaxSmDevices];
 constexpr int kFusedThreads = 1024;
 constexpr int kFusedWarps = kFusedThreads / 32;
 constexpr int kFusedMaxGrid = 256;              // the starts scan loads at most 8 counts per lane
-constexpr int kFusedZeroWords = 32 + 8 * 256;   // barrier counter, per-pass digit totals: zeroed per launch
+constexpr int kFusedDigits = 2048;              // digits of a pass, at most (11-bit digits)
+constexpr int kFusedZeroWords = 32 + 6 * kFusedDigits;  // barrier counter, per-pass digit totals: zeroed per launch
 
 struct FusedArgs {
     unsigned long long* keys[2];
@@ -2249,29 +2251,35 @@ __device__ __forceinline__ unsigned long long forward_key(const GridParams& g, u
            (static_cast<unsigned long long>(y) << g.w[2]) | static_cast<unsigned long long>(z);
 }
 
-template <int K>
+template <int K, int DB>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, FusedArgs f) {
+    constexpr int ND = 1 << DB;              // digits of a pass
+    constexpr unsigned DM = ND - 1;
+    constexpr int kPer = ND / kFusedThreads > 0 ? ND / kFusedThreads : 1;  // digits per thread in digit loops
     extern __shared__ __align__(16) unsigned char fused_smem[];
-    unsigned int* wcnt = reinterpret_cast<unsigned int*>(fused_smem);                          // [32][256]
-    unsigned long long* stage = reinterpret_cast<unsigned long long*>(fused_smem + 4 * 32 * 256);  // [1024 K]
+    // Per-warp digit counters (u16: a warp holds at most 32 K keys), then the
+    // stage of the scatter, then per-digit starts.
+    unsigned short* wcnt = reinterpret_cast<unsigned short*>(fused_smem);                              // [32][ND]
+    unsigned long long* stage = reinterpret_cast<unsigned long long*>(fused_smem + 2 * 32 * ND);      // [1024 K]
+    unsigned int* dstart = reinterpret_cast<unsigned int*>(stage + kFusedThreads * K);  // block-local start of each digit
+    unsigned int* dglob = dstart + ND;     // start of each digit in the output
+    int* gshift = reinterpret_cast<int*>(dglob + ND);   // output position minus block-local position
     __shared__ unsigned int wsum[32];
-    __shared__ unsigned int dstart[256];   // block-local start of each digit
-    __shared__ unsigned int dglob[256];    // start of each digit in the output
-    __shared__ int gshift[256];            // output position minus block-local position, per digit
     __shared__ unsigned int whead[32];     // cell heads of each warp, then their exclusive prefix
     __shared__ unsigned long long bsum[4];
     __shared__ int gave_up;
+    __shared__ unsigned int block_heads;
     __shared__ GridParams g;
 
     Ctrl* ctrl = a.ctrl;
     if (step_void(ctrl)) return;
     const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned int* bar = f.scratch;
-    unsigned int* totals = f.scratch + 32;                 // [8][256]
+    unsigned int* totals = f.scratch + 32;                 // [passes][ND]
     unsigned int* heads = f.scratch + kFusedZeroWords;     // [G]
     unsigned int* iparts = heads + G;                      // [2 G]: heavy, then light items per block
-    unsigned int* counts = iparts + 2 * G;                 // [G][256]
-    unsigned int* offs = counts + 256 * G;                 // [G][256]
+    unsigned int* counts = iparts + 2 * G;                 // [G][ND]
+    unsigned int* offs = counts + kFusedDigits * G;        // [G][ND]
     int* flags = &ctrl->flags;
     const int polls = a.tune.lookback_polls;
     unsigned int target = 0;
@@ -2280,24 +2288,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
     const int R = (n + G - 1) / G;
     const int lo = min(n, b * R);
     const int cnt = min(min(n, lo + R) - lo, K * kFusedThreads);
-    const int passes = a.sort_passes;
+    // The key bits [pack_bits, pack_bits + 8 sort_passes) in passes of DB bits.
+    const int passes = (8 * a.sort_passes + DB - 1) / DB;
     const bool by_ballot = a.tune.sort_rank_ballot != 0;
-
-    // The cell-key hash is cleared here; the inserts come several barriers later.
-    {
-        ulonglong2* h2 = reinterpret_cast<ulonglong2*>(f.hk);
-        const int64_t words = static_cast<int64_t>((f.hmask + 1) >> 1);
-        for (int64_t i = static_cast<int64_t>(b) * kFusedThreads + tid; i < words;
-             i += static_cast<int64_t>(G) * kFusedThreads)
-            h2[i] = make_ulonglong2(kEmpty, kEmpty);
-    }
 
     unsigned long long k[K];
     for (int pass = 0; pass < passes; ++pass) {
         const unsigned long long* in = f.keys[pass & 1];
         unsigned long long* out = f.keys[(pass & 1) ^ 1];
-        const int shift = a.pack_bits + 8 * pass;
-        for (int i = tid; i < 32 * 256; i += kFusedThreads) wcnt[i] = 0;
+        const int shift = a.pack_bits + DB * pass;
+        for (int i = tid; i < 32 * ND / 2; i += kFusedThreads) reinterpret_cast<unsigned int*>(wcnt)[i] = 0u;
 #pragma unroll
         for (int r = 0; r < K; ++r) {
             const int li = warp * 32 * K + r * 32 + lane;
@@ -2309,37 +2309,66 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
 #pragma unroll
         for (int r = 0; r < K; ++r) {
             const bool valid = warp * 32 * K + r * 32 + lane < cnt;
-            const unsigned d = static_cast<unsigned>((k[r] >> shift) & 0xFF);
-            const unsigned peers = digit_peers(d, valid, by_ballot);
-            const unsigned int prior = valid ? wcnt[warp * 256 + d] : 0u;
+            const unsigned d = static_cast<unsigned>(k[r] >> shift) & DM;
+            const unsigned peers = digit_peers<DB>(d, valid, by_ballot);
+            const unsigned int prior = valid ? wcnt[warp * ND + d] : 0u;
             __syncwarp();
-            if (valid && lane == __ffs(peers) - 1) wcnt[warp * 256 + d] = prior + __popc(peers);
+            if (valid && lane == __ffs(peers) - 1) wcnt[warp * ND + d] = static_cast<unsigned short>(prior + __popc(peers));
             __syncwarp();
             rk[r] = prior + __popc(peers & lanemask_lt());
         }
         __syncthreads();
-        unsigned int tot = 0;
-        if (tid < 256) {
-            for (int w = 0; w < kFusedWarps; ++w) {
-                const unsigned int c = wcnt[w * 256 + tid];
-                wcnt[w * 256 + tid] = tot;
-                tot += c;
+        // Per digit: the warps' exclusive prefix (in place) and the block's
+        // count; thread t owns digits kPer t .. kPer t + kPer - 1.
+        unsigned int tot[kPer];
+        unsigned int mine = 0;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            const int d = kPer * tid + e;
+            unsigned int run = 0;
+            if (d < ND) {
+                for (int w = 0; w < kFusedWarps; ++w) {
+                    const unsigned int c = wcnt[w * ND + d];
+                    wcnt[w * ND + d] = static_cast<unsigned short>(run);
+                    run += c;
+                }
             }
+            tot[e] = run;
+            mine += run;
         }
         unsigned int unused;
-        const unsigned int local_start = scan_1024(tid < 256 ? tot : 0u, &unused, wsum);
-        if (tid < 256) {
-            dstart[tid] = local_start;
-            counts[b * 256 + tid] = tot;
-            if (tot) atomicAdd(&totals[pass * 256 + tid], tot);
+        unsigned int start = scan_1024(mine, &unused, wsum);
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            const int d = kPer * tid + e;
+            if (d < ND) {
+                dstart[d] = start;
+                counts[b * ND + d] = tot[e];
+                if (tot[e]) atomicAdd(&totals[pass * ND + d], tot[e]);
+            }
+            start += tot[e];
         }
         grid_sync(bar, target, polls, flags);
         // Starts: digit d's place in the output, then each block's within it.
-        const unsigned int dt = scan_1024(tid < 256 ? __ldcg(totals + pass * 256 + tid) : 0u, &unused, wsum);
-        if (tid < 256) dglob[tid] = dt;
+        {
+            unsigned int tv[kPer];
+            unsigned int sum = 0;
+#pragma unroll
+            for (int e = 0; e < kPer; ++e) {
+                const int d = kPer * tid + e;
+                tv[e] = d < ND ? __ldcg(totals + pass * ND + d) : 0u;
+                sum += tv[e];
+            }
+            unsigned int run = scan_1024(sum, &unused, wsum);
+#pragma unroll
+            for (int e = 0; e < kPer; ++e) {
+                const int d = kPer * tid + e;
+                if (d < ND) dglob[d] = run;
+                run += tv[e];
+            }
+        }
         __syncthreads();
-        if (b + warp * G < 256) {
-            const int d = b + warp * G;
+        for (int d = b + warp * G; d < ND; d += kFusedWarps * G) {
             constexpr int kSeg = kFusedMaxGrid / 32;
             const int S = (G + 31) / 32;
             unsigned int c[kSeg];
@@ -2347,7 +2376,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
 #pragma unroll
             for (int i = 0; i < kSeg; ++i) {
                 const int j = lane * S + i;
-                c[i] = (i < S && j < G) ? __ldcg(counts + j * 256 + d) : 0u;
+                c[i] = (i < S && j < G) ? __ldcg(counts + j * ND + d) : 0u;
                 seg += c[i];
             }
             unsigned int incl = seg;
@@ -2359,24 +2388,25 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
 #pragma unroll
             for (int i = 0; i < kSeg; ++i) {
                 const int j = lane * S + i;
-                if (i < S && j < G) offs[j * 256 + d] = run;
+                if (i < S && j < G) offs[j * ND + d] = run;
                 run += c[i];
             }
         }
         grid_sync(bar, target, polls, flags);
         // Scatter: stage in digit order, store each digit's run from the block's start.
-        if (tid < 256) gshift[tid] = static_cast<int>(__ldcg(offs + b * 256 + tid)) - static_cast<int>(dstart[tid]);
+        for (int d = tid; d < ND; d += kFusedThreads)
+            gshift[d] = static_cast<int>(__ldcg(offs + b * ND + d)) - static_cast<int>(dstart[d]);
 #pragma unroll
         for (int r = 0; r < K; ++r) {
             if (warp * 32 * K + r * 32 + lane < cnt) {
-                const unsigned d = static_cast<unsigned>((k[r] >> shift) & 0xFF);
-                stage[dstart[d] + wcnt[warp * 256 + d] + rk[r]] = k[r];
+                const unsigned d = static_cast<unsigned>(k[r] >> shift) & DM;
+                stage[dstart[d] + wcnt[warp * ND + d] + rk[r]] = k[r];
             }
         }
         __syncthreads();
         for (int q = tid; q < cnt; q += kFusedThreads) {
             const unsigned long long kk = stage[q];
-            const int dst = gshift[static_cast<unsigned>((kk >> shift) & 0xFF)] + q;
+            const int dst = gshift[static_cast<unsigned>(kk >> shift) & DM] + q;
             if (dst >= 0 && dst < n) out[dst] = kk;
         }
         grid_sync(bar, target, polls, flags);
@@ -2416,7 +2446,75 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
             if (lane >= o) incl += y;
         }
         whead[lane] = incl - x;
-        if (lane == 31) heads[b] = incl;
+        if (lane == 31) {
+            heads[b] = incl;
+            block_heads = incl;
+        }
+    }
+    grid_sync(bar, target, polls, flags);
+    // Cells opened by the block's keys: ranges, keys, hash entries.
+    if (warp == 0) {
+        unsigned long long below, all;
+        blocks_sum(heads, G, b, &below, &all);
+        if (lane == 0) {
+            bsum[0] = below;
+            bsum[3] = all;
+        }
+    }
+    __syncthreads();
+    // The hash in use this step: the power of two of at least
+    // hash_slots_per_cell slots per cell (at most the table; 0: the table),
+    // the same in every block (all cell counts are in). The prefix in use is
+    // cleared again at the end.
+    unsigned long long hmask = a.tune.hash_slots_per_cell > 0 ? 15 : f.hmask;
+    while (hmask < f.hmask && hmask + 1 < static_cast<unsigned long long>(a.tune.hash_slots_per_cell) * bsum[3])
+        hmask = 2 * hmask + 1;
+    {
+        // The block's cells take consecutive indices from `first`: ranges and
+        // keys stored from registers, keys listed in shared memory (the
+        // stage of the sort is free now) for the hash inserts, one per thread.
+        const unsigned int first = static_cast<unsigned int>(bsum[0]);
+        const unsigned int base = whead[warp];
+        unsigned int earlier = 0;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            const int li = warp * 32 * K + r * 32 + lane;
+            const int p = lo + li;
+            const bool head = (bal[r] >> lane) & 1u;
+            const unsigned int local = base + earlier + __popc(bal[r] & lanemask_lt()) + (head ? 1u : 0u) - 1u;
+            const int cid = static_cast<int>(first + local);
+            if (head && cid >= 0 && cid < n) {
+                const unsigned long long key = k[r] >> sh;
+                f.cell_begin[cid] = p;
+                f.cell_key[cid] = key;
+                stage[local] = key;
+            }
+            if (li < cnt && p == m - 1 && cid >= 0 && cid < n) {
+                ctrl->n_cells = cid + 1;
+                f.cell_begin[cid + 1] = m;
+            }
+            earlier += __popc(bal[r]);
+        }
+        if (m == 0 && !skip && b == 0 && tid == 0) {
+            ctrl->n_cells = 0;
+            f.cell_begin[0] = 0;
+        }
+        __syncthreads();
+        const int nh = min(static_cast<int>(block_heads), cnt);
+        for (int i = tid; i < nh; i += kFusedThreads) {
+            const int cid = static_cast<int>(first) + i;
+            if (cid >= n) break;
+            const unsigned long long key = stage[i];
+            unsigned long long h = hash_slot(key, hmask);
+            for (unsigned long long probe = 0; probe <= hmask; ++probe) {
+                const unsigned long long prev = atomicCAS(&f.hk[h], kEmpty, key);
+                if (prev == kEmpty || prev == key) {
+                    f.hv[h] = cid;
+                    break;
+                }
+                h = (h + 1) & hmask;
+            }
+        }
     }
     grid_arrive(bar, target);
     // Records in cell order (read only by the pair kernel, after this launch).
@@ -2474,48 +2572,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
         }
     }
     grid_wait(bar, target, polls, flags);
-    // Cells opened by the block's keys: ranges, keys, hash entries.
-    if (warp == 0) {
-        unsigned long long below, all;
-        blocks_sum(heads, G, b, &below, &all);
-        if (lane == 0) bsum[0] = below;
-    }
-    __syncthreads();
-    {
-        const unsigned int base = static_cast<unsigned int>(bsum[0]) + whead[warp];
-        unsigned int earlier = 0;
-#pragma unroll
-        for (int r = 0; r < K; ++r) {
-            const int li = warp * 32 * K + r * 32 + lane;
-            const int p = lo + li;
-            const bool head = (bal[r] >> lane) & 1u;
-            const int cid = static_cast<int>(base + earlier + __popc(bal[r] & lanemask_lt()) + (head ? 1u : 0u)) - 1;
-            if (head && cid >= 0 && cid < n) {
-                const unsigned long long key = k[r] >> sh;
-                f.cell_begin[cid] = p;
-                f.cell_key[cid] = key;
-                unsigned long long h = hash_slot(key, f.hmask);
-                for (unsigned long long probe = 0; probe <= f.hmask; ++probe) {
-                    const unsigned long long prev = atomicCAS(&f.hk[h], kEmpty, key);
-                    if (prev == kEmpty || prev == key) {
-                        f.hv[h] = cid;
-                        break;
-                    }
-                    h = (h + 1) & f.hmask;
-                }
-            }
-            if (li < cnt && p == m - 1 && cid >= 0 && cid < n) {
-                ctrl->n_cells = cid + 1;
-                f.cell_begin[cid + 1] = m;
-            }
-            earlier += __popc(bal[r]);
-        }
-        if (m == 0 && !skip && b == 0 && tid == 0) {
-            ctrl->n_cells = 0;
-            f.cell_begin[0] = 0;
-        }
-    }
-    grid_sync(bar, target, polls, flags);
     // Neighbours, column-list lengths and work-item counts of the block's share of the cells.
     const int nc = launch_gave_up(flags, &gave_up) ? 0 : max(0, min(__ldcg(&ctrl->n_cells), n));
     const int Rc = (nc + G - 1) / G;
@@ -2524,37 +2580,43 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
     unsigned long long cand = 0;
     int biggest = 0;
     unsigned int heavy_sum = 0, light_sum = 0;
-    for (int c = c0 + tid; c < c1; c += kFusedThreads) {
-        const unsigned long long key = __ldcg(f.cell_key + c);
-        const int b0 = __ldcg(f.cell_begin + c);
-        const int kc = __ldcg(f.cell_begin + c + 1) - b0;
-        int other = 0;
-        int* nb_out = f.nbr + 13 * static_cast<int64_t>(c);
+    // Forward neighbours: the block's (cell, offset) lookups spread over its
+    // threads, kLook at a time per thread with their probes in flight together.
+    {
+        constexpr int kLook = 6;
+        const int total = 13 * (c1 - c0);
+        for (int j0 = 0; j0 < total; j0 += kLook * kFusedThreads) {
+            unsigned long long want[kLook];
+            int found[kLook];
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            constexpr int kB = 7;
-            unsigned long long want[kB];
-            int found[kB];
-#pragma unroll
-            for (int i = 0; i < kB; ++i) {
-                const int o = half * kB + i;
-                want[i] = o < 13 ? forward_key(g, key, o) : kEmpty;
+            for (int i = 0; i < kLook; ++i) {
+                const int j = j0 + i * kFusedThreads + tid;
+                want[i] = kEmpty;
+                if (j < total) {
+                    const int c = c0 + j / 13;
+                    want[i] = forward_key(g, __ldcg(f.cell_key + c), j % 13);
+                }
             }
-            hash_find_batch<kB>(f.hk, f.hv, f.hmask, want, found);
-            int beg[kB], end[kB];
+            hash_find_batch<kLook>(f.hk, f.hv, hmask, want, found);
 #pragma unroll
-            for (int i = 0; i < kB; ++i) {
-                const bool ok = found[i] >= 0 && found[i] < nc;
-                beg[i] = ok ? __ldcg(f.cell_begin + found[i]) : 0;
-                end[i] = ok ? __ldcg(f.cell_begin + found[i] + 1) : 0;
-            }
-#pragma unroll
-            for (int i = 0; i < kB; ++i) {
-                const int o = half * kB + i;
-                if (o < 13) nb_out[o] = found[i];
-                other += end[i] - beg[i];
+            for (int i = 0; i < kLook; ++i) {
+                const int j = j0 + i * kFusedThreads + tid;
+                if (j < total) f.nbr[13 * static_cast<int64_t>(c0) + j] = (found[i] >= 0 && found[i] < nc) ? found[i] : -1;
             }
         }
+    }
+    __syncthreads();
+    for (int c = c0 + tid; c < c1; c += kFusedThreads) {
+        const int b0 = __ldcg(f.cell_begin + c);
+        const int kc = __ldcg(f.cell_begin + c + 1) - b0;
+        const int* nb = f.nbr + 13 * static_cast<int64_t>(c);
+        int fo[13];
+#pragma unroll
+        for (int o = 0; o < 13; ++o) fo[o] = __ldcg(nb + o);
+        int other = 0;
+#pragma unroll
+        for (int o = 0; o < 13; ++o)
+            if (fo[o] >= 0) other += __ldcg(f.cell_begin + fo[o] + 1) - __ldcg(f.cell_begin + fo[o]);
         const int L = kc + other;
         f.cell_len[c] = L;
         const unsigned int n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
@@ -2591,6 +2653,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
         }
     }
     __syncthreads();
+    // The hash is no longer read in this step: each block clears its share of
+    // it for the next step (a chunk clears it once before its first step).
+    {
+        ulonglong2* h2 = reinterpret_cast<ulonglong2*>(f.hk);
+        const int64_t words = static_cast<int64_t>((hmask + 1) >> 1);
+        for (int64_t i = static_cast<int64_t>(b) * kFusedThreads + tid; i < words;
+             i += static_cast<int64_t>(G) * kFusedThreads)
+            h2[i] = make_ulonglong2(kEmpty, kEmpty);
+    }
     if (launch_gave_up(flags, &gave_up)) return;
     int64_t heavy_base = static_cast<int64_t>(bsum[1]);
     int64_t light_base = static_cast<int64_t>(bsum[2]);
@@ -2653,7 +2724,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
 // Blocks of the fused kernel per device (0: not available), set up on first use.
 std::atomic<int> g_fused_grid[kMaxSmDevices];
 
-size_t fused_smem_bytes(int K) { return 4 * 32 * 256 + sizeof(unsigned long long) * kFusedThreads * K; }
+// Dynamic shared memory of k_sort_cells<K, DB>: per-warp u16 digit counters,
+// the stage of K keys per thread, three u32 per digit.
+size_t fused_smem_bytes(int K, int DB) {
+    const size_t nd = size_t(1) << DB;
+    return 2 * 32 * nd + sizeof(unsigned long long) * kFusedThreads * K + 3 * 4 * nd;
+}
 
 int grid_for_block(int64_t n, int per_sm_blocks, int block) {
     const int sms = sm_count();
@@ -2698,9 +2774,9 @@ int fused_grid() {
     int blocks = coop ? sm_count() : 0;
     if (blocks > kFusedMaxGrid) blocks = 0;
     bool failed = false;
-    auto setup = [&](auto kernel, int K) {
+    auto setup = [&](auto kernel, int K, int DB) {
         if (blocks <= 0) return;
-        const int smem = static_cast<int>(fused_smem_bytes(K));
+        const int smem = static_cast<int>(fused_smem_bytes(K, DB));
         int occ = 0;
         if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kFusedThreads, smem) != cudaSuccess) {
@@ -2710,16 +2786,18 @@ int fused_grid() {
             blocks = 0;
         }
     };
-    setup(k_sort_cells<4>, 4);
-    setup(k_sort_cells<8>, 8);
-    setup(k_sort_cells<12>, 12);
+    setup(k_sort_cells<4, 8>, 4, 8);
+    setup(k_sort_cells<8, 8>, 8, 8);
+    setup(k_sort_cells<12, 8>, 12, 8);
+    setup(k_sort_cells<4, 11>, 4, 11);
+    setup(k_sort_cells<8, 11>, 8, 11);
     if (failed) cudaGetLastError();  // the attribute query's error, not a launch's
     g_fused_grid[dev].store(blocks > 0 ? blocks : -1, std::memory_order_relaxed);
     return blocks;
 }
 
 int64_t fused_scratch_words(int grid) {
-    return kFusedZeroWords + 3 * static_cast<int64_t>(grid) + 2 * 256 * static_cast<int64_t>(grid);
+    return kFusedZeroWords + 3 * static_cast<int64_t>(grid) + 2 * static_cast<int64_t>(kFusedDigits) * grid;
 }
 
 namespace {
@@ -2739,9 +2817,20 @@ bool sort_cells_fused(const DeviceBuffers& b, const StepArgs& a) {
     return grid > 0 && grid <= b.fused_grid && fused_keys_per_thread(a.n, grid) > 0;
 }
 
+// Digit width of the fused sort: 8 bits, or with tuning "sort_digit_bits" 11,
+// 11 bits (three passes where 8-bit digits take four) where its counters fit
+// next to the keys (K <= 8) and it saves a pass. At 1M objects the 11-bit form
+// is slower (173 vs 130 us a step): its 128 KB of per-warp counters leave L1
+// a fifth of its room for the cell phases' gathers and probes.
+int fused_digit_bits(const StepArgs& a, int K) {
+    if (a.tune.sort_digit_bits != 11 || K > 8) return 8;
+    return (8 * a.sort_passes + 10) / 11 < a.sort_passes ? 11 : 8;
+}
+
 void launch_sort_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     const int grid = fused_grid();
     const int K = fused_keys_per_thread(a.n, grid);
+    const int DB = fused_digit_bits(a, K);
     cudaMemsetAsync(b.fused, 0, sizeof(unsigned int) * kFusedZeroWords, stream);
     FusedArgs f{};
     f.keys[0] = b.keys[0];
@@ -2765,16 +2854,23 @@ void launch_sort_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t s
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kFusedThreads);
-    cfg.dynamicSmemBytes = fused_smem_bytes(K);
+    cfg.dynamicSmemBytes = fused_smem_bytes(K, DB);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (K == 4) cudaLaunchKernelEx(&cfg, k_sort_cells<4>, a, f);
-    else if (K == 8) cudaLaunchKernelEx(&cfg, k_sort_cells<8>, a, f);
-    else cudaLaunchKernelEx(&cfg, k_sort_cells<12>, a, f);
+    if (DB == 11) {
+        if (K == 4) cudaLaunchKernelEx(&cfg, k_sort_cells<4, 11>, a, f);
+        else cudaLaunchKernelEx(&cfg, k_sort_cells<8, 11>, a, f);
+    } else if (K == 4) {
+        cudaLaunchKernelEx(&cfg, k_sort_cells<4, 8>, a, f);
+    } else if (K == 8) {
+        cudaLaunchKernelEx(&cfg, k_sort_cells<8, 8>, a, f);
+    } else {
+        cudaLaunchKernelEx(&cfg, k_sort_cells<12, 8>, a, f);
+    }
 }
 
 void launch_chunk_init(const DeviceBuffers& b, int k_steps, cudaStream_t stream, bool checkpoint) {

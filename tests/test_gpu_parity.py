@@ -249,25 +249,32 @@ def test_fused_sort_and_cell_build_reproduce_the_reference(engine, name, steps, 
         engine.set_tuning("sort_rank_ballot", 0)
 
 
-@pytest.mark.parametrize("n_total,age", [(300_000, 3600.0), (1_100_000, 86400.0)])
+@pytest.mark.parametrize("n_total,age", [(300_000, 3600.0), (1_100_000, 86400.0), (1_500_000, 86400.0)])
 def test_fused_sort_and_cell_build_equal_the_separate_kernels(engine, ks, n_total, age):
-    """Larger populations (3 and 8 keys per thread of the fused kernel; the
-    second near its 8-key limit): every record, counter and state equal with
-    the fused launch and with the separate kernels."""
+    """Larger populations (4, 8 and 12 keys per thread of the fused kernel;
+    the second near its 8-key limit), with 8-bit and 11-bit digits and with
+    the whole hash or a crowded part of it (2 slots per cell: longer probe
+    sequences): every record, counter and state equal with the fused launch and
+    with the separate kernels."""
     st, sz, al = ks.generate_population(77, 20000, n_total, 60, age)
     runs = []
     try:
-        for fused in (1, 0):
+        for fused, bits, slots in ((1, 8, 0), (1, 11, 4), (1, 8, 2), (0, 8, 0)):
             engine.set_tuning("sort_fused", fused)
+            engine.set_tuning("sort_digit_bits", bits)
+            engine.set_tuning("hash_slots_per_cell", slots)
             runs.append(run_engine(engine, st, sz, al, 6, spg=3))
             assert engine.timing()["sort_cells_fused"] == fused
     finally:
         engine.set_tuning("sort_fused", 1)
-    (fs1, fa1, c1, s1), (fs0, fa0, c0, s0) = runs
-    assert len(c1) > 0
-    assert np.array_equal(fs1, fs0) and np.array_equal(fa1, fa0)
-    assert_same_conj(c1, c0)
-    assert_same_stats(s1, s0)
+        engine.set_tuning("sort_digit_bits", 8)
+        engine.set_tuning("hash_slots_per_cell", 0)
+    fs0, fa0, c0, s0 = runs[-1]
+    assert len(c0) > 0
+    for fs1, fa1, c1, s1 in runs[:-1]:
+        assert np.array_equal(fs1, fs0) and np.array_equal(fa1, fa0)
+        assert_same_conj(c1, c0)
+        assert_same_stats(s1, s0)
 
 
 def test_prepared_graphs_give_the_same_run(engine):
