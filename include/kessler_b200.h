@@ -103,10 +103,11 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * precision's pair kernel: 0 FP64 gate, two columns per lane; 1 FP64 gate, one
  * column per lane; 2, the default, the split kernel's FP32 gate on
  * cell-relative records; every variant decides with the exact FP64 filter),
- * "pair_blocks_per_sm" (0 = default),
+ * "pair_blocks_per_sm" (0 = default: 4 for the split kernel; 5 compiles it for
+ * 48 registers),
  * "subcell_bits" (0..3: Morton order of objects inside a cell; default 1), "box_min_rows"
  * (split pair kernel: skip tiles whose row and column blocks are provably
- * apart, for tiles of at least this many rows; 0 = off), "cell_scale_permille"
+ * apart, for tiles of at least this many rows; default 4; 0 = off), "cell_scale_permille"
  * (1000..4000: grid cell edge = the reference's edge x value/1000),
  * "prop_block" (32..128, threads per block of the propagation kernels),
  * "item_col_blocks" (1..64, column blocks of 32 per pair-kernel work item),

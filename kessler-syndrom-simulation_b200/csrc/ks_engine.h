@@ -179,7 +179,7 @@ struct Tuning {
     int pair_variant = 2;         // FP64 gate: 0 two columns per lane, 1 one; 2: FP32 gate on cell-relative records
     int pair_blocks_per_sm = 0;   // resident blocks of the pair kernel
     int subcell_bits = 1;         // Morton order inside cells, bits per axis (0..3)
-    int box_min_rows = 8;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
+    int box_min_rows = 4;         // split pairs: block-box pruning for tiles with at least this many rows (0: off)
     double cell_scale = 1.0;      // cell edge = reference edge x this (>= 1; changes only candidate counts)
     int prop_block = 128;         // threads per block of the propagation kernels (32..128, multiple of 32)
     int item_col_blocks = 16;     // column blocks of 32 per pair work item (1..64)

@@ -34,11 +34,16 @@ constexpr int kWarps = kBlock / 32;
 constexpr int kCellTile = 1024;            // sorted entries per cell-build tile
 constexpr int kPropBlock = 128;            // propagation: 4 blocks per SM (at most 128 registers)
 
-// Forward neighbour offsets (src/core/collision_filter.hpp:137-140): with the
-// pairs inside a cell they visit every pair of neighbouring cells once.
-__constant__ int c_forward[13][3] = {{1, -1, -1}, {1, -1, 0}, {1, -1, 1}, {1, 0, -1}, {1, 0, 0},
-                                      {1, 0, 1},   {1, 1, -1}, {1, 1, 0},  {1, 1, 1},  {0, 1, -1},
-                                      {0, 1, 0},   {0, 1, 1},  {0, 0, 1}};
+// Forward neighbour offset o in 0..12 (src/core/collision_filter.hpp:137-140):
+// with the pairs inside a cell they visit every pair of neighbouring cells
+// once. o < 9 is (1, o/3 - 1, o%3 - 1), 9..11 is (0, 1, o - 10), 12 is
+// (0, 0, 1); computed rather than read from a table at a lane-varying index,
+// which constant memory serialises.
+__device__ __forceinline__ void forward_offset(int o, int& dx, int& dy, int& dz) {
+    dx = o < 9 ? 1 : 0;
+    dy = o < 9 ? o / 3 - 1 : (o < 12 ? 1 : 0);
+    dz = o < 9 ? o % 3 - 1 : (o < 12 ? o - 10 : 1);
+}
 
 // Order-preserving map of doubles to u64 (for atomicMin / atomicMax).
 __device__ __forceinline__ unsigned long long enc_double(double x) {
@@ -1046,12 +1051,8 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
     for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
          t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int c = static_cast<int>(t / 13), o = static_cast<int>(t - 13 * static_cast<int64_t>(c));
-        // Offset o of c_forward, computed rather than read from constant memory
-        // at a lane-varying index (which serialises): o < 9 is (1, o/3 - 1, o%3 - 1),
-        // 9..11 is (0, 1, o - 10), 12 is (0, 0, 1).
-        const int dx = o < 9 ? 1 : 0;
-        const int dy = o < 9 ? o / 3 - 1 : (o < 12 ? 1 : 0);
-        const int dz = o < 9 ? o % 3 - 1 : (o < 12 ? o - 10 : 1);
+        int dx, dy, dz;
+        forward_offset(o, dx, dy, dz);
         const unsigned long long key = cell_key_in[c];
         const unsigned long long rid = key >> (g.w[0] + g.w[1] + g.w[2]);
         const long long x = static_cast<long long>((key >> (g.w[1] + g.w[2])) & ((1ull << g.w[0]) - 1)) + dx;
@@ -1430,6 +1431,20 @@ __device__ __forceinline__ int locate(const SegTable& t, int nseg, int p, int* s
     return t.begin[lo] + (p - t.start[lo]);
 }
 
+// Column index p -> sorted position and the index of its segment in the table.
+__device__ __forceinline__ int locate_segment(const SegTable& t, int nseg, int p, int* seg) {
+    int lo = 0, hi = nseg - 1;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+        const int mid = (lo + hi + 1) >> 1;
+        const bool ge = t.start[mid] <= p;
+        lo = ge ? mid : lo;
+        hi = ge ? hi : mid - 1;
+    }
+    *seg = lo;
+    return t.begin[lo] + (p - t.start[lo]);
+}
+
 // Position / velocity bounding box of the 32 lanes' FP64 states.
 struct BoxD {
     double pmin[3], pmax[3], vmin[3], vmax[3];
@@ -1616,7 +1631,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
 // (filter_pair on the FP64 states) for the pairs the FP32 tests cannot
 // reject. Rows and columns are FP32 records relative to their own cell's
 // corner; a column from forward neighbour o is moved into the row cell's
-// frame by c_forward[o] cell edges. Tiles whose row block and column block
+// frame by forward_offset(o) cell edges. Tiles whose row block and column block
 // are provably apart over the whole step (position and velocity boxes) are
 // skipped before the row loop.
 // ---------------------------------------------------------------------------
@@ -1799,6 +1814,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
     // Per-warp queue of flagged (column lane, row) pairs for the compacted second stage.
     __shared__ unsigned short pq[kWarps][64];
+    // Per segment of the item's column list: the move of its records into the
+    // row cell's frame (the forward offset times the cell edge; 0 for the cell itself).
+    __shared__ float4 segoff[kWarps][16];
     __shared__ int2 fq[kWarps][64];
     if (step_void(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1831,6 +1849,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
         __syncwarp();
         int nseg;
         const int L = build_segments(segs[warp], c, b0, k, cell_begin, nbr, &nseg);
+        if (lane < nseg) {
+            // Segment id 0 is the cell itself, 1 + o its forward neighbour o.
+            const int o = segs[warp].id[lane] - 1;
+            int dx = 0, dy = 0, dz = 0;
+            if (o >= 0) forward_offset(o, dx, dy, dz);
+            // dx cell_f is exact (dx in {-1, 0, 1}): adding it rounds once, as fma(dx, cell_f, x) did.
+            segoff[warp][lane] = make_float4(static_cast<float>(dx) * cell_f, static_cast<float>(dy) * cell_f,
+                                             static_cast<float>(dz) * cell_f, 0.0f);
+        }
         const int r0 = 32 * ra;
         const int nr = min(32, k - r0);
         const unsigned nrmask = nr >= 32 ? 0xffffffffu : ((1u << nr) - 1u);
@@ -1882,14 +1909,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
         for (int cb = cb0; cb < cb0 + ncb; ++cb) {
             const int p = 32 * cb + lane;
             const bool ok = p < L;
-            int sid = 0;
-            const int q = ok ? locate(segs[warp], nseg, p, &sid) : b0;
+            int seg = 0;
+            const int q = ok ? locate_segment(segs[warp], nseg, p, &seg) : b0;
             float4 cp = sorted32[2 * static_cast<int64_t>(q)];
             const float4 cv = sorted32[2 * static_cast<int64_t>(q) + 1];
-            if (sid > 0) {
-                cp.x = fmaf(static_cast<float>(c_forward[sid - 1][0]), cell_f, cp.x);
-                cp.y = fmaf(static_cast<float>(c_forward[sid - 1][1]), cell_f, cp.y);
-                cp.z = fmaf(static_cast<float>(c_forward[sid - 1][2]), cell_f, cp.z);
+            if (seg > 0) {
+                const float4 o = segoff[warp][seg];
+                cp.x += o.x;
+                cp.y += o.y;
+                cp.z += o.z;
             }
             const unsigned valid = ok ? (cb == ra ? lanes_below : 0xffffffffu) & nrmask : 0u;
             if (!use_box) {
@@ -2238,9 +2266,8 @@ __device__ __forceinline__ void hash_find_batch(const unsigned long long* hk, co
 
 // Key of forward neighbour o of the cell with key `key`, or kEmpty outside the grid.
 __device__ __forceinline__ unsigned long long forward_key(const GridParams& g, unsigned long long key, int o) {
-    const int dx = o < 9 ? 1 : 0;
-    const int dy = o < 9 ? o / 3 - 1 : (o < 12 ? 1 : 0);
-    const int dz = o < 9 ? o % 3 - 1 : (o < 12 ? o - 10 : 1);
+    int dx, dy, dz;
+    forward_offset(o, dx, dy, dz);
     const int wyz = g.w[1] + g.w[2];
     const unsigned long long rid = key >> (g.w[0] + wyz);
     const long long x = static_cast<long long>((key >> wyz) & ((1ull << g.w[0]) - 1)) + dx;
@@ -3092,10 +3119,15 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
 void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream) {
     // Default: the resident block count of each kernel.
     if (f32_records(a)) {
-        // Register budget for 3 resident blocks per SM (80 registers), or for 4
-        // (64; the default: the higher occupancy outweighs a few spilled registers).
+        // Register budget for 3 resident blocks per SM (80 registers), for 4
+        // (64; the default: the higher occupancy outweighs a few spilled
+        // registers) or for 5 (48; the most its shared memory allows).
         const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 4;
-        if (bps >= 4)
+        if (bps >= 5)
+            k_pairs_split<5><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
+                                                                     b.cell_begin, b.nbr, b.items, b.items_cap,
+                                                                     b.survivors, b.surv_cap);
+        else if (bps == 4)
             k_pairs_split<4><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
                                                                      b.cell_begin, b.nbr, b.items, b.items_cap,
                                                                      b.survivors, b.surv_cap);

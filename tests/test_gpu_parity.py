@@ -69,6 +69,7 @@ def test_chunking_and_graph_parity_do_not_change_results(engine):
 
 
 @pytest.mark.parametrize("variant,bps,x2,s2", [(0, 0, 1, 1), (0, 1, 1, 1), (1, 5, 1, 1), (1, 0, 1, 1), (2, 3, 1, 1),
+                                               (2, 5, 1, 1),
                                                (2, 1, 1, 1), (2, 0, 0, 1), (2, 3, 0, 0), (2, 0, 1, 0), (2, 0, 1, 2),
                                                (2, 3, 0, 2)])
 def test_tuning_knobs_do_not_change_results(engine, variant, bps, x2, s2):

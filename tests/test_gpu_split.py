@@ -134,7 +134,7 @@ def test_grid_order_and_pruning_knobs_do_not_change_results(engine, ks, prec, su
         got = run()
     finally:
         engine.set_tuning("subcell_bits", 1)
-        engine.set_tuning("box_min_rows", 8)
+        engine.set_tuning("box_min_rows", 4)
         engine.set_precision(ks.PRECISION_FP64)
     assert np.array_equal(got[0][0], base[0][0])
     same_conj(got[1], base[1])

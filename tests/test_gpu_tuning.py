@@ -42,7 +42,7 @@ def test_autotune_keeps_results(engine, oracle, ks, precision):
         else:
             # the same split run with the default configuration
             for key, val in (("pair_variant", 2), ("pair_blocks_per_sm", 0), ("subcell_bits", 1),
-                             ("box_min_rows", 8), ("cell_scale_permille", 1000), ("prop_block", 128)):
+                             ("box_min_rows", 4), ("cell_scale_permille", 1000), ("prop_block", 128)):
                 engine.set_tuning(key, val)
             engine.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, 10.0)
             engine.set_population(st, sz, al)
@@ -54,7 +54,7 @@ def test_autotune_keeps_results(engine, oracle, ks, precision):
             assert_same_conj(conj, engine.take_conjunctions())
             engine.take_step_stats()
     finally:
-        for key, val in (("pair_variant", 2), ("pair_blocks_per_sm", 0), ("subcell_bits", 1), ("box_min_rows", 8),
+        for key, val in (("pair_variant", 2), ("pair_blocks_per_sm", 0), ("subcell_bits", 1), ("box_min_rows", 4),
                          ("cell_scale_permille", 1000), ("prop_block", 128)):
             engine.set_tuning(key, val)
         engine.set_steps_per_graph(32)
