@@ -305,7 +305,7 @@ typedef struct ks_timing {
     double chunk_ms;       /* device work of the chunks outside their steps: set-up, checkpoint,
                               ordering of the chunk's conjunction records, replays (L2 flushes excluded) */
     int64_t sort_cells_fused;  /* 1: the last steps sorted and built the cells in one cooperative launch
-                                  (sort_ms then holds both, cells_ms is 0) */
+                                  (sort_ms then holds both, cells_ms is 0); 0: separate kernels */
     /* Host wall time of the run's chunks (fragmentation on the host), always
      * measured: in all, before the first launch of each chunk (parameters,
      * buffer sizing, graph capture), in the launch calls, waiting for the

@@ -207,6 +207,8 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
         KS_CUDA(cudaMalloc(&b.fused, sizeof(unsigned int) * ks::fused_scratch_words(fg)));
         b.fused_grid = fg;
     }
+    // Every path leaves the cell-key hash empty after a step; it starts so.
+    KS_CUDA(cudaMemset(b.hash_keys, 0xFF, sizeof(unsigned long long) * h));
     if (ctx->dev_sbm) {
         KS_CUDA(cudaMalloc(&b.n_live, sizeof(int)));
         KS_CUDA(cudaMalloc(&b.mass_kg, sizeof(double) * cap));
@@ -432,6 +434,11 @@ StepArgs step_args(ks_ctx* ctx, int k, int k_steps, int src) {
     return a;
 }
 
+// Which cell build the steps take: 0 separate kernels, 1 the fused launch.
+int fused_form(ks_ctx* ctx) {
+    return ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, 1, 0)) ? 1 : 0;
+}
+
 ks::SbmArgs sbm_args(const ks_ctx* ctx) {
     ks::SbmArgs s{};
     s.lc_m = ctx->bk.params.lc_m;
@@ -464,10 +471,6 @@ void enqueue_chunk(ks_ctx* ctx, int k_steps, int src0, bool capturing) {
     cudaStream_t s = ctx->stream;
     cudaMemcpyAsync(ctx->b.params, ctx->h_params, sizeof(StepParams) * k_steps, cudaMemcpyHostToDevice, s);
     ks::launch_chunk_init(ctx->b, k_steps, s, true);
-    // The fused sort + cell build leaves the cell-key hash empty for the next
-    // step; it is cleared once here for the chunk's first.
-    if (ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, k_steps, src0)))
-        cudaMemsetAsync(ctx->b.hash_keys, 0xFF, sizeof(unsigned long long) * ctx->b.hash_cap, s);
     int src = src0;
     for (int k = 0; k < k_steps; ++k) {
         const StepArgs a = step_args(ctx, k, k_steps, src);
@@ -753,7 +756,7 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     accumulate_timing(ctx, done);
     ctx->timing.steps += done;
     ctx->timing.sort_passes = ctx->sort_passes;
-    ctx->timing.sort_cells_fused = ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, 1, 0)) ? 1 : 0;
+    ctx->timing.sort_cells_fused = fused_form(ctx);
     ctx->steps_done += done;
     ctx->t = done == k_steps ? t_end : ctx->h_params[done].t0;
     if (done & 1) ctx->cur ^= 1;
@@ -952,7 +955,7 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     accumulate_timing(ctx, k_steps);
     ctx->timing.steps += k_steps;
     ctx->timing.sort_passes = ctx->sort_passes;
-    ctx->timing.sort_cells_fused = ctx->screening && ks::sort_cells_fused(ctx->b, step_args(ctx, 0, 1, 0)) ? 1 : 0;
+    ctx->timing.sort_cells_fused = fused_form(ctx);
     ctx->steps_done += k_steps;
     ctx->t = t_end;
     if (k_steps & 1) ctx->cur ^= 1;

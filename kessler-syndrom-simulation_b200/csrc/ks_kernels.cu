@@ -2278,6 +2278,161 @@ __device__ __forceinline__ unsigned long long forward_key(const GridParams& g, u
            (static_cast<unsigned long long>(y) << g.w[2]) | static_cast<unsigned long long>(z);
 }
 
+// The cell phases both fused launches share, once the step's cell table
+// (cell_begin, cell_key, n_cells) and hash are complete: each block's share of
+// the cells gets its 13 forward neighbours (lookups spread over the threads),
+// its column-list lengths and work-item counts (heavy and light totals per
+// block; barrier), then the work list, heavy cells' items first, each group in
+// cell order. `clear` runs once the hash is no longer read.
+template <typename Clear>
+__device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedArgs& f, Ctrl* ctrl, int n,
+                                                 unsigned long long hmask, const GridParams& g, unsigned int* wsum,
+                                                 unsigned long long* bsum, int* gave_up, unsigned int* iparts,
+                                                 unsigned int* bar, unsigned int& target, int polls, int* flags,
+                                                 Clear clear) {
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // Neighbours, column-list lengths and work-item counts of the block's share of the cells.
+    const int nc = launch_gave_up(flags, gave_up) ? 0 : max(0, min(__ldcg(&ctrl->n_cells), n));
+    const int Rc = (nc + G - 1) / G;
+    const int c0 = min(nc, b * Rc), c1 = min(nc, c0 + Rc);
+    const int per = f.per;
+    unsigned long long cand = 0;
+    int biggest = 0;
+    unsigned int heavy_sum = 0, light_sum = 0;
+    // Forward neighbours: the block's (cell, offset) lookups spread over its
+    // threads, kLook at a time per thread with their probes in flight together.
+    {
+        constexpr int kLook = 6;
+        const int total = 13 * (c1 - c0);
+        for (int j0 = 0; j0 < total; j0 += kLook * kFusedThreads) {
+            unsigned long long want[kLook];
+            int found[kLook];
+#pragma unroll
+            for (int i = 0; i < kLook; ++i) {
+                const int j = j0 + i * kFusedThreads + tid;
+                want[i] = kEmpty;
+                if (j < total) {
+                    const int c = c0 + j / 13;
+                    want[i] = forward_key(g, __ldcg(f.cell_key + c), j % 13);
+                }
+            }
+            hash_find_batch<kLook>(f.hk, f.hv, hmask, want, found);
+#pragma unroll
+            for (int i = 0; i < kLook; ++i) {
+                const int j = j0 + i * kFusedThreads + tid;
+                if (j < total) f.nbr[13 * static_cast<int64_t>(c0) + j] = (found[i] >= 0 && found[i] < nc) ? found[i] : -1;
+            }
+        }
+    }
+    __syncthreads();
+    for (int c = c0 + tid; c < c1; c += kFusedThreads) {
+        const int b0 = __ldcg(f.cell_begin + c);
+        const int kc = __ldcg(f.cell_begin + c + 1) - b0;
+        const int* nb = f.nbr + 13 * static_cast<int64_t>(c);
+        int fo[13];
+#pragma unroll
+        for (int o = 0; o < 13; ++o) fo[o] = __ldcg(nb + o);
+        int other = 0;
+#pragma unroll
+        for (int o = 0; o < 13; ++o)
+            if (fo[o] >= 0) other += __ldcg(f.cell_begin + fo[o] + 1) - __ldcg(f.cell_begin + fo[o]);
+        const int L = kc + other;
+        f.cell_len[c] = L;
+        const unsigned int n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
+        if (heavy_cell(kc, L)) heavy_sum += n_items;
+        else light_sum += n_items;
+        cand += static_cast<unsigned long long>(kc) * (kc - 1) / 2 + static_cast<unsigned long long>(kc) * other;
+        biggest = max(biggest, kc);
+    }
+    cand = warp_sum(cand);
+    biggest = warp_max(biggest);
+    if (lane == 0) {
+        if (cand) atomicAdd(&ctrl->candidates, cand);
+        if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
+    }
+    {
+        unsigned int ht, lt;
+        scan_1024(heavy_sum, &ht, wsum);
+        scan_1024(light_sum, &lt, wsum);
+        if (tid == 0) {
+            iparts[b] = ht;
+            iparts[G + b] = lt;
+        }
+    }
+    grid_sync(bar, target, polls, flags);
+    // Work list: heavy cells' items first, then the light cells', each in cell order.
+    if (warp == 0) {
+        unsigned long long hb, ha, lb, la;
+        blocks_sum(iparts, G, b, &hb, &ha);
+        blocks_sum(iparts + G, G, b, &lb, &la);
+        if (lane == 0) {
+            bsum[1] = hb;
+            bsum[2] = ha + lb;
+            if (b == 0) ctrl->n_items = static_cast<unsigned int>(ha + la);
+        }
+    }
+    __syncthreads();
+    // The hash is no longer read in this step.
+    clear();
+    if (launch_gave_up(flags, gave_up)) return;
+    int64_t heavy_base = static_cast<int64_t>(bsum[1]);
+    int64_t light_base = static_cast<int64_t>(bsum[2]);
+    bool over = false;
+    for (int blk = c0; blk < c1; blk += kFusedThreads) {
+        const int c = blk + tid;
+        int kc = 0, L = 0;
+        unsigned int n_items = 0;
+        bool heavy = false;
+        if (c < c1) {
+            kc = __ldcg(f.cell_begin + c + 1) - __ldcg(f.cell_begin + c);
+            L = __ldcg(f.cell_len + c);
+            heavy = heavy_cell(kc, L);
+            n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
+        }
+        unsigned int ht, lt;
+        const int64_t hoff = heavy_base + scan_1024(heavy ? n_items : 0u, &ht, wsum);
+        const int64_t loff = light_base + scan_1024(c < c1 && !heavy ? n_items : 0u, &lt, wsum);
+        heavy_base += ht;
+        light_base += lt;
+        const bool small = c < c1 && n_items <= 32;
+        if (small) {
+            const int ta = (kc + 31) >> 5, tc = (L + 31) >> 5;
+            int64_t w = heavy ? hoff : loff;
+            for (int ra = 0; ra < ta; ++ra)
+                for (int cb = ra; cb < tc; cb += per, ++w) {
+                    if (w < f.items_cap) f.items[w] = make_int4(c, ra, cb, min(per, tc - cb));
+                    else over = true;
+                }
+        }
+        // Cells with more than 32 items (all heavy): the warp writes them together.
+        unsigned big = __ballot_sync(0xffffffffu, c < c1 && !small);
+        while (big) {
+            const int src = __ffs(big) - 1;
+            big &= big - 1;
+            const int cc = blk + (tid & ~31) + src;
+            const int kk = __shfl_sync(0xffffffffu, kc, src), LL = __shfl_sync(0xffffffffu, L, src);
+            const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
+            int64_t wbase = __shfl_sync(0xffffffffu, hoff, src);
+            for (int a0 = 0; a0 < ta; a0 += 32) {
+                const int ra = a0 + lane;
+                const unsigned int mine = ra < ta ? row_block_items(ra, tc, per) : 0u;
+                unsigned int incl = mine;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                int64_t w = wbase + (incl - mine);
+                for (int cb = ra; ra < ta && cb < tc; cb += per, ++w) {
+                    if (w < f.items_cap) f.items[w] = make_int4(cc, ra, cb, min(per, tc - cb));
+                    else over = true;
+                }
+                wbase += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+    }
+    if (over) atomicOr(flags, FLAG_ITEMS_OVERFLOW);
+}
+
 template <int K, int DB>
 __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, FusedArgs f) {
     constexpr int ND = 1 << DB;              // digits of a pass
@@ -2599,154 +2754,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
         }
     }
     grid_wait(bar, target, polls, flags);
-    // Neighbours, column-list lengths and work-item counts of the block's share of the cells.
-    const int nc = launch_gave_up(flags, &gave_up) ? 0 : max(0, min(__ldcg(&ctrl->n_cells), n));
-    const int Rc = (nc + G - 1) / G;
-    const int c0 = min(nc, b * Rc), c1 = min(nc, c0 + Rc);
-    const int per = f.per;
-    unsigned long long cand = 0;
-    int biggest = 0;
-    unsigned int heavy_sum = 0, light_sum = 0;
-    // Forward neighbours: the block's (cell, offset) lookups spread over its
-    // threads, kLook at a time per thread with their probes in flight together.
-    {
-        constexpr int kLook = 6;
-        const int total = 13 * (c1 - c0);
-        for (int j0 = 0; j0 < total; j0 += kLook * kFusedThreads) {
-            unsigned long long want[kLook];
-            int found[kLook];
-#pragma unroll
-            for (int i = 0; i < kLook; ++i) {
-                const int j = j0 + i * kFusedThreads + tid;
-                want[i] = kEmpty;
-                if (j < total) {
-                    const int c = c0 + j / 13;
-                    want[i] = forward_key(g, __ldcg(f.cell_key + c), j % 13);
-                }
-            }
-            hash_find_batch<kLook>(f.hk, f.hv, hmask, want, found);
-#pragma unroll
-            for (int i = 0; i < kLook; ++i) {
-                const int j = j0 + i * kFusedThreads + tid;
-                if (j < total) f.nbr[13 * static_cast<int64_t>(c0) + j] = (found[i] >= 0 && found[i] < nc) ? found[i] : -1;
-            }
-        }
-    }
-    __syncthreads();
-    for (int c = c0 + tid; c < c1; c += kFusedThreads) {
-        const int b0 = __ldcg(f.cell_begin + c);
-        const int kc = __ldcg(f.cell_begin + c + 1) - b0;
-        const int* nb = f.nbr + 13 * static_cast<int64_t>(c);
-        int fo[13];
-#pragma unroll
-        for (int o = 0; o < 13; ++o) fo[o] = __ldcg(nb + o);
-        int other = 0;
-#pragma unroll
-        for (int o = 0; o < 13; ++o)
-            if (fo[o] >= 0) other += __ldcg(f.cell_begin + fo[o] + 1) - __ldcg(f.cell_begin + fo[o]);
-        const int L = kc + other;
-        f.cell_len[c] = L;
-        const unsigned int n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
-        if (heavy_cell(kc, L)) heavy_sum += n_items;
-        else light_sum += n_items;
-        cand += static_cast<unsigned long long>(kc) * (kc - 1) / 2 + static_cast<unsigned long long>(kc) * other;
-        biggest = max(biggest, kc);
-    }
-    cand = warp_sum(cand);
-    biggest = warp_max(biggest);
-    if (lane == 0) {
-        if (cand) atomicAdd(&ctrl->candidates, cand);
-        if (biggest > 0) atomicMax(&ctrl->max_cell, biggest);
-    }
-    {
-        unsigned int ht, lt;
-        scan_1024(heavy_sum, &ht, wsum);
-        scan_1024(light_sum, &lt, wsum);
-        if (tid == 0) {
-            iparts[b] = ht;
-            iparts[G + b] = lt;
-        }
-    }
-    grid_sync(bar, target, polls, flags);
-    // Work list: heavy cells' items first, then the light cells', each in cell order.
-    if (warp == 0) {
-        unsigned long long hb, ha, lb, la;
-        blocks_sum(iparts, G, b, &hb, &ha);
-        blocks_sum(iparts + G, G, b, &lb, &la);
-        if (lane == 0) {
-            bsum[1] = hb;
-            bsum[2] = ha + lb;
-            if (b == 0) ctrl->n_items = static_cast<unsigned int>(ha + la);
-        }
-    }
-    __syncthreads();
-    // The hash is no longer read in this step: each block clears its share of
-    // it for the next step (a chunk clears it once before its first step).
-    {
+    // Neighbours, column-list lengths and work-item counts, then the work list;
+    // the hash is cleared for the next step once no longer read (a chunk also
+    // clears it once before its first step).
+    fused_cells_tail(a, f, ctrl, n, hmask, g, wsum, bsum, &gave_up, iparts, bar, target, polls, flags, [&]() {
         ulonglong2* h2 = reinterpret_cast<ulonglong2*>(f.hk);
         const int64_t words = static_cast<int64_t>((hmask + 1) >> 1);
         for (int64_t i = static_cast<int64_t>(b) * kFusedThreads + tid; i < words;
              i += static_cast<int64_t>(G) * kFusedThreads)
             h2[i] = make_ulonglong2(kEmpty, kEmpty);
-    }
-    if (launch_gave_up(flags, &gave_up)) return;
-    int64_t heavy_base = static_cast<int64_t>(bsum[1]);
-    int64_t light_base = static_cast<int64_t>(bsum[2]);
-    bool over = false;
-    for (int blk = c0; blk < c1; blk += kFusedThreads) {
-        const int c = blk + tid;
-        int kc = 0, L = 0;
-        unsigned int n_items = 0;
-        bool heavy = false;
-        if (c < c1) {
-            kc = __ldcg(f.cell_begin + c + 1) - __ldcg(f.cell_begin + c);
-            L = __ldcg(f.cell_len + c);
-            heavy = heavy_cell(kc, L);
-            n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
-        }
-        unsigned int ht, lt;
-        const int64_t hoff = heavy_base + scan_1024(heavy ? n_items : 0u, &ht, wsum);
-        const int64_t loff = light_base + scan_1024(c < c1 && !heavy ? n_items : 0u, &lt, wsum);
-        heavy_base += ht;
-        light_base += lt;
-        const bool small = c < c1 && n_items <= 32;
-        if (small) {
-            const int ta = (kc + 31) >> 5, tc = (L + 31) >> 5;
-            int64_t w = heavy ? hoff : loff;
-            for (int ra = 0; ra < ta; ++ra)
-                for (int cb = ra; cb < tc; cb += per, ++w) {
-                    if (w < f.items_cap) f.items[w] = make_int4(c, ra, cb, min(per, tc - cb));
-                    else over = true;
-                }
-        }
-        // Cells with more than 32 items (all heavy): the warp writes them together.
-        unsigned big = __ballot_sync(0xffffffffu, c < c1 && !small);
-        while (big) {
-            const int src = __ffs(big) - 1;
-            big &= big - 1;
-            const int cc = blk + (tid & ~31) + src;
-            const int kk = __shfl_sync(0xffffffffu, kc, src), LL = __shfl_sync(0xffffffffu, L, src);
-            const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
-            int64_t wbase = __shfl_sync(0xffffffffu, hoff, src);
-            for (int a0 = 0; a0 < ta; a0 += 32) {
-                const int ra = a0 + lane;
-                const unsigned int mine = ra < ta ? row_block_items(ra, tc, per) : 0u;
-                unsigned int incl = mine;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                int64_t w = wbase + (incl - mine);
-                for (int cb = ra; ra < ta && cb < tc; cb += per, ++w) {
-                    if (w < f.items_cap) f.items[w] = make_int4(cc, ra, cb, min(per, tc - cb));
-                    else over = true;
-                }
-                wbase += __shfl_sync(0xffffffffu, incl, 31);
-            }
-        }
-    }
-    if (over) atomicOr(flags, FLAG_ITEMS_OVERFLOW);
+    });
 }
+
 
 // Blocks of the fused kernel per device (0: not available), set up on first use.
 std::atomic<int> g_fused_grid[kMaxSmDevices];
@@ -3107,6 +3126,8 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
                                                f32_records(a) ? b.sorted32 : nullptr, b.rec32, a.pack_bits);
     k_neighbours<<<grid_for(13 * static_cast<int64_t>(a.n), 8), kBlock, 0, stream>>>(
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
+    // Left empty for the fused launches, which take it so.
+    cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
     k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.item_part,
                                                            a.tune.item_col_blocks);
     // Offsets of the heavy, then the light cells' items per chunk of cells, and their total.
