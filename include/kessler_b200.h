@@ -131,9 +131,10 @@ int ks_set_l2_flush(ks_ctx* ctx, int64_t bytes);
  * "sort_digit_bits" (8, the default: the fused sort takes 8-bit digits; 11:
  * 11-bit digits where that saves a pass and their counters fit, three passes
  * for the four 8-bit ones of 32 key bits),
- * "hash_slots_per_cell" (0..64, default 0: the fused cell build probes the
- * whole cell-key hash, 2 slots per object; n: only the power of two of at
- * least n slots per cell of the step),
+ * "hash_slots_per_cell" (0..64, default 0: the fused cell build keeps its
+ * cell table as (key, cell) words in buckets of four, 4 slots per cell, where
+ * the cell keys take at most 40 bits, else the whole hash; n: (key, cell)
+ * pairs over the power of two of at least n slots per cell of the step),
  * "lookback_polls" (0..2^30, default 2^22: polls a radix-sort tile makes of a
  * predecessor's unpublished digit counts, or a block of the fused sort makes of
  * a grid barrier, before it gives up; a wait that runs out fails the run with

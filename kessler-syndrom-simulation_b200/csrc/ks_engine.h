@@ -190,7 +190,8 @@ struct Tuning {
     int prop_min_blocks = 4;      // FP64 propagation: resident 128-thread blocks per SM it is compiled for (4..6)
     int sort_fused = 1;           // object sort and cell build in one cooperative launch (k_sort_cells) where it fits
     int sort_digit_bits = 8;      // fused sort: 8-bit digits; 11: 11-bit digits where they save a pass and fit
-    int hash_slots_per_cell = 0;  // fused cell build: hash slots in use per cell, rounded up to a power of two (0: all)
+    int hash_slots_per_cell = 0;  // fused cell build: 0 packed buckets (4 slots a cell) where keys fit, else the whole
+                                  // table; n: (key, cell) pairs over n slots a cell (rounded to a power of two)
 };
 
 // Time from a fragmentation event to the end of its step and the lunar stages

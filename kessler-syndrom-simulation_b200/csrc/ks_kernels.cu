@@ -2264,6 +2264,64 @@ __device__ __forceinline__ void hash_find_batch(const unsigned long long* hk, co
     }
 }
 
+// The fused launch's cell table where cell keys leave room (at most 40 bits,
+// fewer than 2^24 - 1 cells): entries (cell key << 24 | cell index) in
+// buckets of four slots, one 32-byte sector each, filled in slot order; a
+// lookup reads its bucket in one sector and finds the cell or an empty slot
+// (the key is absent), and moves to the next bucket only past four entries.
+constexpr int kCellIdBits = 24;
+
+__device__ __forceinline__ unsigned long long cell_entry(unsigned long long key, int cid) {
+    return (key << kCellIdBits) | static_cast<unsigned long long>(cid);
+}
+
+__device__ __forceinline__ void cell_insert_packed(unsigned long long* hk, unsigned long long bmask,
+                                                   unsigned long long key, int cid) {
+    const unsigned long long e = cell_entry(key, cid);
+    unsigned long long bk = hash_slot(key, bmask);
+    for (unsigned long long probe = 0; probe <= bmask; ++probe) {
+        for (int j = 0; j < 4; ++j)
+            if (atomicCAS(&hk[4 * bk + j], kEmpty, e) == kEmpty) return;
+        bk = (bk + 1) & bmask;
+    }
+}
+
+template <int B>
+__device__ __forceinline__ void cell_find_batch_packed(const unsigned long long* hk, unsigned long long bmask,
+                                                       const unsigned long long (&want)[B], int (&found)[B]) {
+    ulonglong2 lo[B], hi[B];
+    unsigned long long bk[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        bk[i] = hash_slot(want[i], bmask);
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(hk + 4 * bk[i]);
+        lo[i] = want[i] != kEmpty ? __ldcg(p) : make_ulonglong2(kEmpty, kEmpty);
+        hi[i] = want[i] != kEmpty ? __ldcg(p + 1) : make_ulonglong2(kEmpty, kEmpty);
+    }
+    const unsigned long long idmask = (1ull << kCellIdBits) - 1;
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        found[i] = -1;
+        if (want[i] == kEmpty) continue;
+        unsigned long long e[4] = {lo[i].x, lo[i].y, hi[i].x, hi[i].y};
+        for (unsigned long long probe = 0; probe <= bmask; ++probe) {
+            bool done = false;
+            for (int j = 0; j < 4 && !done; ++j) {
+                if (e[j] == kEmpty) done = true;
+                else if ((e[j] >> kCellIdBits) == want[i]) {
+                    found[i] = static_cast<int>(e[j] & idmask);
+                    done = true;
+                }
+            }
+            if (done) break;
+            bk[i] = (bk[i] + 1) & bmask;   // a full bucket without the key: the next one
+            const ulonglong2* p = reinterpret_cast<const ulonglong2*>(hk + 4 * bk[i]);
+            const ulonglong2 a2 = __ldcg(p), b2 = __ldcg(p + 1);
+            e[0] = a2.x; e[1] = a2.y; e[2] = b2.x; e[3] = b2.y;
+        }
+    }
+}
+
 // Key of forward neighbour o of the cell with key `key`, or kEmpty outside the grid.
 __device__ __forceinline__ unsigned long long forward_key(const GridParams& g, unsigned long long key, int o) {
     int dx, dy, dz;
@@ -2286,7 +2344,8 @@ __device__ __forceinline__ unsigned long long forward_key(const GridParams& g, u
 // cell order. `clear` runs once the hash is no longer read.
 template <typename Clear>
 __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedArgs& f, Ctrl* ctrl, int n,
-                                                 unsigned long long hmask, const GridParams& g, unsigned int* wsum,
+                                                 unsigned long long hmask, bool packed, const GridParams& g,
+                                                 unsigned int* wsum,
                                                  unsigned long long* bsum, int* gave_up, unsigned int* iparts,
                                                  unsigned int* bar, unsigned int& target, int polls, int* flags,
                                                  Clear clear) {
@@ -2316,7 +2375,25 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
                     want[i] = forward_key(g, __ldcg(f.cell_key + c), j % 13);
                 }
             }
-            hash_find_batch<kLook>(f.hk, f.hv, hmask, want, found);
+            if (packed) {
+                // Two halves: each bucket read holds four entries in registers.
+                unsigned long long w0[kLook / 2], w1[kLook / 2];
+                int f0[kLook / 2], f1[kLook / 2];
+#pragma unroll
+                for (int i = 0; i < kLook / 2; ++i) {
+                    w0[i] = want[i];
+                    w1[i] = want[kLook / 2 + i];
+                }
+                cell_find_batch_packed<kLook / 2>(f.hk, hmask >> 2, w0, f0);
+                cell_find_batch_packed<kLook / 2>(f.hk, hmask >> 2, w1, f1);
+#pragma unroll
+                for (int i = 0; i < kLook / 2; ++i) {
+                    found[i] = f0[i];
+                    found[kLook / 2 + i] = f1[i];
+                }
+            } else {
+                hash_find_batch<kLook>(f.hk, f.hv, hmask, want, found);
+            }
 #pragma unroll
             for (int i = 0; i < kLook; ++i) {
                 const int j = j0 + i * kFusedThreads + tid;
@@ -2644,13 +2721,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
         }
     }
     __syncthreads();
-    // The hash in use this step: the power of two of at least
-    // hash_slots_per_cell slots per cell (at most the table; 0: the table),
-    // the same in every block (all cell counts are in). The prefix in use is
+    // The table in use this step, the same in every block (all cell counts
+    // are in): by default (hash_slots_per_cell 0), where the cell keys leave
+    // room, the packed bucketed table with 4 slots per cell (at 1M objects 87k
+    // cells in 512k slots, 4 MB, in L2); else (key, cell) pairs over
+    // hash_slots_per_cell slots per cell, or over the whole table. Either way
+    // a power of two of slots at most the table's, whose prefix in use is
     // cleared again at the end.
-    unsigned long long hmask = a.tune.hash_slots_per_cell > 0 ? 15 : f.hmask;
-    while (hmask < f.hmask && hmask + 1 < static_cast<unsigned long long>(a.tune.hash_slots_per_cell) * bsum[3])
-        hmask = 2 * hmask + 1;
+    const bool packed = a.tune.hash_slots_per_cell == 0 && g.bits - 3 * g.sub <= 64 - kCellIdBits &&
+                        bsum[3] + 1 < (1ull << kCellIdBits);
+    const unsigned long long per_cell = packed ? 4ull : static_cast<unsigned long long>(a.tune.hash_slots_per_cell);
+    unsigned long long hmask = per_cell > 0 ? 63 : f.hmask;
+    while (hmask < f.hmask && hmask + 1 < per_cell * bsum[3]) hmask = 2 * hmask + 1;
     {
         // The block's cells take consecutive indices from `first`: ranges and
         // keys stored from registers, keys listed in shared memory (the
@@ -2687,6 +2769,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
             const int cid = static_cast<int>(first) + i;
             if (cid >= n) break;
             const unsigned long long key = stage[i];
+            if (packed) {
+                cell_insert_packed(f.hk, hmask >> 2, key, cid);
+                continue;
+            }
             unsigned long long h = hash_slot(key, hmask);
             for (unsigned long long probe = 0; probe <= hmask; ++probe) {
                 const unsigned long long prev = atomicCAS(&f.hk[h], kEmpty, key);
@@ -2757,7 +2843,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
     // Neighbours, column-list lengths and work-item counts, then the work list;
     // the hash is cleared for the next step once no longer read (a chunk also
     // clears it once before its first step).
-    fused_cells_tail(a, f, ctrl, n, hmask, g, wsum, bsum, &gave_up, iparts, bar, target, polls, flags, [&]() {
+    fused_cells_tail(a, f, ctrl, n, hmask, packed, g, wsum, bsum, &gave_up, iparts, bar, target, polls, flags, [&]() {
         ulonglong2* h2 = reinterpret_cast<ulonglong2*>(f.hk);
         const int64_t words = static_cast<int64_t>((hmask + 1) >> 1);
         for (int64_t i = static_cast<int64_t>(b) * kFusedThreads + tid; i < words;
