@@ -147,7 +147,7 @@ void free_objects(ks_ctx* ctx) {
     for (int k = 0; k < 2; ++k) { dfree(b.state[k]); dfree(b.alive[k]); dfree(b.keys[k]); dfree(b.idx[k]); }
     dfree(b.size_m); dfree(b.real_id); dfree(b.ckpt_state); dfree(b.ckpt_alive); dfree(b.block_counts);
     dfree(b.sort_hist); dfree(b.sort_status); dfree(b.sort_ctr);
-    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
+    dfree(b.cell_begin); dfree(b.cell_key); dfree(b.nbr); dfree(b.cell_len); dfree(b.col_tab); dfree(b.item_part); dfree(b.hash_keys); dfree(b.hash_vals);
     dfree(b.sorted); dfree(b.sorted32); dfree(b.rec32); dfree(b.sorted_orig); dfree(b.fused);
     b.fused_grid = 0;
     dfree(b.n_live); dfree(b.mass_kg); dfree(b.a2m); dfree(b.event_of); dfree(b.coll); dfree(b.sbm_work);
@@ -191,6 +191,7 @@ int ensure_objects(ks_ctx* ctx, int64_t n) {
     KS_CUDA(cudaMalloc(&b.cell_key, sizeof(unsigned long long) * cap));
     KS_CUDA(cudaMalloc(&b.nbr, sizeof(int) * 13 * cap));
     KS_CUDA(cudaMalloc(&b.cell_len, sizeof(int) * cap));
+    KS_CUDA(cudaMalloc(&b.col_tab, sizeof(int2) * 16 * cap));
     KS_CUDA(cudaMalloc(&b.item_part, sizeof(unsigned int) * 2 * ((cap + 255) / 256 + 1)));
     int64_t h = 16;
     while (h < 2 * cap) h <<= 1;

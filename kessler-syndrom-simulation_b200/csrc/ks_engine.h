@@ -130,6 +130,7 @@ struct DeviceBuffers {
     unsigned long long* cell_key = nullptr;
     int* nbr = nullptr;                    // 13 per cell
     int* cell_len = nullptr;               // per cell: length of its column list
+    int2* col_tab = nullptr;               // per cell: its column list's segments for the pair kernel (16 int2)
     unsigned int* item_part = nullptr;     // heavy, then light cells' work items per chunk of 256 cells, then offsets
     int4* items = nullptr;
     int64_t items_cap = 0;

@@ -1070,6 +1070,34 @@ __global__ void __launch_bounds__(kBlock) k_neighbours(Ctrl* ctrl, const unsigne
     }
 }
 
+// A cell's column list for the pair kernel, 16 int2: entries 0..nseg-1 the
+// (first column, first sorted position) of each non-empty segment (the cell
+// itself, then its forward neighbours in offset order); entry 14 the
+// segments' ids, 4 bits each (0 the cell, 1 + o forward neighbour o); entry
+// 15 (column-list length L, nseg). One warp reads it in one 128-byte load.
+__device__ __forceinline__ void write_column_table(int2* __restrict__ t, int b0, int k, const int (&nb_begin)[13],
+                                                   const int (&nb_len)[13]) {
+    unsigned long long ids = 0;
+    int nseg = 1, start = k;
+    t[0] = make_int2(0, b0);
+#pragma unroll
+    for (int o = 0; o < 13; ++o) {
+        if (nb_len[o] <= 0) continue;
+        t[nseg] = make_int2(start, nb_begin[o]);
+        ids |= static_cast<unsigned long long>(o + 1) << (4 * nseg);
+        ++nseg;
+        start += nb_len[o];
+    }
+    t[14] = make_int2(static_cast<int>(static_cast<unsigned int>(ids)), static_cast<int>(static_cast<unsigned int>(ids >> 32)));
+    t[15] = make_int2(start, nseg);
+}
+
+// A pair work item, int4: (cell, row block | column blocks << 24, first column
+// block, the cell's first sorted position).
+__device__ __forceinline__ int4 work_item(int c, int row_block, int col_block, int col_blocks, int b0) {
+    return make_int4(c, row_block | (col_blocks << 24), col_block, b0);
+}
+
 // Number of work items of row block a: its column blocks a .. tc-1 in groups.
 __device__ __forceinline__ unsigned int row_block_items(int a, int tc, int per) {
     return static_cast<unsigned int>((tc - a + per - 1) / per);
@@ -1095,7 +1123,8 @@ __device__ __forceinline__ unsigned int cell_items(int ta, int tc, int per) {
 // heavy item before every light item, each group in cell order.
 __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* __restrict__ cell_begin,
                                                         const int* __restrict__ nbr, int* __restrict__ cell_len,
-                                                        unsigned int* __restrict__ part, int per) {
+                                                        int2* __restrict__ col_tab, unsigned int* __restrict__ part,
+                                                        int per) {
     if (step_void(ctrl)) return;
     const int nc = ctrl->n_cells;
     const int chunks = (nc + kBlock - 1) / kBlock;
@@ -1110,11 +1139,15 @@ __global__ void __launch_bounds__(kBlock) k_items_count(Ctrl* ctrl, const int* _
             const int k = cell_begin[c + 1] - b0;
             int other = 0;
             const int* nb = nbr + 13 * static_cast<int64_t>(c);
+            int nb_begin[13], nb_len[13];
 #pragma unroll
             for (int o = 0; o < 13; ++o) {
                 const int f = nb[o];
-                if (f >= 0) other += cell_begin[f + 1] - cell_begin[f];
+                nb_begin[o] = f >= 0 ? cell_begin[f] : 0;
+                nb_len[o] = f >= 0 ? cell_begin[f + 1] - nb_begin[o] : 0;
+                other += nb_len[o];
             }
+            write_column_table(col_tab + 16 * static_cast<int64_t>(c), b0, k, nb_begin, nb_len);
             const int L = k + other;
             const unsigned int n_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
             if (heavy_cell(k, L)) heavy_items = n_items;
@@ -1159,8 +1192,10 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
         int k = 0, L = 0;
         unsigned int n_items = 0;
         bool heavy = false;
+        int b0 = 0;
         if (c < nc) {
-            k = cell_begin[c + 1] - cell_begin[c];
+            b0 = cell_begin[c];
+            k = cell_begin[c + 1] - b0;
             L = cell_len[c];
             heavy = heavy_cell(k, L);
             n_items = cell_items((k + 31) >> 5, (L + 31) >> 5, per);
@@ -1176,7 +1211,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
             int64_t w = heavy ? hoff : loff;
             for (int a = 0; a < ta; ++a)
                 for (int cb = a; cb < tc; cb += per, ++w) {
-                    if (w < items_cap) items[w] = make_int4(c, a, cb, min(per, tc - cb));
+                    if (w < items_cap) items[w] = work_item(c, a, cb, min(per, tc - cb), b0);
                     else over = true;
                 }
         }
@@ -1187,6 +1222,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
             big &= big - 1;
             const int cc = blk + (threadIdx.x & ~31) + src;
             const int kk = __shfl_sync(0xffffffffu, k, src), LL = __shfl_sync(0xffffffffu, L, src);
+            const int bb = __shfl_sync(0xffffffffu, b0, src);
             const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
             int64_t wbase = __shfl_sync(0xffffffffu, hoff, src);
             for (int a0 = 0; a0 < ta; a0 += 32) {
@@ -1199,7 +1235,7 @@ __global__ void __launch_bounds__(kBlock) k_items_write(Ctrl* ctrl, const int* _
                 }
                 int64_t w = wbase + (incl - mine);
                 for (int cb = a; a < ta && cb < tc; cb += per, ++w) {
-                    if (w < items_cap) items[w] = make_int4(cc, a, cb, min(per, tc - cb));
+                    if (w < items_cap) items[w] = work_item(cc, a, cb, min(per, tc - cb), bb);
                     else over = true;
                 }
                 wbase += __shfl_sync(0xffffffffu, incl, 31);
@@ -1431,20 +1467,6 @@ __device__ __forceinline__ int locate(const SegTable& t, int nseg, int p, int* s
     return t.begin[lo] + (p - t.start[lo]);
 }
 
-// Column index p -> sorted position and the index of its segment in the table.
-__device__ __forceinline__ int locate_segment(const SegTable& t, int nseg, int p, int* seg) {
-    int lo = 0, hi = nseg - 1;
-#pragma unroll
-    for (int it = 0; it < 4; ++it) {
-        const int mid = (lo + hi + 1) >> 1;
-        const bool ge = t.start[mid] <= p;
-        lo = ge ? mid : lo;
-        hi = ge ? hi : mid - 1;
-    }
-    *seg = lo;
-    return t.begin[lo] + (p - t.start[lo]);
-}
-
 // Position / velocity bounding box of the 32 lanes' FP64 states.
 struct BoxD {
     double pmin[3], pmax[3], vmin[3], vmax[3];
@@ -1517,7 +1539,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_pairs_tiles(StepArgs a, const dou
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
         const int4 item = items[it];
-        const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
+        const int c = item.x, ra = item.y & 0xFFFFFF, cb0 = item.z;
+        const int ncb = static_cast<int>(static_cast<unsigned int>(item.y) >> 24);
         const int b0 = cell_begin[c];
         const int k = cell_begin[c + 1] - b0;
         __syncwarp();
@@ -1799,14 +1822,12 @@ template <int kMinBlocks>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, const double* __restrict__ before,
                                                         const float4* __restrict__ sorted32,
                                                         const int* __restrict__ orig,
-                                                        const int* __restrict__ cell_begin,
-                                                        const int* __restrict__ nbr, const int4* __restrict__ items,
+                                                        const int2* __restrict__ col_tab, const int4* __restrict__ items,
                                                         int64_t items_cap, int2* __restrict__ surv, int64_t surv_cap) {
     __shared__ float4 rows32[kWarps][32][2];
     // The same rows in pairs, components interleaved, for the packed gate.
     __shared__ float2 rows2[kWarps][16][6];
     __shared__ int rorig[kWarps][32];
-    __shared__ SegTable segs[kWarps];
     // Per-warp queue of columns that survived the row-box test, drained 32 at a time.
     __shared__ float4 qcol[kWarps][64][2];
     __shared__ int qidx[kWarps][64];
@@ -1814,9 +1835,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     // Per-warp queue of pairs for the exact filter (column's sorted position, row).
     // Per-warp queue of flagged (column lane, row) pairs for the compacted second stage.
     __shared__ unsigned short pq[kWarps][64];
-    // Per segment of the item's column list: the move of its records into the
-    // row cell's frame (the forward offset times the cell edge; 0 for the cell itself).
-    __shared__ float4 segoff[kWarps][16];
     __shared__ int2 fq[kWarps][64];
     if (step_void(a.ctrl)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1838,36 +1856,59 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
     const double vme = sqrt(a.vmin2) + ev_d;
     const float vmin2e = static_cast<float>(vme * vme * (1.0 + 1e-6));
     const int box_rows = a.tune.box_min_rows;
+    const int last_record = max(0, a.ctrl->n_alive - 1);
     PairCounters pc;
     int fcount = 0;
     // Items are handed out dynamically: their costs differ by orders of magnitude.
     for (int it = next_item(a.ctrl); it < n_items; it = next_item(a.ctrl)) {
         const int4 item = items[it];
-        const int c = item.x, ra = item.y, cb0 = item.z, ncb = item.w;
-        const int b0 = cell_begin[c];
-        const int k = cell_begin[c + 1] - b0;
-        __syncwarp();
-        int nseg;
-        const int L = build_segments(segs[warp], c, b0, k, cell_begin, nbr, &nseg);
-        if (lane < nseg) {
-            // Segment id 0 is the cell itself, 1 + o its forward neighbour o.
-            const int o = segs[warp].id[lane] - 1;
-            int dx = 0, dy = 0, dz = 0;
-            if (o >= 0) forward_offset(o, dx, dy, dz);
-            // dx cell_f is exact (dx in {-1, 0, 1}): adding it rounds once, as fma(dx, cell_f, x) did.
-            segoff[warp][lane] = make_float4(static_cast<float>(dx) * cell_f, static_cast<float>(dy) * cell_f,
-                                             static_cast<float>(dz) * cell_f, 0.0f);
-        }
+        const int c = item.x, ra = item.y & 0xFFFFFF, cb0 = item.z, b0 = item.w;
+        const int ncb = static_cast<int>(static_cast<unsigned int>(item.y) >> 24);
         const int r0 = 32 * ra;
+        // The cell's column table and its rows, loaded together (the rows of
+        // lanes past the cell's end are replaced below).
+        const int2 te = col_tab[16 * static_cast<int64_t>(c) + (lane & 15)];
+        const int rl = min(b0 + r0 + lane, last_record);
+        float4 my_rp = sorted32[2 * static_cast<int64_t>(rl)];
+        float4 my_rv = sorted32[2 * static_cast<int64_t>(rl) + 1];
+        const int my_orig = orig[rl];
+        const int L = __shfl_sync(0xffffffffu, te.x, 15), nseg = __shfl_sync(0xffffffffu, te.y, 15);
+        const unsigned id_lo = static_cast<unsigned>(__shfl_sync(0xffffffffu, te.x, 14));
+        const unsigned id_hi = static_cast<unsigned>(__shfl_sync(0xffffffffu, te.y, 14));
+        const int second = __shfl_sync(0xffffffffu, te.x, 1);
+        const int k = nseg > 1 ? second : L;
         const int nr = min(32, k - r0);
         const unsigned nrmask = nr >= 32 ? 0xffffffffu : ((1u << nr) - 1u);
-        const int rl = b0 + r0 + (lane < nr ? lane : 0);
-        const float4 my_rp = sorted32[2 * static_cast<int64_t>(rl)];
-        const float4 my_rv = sorted32[2 * static_cast<int64_t>(rl) + 1];
+        {
+            // Rows past nr repeat the first row (their bits are masked off).
+            const float4 p0 = make_float4(__shfl_sync(0xffffffffu, my_rp.x, 0), __shfl_sync(0xffffffffu, my_rp.y, 0),
+                                          __shfl_sync(0xffffffffu, my_rp.z, 0), my_rp.w);
+            const float4 v0 = make_float4(__shfl_sync(0xffffffffu, my_rv.x, 0), __shfl_sync(0xffffffffu, my_rv.y, 0),
+                                          __shfl_sync(0xffffffffu, my_rv.z, 0), my_rv.w);
+            if (lane >= nr) {
+                my_rp = p0;
+                my_rv = v0;
+            }
+        }
+        // Lane j < nseg holds segment j: its first column, the sorted position
+        // minus that column, and its move into the row cell's frame (the
+        // forward offset times the cell edge; none for the cell itself).
+        const int seg_start = lane < nseg ? te.x : 0x7FFFFFFF;
+        const int seg_base = lane < nseg ? te.y - te.x : 0;
+        const unsigned seg_id = lane < nseg ? (((lane < 8 ? id_lo >> (4 * lane) : id_hi >> (4 * (lane - 8)))) & 15u) : 0u;
+        float4 seg_off = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (seg_id > 0) {
+            int dx, dy, dz;
+            forward_offset(static_cast<int>(seg_id) - 1, dx, dy, dz);
+            // dx cell_f is exact (dx in {-1, 0, 1}): adding it rounds once, as fma(dx, cell_f, x) would.
+            seg_off = make_float4(static_cast<float>(dx) * cell_f, static_cast<float>(dy) * cell_f,
+                                  static_cast<float>(dz) * cell_f, 0.0f);
+        }
+        __syncwarp();
         if (lane < nr) {
             rows32[warp][lane][0] = my_rp;
             rows32[warp][lane][1] = my_rv;
-            rorig[warp][lane] = orig[rl];
+            rorig[warp][lane] = my_orig;
         }
         if (gate_x2) {
             // Lane l writes its row into pair l / 2, half l % 2 (rows past nr
@@ -1906,18 +1947,28 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_pairs_split(StepArgs a, 
             __syncwarp();
         };
         int queued = 0;
+        // A column block's lanes find their segments by one ballot (the
+        // segment of its first column) and one OR of the segment starts inside it.
         for (int cb = cb0; cb < cb0 + ncb; ++cb) {
-            const int p = 32 * cb + lane;
+            const int p0 = 32 * cb;
+            const int p = p0 + lane;
             const bool ok = p < L;
-            int seg = 0;
-            const int q = ok ? locate_segment(segs[warp], nseg, p, &seg) : b0;
+            const unsigned at_or_before = __ballot_sync(0xffffffffu, seg_start <= p0);
+            const int seg0 = 31 - __clz(at_or_before);
+            const unsigned inside = __reduce_or_sync(
+                0xffffffffu, (seg_start > p0 && seg_start - p0 < 32) ? (1u << (seg_start - p0)) : 0u);
+            const int seg = seg0 + __popc(inside & ((2u << lane) - 1u));
+            const int sb = __shfl_sync(0xffffffffu, seg_base, seg);  // every lane: a full-mask shuffle
+            const int q = ok ? sb + p : b0;
+            const float ox = __shfl_sync(0xffffffffu, seg_off.x, seg);
+            const float oy = __shfl_sync(0xffffffffu, seg_off.y, seg);
+            const float oz = __shfl_sync(0xffffffffu, seg_off.z, seg);
             float4 cp = sorted32[2 * static_cast<int64_t>(q)];
             const float4 cv = sorted32[2 * static_cast<int64_t>(q) + 1];
             if (seg > 0) {
-                const float4 o = segoff[warp][seg];
-                cp.x += o.x;
-                cp.y += o.y;
-                cp.z += o.z;
+                cp.x += ox;
+                cp.y += oy;
+                cp.z += oz;
             }
             const unsigned valid = ok ? (cb == ra ? lanes_below : 0xffffffffu) & nrmask : 0u;
             if (!use_box) {
@@ -2146,6 +2197,7 @@ struct FusedArgs {
     const float4* rec32;     // FP32 records in object order (used when sorted is null)
     int* nbr;
     int* cell_len;
+    int2* col_tab;
     int4* items;
     int64_t items_cap;
     int per;
@@ -2410,9 +2462,14 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
 #pragma unroll
         for (int o = 0; o < 13; ++o) fo[o] = __ldcg(nb + o);
         int other = 0;
+        int nb_begin[13], nb_len[13];
 #pragma unroll
-        for (int o = 0; o < 13; ++o)
-            if (fo[o] >= 0) other += __ldcg(f.cell_begin + fo[o] + 1) - __ldcg(f.cell_begin + fo[o]);
+        for (int o = 0; o < 13; ++o) {
+            nb_begin[o] = fo[o] >= 0 ? __ldcg(f.cell_begin + fo[o]) : 0;
+            nb_len[o] = fo[o] >= 0 ? __ldcg(f.cell_begin + fo[o] + 1) - nb_begin[o] : 0;
+            other += nb_len[o];
+        }
+        write_column_table(f.col_tab + 16 * static_cast<int64_t>(c), b0, kc, nb_begin, nb_len);
         const int L = kc + other;
         f.cell_len[c] = L;
         const unsigned int n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
@@ -2460,8 +2517,10 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
         int kc = 0, L = 0;
         unsigned int n_items = 0;
         bool heavy = false;
+        int b0 = 0;
         if (c < c1) {
-            kc = __ldcg(f.cell_begin + c + 1) - __ldcg(f.cell_begin + c);
+            b0 = __ldcg(f.cell_begin + c);
+            kc = __ldcg(f.cell_begin + c + 1) - b0;
             L = __ldcg(f.cell_len + c);
             heavy = heavy_cell(kc, L);
             n_items = cell_items((kc + 31) >> 5, (L + 31) >> 5, per);
@@ -2477,7 +2536,7 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
             int64_t w = heavy ? hoff : loff;
             for (int ra = 0; ra < ta; ++ra)
                 for (int cb = ra; cb < tc; cb += per, ++w) {
-                    if (w < f.items_cap) f.items[w] = make_int4(c, ra, cb, min(per, tc - cb));
+                    if (w < f.items_cap) f.items[w] = work_item(c, ra, cb, min(per, tc - cb), b0);
                     else over = true;
                 }
         }
@@ -2488,6 +2547,7 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
             big &= big - 1;
             const int cc = blk + (tid & ~31) + src;
             const int kk = __shfl_sync(0xffffffffu, kc, src), LL = __shfl_sync(0xffffffffu, L, src);
+            const int bb = __shfl_sync(0xffffffffu, b0, src);
             const int ta = (kk + 31) >> 5, tc = (LL + 31) >> 5;
             int64_t wbase = __shfl_sync(0xffffffffu, hoff, src);
             for (int a0 = 0; a0 < ta; a0 += 32) {
@@ -2500,7 +2560,7 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
                 }
                 int64_t w = wbase + (incl - mine);
                 for (int cb = ra; ra < ta && cb < tc; cb += per, ++w) {
-                    if (w < f.items_cap) f.items[w] = make_int4(cc, ra, cb, min(per, tc - cb));
+                    if (w < f.items_cap) f.items[w] = work_item(cc, ra, cb, min(per, tc - cb), bb);
                     else over = true;
                 }
                 wbase += __shfl_sync(0xffffffffu, incl, 31);
@@ -2980,6 +3040,7 @@ void launch_sort_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t s
     f.rec32 = b.rec32;
     f.nbr = b.nbr;
     f.cell_len = b.cell_len;
+    f.col_tab = b.col_tab;
     f.items = b.items;
     f.items_cap = b.items_cap;
     f.per = a.tune.item_col_blocks;
@@ -3214,7 +3275,7 @@ void launch_cells(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
         a.ctrl, b.cell_key, b.hash_keys, b.hash_vals, static_cast<unsigned long long>(b.hash_cap - 1), b.nbr);
     // Left empty for the fused launches, which take it so.
     cudaMemsetAsync(b.hash_keys, 0xFF, sizeof(unsigned long long) * b.hash_cap, stream);
-    k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.item_part,
+    k_items_count<<<grid_for(a.n, 8), kBlock, 0, stream>>>(a.ctrl, b.cell_begin, b.nbr, b.cell_len, b.col_tab, b.item_part,
                                                            a.tune.item_col_blocks);
     // Offsets of the heavy, then the light cells' items per chunk of cells, and their total.
     k_scan_small<<<1, 1024, 0, stream>>>(b.item_part, static_cast<int>(2 * ((b.cap + kBlock - 1) / kBlock)),
@@ -3232,15 +3293,15 @@ void launch_pairs(const DeviceBuffers& b, const StepArgs& a, cudaStream_t stream
         const int bps = a.tune.pair_blocks_per_sm > 0 ? a.tune.pair_blocks_per_sm : 4;
         if (bps >= 5)
             k_pairs_split<5><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
-                                                                     b.cell_begin, b.nbr, b.items, b.items_cap,
+                                                                     b.col_tab, b.items, b.items_cap,
                                                                      b.survivors, b.surv_cap);
         else if (bps == 4)
             k_pairs_split<4><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
-                                                                     b.cell_begin, b.nbr, b.items, b.items_cap,
+                                                                     b.col_tab, b.items, b.items_cap,
                                                                      b.survivors, b.surv_cap);
         else
             k_pairs_split<3><<<sm_count() * bps, kBlock, 0, stream>>>(a, b.state[a.src], b.sorted32, b.sorted_orig,
-                                                                     b.cell_begin, b.nbr, b.items, b.items_cap,
+                                                                     b.col_tab, b.items, b.items_cap,
                                                                      b.survivors, b.surv_cap);
         return;
     }

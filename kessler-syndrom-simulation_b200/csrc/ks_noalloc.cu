@@ -51,6 +51,7 @@ constexpr int64_t scratch_bytes() {
     b += align256(sizeof(unsigned long long) * n);       // cell_key
     b += align256(sizeof(int) * 13 * n);                 // nbr
     b += align256(sizeof(int) * n);                      // cell_len
+    b += align256(sizeof(int2) * 16 * n);                // col_tab
     b += align256(sizeof(unsigned int) * 2 * ((n + 255) / 256 + 1));  // item_part
     b += align256(sizeof(int4) * kNoAllocItems);         // items
     b += align256(sizeof(unsigned long long) * kNoAllocHash);  // hash keys
@@ -110,6 +111,7 @@ ks::DeviceBuffers carve(unsigned char* base) {
     b.cell_key = take<unsigned long long>(p, sizeof(unsigned long long) * n);
     b.nbr = take<int>(p, sizeof(int) * 13 * n);
     b.cell_len = take<int>(p, sizeof(int) * n);
+    b.col_tab = take<int2>(p, sizeof(int2) * 16 * n);
     b.item_part = take<unsigned int>(p, sizeof(unsigned int) * 2 * ((n + 255) / 256 + 1));
     b.items = take<int4>(p, sizeof(int4) * kNoAllocItems);
     b.items_cap = kNoAllocItems;
