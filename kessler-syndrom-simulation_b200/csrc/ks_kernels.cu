@@ -182,6 +182,34 @@ __device__ __forceinline__ T warp_min(T v) {
     return v;
 }
 
+// One 256-bit access (sm_100 ld/st .v8.f32, .v4.u64) for a 32-byte FP32
+// record or a four-slot hash bucket: half the load instructions of two
+// 16-byte accesses, which is what bounds the cell build's divergent gathers
+// and bucket reads. Record arrays and the hash start at allocation
+// boundaries, so record i and bucket k sit at 32-byte aligned addresses.
+// ld_rec32 reads records no kernel writes while it runs (no memory clobber).
+struct __align__(32) Rec32 {
+    float4 p, v;
+};
+__device__ __forceinline__ Rec32 ld_rec32(const float4* q) {
+    Rec32 r;
+    asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(r.p.x), "=f"(r.p.y), "=f"(r.p.z), "=f"(r.p.w), "=f"(r.v.x), "=f"(r.v.y), "=f"(r.v.z), "=f"(r.v.w)
+                 : "l"(q));
+    return r;
+}
+__device__ __forceinline__ void st_rec32(float4* q, const Rec32& r) {
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(q), "f"(r.p.x), "f"(r.p.y), "f"(r.p.z),
+                 "f"(r.p.w), "f"(r.v.x), "f"(r.v.y), "f"(r.v.z), "f"(r.v.w)
+                 : "memory");
+}
+__device__ __forceinline__ void ld_bucket_cg(const unsigned long long* q, unsigned long long (&e)[4]) {
+    asm volatile("ld.global.cg.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(e[0]), "=l"(e[1]), "=l"(e[2]), "=l"(e[3])
+                 : "l"(q)
+                 : "memory");
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -200,6 +228,19 @@ __device__ __forceinline__ void st6(double* __restrict__ base, int64_t i, const 
     p[0] = make_double2(s[0], s[1]);
     p[1] = make_double2(s[2], s[3]);
     p[2] = make_double2(s[4], s[5]);
+}
+// Streaming (evict-first) forms for the propagation: each state is read and
+// written once per step, so they do not displace the step's keys and records in L2.
+__device__ __forceinline__ void ld6s(const double* __restrict__ base, int64_t i, double s[6]) {
+    const double2* p = reinterpret_cast<const double2*>(base + 6 * i);
+    const double2 a = __ldcs(p), b = __ldcs(p + 1), c = __ldcs(p + 2);
+    s[0] = a.x; s[1] = a.y; s[2] = b.x; s[3] = b.y; s[4] = c.x; s[5] = c.y;
+}
+__device__ __forceinline__ void st6s(double* __restrict__ base, int64_t i, const double s[6]) {
+    double2* p = reinterpret_cast<double2*>(base + 6 * i);
+    __stcs(p, make_double2(s[0], s[1]));
+    __stcs(p + 1, make_double2(s[2], s[3]));
+    __stcs(p + 2, make_double2(s[4], s[5]));
 }
 
 // Reduces per-thread speculation values over the block and applies them with
@@ -384,9 +425,9 @@ __global__ void __launch_bounds__(kPropBlock, kMinBlocks) k_propagate_exact(Step
         unsigned long long out_key = 0ull;
         if (i < n) {
             double s[6];
-            ld6(in, i, s);
+            ld6s(in, i, s);
             if (!alive_in[i]) {
-                st6(out, i, s);
+                st6s(out, i, s);
                 alive_out[i] = 0;
                 out_key = dead_key(g);
             } else {
@@ -399,7 +440,7 @@ __global__ void __launch_bounds__(kPropBlock, kMinBlocks) k_propagate_exact(Step
                     if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
                 }
                 rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
-                st6(out, i, s);
+                st6s(out, i, s);
                 // Re-entry (src/core/orbital.cpp:297).
                 const bool alive = !(xsqrt(xdot3(s[0], s[1], s[2])) < fc.r_earth);
                 alive_out[i] = alive ? 1 : 0;
@@ -504,9 +545,9 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
         unsigned long long out_key = 0ull;
         if (i < n) {
             double s[6];
-            ld6(in, i, s);
+            ld6s(in, i, s);
             if (!alive_in[i]) {
-                st6(out, i, s);
+                st6s(out, i, s);
                 alive_out[i] = 0;
                 out_key = dead_key(g);
             } else {
@@ -519,7 +560,7 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
                     if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
                 }
                 rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
-                st6(out, i, s);
+                st6s(out, i, s);
                 const bool alive = !(fma(s[0], s[0], fma(s[1], s[1], s[2] * s[2])) < re2);
                 alive_out[i] = alive ? 1 : 0;
                 if (alive) {
@@ -2341,21 +2382,20 @@ __device__ __forceinline__ void cell_insert_packed(unsigned long long* hk, unsig
 template <int B>
 __device__ __forceinline__ void cell_find_batch_packed(const unsigned long long* hk, unsigned long long bmask,
                                                        const unsigned long long (&want)[B], int (&found)[B]) {
-    ulonglong2 lo[B], hi[B];
+    unsigned long long ent[B][4];
     unsigned long long bk[B];
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         bk[i] = hash_slot(want[i], bmask);
-        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(hk + 4 * bk[i]);
-        lo[i] = want[i] != kEmpty ? __ldcg(p) : make_ulonglong2(kEmpty, kEmpty);
-        hi[i] = want[i] != kEmpty ? __ldcg(p + 1) : make_ulonglong2(kEmpty, kEmpty);
+        if (want[i] != kEmpty) ld_bucket_cg(hk + 4 * bk[i], ent[i]);
+        else ent[i][0] = ent[i][1] = ent[i][2] = ent[i][3] = kEmpty;
     }
     const unsigned long long idmask = (1ull << kCellIdBits) - 1;
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         found[i] = -1;
         if (want[i] == kEmpty) continue;
-        unsigned long long e[4] = {lo[i].x, lo[i].y, hi[i].x, hi[i].y};
+        unsigned long long e[4] = {ent[i][0], ent[i][1], ent[i][2], ent[i][3]};
         for (unsigned long long probe = 0; probe <= bmask; ++probe) {
             bool done = false;
             for (int j = 0; j < 4 && !done; ++j) {
@@ -2367,9 +2407,7 @@ __device__ __forceinline__ void cell_find_batch_packed(const unsigned long long*
             }
             if (done) break;
             bk[i] = (bk[i] + 1) & bmask;   // a full bucket without the key: the next one
-            const ulonglong2* p = reinterpret_cast<const ulonglong2*>(hk + 4 * bk[i]);
-            const ulonglong2 a2 = __ldcg(p), b2 = __ldcg(p + 1);
-            e[0] = a2.x; e[1] = a2.y; e[2] = b2.x; e[3] = b2.y;
+            ld_bucket_cg(hk + 4 * bk[i], e);
         }
     }
 }
@@ -2496,9 +2534,22 @@ __device__ __forceinline__ void fused_cells_tail(const StepArgs& a, const FusedA
     grid_sync(bar, target, polls, flags);
     // Work list: heavy cells' items first, then the light cells', each in cell order.
     if (warp == 0) {
-        unsigned long long hb, ha, lb, la;
-        blocks_sum(iparts, G, b, &hb, &ha);
-        blocks_sum(iparts + G, G, b, &lb, &la);
+        // Heavy totals, then light: one copy of the code run twice. Code that
+        // runs once per launch is fetched from DRAM (the step's traffic has
+        // evicted it), so two inlined copies took ~4 us each, this loop ~1.
+        unsigned long long hb = 0, ha = 0, lb = 0, la = 0;
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            unsigned long long x, y;
+            blocks_sum(iparts + h * G, G, b, &x, &y);
+            if (h == 0) {
+                hb = x;
+                ha = y;
+            } else {
+                lb = x;
+                la = y;
+            }
+        }
         if (lane == 0) {
             bsum[1] = hb;
             bsum[2] = ha + lb;
@@ -2859,20 +2910,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
             o[j] = (kk[j] != kEmpty && oi < static_cast<unsigned long long>(n)) ? static_cast<int>(oi) : -1;
         }
         if (!f.sorted) {
-            float4 rr[4][2];
+            Rec32 rr[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (o[j] < 0) continue;
-                rr[j][0] = f.rec32[2 * static_cast<int64_t>(o[j])];
-                rr[j][1] = f.rec32[2 * static_cast<int64_t>(o[j]) + 1];
+                rr[j] = ld_rec32(f.rec32 + 2 * static_cast<int64_t>(o[j]));
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (o[j] < 0) continue;
                 const int64_t p = lo + (r0 + j) * kFusedThreads + tid;
                 f.sorted_orig[p] = o[j];
-                f.sorted32[2 * p] = rr[j][0];
-                f.sorted32[2 * p + 1] = rr[j][1];
+                st_rec32(f.sorted32 + 2 * p, rr[j]);
             }
         } else {
             double2 st[4][3];
