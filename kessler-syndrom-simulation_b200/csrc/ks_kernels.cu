@@ -2738,34 +2738,62 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_sort_cells(StepArgs a, Fus
             }
         }
         __syncthreads();
-        for (int d = b + warp * G; d < ND; d += kFusedWarps * G) {
-            constexpr int kSeg = kFusedMaxGrid / 32;
-            const int S = (G + 31) / 32;
-            unsigned int c[kSeg];
-            unsigned int seg = 0;
+        if constexpr (4 * ND <= kFusedThreads) {
+            // Each block its own starts, without a second barrier: digit d's
+            // keys of the blocks below it are the column sum of the count
+            // matrix over rows j < b, or, for the upper half of the blocks,
+            // the digit's total minus the rows j >= b (at most G / 2 rows,
+            // split over kFusedThreads / ND threads per digit, coalesced
+            // across the digits of a row).
+            constexpr int kParts = kFusedThreads / ND;
+            unsigned int* psum = reinterpret_cast<unsigned int*>(stage);   // [kParts][ND]; the stage is free
+            const int d = tid % ND, part = tid / ND;
+            const bool upper = 2 * b >= G;
+            const int j0 = upper ? b : 0, span = upper ? G - b : b;
+            const int r0 = j0 + span * part / kParts, r1 = j0 + span * (part + 1) / kParts;
+            unsigned int acc = 0;
+#pragma unroll 4
+            for (int j = r0; j < r1; ++j) acc += __ldcg(counts + j * ND + d);
+            psum[part * ND + d] = acc;
+            __syncthreads();
+            if (tid < ND) {
+                unsigned int sum = 0;
 #pragma unroll
-            for (int i = 0; i < kSeg; ++i) {
-                const int j = lane * S + i;
-                c[i] = (i < S && j < G) ? __ldcg(counts + j * ND + d) : 0u;
-                seg += c[i];
+                for (int q = 0; q < kParts; ++q) sum += psum[q * ND + tid];
+                const unsigned int below = upper ? __ldcg(totals + pass * ND + tid) - sum : sum;
+                gshift[tid] = static_cast<int>(dglob[tid] + below) - static_cast<int>(dstart[tid]);
             }
-            unsigned int incl = seg;
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            unsigned int run = dglob[d] + incl - seg;
+            __syncthreads();
+        } else {
+            for (int d = b + warp * G; d < ND; d += kFusedWarps * G) {
+                constexpr int kSeg = kFusedMaxGrid / 32;
+                const int S = (G + 31) / 32;
+                unsigned int c[kSeg];
+                unsigned int seg = 0;
 #pragma unroll
-            for (int i = 0; i < kSeg; ++i) {
-                const int j = lane * S + i;
-                if (i < S && j < G) offs[j * ND + d] = run;
-                run += c[i];
+                for (int i = 0; i < kSeg; ++i) {
+                    const int j = lane * S + i;
+                    c[i] = (i < S && j < G) ? __ldcg(counts + j * ND + d) : 0u;
+                    seg += c[i];
+                }
+                unsigned int incl = seg;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                unsigned int run = dglob[d] + incl - seg;
+#pragma unroll
+                for (int i = 0; i < kSeg; ++i) {
+                    const int j = lane * S + i;
+                    if (i < S && j < G) offs[j * ND + d] = run;
+                    run += c[i];
+                }
             }
+            grid_sync(bar, target, polls, flags);
+            for (int d = tid; d < ND; d += kFusedThreads)
+                gshift[d] = static_cast<int>(__ldcg(offs + b * ND + d)) - static_cast<int>(dstart[d]);
         }
-        grid_sync(bar, target, polls, flags);
         // Scatter: stage in digit order, store each digit's run from the block's start.
-        for (int d = tid; d < ND; d += kFusedThreads)
-            gshift[d] = static_cast<int>(__ldcg(offs + b * ND + d)) - static_cast<int>(dstart[d]);
 #pragma unroll
         for (int r = 0; r < K; ++r) {
             if (warp * 32 * K + r * 32 + lane < cnt) {
