@@ -743,21 +743,19 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision, steps=None):
     eng.set_screening(True, a.conj_km, 1.0, 0.01)
     eng.set_steps_per_graph(chunk)
     # Untimed warm-up on the same population: device buffers reach their
-    # working sizes and the chunk graphs are built, as after a run's first
-    # chunk; it also sizes the caller's pinned record buffer, reused by every take.
+    # working sizes and the chunk graphs are built, as after a run's first chunk.
     eng.set_population(pin_st, pin_sz, pin_al)
     eng.run(min(steps, chunk))
-    warm = len(eng.take_conjunctions())
+    eng.take_conjunctions()
     eng.take_step_stats()
     eng.prepare_run()
-    rec = torch.empty(max(4096, 2 * warm) * ks.CONJ_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
-    rec = rec.view(ks.CONJ_DTYPE)
     eng.set_clock(ks.DEFAULT_EPOCH_JD, 0.0, a.dt)
     barrier()
     t0 = time.perf_counter()
     eng.set_population(pin_st, pin_sz, pin_al)
     t_up = time.perf_counter()
     nconj = nstats = 0
+    last_t = 0.0
     run_s = take_s = 0.0
     host = {"prep_ms": 0.0, "launch_ms": 0.0, "sync_ms": 0.0, "after_ms": 0.0}
     for done in range(0, steps, chunk):
@@ -769,11 +767,14 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision, steps=None):
         host["launch_ms"] += tm["host_launch_ms"]
         host["sync_ms"] += tm["host_sync_ms"]
         host["after_ms"] += tm["host_chunk_ms"] - tm["host_prep_ms"] - tm["host_launch_ms"] - tm["host_sync_ms"]
+        # Zero-copy takes: the records where the device copied them (pinned
+        # host memory), read before the next run reuses that memory.
         while True:
-            got = len(eng.take_conjunctions(rec))
-            nconj += got
-            if got < len(rec):
+            v = eng.take_conjunctions_view()
+            if len(v) == 0:
                 break
+            nconj += len(v)
+            last_t = max(last_t, float(v["t"][-1]))
         nstats += len(eng.take_step_stats())
         run_s += r1 - r0
         take_s += time.perf_counter() - r1
@@ -797,8 +798,9 @@ def e2e_run(ks, a, st, sz, al, device, barrier, pg, precision, steps=None):
             "steps": steps, "steps_per_call": chunk, "phases_ms": phases,
             "what": f"ks_set_population from pinned host memory, then ks_run of {chunk}-step chunks (per step: "
                     "host->device lunar rows, device->host conjunction records in (t, i, j) order and counters, "
-                    "taken after each call), then ks_get_population into pinned host memory; wall clock, max over "
-                    "ranks"}
+                    "taken after each call with the zero-copy take, ks_take_conjunctions_view, from the pinned "
+                    "memory the device copied them into), then ks_get_population into pinned host memory; wall "
+                    "clock, max over ranks"}
 
 
 if __name__ == "__main__":

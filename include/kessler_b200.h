@@ -184,6 +184,15 @@ int ks_prepare_run(ks_ctx* ctx);
  * orders them (src/core/collision.cpp:743-747). With out == NULL only *count is
  * set (number available). Otherwise up to cap records are moved out. */
 int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t* count);
+/* Zero-copy form of ks_take_conjunctions (no counterpart in the reference,
+ * whose records are already host vectors): *first points at the oldest
+ * *count records not yet taken, in the same (t, i, j) order, inside the
+ * engine's host memory (the pinned buffer the device copied the last chunk's
+ * records into, or a holder of older ones), and those records count as taken.
+ * Call it until *count is 0 to get every record. The memory stays valid until
+ * the next call on ctx that runs steps, sets the population or takes records
+ * again; read or copy the records before that. */
+int ks_take_conjunctions_view(ks_ctx* ctx, const ks_conjunction** first, int64_t* count);
 int ks_take_step_stats(ks_ctx* ctx, ks_step_stats* out, int64_t cap, int64_t* count);
 
 /* --- fragmentation: Fragmentation (src/core/breakup.hpp:100-153), the CLI's

@@ -173,6 +173,20 @@ class Engine:
             self._check(self._lib.ks_take_conjunctions(self._h, ptr(res), cnt.value, C.byref(cnt)))
         return res[: cnt.value]
 
+    def take_conjunctions_view(self):
+        """Zero-copy take: the oldest records not yet taken, as a CONJ_DTYPE array
+        over the engine's own host memory (no copy), in (t, i, j) order; call
+        until it returns an empty array. The array is valid only until the
+        next run, population change or take on this engine: copy what must
+        outlive that."""
+        first = C.c_void_p()
+        cnt = C.c_int64()
+        self._check(self._lib.ks_take_conjunctions_view(self._h, C.byref(first), C.byref(cnt)))
+        if cnt.value == 0 or not first.value:
+            return np.empty(0, dtype=CONJ_DTYPE)
+        buf = (C.c_char * (cnt.value * CONJ_DTYPE.itemsize)).from_address(first.value)
+        return np.frombuffer(buf, dtype=CONJ_DTYPE, count=cnt.value)
+
     def take_step_stats(self):
         cnt = C.c_int64()
         self._check(self._lib.ks_take_step_stats(self._h, None, 0, C.byref(cnt)))

@@ -79,6 +79,7 @@ SIGNATURES = {
     "ks_prepare_run": (C.c_int, [_P]),
     "ks_autotune": (C.c_int, [_P, C.c_int32, C.POINTER(TuningChoice)]),
     "ks_take_conjunctions": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
+    "ks_take_conjunctions_view": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_I64)]),
     "ks_take_step_stats": (C.c_int, [_P, _P, _I64, C.POINTER(_I64)]),
     "ks_set_breakup": (C.c_int, [_P, C.c_int, _D, _D, C.c_uint64]),
     "ks_set_masses": (C.c_int, [_P, _I64, _P]),

@@ -64,6 +64,7 @@ struct ks_ctx {
     ks_conjunction* h_conj = nullptr;
     int64_t h_conj_cap = 0;
     std::vector<ks_conjunction> conj_out;
+    std::vector<ks_conjunction> conj_view;  // older records handed out by the last zero-copy take
     // The last chunk's ordered records, still in h_conj[pend_begin, pend_end):
     // newer than conj_out, moved into it before anything reuses h_conj, so
     // that a caller taking records after every step copies them only once.
@@ -1848,6 +1849,24 @@ int ks_take_conjunctions(ks_ctx* ctx, ks_conjunction* out, int64_t cap, int64_t*
         ctx->pend_begin += m - m1;
     }
     *count = m;
+    return KS_OK;
+}
+
+int ks_take_conjunctions_view(ks_ctx* ctx, const ks_conjunction** first, int64_t* count) {
+    if (!ctx || !first || !count) return KS_ERR_ARG;
+    if (!ctx->conj_out.empty()) {
+        // Older records (chunks not taken before the next one ran): handed out
+        // from a holder that the next call of this function or ks_run replaces.
+        ctx->conj_view.clear();
+        ctx->conj_view.swap(ctx->conj_out);
+        *first = ctx->conj_view.data();
+        *count = static_cast<int64_t>(ctx->conj_view.size());
+        return KS_OK;
+    }
+    // The last chunk's records where the device copied them (pinned memory).
+    *first = ctx->h_conj ? ctx->h_conj + ctx->pend_begin : nullptr;
+    *count = ctx->pend_end - ctx->pend_begin;
+    ctx->pend_begin = ctx->pend_end;
     return KS_OK;
 }
 

@@ -225,6 +225,18 @@ public:
         out.resize(static_cast<size_t>(n));
         return out;
     }
+    // The same records without a copy: f(const ks_conjunction&) is called on
+    // each, in (t, i, j) order, where the engine holds them (ks_take_conjunctions_view).
+    template <typename F>
+    void for_each_conjunction(F&& f) {
+        for (;;) {
+            const ks_conjunction* first = nullptr;
+            int64_t n = 0;
+            check(ctx_.get(), ks_take_conjunctions_view(ctx_.get(), &first, &n), "ks_take_conjunctions_view");
+            if (n <= 0) return;
+            for (int64_t q = 0; q < n; ++q) f(first[q]);
+        }
+    }
     std::vector<ks_step_stats> take_step_stats() {
         int64_t n = 0;
         check(ctx_.get(), ks_take_step_stats(ctx_.get(), nullptr, 0, &n), "ks_take_step_stats");

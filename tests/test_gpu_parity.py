@@ -292,3 +292,31 @@ def test_prepared_graphs_give_the_same_run(engine):
     assert np.array_equal(fs, fx["final_states"]) and np.array_equal(fa, fx["final_alive"])
     assert_same_conj(engine.take_conjunctions(), fx["conj"])
     assert_same_stats(engine.take_step_stats(), fx["stats"])
+
+
+def test_zero_copy_take_returns_the_same_records(engine, ks):
+    """ks_take_conjunctions_view hands out the records where the engine holds
+    them, older chunks' first, in the order of one copying take after the run;
+    each view stays readable until the next run."""
+    st, sz, al = ks.generate_population(505, 5000, 30000, 8, 3600.0)
+    want = run_engine(engine, st, sz, al, 24, spg=8)[2]
+    assert len(want) > 40
+    engine.set_steps_per_graph(8)
+    engine.set_clock(2461253.916666667, 0.0, 10.0)
+    engine.set_screening(True, 5.0, 1.0, 0.01)
+    engine.set_population(st, sz, al)
+    parts = []
+    engine.run(8)
+    parts.append(engine.take_conjunctions_view().copy())   # the chunk's records in pinned memory
+    assert len(engine.take_conjunctions_view()) == 0
+    engine.run(8)
+    engine.run(8)                                          # the second chunk's records move behind
+    while True:
+        v = engine.take_conjunctions_view()
+        if len(v) == 0:
+            break
+        parts.append(v.copy())
+    assert len(engine.take_conjunctions()) == 0
+    engine.take_step_stats()
+    got = np.concatenate(parts)
+    assert_same_conj(got, want)
