@@ -725,7 +725,7 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     for (int64_t q = 0; q < nc; ++q)
         if (ctx->h_conj[q].step < last_step) ctx->h_conj[kept++] = ctx->h_conj[q];
     if (kept > 0) {
-        finish_order(ctx->h_conj, ctx->h_conj + kept);
+        if (ctx->h_chunk->flags & ks::FLAG_CONJ_TIES) finish_order(ctx->h_conj, ctx->h_conj + kept);
         ctx->pend_begin = 0;
         ctx->pend_end = kept;
     }
@@ -929,7 +929,9 @@ int run_chunk(ks_ctx* ctx, int k_steps) {
     std::vector<ks_conjunction> hits;
     const double t_last = ctx->h_params[k_steps - 1].t0;
     if (nc > 0) {
-        finish_order(ctx->h_conj, ctx->h_conj + nc);
+        // The device ordered the records by (t, i, j), ties of its key included,
+        // unless a run of ties was longer than it takes.
+        if (ctx->h_chunk->flags & ks::FLAG_CONJ_TIES) finish_order(ctx->h_conj, ctx->h_conj + nc);
         ctx->pend_begin = 0;
         ctx->pend_end = nc;
         if (ctx->bk.on)

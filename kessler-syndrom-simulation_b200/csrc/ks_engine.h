@@ -68,6 +68,7 @@ enum : int {
     FLAG_COLL_OVERFLOW = 512,   // device SBM: more collisions in one step than its event buffer holds
     FLAG_POP_BUDGET = 1024,     // device SBM: fragments would pass the population's capacity
     FLAG_HALTED = 2048,         // device SBM: an earlier step of the chunk was left void; this step does nothing
+    FLAG_CONJ_TIES = 4096,      // records sharing an ordering key in a run longer than the device orders: the host orders
 };
 
 

@@ -3256,6 +3256,49 @@ __global__ void __launch_bounds__(kBlock) k_conj_gather(const ks_conjunction* __
 // k_conj_keys (14 index bits here) sorted by a bitonic network in shared
 // memory, then the records gathered. With more records it sets
 // FLAG_CONJ_LARGE and leaves them to the multi-block sort.
+// (t, i, j) order of records (src/core/collision.cpp:743-747).
+__device__ __forceinline__ bool conj_before(const ks_conjunction& a, const ks_conjunction& b) {
+    if (a.t != b.t) return a.t < b.t;
+    if (a.i != b.i) return a.i < b.i;
+    return a.j < b.j;
+}
+
+// Records ordered by a key monotone in t keep, among those sharing a key, the
+// order they were appended in: the thread at the start of such a run orders it
+// by (t, i, j) in place (insertion sort; runs are a few records). A run longer
+// than kTieRun is left to the host (FLAG_CONJ_TIES).
+constexpr int kTieRun = 64;
+template <typename KeyAt>
+__device__ __forceinline__ void order_tie_run(int q, int n, KeyAt key_at, ks_conjunction* __restrict__ out,
+                                              ChunkCtrl* chunk) {
+    const unsigned long long k = key_at(q);
+    if (q > 0 && key_at(q - 1) == k) return;
+    int e = q + 1;
+    while (e < n && e - q <= kTieRun && key_at(e) == k) ++e;
+    if (e - q < 2) return;
+    if (e - q > kTieRun) {
+        atomicOr(&chunk->flags, FLAG_CONJ_TIES);
+        return;
+    }
+    for (int u = q + 1; u < e; ++u) {
+        const ks_conjunction v = out[u];
+        int w = u;
+        while (w > q && conj_before(v, out[w - 1])) {
+            out[w] = out[w - 1];
+            --w;
+        }
+        out[w] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_conj_ties(const unsigned long long* __restrict__ order, int pb,
+                                                      ChunkCtrl* chunk, ks_conjunction* __restrict__ out) {
+    const int n = chunk->sort_n;
+    auto key_at = [&](int p) { return order[p] >> pb; };
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        order_tie_run(q, n, key_at, out, chunk);
+}
+
 __global__ void __launch_bounds__(1024) k_conj_sort_small(const ks_conjunction* __restrict__ conj, int64_t cap,
                                                           ChunkCtrl* chunk, const double* __restrict__ t_start,
                                                           double span_s, ks_conjunction* __restrict__ out) {
@@ -3297,6 +3340,9 @@ __global__ void __launch_bounds__(1024) k_conj_sort_small(const ks_conjunction* 
             __syncthreads();
         }
     for (int q = threadIdx.x; q < n; q += blockDim.x) out[q] = conj[static_cast<int>(sk[q] & 0x3FFFull)];
+    __syncthreads();
+    auto key_at = [&](int p) { return sk[p] >> 14; };
+    for (int q = threadIdx.x; q < n; q += blockDim.x) order_tie_run(q, n, key_at, out, chunk);
 }
 
 void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_start, double span_s, bool small,
@@ -3329,6 +3375,7 @@ void launch_conj_sort(const DeviceBuffers& b, ChunkCtrl* chunk, const double* t_
     }
     k_conj_gather<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj, b.conj_keys[kPasses & 1], (1ull << pb) - 1, chunk,
                                                          b.conj_sorted);
+    k_conj_ties<<<sm_count() * 4, kBlock, 0, stream>>>(b.conj_keys[kPasses & 1], pb, chunk, b.conj_sorted);
 }
 
 // The pair kernel gates on FP32 cell-relative records (and decides with the
