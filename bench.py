@@ -656,7 +656,8 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     counter-based draws, one stream per realisation), split precision, 5 km,
     10 m/s, within a fixed population budget. Every collision fragments inside
     the step that found it, so chunks of steps run through collisions. Timed on
-    the device (CUDA events) with the wall time beside it."""
+    the device (CUDA events) with the wall time beside it (chunks run by ks_run
+    calls, their records taken after each call) and the host's share of it."""
     R = a.cascade_realisations
     n0 = len(sz)
     budget = int(R * n0 * a.cascade_budget)
@@ -677,15 +678,34 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     warm_events = eng.take_breakups()
     n_start = eng.population_size()
     eng.set_profiling(True)
+    # A caller streams the records out as the run goes: ks_run over chunks of
+    # steps, each chunk's conjunction records taken with the zero-copy take
+    # (counted, collisions tallied) and its breakup records and counters taken
+    # after each call.
+    chunk = timed_chunk(a.cascade_steps, a.steps_per_graph)
+    tm = {k: 0.0 for k in ("total_ms", "chunk_ms", "object_steps", "steps", "host_chunk_ms", "host_prep_ms",
+                           "host_launch_ms", "host_sync_ms")}
+    n_conj = n_coll = 0
+    evs, stats = [], []
     barrier()
     w0 = time.perf_counter()
-    eng.run(a.cascade_steps)
+    for done in range(0, a.cascade_steps, chunk):
+        eng.run(min(chunk, a.cascade_steps - done))
+        t = eng.timing()
+        for k in tm:
+            tm[k] += t[k]
+        while True:
+            v = eng.take_conjunctions_view()
+            if len(v) == 0:
+                break
+            n_conj += len(v)
+            n_coll += int(v["collision"].sum())
+        evs.append(eng.take_breakups())
+        stats.append(eng.take_step_stats())
     barrier()
     wall = time.perf_counter() - w0
-    tm = eng.timing()
-    ev = eng.take_breakups()
-    conj = eng.take_conjunctions()
-    stats = eng.take_step_stats()
+    ev = np.concatenate(evs)
+    stats = np.concatenate(stats)
     n_end = eng.population_size()
     props = eng.objects()
     eng.close()
@@ -705,7 +725,11 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
             "fragments_created": int(ev["fragments"].sum()) if len(ev) else 0,
             "escaped": int(ev["escaped"].sum()) if len(ev) else 0,
             "events_per_realisation": {"min": int(per_real.min()), "max": int(per_real.max())},
-            "collisions": int(conj["collision"].sum()), "conjunctions": int(len(conj)),
+            "collisions": n_coll, "conjunctions": n_conj, "steps_per_call": chunk,
+            "host_ms": {"runs": tm["host_chunk_ms"], "prep": tm["host_prep_ms"], "launch": tm["host_launch_ms"],
+                        "wait_for_device": tm["host_sync_ms"],
+                        "records_and_counters": tm["host_chunk_ms"] - tm["host_prep_ms"] - tm["host_launch_ms"] -
+                        tm["host_sync_ms"]},
             "fragment_sizes_m": {"n_gt_lc": int((size > 0.1).sum()), "ratio_n_gt_2lc": float((size > 0.2).sum() /
                                  max(1, (size > 0.1).sum())), "untruncated_power_law_ratio": 2 ** -1.71,
                                  "note": "SBM sizes are drawn from L^-1.71 truncated to [L_c, parent size] and "

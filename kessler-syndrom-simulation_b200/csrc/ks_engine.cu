@@ -680,6 +680,7 @@ int plan_records(ks_ctx* ctx, int k_steps) {
 // at the void step from the states the chunk left (a void step never writes
 // its start-of-step buffer).
 int run_chunk_dev(ks_ctx* ctx, int k_steps) {
+    const HostClock::time_point h0 = HostClock::now();
     stash_pending(ctx);
     int rc = ensure_chunk(ctx, k_steps);
     if (rc) return rc;
@@ -688,9 +689,14 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     if ((rc = plan_records(ctx, k_steps))) return rc;
     if ((rc = ensure_graph(ctx, k_steps))) return rc;
     if (ctx->profiling) KS_CUDA(cudaEventRecord(ctx->ev_chunk[0], ctx->stream));
+    const HostClock::time_point hl = HostClock::now();
+    ctx->timing.host_prep_ms += host_ms(h0, hl);
     rc = launch_chunk(ctx, k_steps);
     if (rc) return rc;
+    const HostClock::time_point hs = HostClock::now();
     KS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->timing.host_launch_ms += host_ms(hl, hs);
+    ctx->timing.host_sync_ms += host_ms(hs, HostClock::now());
     const ks::ChunkCtrl ch = *ctx->h_chunk;
     if (ch.flags & ks::FLAG_POP_BUDGET)
         return fail(ctx, KS_ERR_OVERFLOW, "fragments would pass the population budget of " +
@@ -721,9 +727,11 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
                                 cudaMemcpyDeviceToHost, ctx->stream));
         KS_CUDA(cudaStreamSynchronize(ctx->stream));
     }
-    int64_t kept = 0;
-    for (int64_t q = 0; q < nc; ++q)
-        if (ctx->h_conj[q].step < last_step) ctx->h_conj[kept++] = ctx->h_conj[q];
+    // Without a void step every record is kept: no pass over them.
+    int64_t kept = h < 0 ? nc : 0;
+    if (h >= 0)
+        for (int64_t q = 0; q < nc; ++q)
+            if (ctx->h_conj[q].step < last_step) ctx->h_conj[kept++] = ctx->h_conj[q];
     if (kept > 0) {
         if (ctx->h_chunk->flags & ks::FLAG_CONJ_TIES) finish_order(ctx->h_conj, ctx->h_conj + kept);
         ctx->pend_begin = 0;
