@@ -669,7 +669,9 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     # step (radii 2.5-12.5 m there) still overlap at the next step and collide
     # with each other, pairs by the hundred per event, past any per-step limit.
     eng.set_screening(True, a.conj_km, 5.0, 0.01)
-    eng.set_steps_per_graph(a.steps_per_graph)
+    # Each ks_run call below is one chunk, run as one captured graph.
+    chunk = timed_chunk(a.cascade_steps, a.steps_per_graph)
+    eng.set_steps_per_graph(chunk)
     eng.set_population_batch(np.arange(R + 1) * n0, np.tile(st, (R, 1)), np.tile(sz, R), np.tile(al, R))
     eng.set_breakup(True, 0.10, 40.0, realisation_seed(a.seed, rank))
     eng.run(a.warmup)
@@ -682,18 +684,19 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
     # steps, each chunk's conjunction records taken with the zero-copy take
     # (counted, collisions tallied) and its breakup records and counters taken
     # after each call.
-    chunk = timed_chunk(a.cascade_steps, a.steps_per_graph)
     tm = {k: 0.0 for k in ("total_ms", "chunk_ms", "object_steps", "steps", "host_chunk_ms", "host_prep_ms",
                            "host_launch_ms", "host_sync_ms")}
     n_conj = n_coll = 0
     evs, stats = [], []
     barrier()
     w0 = time.perf_counter()
+    prep_calls = []
     for done in range(0, a.cascade_steps, chunk):
         eng.run(min(chunk, a.cascade_steps - done))
         t = eng.timing()
         for k in tm:
             tm[k] += t[k]
+        prep_calls.append(round(t["host_prep_ms"], 2))
         while True:
             v = eng.take_conjunctions_view()
             if len(v) == 0:
@@ -721,7 +724,7 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
             "wall_s": wall, "wall_object_steps_per_s": obj / wall, "steps": a.cascade_steps,
             "simulated_hours": a.cascade_steps * a.dt / 3600.0,
             "objects_start": int(n_start), "objects_end": int(n_end), "events": int(len(ev)),
-            "events_in_warmup": int(len(warm_events)), "catastrophic": int(ev["catastrophic"].sum()) if len(ev) else 0,
+            "warmup_steps": a.warmup, "events_in_warmup": int(len(warm_events)), "catastrophic": int(ev["catastrophic"].sum()) if len(ev) else 0,
             "fragments_created": int(ev["fragments"].sum()) if len(ev) else 0,
             "escaped": int(ev["escaped"].sum()) if len(ev) else 0,
             "events_per_realisation": {"min": int(per_real.min()), "max": int(per_real.max())},
@@ -729,7 +732,7 @@ def cascade_run(ks, a, device, barrier, pg, rank, st, sz, al):
             "host_ms": {"runs": tm["host_chunk_ms"], "prep": tm["host_prep_ms"], "launch": tm["host_launch_ms"],
                         "wait_for_device": tm["host_sync_ms"],
                         "records_and_counters": tm["host_chunk_ms"] - tm["host_prep_ms"] - tm["host_launch_ms"] -
-                        tm["host_sync_ms"]},
+                        tm["host_sync_ms"], "prep_per_call": prep_calls},
             "fragment_sizes_m": {"n_gt_lc": int((size > 0.1).sum()), "ratio_n_gt_2lc": float((size > 0.2).sum() /
                                  max(1, (size > 0.1).sum())), "untruncated_power_law_ratio": 2 ** -1.71,
                                  "note": "SBM sizes are drawn from L^-1.71 truncated to [L_c, parent size] and "

@@ -652,9 +652,13 @@ int apply_collisions(ks_ctx* ctx, int64_t step, double t0, const std::vector<ks_
 int plan_records(ks_ctx* ctx, int k_steps) {
     int rc = KS_OK;
     // Room for the chunk's records at the largest per-step count seen so far,
-    // so that a longer chunk does not overflow and replay.
+    // so that a longer chunk does not overflow and replay; sized for a whole
+    // graph's chunk even when this one is shorter (a run's first chunks end
+    // early while the counts are learnt), so that the first full chunk does
+    // not grow the buffers (pinned host memory included) again.
     if (ctx->screening && ctx->max_step_conj > 0) {
-        const int64_t want = std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, int64_t(1) << 30);
+        const int64_t span = std::max<int64_t>(k_steps, ctx->steps_per_graph);
+        const int64_t want = std::min<int64_t>(ctx->max_step_conj * span * 5 / 4 + 256, int64_t(1) << 30);
         if (want > ctx->b.conj_cap && (rc = ensure_conj(ctx, want))) return rc;
     }
     // One-block ordering of the records where the chunk should hold few.
@@ -804,29 +808,9 @@ int run_chunk_dev(ks_ctx* ctx, int k_steps) {
     return KS_OK;
 }
 
-// Buffer sizes and graph shape of a chunk of k_steps steps (fragmentation on
-// the host): room for its records at the largest per-step count seen so far
-// (so that a longer chunk does not overflow and replay), one-block ordering of
-// the records where it should hold few, and how many records come back with
-// its control blocks (up to the expected count: one host round trip).
-int plan_chunk(ks_ctx* ctx, int k_steps) {
-    int rc = KS_OK;
-    if (ctx->screening && ctx->max_step_conj > 0) {
-        const int64_t want = std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, int64_t(1) << 30);
-        if (want > ctx->b.conj_cap && (rc = ensure_conj(ctx, want))) return rc;
-    }
-    const bool small = ctx->screening && ctx->max_step_conj > 0 &&
-                       ctx->max_step_conj * k_steps * 5 / 4 + 256 <= ks::kConjSmall;
-    if (small != ctx->conj_small) {
-        ctx->conj_small = small;
-        drop_graphs(ctx);
-    }
-    const int64_t spec = ctx->screening ? std::min<int64_t>(ctx->max_step_conj * k_steps * 5 / 4 + 256, ctx->b.conj_cap) : 0;
-    ctx->chunk_spec = ctx->max_step_conj > 0 && spec <= (int64_t(1) << 16) ? spec : 0;
-    const bool use_graph = ctx->steps_per_graph > 0 && k_steps == ctx->steps_per_graph;
-    if (use_graph && ctx->graph_exec[ctx->cur] && ctx->graph_spec[ctx->cur] < ctx->chunk_spec) drop_graphs(ctx);
-    return KS_OK;
-}
+// Buffer sizes and graph shape of a chunk of k_steps steps with fragmentation
+// on the host: the plan of plan_records.
+int plan_chunk(ks_ctx* ctx, int k_steps) { return plan_records(ctx, k_steps); }
 
 int run_chunk(ks_ctx* ctx, int k_steps) {
     if (ctx->dev_sbm) return run_chunk_dev(ctx, k_steps);
