@@ -1725,9 +1725,12 @@ __device__ __forceinline__ Box warp_box(float4 p, float4 v) {
 }
 
 // True if every pair (row in box a, column in box b) stays farther apart than
-// gate over [0, dt]: box distance minus dt times the largest relative speed.
-// gate already carries the FP32 record errors; the factor covers the FP32
-// rounding of this test.
+// gate over [0, dt]: the box distance d exceeds gate + dt w, w the largest
+// relative speed. gate already carries the FP32 record errors. The distance is
+// compared squared; w takes one approximate square root (sqrt.approx.f32,
+// error a few units in the last place), raised by 1e-4, some 800 times 2^-23;
+// the other factors cover the FP32 rounding of this test, so that it is at
+// least as strict as d (1 - 1e-5) - dt w (1 + 1e-5) > gate.
 __device__ __forceinline__ bool boxes_apart(const Box& a, const Box& b, float dt, float gate) {
     float d2 = 0.f, w2 = 0.f;
 #pragma unroll
@@ -1737,7 +1740,10 @@ __device__ __forceinline__ bool boxes_apart(const Box& a, const Box& b, float dt
         const float w = fmaxf(fabsf(b.vmax[q] - a.vmin[q]), fabsf(b.vmin[q] - a.vmax[q]));
         w2 = fmaf(w, w, w2);
     }
-    return sqrtf(d2) * (1.0f - 1e-5f) - dt * sqrtf(w2) * (1.0f + 1e-5f) > gate;
+    float w;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(w) : "f"(w2));
+    const float reach = fmaf(dt, w * (1.0f + 1e-4f), gate);
+    return d2 * (1.0f - 4e-5f) > reach * reach * (1.0f + 1e-5f);
 }
 
 // Second FP32 stage for the pairs the gate lets through, on FP32 records whose
