@@ -47,6 +47,7 @@ struct StepParams {
 // the grid.
 struct GridParams {
     double cell;
+    double inv_cell;     // 1 / cell, correctly rounded (cell_key's fast quotient)
     long long lo[3];
     long long span[3];   // hi - lo per axis
     int w[3];

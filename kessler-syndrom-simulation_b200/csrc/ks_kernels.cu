@@ -65,6 +65,7 @@ __device__ void make_grid(double vmax, const unsigned long long* bb_min, const u
                           xmul(xmul(xmul(xmul(kGravityGradient, vrel), dt), dt), dt));
     g.cell = c > 1.0 ? c : 1.0;
     if (scale > 1.0) g.cell = xmul(g.cell, scale);
+    g.inv_cell = xdiv(1.0, g.cell);
     int bits = 0;
     for (int a = 0; a < 3; ++a) {
         const double mn = dec_double(bb_min[a]), mx = dec_double(bb_max[a]);
@@ -88,13 +89,35 @@ __device__ __forceinline__ unsigned sub_coord(double q, double fq, int sub) {
     return static_cast<unsigned>(min(max(s, 0), (1 << sub) - 1));
 }
 
+// floor(x / c) of the correctly rounded quotient, the reference's cell
+// coordinate (src/core/collision.cpp:393-395), without a division where it
+// can: y = x * (1/c), both rounded once, lies within 2 units in the last place
+// of the quotient, so where y is farther than 2^-50 |y| (4 units) from every
+// integer the two have the same floor (the distances below are computed
+// exactly or within an ulp of themselves); elsewhere the quotient is divided
+// out exactly. *q receives y or the quotient, for the sub-cell code: any value
+// inside the cell serves there, as the order of objects within a cell changes
+// no result.
+__device__ __forceinline__ double floor_quot(double x, double c, double inv_c, double* q) {
+    const double y = x * inv_c;
+    const double f = floor(y);
+    const double tol = fabs(y) * 0x1p-50 + 0x1p-1000;
+    if (y - f > tol && (f + 1.0) - y > tol) {
+        *q = y;
+        return f;
+    }
+    *q = xdiv(x, c);
+    return floor(*q);
+}
+
 // Key of a start-of-step position: realisation index, then compact cell
 // coordinates (floor(r / cell), the reference's cell, src/core/collision.cpp:393-395),
 // then the Morton code of the sub-cell; sets *bad if the cell lies outside the bounds.
 __device__ __forceinline__ unsigned long long cell_key(const GridParams& g, double x, double y, double z,
                                                        unsigned rid, int* bad) {
-    const double qx = xdiv(x, g.cell), qy = xdiv(y, g.cell), qz = xdiv(z, g.cell);
-    const double fx = floor(qx), fy = floor(qy), fz = floor(qz);
+    double qx, qy, qz;
+    const double fx = floor_quot(x, g.cell, g.inv_cell, &qx), fy = floor_quot(y, g.cell, g.inv_cell, &qy),
+                 fz = floor_quot(z, g.cell, g.inv_cell, &qz);
     const long long cx = static_cast<long long>(fx) - g.lo[0];
     const long long cy = static_cast<long long>(fy) - g.lo[1];
     const long long cz = static_cast<long long>(fz) - g.lo[2];
@@ -245,14 +268,17 @@ __device__ __forceinline__ void st6s(double* __restrict__ base, int64_t i, const
 
 // Reduces per-thread speculation values over the block and applies them with
 // one atomic per quantity per block.
+// Squared speeds are accumulated (one square root per block, in flush_spec):
+// square roots are correctly rounded and monotone, so the root of the largest
+// square is exactly the largest of the roots.
 struct SpecAccum {
-    double vtrue, vnext;
+    double vtrue2, vnext2;
     unsigned long long mn[3], mx[3];
     int alive;
     unsigned long long props;
     int bad;
     __device__ void init() {
-        vtrue = 0.0; vnext = 0.0;
+        vtrue2 = 0.0; vnext2 = 0.0;
         for (int a = 0; a < 3; ++a) { mn[a] = kEmpty; mx[a] = 0ull; }
         alive = 0; props = 0; bad = 0;
     }
@@ -263,8 +289,8 @@ __device__ void flush_spec(SpecAccum& s, Ctrl* cur, Ctrl* next, bool screening) 
     __shared__ int sh_alive[kWarps], sh_bad[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long vals[10];
-    vals[0] = warp_max(static_cast<unsigned long long>(__double_as_longlong(s.vtrue)));
-    vals[1] = warp_max(static_cast<unsigned long long>(__double_as_longlong(s.vnext)));
+    vals[0] = warp_max(static_cast<unsigned long long>(__double_as_longlong(s.vtrue2)));
+    vals[1] = warp_max(static_cast<unsigned long long>(__double_as_longlong(s.vnext2)));
     for (int a = 0; a < 3; ++a) { vals[2 + a] = warp_min(s.mn[a]); vals[5 + a] = warp_max(s.mx[a]); }
     vals[8] = warp_sum(s.props);
     vals[9] = 0;
@@ -289,8 +315,11 @@ __device__ void flush_spec(SpecAccum& s, Ctrl* cur, Ctrl* next, bool screening) 
         atomicAdd(&cur->n_alive, alive);
         atomicAdd(&cur->object_steps, vals[8]);
         if (screening) {
-            atomicMax(&cur->vmax_true, vals[0]);
-            atomicMax(&next->spec_vmax, vals[1]);
+            // Bit patterns of non-negative doubles order like their values.
+            const double vt = xsqrt(__longlong_as_double(static_cast<long long>(vals[0])));
+            const double vn = xsqrt(__longlong_as_double(static_cast<long long>(vals[1])));
+            atomicMax(&cur->vmax_true, static_cast<unsigned long long>(__double_as_longlong(vt)));
+            atomicMax(&next->spec_vmax, static_cast<unsigned long long>(__double_as_longlong(vn)));
             for (int a = 0; a < 3; ++a) {
                 atomicMin(&next->bb_min[a], vals[2 + a]);
                 atomicMax(&next->bb_max[a], vals[5 + a]);
@@ -349,7 +378,7 @@ __global__ void k_seed_ctrl(const double* __restrict__ st, const uint8_t* __rest
         if (!alive[i]) continue;
         double x[6];
         ld6(st, i, x);
-        s.vnext = fmax(s.vnext, xsqrt(xdot3(x[3], x[4], x[5])));
+        s.vnext2 = fmax(s.vnext2, xdot3(x[3], x[4], x[5]));
         for (int a = 0; a < 3; ++a) {
             const unsigned long long e = enc_double(x[a]);
             s.mn[a] = min(s.mn[a], e);
@@ -433,10 +462,10 @@ __global__ void __launch_bounds__(kPropBlock, kMinBlocks) k_propagate_exact(Step
             } else {
                 acc.props += 1;
                 unsigned long long key = 0ull;
-                double vb = 0.0;
+                double vb2 = 0.0;
                 if (a.screening) {
                     key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
-                    vb = xsqrt(xdot3(s[3], s[4], s[5]));
+                    vb2 = xdot3(s[3], s[4], s[5]);
                     if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
                 }
                 rk4_exact(fc, a.dt, moon[0], moon[1], moon[2], s);
@@ -447,8 +476,8 @@ __global__ void __launch_bounds__(kPropBlock, kMinBlocks) k_propagate_exact(Step
                 if (alive) {
                     acc.alive += 1;
                     if (a.screening) {
-                        acc.vtrue = fmax(acc.vtrue, vb);
-                        acc.vnext = fmax(acc.vnext, xsqrt(xdot3(s[3], s[4], s[5])));
+                        acc.vtrue2 = fmax(acc.vtrue2, vb2);
+                        acc.vnext2 = fmax(acc.vnext2, xdot3(s[3], s[4], s[5]));
                         for (int q = 0; q < 3; ++q) {
                             const unsigned long long e = enc_double(s[q]);
                             acc.mn[q] = min(acc.mn[q], e);
@@ -553,10 +582,10 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
             } else {
                 acc.props += 1;
                 unsigned long long key = 0ull;
-                double vb = 0.0;
+                double vb2 = 0.0;
                 if (a.screening) {
                     key = cell_key(g, s[0], s[1], s[2], a.real_id ? a.real_id[i] : 0u, &acc.bad);
-                    vb = xsqrt(xdot3(s[3], s[4], s[5]));
+                    vb2 = xdot3(s[3], s[4], s[5]);
                     if (a.rec32) f32_record(g, key, s[0], s[1], s[2], s[3], s[4], s[5], a.rec32 + 2 * static_cast<int64_t>(i));
                 }
                 rk4_split(sc, a.dt, moon[0], moon[1], moon[2], s);
@@ -566,8 +595,8 @@ __global__ void __launch_bounds__(kPropBlock, 5) k_propagate_split(StepArgs a, c
                 if (alive) {
                     acc.alive += 1;
                     if (a.screening) {
-                        acc.vtrue = fmax(acc.vtrue, vb);
-                        acc.vnext = fmax(acc.vnext, xsqrt(xdot3(s[3], s[4], s[5])));
+                        acc.vtrue2 = fmax(acc.vtrue2, vb2);
+                        acc.vnext2 = fmax(acc.vnext2, xdot3(s[3], s[4], s[5]));
                         for (int q = 0; q < 3; ++q) {
                             const unsigned long long e = enc_double(s[q]);
                             acc.mn[q] = min(acc.mn[q], e);
