@@ -380,6 +380,11 @@ def roofline_of(tm, a, fp64_rate, fp32_rates, split):
                   for k, v in fp32_rates.items()}
     return {"bound": d["pipe"], "kernel": dom, "achieved": d["tflops"], "peak": d["peak"] / 1e12,
             "unit": "TFLOP/s", "frac": d["frac"], "traffic": traffic_of(dom, split),
+            # How busy the pipes really are (the pair kernel prunes most candidates
+            # before its gate, so the algorithmic rate above can near the issue rate).
+            "pipes_ncu": pipes_of(dom, split),
+            "pipes_ncu_source": "ncu --set full of one launch at 400k objects (the committed profile summaries), "
+                                "not measured in this run",
             "peak_source": "measured on this GPU by the project microbenchmarks (dependent chains of FP32 add/mul, "
                            "FMA and packed FFMA2, FP64 add/mul; the highest FP32 rate is the peak); "
                            "MEASURED_PEAKS.json has no FP64/FP32 SIMT figure",
@@ -392,6 +397,22 @@ def roofline_of(tm, a, fp64_rate, fp32_rates, split):
                     "peak_source": ("copy bandwidth measured on this pool (MEASURED_PEAKS.json hbm_gbs)"
                                     if peak_src == "measured" else "the profiling recipe's fallback (6.65 TB/s)"),
                     "phases": hbm_kernels}}
+
+
+def pipes_of(kernel, split):
+    """Pipe and issue utilisation of the kernel (fractions of peak, active
+    cycles; DRAM of elapsed) from the committed ncu summaries, if present."""
+    path = os.path.join(ROOT, "profiles", "pipes_per_kernel.txt")
+    key = "pairs_split" if kernel == "pairs" else f"{kernel}_{'split' if split else 'exact'}"
+    out = {}
+    try:
+        for line in open(path):
+            f = line.split()
+            if len(f) >= 3 and f[0] == key:
+                out[f[1]] = float(f[2])
+    except (OSError, ValueError):
+        return None
+    return out or None
 
 
 def traffic_of(kernel, split):

@@ -2,7 +2,7 @@
 
 This is the maintainer's side of the drop-in, done by a script: it copies the
 reference's src/ tree to a temporary directory (the reference itself is never
-modified), makes there the edits that INTEGRATION.md sections 2 and 3 describe,
+modified), inserts there the engine behind the reference's screening and step calls,
 and builds the reference's own main.cpp against libkessler_b200.so:
 
   src/core/collision.cpp   Screener::set_gpu / gpu / gpu_compiled / begin /

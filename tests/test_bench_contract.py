@@ -29,6 +29,9 @@ def test_roofline_names_the_pair_kernel_and_its_fp32_rate(bench):
     assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
     # both precisions screen with the FP32-gated kernel
     assert bench.roofline_of(timing(), None, 17.6e12, 35.9e12, False)["bound"] == "fp32"
+    # the pipes the committed ncu capture saw beside the algorithmic rate
+    pipes = r["pipes_ncu"]
+    assert 0.0 < pipes["issue_active"] <= 1.0 and 0.0 < pipes["fma_pipe"] <= 1.0
 
 
 def test_hbm_phases_use_algorithmic_bytes(bench):

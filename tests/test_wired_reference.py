@@ -1,7 +1,7 @@
 """The drop-in behind the reference's own calls: its CLI with --gpu.
 
 kessler-syndrom-simulation_b200/host/wire_reference.py copies the reference's
-src/ tree, makes the edits of INTEGRATION.md sections 2-3 (Screener::set_gpu,
+src/ tree, inserts the engine behind the reference's calls (Screener::set_gpu,
 gpu, begin, finish and Simulation::step call the engine through
 host/kessler_b200.hpp with the reference's own State / Object / Conjunction
 types) and builds the reference's main.cpp against libkessler_b200.so into
