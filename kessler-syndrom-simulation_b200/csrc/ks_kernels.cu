@@ -94,8 +94,9 @@ __device__ __forceinline__ unsigned sub_coord(double q, double fq, int sub) {
 // can: y = x * (1/c), both rounded once, lies within 2 units in the last place
 // of the quotient, so where y is farther than 2^-50 |y| (4 units) from every
 // integer the two have the same floor (the distances below are computed
-// exactly or within an ulp of themselves); elsewhere the quotient is divided
-// out exactly. *q receives y or the quotient, for the sub-cell code: any value
+// exactly or within an ulp of themselves; where the compiler fuses the product
+// into them, they are those of the exact product, within the same bound);
+// elsewhere the quotient is divided out exactly. *q receives y or the quotient, for the sub-cell code: any value
 // inside the cell serves there, as the order of objects within a cell changes
 // no result.
 __device__ __forceinline__ double floor_quot(double x, double c, double inv_c, double* q) {
